@@ -1,0 +1,261 @@
+/*
+ * banshee_gpu.h -- C ABI of the B200 (sm_100a) ray-casting and path-tracing
+ * library that drops in behind Banshee's intersection and tracer plugin
+ * surfaces.
+ *
+ * Every entry point returns an int status: BG_OK (0) on success, a negative
+ * BG_ERR_* code otherwise; bg_last_error() returns a thread-local message for
+ * the last failure.  No C++ exception crosses this boundary.  Pointers named
+ * *_dev are device pointers (cudaMalloc'd or managed) and calls taking them are
+ * asynchronous on the given CUDA stream (a cudaStream_t passed as void*, NULL
+ * for the legacy default stream).  Calls named *_host take host pointers and
+ * are synchronous; the host<->device copies happen inside the call.
+ *
+ * Reference interfaces replaced (paths relative to FireRays/Banshee/):
+ *   Intersectable::Intersect(ray const&, Hit&)   accelerator/intersectable.h:46
+ *   Intersectable::Intersect(ray const&)         accelerator/intersectable.h:48
+ *   World::Commit / World::Intersect             world/world.cpp:5-29
+ *   Mesh::Mesh(...) + ShapeBundle::SetTransform  primitive/mesh.h:69-76,
+ *                                                primitive/shapebundle.h:139
+ *   Renderer::Render(World const&)               renderer/renderer.h:49
+ *   Tracer::GetLi (GiTracer / DiTracer)          tracer/tracer.h:53,
+ *                                                tracer/gitracer.cpp:13,
+ *                                                tracer/ditracer.cpp:19
+ *   Sampler / Camera plugins                     sampler/sampler.h:57-66,
+ *                                                camera/camera.h:53
+ */
+#ifndef BANSHEE_GPU_H
+#define BANSHEE_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+#define BG_OK                  0
+#define BG_ERR_INVALID_ARG    -1  /* bad pointer, size or descriptor field   */
+#define BG_ERR_CUDA           -2  /* a CUDA runtime call failed              */
+#define BG_ERR_OOM            -3  /* device or host allocation failed        */
+#define BG_ERR_STATE          -4  /* call order (e.g. intersect before commit)*/
+#define BG_ERR_OVERFLOW       -5  /* a device-side bound was hit (stack, queue)*/
+#define BG_ERR_TIMEOUT        -6  /* a bounded device wait gave up           */
+#define BG_ERR_UNSUPPORTED    -7  /* valid in Banshee, not on this path      */
+#define BG_ERR_NO_DEVICE      -8  /* no CUDA device / extension not usable   */
+
+/* Device-side error word bits, read with bg_scene_error_flags(). */
+#define BG_FLAG_STACK_OVERFLOW 0x1u
+#define BG_FLAG_QUEUE_OVERFLOW 0x2u
+#define BG_FLAG_BAD_INDEX      0x4u
+#define BG_FLAG_TIMEOUT        0x8u
+
+typedef struct bg_ctx bg_ctx;
+typedef struct bg_scene bg_scene;
+
+/* -------------------------------------------------------------- rays/hits */
+/* 32 bytes: float4(o, tmin), float4(d, tmax).  Mirrors class ray
+ * (math/ray.h:42-62): o, d and the interval t = (tmin, tmax).  Arrays must be
+ * 16-byte aligned. */
+typedef struct bg_ray {
+    float o[3];
+    float tmin;
+    float d[3];
+    float tmax;
+} bg_ray;
+
+/* 16 bytes.  primid is the global triangle index (faces numbered mesh by mesh
+ * in the order meshes were added), -1 on a miss; (u, v) are the Moller-Trumbore
+ * barycentrics (b1, b2) of mesh.cpp:20-26, t the hit distance.  Banshee's Hit
+ * (primitive/shapebundle.h:156-176) carries no primitive id; the shading
+ * fields it does carry are recomputed from (primid, u, v) by the shade stage. */
+typedef struct bg_hit {
+    float t;
+    int32_t primid;
+    float u;
+    float v;
+} bg_hit;
+
+/* ------------------------------------------------------------------ scene */
+/* Mirrors the Mesh constructor (primitive/mesh.h:69-76, mesh.cpp:126-214):
+ * separately indexed vertices/normals/uvs with byte strides (0 = packed for
+ * vertex, normal, uv and the three index arrays) and one material index per
+ * face.  As in mesh.cpp:212, mstride is NOT defaulted: 0 makes every face read
+ * materials[0].  uvs may be NULL (all uvs (0,0), mesh.cpp:165-181).  m/minv is
+ * the row-major bundle transform of ShapeBundle::SetTransform. */
+typedef struct bg_mesh_desc {
+    const float*   vertices; int32_t nvertices; int32_t vstride;
+    const float*   normals;  int32_t nnormals;  int32_t nstride;
+    const float*   uvs;      int32_t nuvs;      int32_t ustride;
+    const int32_t* vidx;     int32_t vistride;
+    const int32_t* nidx;     int32_t nistride;
+    const int32_t* uidx;     int32_t uistride;
+    const int32_t* materials; int32_t mstride;
+    int32_t nfaces;
+    float m[16];
+    float minv[16];
+} bg_mesh_desc;
+
+enum {
+    BG_MAT_LAMBERT        = 0, /* SimpleMaterial(Lambert(kd))          bsdf/lambert.h       */
+    BG_MAT_MICROFACET_GGX = 1, /* SimpleMaterial(Microfacet(eta, ks, FresnelDielectric,
+                                  GgxDistribution(roughness)))       bsdf/microfacet.h    */
+    BG_MAT_EMISSIVE       = 2  /* Emissive(e)                         material/emissive.h  */
+};
+
+typedef struct bg_material_desc {
+    int32_t type;
+    float kd[3];
+    float ks[3];
+    float eta;
+    float roughness;
+    float e[3];
+} bg_material_desc;
+
+enum {
+    BG_LIGHT_AREA        = 0, /* AreaLight(face, mesh, material of that face) light/arealight.cpp:11 */
+    BG_LIGHT_DIRECTIONAL = 1, /* DirectionalLight(d, e)      light/directional_light.h:42        */
+    BG_LIGHT_ENVIRONMENT = 2  /* EnvironmentLight over a constant texture e, (scale, gamma)
+                                 light/environment_light.h:45                                   */
+};
+
+typedef struct bg_light_desc {
+    int32_t type;
+    int32_t mesh;   /* area: mesh index        */
+    int32_t face;   /* area: face within mesh  */
+    float d[3];     /* directional: direction  */
+    float e[3];     /* directional: radiance; environment: constant texel */
+    float scale;    /* environment: radiance scale */
+    float gamma;    /* environment: gamma applied as pow(texel, 1/gamma) */
+} bg_light_desc;
+
+/* PerscpectiveCamera(eye, at, up, zcap=(znear,zfar), fovy, aspect),
+ * camera/perspective_camera.cpp:5-23.  As in the reference, "fovy" sets the
+ * image-plane WIDTH: dim.x = 2 tan(fovy/2) znear, dim.y = dim.x / aspect. */
+typedef struct bg_camera_desc {
+    float eye[3];
+    float at[3];
+    float up[3];
+    float znear, zfar;
+    float fovy;
+    float aspect;
+} bg_camera_desc;
+
+typedef struct bg_build_opts {
+    int32_t node_width;     /* BVH fan-out: 4 or 8 (0 = default 8)      */
+    int32_t max_leaf_size;  /* triangles per leaf, 1..8 (0 = default 4) */
+    int32_t sah_bins;       /* binned-SAH bins (0 = default 32)         */
+    int32_t reserved;
+} bg_build_opts;
+
+typedef struct bg_scene_info {
+    int64_t ntriangles;
+    int64_t nnodes;
+    int64_t node_bytes;     /* device bytes of the node array            */
+    int64_t tri_bytes;      /* device bytes of the traversal triangles   */
+    int64_t shade_bytes;    /* device bytes of the shading records       */
+    int32_t node_stride;    /* bytes per node                             */
+    int32_t max_depth;      /* deepest node level                         */
+    int32_t max_stack;      /* traversal stack entries a ray may need     */
+    int32_t nmeshes;
+    int32_t nmaterials;
+    int32_t nlights;
+    double  build_ms;       /* host build + upload time                   */
+} bg_scene_info;
+
+/* ---------------------------------------------------------------- tracing */
+enum {
+    BG_TRACER_GI = 0,       /* GiTracer(maxdepth), tracer/gitracer.cpp    */
+    BG_TRACER_DI = 1        /* DiTracer, tracer/ditracer.cpp:19-55        */
+};
+
+typedef struct bg_tracer_desc {
+    int32_t kind;
+    int32_t maxdepth;
+} bg_tracer_desc;
+
+/* Sampler plugin: every camera sample (pixel p, sample index s) gets fresh
+ * RandomSampler(McRng) image, light and BSDF samplers
+ * (sampler/random_sampler.h:48-80, rng/mcrng.h:45-76) whose McRng seeds, and
+ * the global rand() draws of GiTracer (light pick, Russian roulette,
+ * gitracer.cpp:75,119), come from a counter-keyed generator:
+ *   rand() = splitmix64(k ^ (counter * 0xD1B54A32D192ED03)) >> 33,
+ *   k = splitmix64(seed ^ splitmix64(p << 32 | s)),
+ * counter = 0, 1, 2, ... within that camera sample.  This is the determinism
+ * contract shared with the CPU oracle. */
+typedef struct bg_sampler_desc {
+    int32_t kind;           /* 0 = keyed RandomSampler(McRng)             */
+    int32_t spp;            /* camera samples per pixel in this call      */
+    uint64_t seed;
+    int32_t sample_offset;  /* index of the first sample of this call     */
+    int32_t reserved;
+} bg_sampler_desc;
+
+typedef struct bg_render_stats {
+    int64_t camera_samples;
+    int64_t rays_closest;   /* extension + MIS closest-hit rays           */
+    int64_t rays_any;       /* shadow rays                                */
+    float   ms_total;
+    float   ms_extend;      /* closest-hit traversal                      */
+    float   ms_shadow;      /* any-hit traversal                          */
+    float   ms_shade;       /* generate + shade + resolve + accumulate    */
+} bg_render_stats;
+
+/* ------------------------------------------------------------------- API */
+const char* bg_last_error(void);
+int bg_version(int32_t* major, int32_t* minor);
+
+int bg_ctx_create(int32_t device, bg_ctx** out);
+int bg_ctx_destroy(bg_ctx* ctx);
+int bg_ctx_sync(bg_ctx* ctx);
+
+/* World assembly.  Mirrors World::shapebundles_/materials_/lights_/bgcolor_
+ * (world/world.h:75-87) and World::Commit (world/world.cpp:5-16). */
+int bg_scene_create(bg_ctx* ctx, bg_scene** out);
+int bg_scene_destroy(bg_scene* scene);
+int bg_scene_add_mesh(bg_scene* scene, const bg_mesh_desc* mesh, int32_t* index);
+int bg_scene_add_material(bg_scene* scene, const bg_material_desc* mat, int32_t* index);
+int bg_scene_add_light(bg_scene* scene, const bg_light_desc* light, int32_t* index);
+int bg_scene_set_background(bg_scene* scene, const float rgb[3]);
+int bg_scene_commit(bg_scene* scene, const bg_build_opts* opts);
+int bg_scene_info_get(bg_scene* scene, bg_scene_info* info);
+int bg_scene_error_flags(bg_scene* scene, uint32_t* flags, int32_t clear);
+
+/* Closest hit: replaces World::Intersect(ray, Hit&) -> Bvh::Intersect
+ * (world/world.cpp:19-23, accelerator/bvh.cpp:499-573).  A triangle is
+ * accepted when its Moller-Trumbore t lies in (tmin, tmax] (mesh.cpp:33). */
+int bg_intersect_closest(bg_scene* scene, const bg_ray* rays_dev, bg_hit* hits_dev,
+                         int64_t n, void* stream);
+/* Any hit: replaces World::Intersect(ray) -> Bvh::Intersect(ray)
+ * (world/world.cpp:26-29, accelerator/bvh.cpp:575-647).  occluded_dev[i] = 1
+ * if some triangle has t in (tmin, tmax]. */
+int bg_intersect_any(bg_scene* scene, const bg_ray* rays_dev, uint8_t* occluded_dev,
+                     int64_t n, void* stream);
+int bg_intersect_closest_host(bg_scene* scene, const bg_ray* rays, bg_hit* hits, int64_t n);
+int bg_intersect_any_host(bg_scene* scene, const bg_ray* rays, uint8_t* occluded, int64_t n);
+
+/* Instrumented replay of the same traversal: total nodes fetched and
+ * triangles tested over the n rays (the per-ray byte model of the roofline). */
+int bg_traversal_counts(bg_scene* scene, const bg_ray* rays_dev, int64_t n, int32_t any_hit,
+                        uint64_t* nodes, uint64_t* triangles, void* stream);
+
+/* Renderer::Render for ImageRenderer/MtImageRenderer + the tracer plugin
+ * (renderer/imagerenderer.cpp:9-59).  Adds spp samples per pixel into
+ * accum_rgbw_dev (width*height float4: rgb sum and sample count in w), rows
+ * flipped as FileImagePlane::WriteSample does (imageplane/fileimageplane.cpp:29-34).
+ * The caller zeroes the buffer once and may call repeatedly with increasing
+ * sample_offset to accumulate progressively.  stats may be NULL. */
+int bg_render(bg_scene* scene, const bg_camera_desc* camera, const bg_tracer_desc* tracer,
+              const bg_sampler_desc* sampler, int32_t width, int32_t height,
+              float* accum_rgbw_dev, bg_render_stats* stats, void* stream);
+/* Same, with the accumulation buffer in host memory: it is copied in, the
+ * samples are added on the device and the result is copied back. */
+int bg_render_host(bg_scene* scene, const bg_camera_desc* camera, const bg_tracer_desc* tracer,
+                   const bg_sampler_desc* sampler, int32_t width, int32_t height,
+                   float* accum_rgbw, bg_render_stats* stats);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BANSHEE_GPU_H */
