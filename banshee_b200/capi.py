@@ -1,0 +1,197 @@
+"""ctypes binding of libbanshee_gpu.so (include/banshee_gpu.h).
+
+There is no fallback: if the shared library is missing or no sm_100 device is
+present, constructing a Context raises.  Device buffers are torch CUDA tensors
+(torch supplies device memory and streams only; all compute runs in the
+library's own kernels).
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libbanshee_gpu.so")
+
+_vp = C.c_void_p
+_i32 = C.c_int32
+_i64 = C.c_int64
+_lib = None
+
+
+class BansheeError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("%s (%d): %s" % (abi.BG_ERR.get(code, "BG_ERR"), code, msg))
+        self.code = code
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError("libbanshee_gpu.so is not built (%s); run banshee_b200/build.py" % LIB_PATH)
+        L = C.CDLL(LIB_PATH)
+        L.bg_last_error.restype = C.c_char_p
+        sig = {
+            "bg_version": [C.POINTER(_i32), C.POINTER(_i32)],
+            "bg_ctx_create": [_i32, C.POINTER(_vp)],
+            "bg_ctx_destroy": [_vp],
+            "bg_ctx_sync": [_vp],
+            "bg_scene_create": [_vp, C.POINTER(_vp)],
+            "bg_scene_destroy": [_vp],
+            "bg_scene_add_mesh": [_vp, C.POINTER(abi.MeshDesc), C.POINTER(_i32)],
+            "bg_scene_add_material": [_vp, C.POINTER(abi.MaterialDesc), C.POINTER(_i32)],
+            "bg_scene_add_light": [_vp, C.POINTER(abi.LightDesc), C.POINTER(_i32)],
+            "bg_scene_set_background": [_vp, C.POINTER(C.c_float)],
+            "bg_scene_commit": [_vp, C.POINTER(abi.BuildOpts)],
+            "bg_scene_info_get": [_vp, C.POINTER(abi.SceneInfo)],
+            "bg_scene_error_flags": [_vp, C.POINTER(C.c_uint32), _i32],
+            "bg_intersect_closest": [_vp, _vp, _vp, _i64, _vp],
+            "bg_intersect_any": [_vp, _vp, _vp, _i64, _vp],
+            "bg_intersect_closest_host": [_vp, _vp, _vp, _i64],
+            "bg_intersect_any_host": [_vp, _vp, _vp, _i64],
+            "bg_traversal_counts": [_vp, _vp, _i64, _i32, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), _vp],
+            "bg_render": [_vp, C.POINTER(abi.CameraDesc), C.POINTER(abi.TracerDesc), C.POINTER(abi.SamplerDesc),
+                          _i32, _i32, _vp, C.POINTER(abi.RenderStats), _vp],
+            "bg_render_host": [_vp, C.POINTER(abi.CameraDesc), C.POINTER(abi.TracerDesc),
+                               C.POINTER(abi.SamplerDesc), _i32, _i32, _vp, C.POINTER(abi.RenderStats)],
+        }
+        for name, args in sig.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def check(rc):
+    if rc != abi.BG_OK:
+        raise BansheeError(rc, lib().bg_last_error().decode(errors="replace"))
+    return rc
+
+
+def _stream_handle(stream):
+    if stream is None:
+        import torch
+        return torch.cuda.current_stream().cuda_stream
+    return int(stream)
+
+
+class Context:
+    """bg_ctx: one per CUDA device."""
+
+    def __init__(self, device=0):
+        self.h = _vp()
+        check(lib().bg_ctx_create(int(device), C.byref(self.h)))
+        self.device = int(device)
+
+    def sync(self):
+        check(lib().bg_ctx_sync(self.h))
+
+    def close(self):
+        if self.h:
+            lib().bg_ctx_destroy(self.h)
+            self.h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class GpuScene:
+    """A committed scene on the device: World::Commit + the Intersectable surface."""
+
+    def __init__(self, ctx, scene, node_width=4, max_leaf=4, bins=32):
+        self.ctx = ctx
+        self.scene = scene
+        self.h = _vp()
+        L = lib()
+        check(L.bg_scene_create(ctx.h, C.byref(self.h)))
+        for m in scene.meshes:
+            d = m.desc()
+            check(L.bg_scene_add_mesh(self.h, C.byref(d), None))
+        for md in scene.materials:
+            from .scene import material_desc
+            d = material_desc(md)
+            check(L.bg_scene_add_material(self.h, C.byref(d), None))
+        for ld in scene.lights:
+            from .scene import light_desc
+            d = light_desc(ld)
+            check(L.bg_scene_add_light(self.h, C.byref(d), None))
+        bg = (C.c_float * 3)(*scene.bgcolor)
+        check(L.bg_scene_set_background(self.h, bg))
+        opts = abi.BuildOpts(node_width, max_leaf, bins, 0)
+        check(L.bg_scene_commit(self.h, C.byref(opts)))
+
+    def info(self):
+        i = abi.SceneInfo()
+        check(lib().bg_scene_info_get(self.h, C.byref(i)))
+        return {k: getattr(i, k) for k, _ in abi.SceneInfo._fields_}
+
+    def error_flags(self, clear=True):
+        f = C.c_uint32()
+        check(lib().bg_scene_error_flags(self.h, C.byref(f), int(clear)))
+        return f.value
+
+    # -- host-buffer entry points (synchronous) --------------------------------
+    def intersect_closest_host(self, rays):
+        rays = np.ascontiguousarray(rays, dtype=abi.RAY_DTYPE)
+        hits = np.zeros(rays.shape[0], dtype=abi.HIT_DTYPE)
+        check(lib().bg_intersect_closest_host(self.h, rays.ctypes.data, hits.ctypes.data, rays.shape[0]))
+        return hits
+
+    def intersect_any_host(self, rays):
+        rays = np.ascontiguousarray(rays, dtype=abi.RAY_DTYPE)
+        occ = np.zeros(rays.shape[0], dtype=np.uint8)
+        check(lib().bg_intersect_any_host(self.h, rays.ctypes.data, occ.ctypes.data, rays.shape[0]))
+        return occ
+
+    # -- device-buffer entry points (async on a stream) ------------------------
+    def intersect_closest(self, rays_dev, hits_dev, n, stream=None):
+        check(lib().bg_intersect_closest(self.h, rays_dev, hits_dev, int(n), _stream_handle(stream)))
+
+    def intersect_any(self, rays_dev, occ_dev, n, stream=None):
+        check(lib().bg_intersect_any(self.h, rays_dev, occ_dev, int(n), _stream_handle(stream)))
+
+    def traversal_counts(self, rays_dev, n, any_hit=False, stream=None):
+        a, b = C.c_uint64(), C.c_uint64()
+        check(lib().bg_traversal_counts(self.h, rays_dev, int(n), int(any_hit), C.byref(a), C.byref(b),
+                                        _stream_handle(stream)))
+        return a.value, b.value
+
+    def render(self, accum_dev, width, height, spp, seed=1, sample_offset=0, tracer=abi.BG_TRACER_GI,
+               maxdepth=5, camera=None, stream=None):
+        cam = self.scene.camera_desc() if camera is None else camera
+        tr = abi.TracerDesc(tracer, maxdepth)
+        sm = abi.SamplerDesc(0, spp, seed, sample_offset, 0)
+        st = abi.RenderStats()
+        check(lib().bg_render(self.h, C.byref(cam), C.byref(tr), C.byref(sm), int(width), int(height),
+                              accum_dev, C.byref(st), _stream_handle(stream)))
+        return {k: getattr(st, k) for k, _ in abi.RenderStats._fields_}
+
+    def render_host(self, width, height, spp, seed=1, sample_offset=0, tracer=abi.BG_TRACER_GI, maxdepth=5,
+                    camera=None, accum=None):
+        cam = self.scene.camera_desc() if camera is None else camera
+        if accum is None:
+            accum = np.zeros((height, width, 4), dtype=np.float32)
+        tr = abi.TracerDesc(tracer, maxdepth)
+        sm = abi.SamplerDesc(0, spp, seed, sample_offset, 0)
+        st = abi.RenderStats()
+        check(lib().bg_render_host(self.h, C.byref(cam), C.byref(tr), C.byref(sm), int(width), int(height),
+                                   accum.ctypes.data, C.byref(st)))
+        return accum
+
+    def close(self):
+        if self.h:
+            lib().bg_scene_destroy(self.h)
+            self.h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,622 @@
+// C ABI (include/banshee_gpu.h): context, scene assembly and commit, ray casts.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+
+#include "bvh_build.h"
+#include "internal.h"
+#include "traverse.cuh"
+
+namespace bg {
+
+static thread_local std::string g_error;
+
+static inline float i2f(int32_t v) {
+    float f;
+    memcpy(&f, &v, sizeof(f));
+    return f;
+}
+
+int set_error(int code, const char* fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_error = buf;
+    return code;
+}
+
+int DevBuf::ensure(size_t need) {
+    if (need <= bytes && ptr) return BG_OK;
+    release();
+    size_t want = std::max<size_t>(need, 256);
+    cudaError_t e = cudaMalloc(&ptr, want);
+    if (e != cudaSuccess) {
+        ptr = nullptr;
+        bytes = 0;
+        cudaGetLastError();
+        return set_error(BG_ERR_OOM, "cudaMalloc(%zu) failed: %s", want, cudaGetErrorString(e));
+    }
+    bytes = want;
+    return BG_OK;
+}
+
+void DevBuf::release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+}
+
+// ------------------------------------------------------------ trace kernel
+// Persistent threads with per-lane dynamic fetch: lanes whose ray finished
+// take new ray indices from one global counter with a single warp-aggregated
+// atomicAdd, every kRefillSteps traversal steps.  Termination: the counter is
+// monotone and every ray finishes after at most one visit per node.
+template <bool ANY, bool COUNT>
+__global__ void __launch_bounds__(kTraceThreads)
+k_trace(DevScene S, const float4* __restrict__ rays, int64_t n_static, const int* __restrict__ n_dev,
+        bg_hit* __restrict__ hits, uint8_t* __restrict__ occ, unsigned long long* __restrict__ work,
+        unsigned long long* __restrict__ counters) {
+    const int64_t n = n_dev ? int64_t(*n_dev) : n_static;
+    const unsigned lane = threadIdx.x & 31u;
+    int2 stack[kStackSize];
+    TravState s;
+    Counters cnt{0ull, 0ull};
+    int64_t ridx = -1;
+    bool active = false, exhausted = false;
+    for (;;) {
+        if (!exhausted) {
+            unsigned need = __ballot_sync(0xffffffffu, !active);
+            if (need) {
+                int c = __popc(need);
+                int leader = __ffs(need) - 1;
+                unsigned long long base = 0;
+                if (lane == unsigned(leader)) base = atomicAdd(work, (unsigned long long)c);
+                base = __shfl_sync(0xffffffffu, base, leader);
+                if (base + c >= (unsigned long long)n) exhausted = true;
+                if (!active) {
+                    int64_t my = int64_t(base) + __popc(need & ((1u << lane) - 1u));
+                    if (my < n) {
+                        ridx = my;
+                        float4 a = __ldg(rays + 2 * my), b = __ldg(rays + 2 * my + 1);
+                        trav_init(s, a, b);
+                        active = true;
+                    }
+                }
+            }
+        }
+        if (!__any_sync(0xffffffffu, active)) break;
+        if (active) {
+            if (trav_steps<ANY, COUNT>(S, s, stack, kRefillSteps, cnt)) {
+                if (ANY) {
+                    occ[ridx] = s.prim >= 0 ? 1 : 0;
+                } else {
+                    bg_hit h;
+                    h.t = s.prim >= 0 ? s.best : s.r.tmax;
+                    h.primid = s.prim;
+                    h.u = s.u;
+                    h.v = s.v;
+                    reinterpret_cast<float4*>(hits)[ridx] = *reinterpret_cast<float4*>(&h);
+                }
+                active = false;
+            }
+        }
+    }
+    if (COUNT) {
+        for (int off = 16; off > 0; off >>= 1) {
+            cnt.nodes += __shfl_down_sync(0xffffffffu, cnt.nodes, off);
+            cnt.tris += __shfl_down_sync(0xffffffffu, cnt.tris, off);
+        }
+        if (lane == 0) {
+            atomicAdd(counters, cnt.nodes);
+            atomicAdd(counters + 1, cnt.tris);
+        }
+    }
+}
+
+template <bool ANY, bool COUNT>
+static int trace_blocks(bg_scene* s) {
+    int nb = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_trace<ANY, COUNT>, kTraceThreads, 0);
+    if (nb < 1) nb = 1;
+    return nb * s->ctx->num_sms;
+}
+
+unsigned long long* next_work_counter(bg_scene* s) {
+    unsigned slot = s->work_slot.fetch_add(1) % kWorkSlots;
+    return s->work.as<unsigned long long>() + slot;
+}
+
+int launch_trace(bg_scene* s, bool any_hit, const float4* rays, int64_t n_static, const int* n_dev,
+                 bg_hit* hits, uint8_t* occ, cudaStream_t st) {
+    unsigned long long* w = next_work_counter(s);
+    BG_CUDA(cudaMemsetAsync(w, 0, sizeof(unsigned long long), st));
+    if (any_hit)
+        k_trace<true, false><<<s->trace_blocks_any, kTraceThreads, 0, st>>>(s->dev, rays, n_static, n_dev, hits, occ, w, nullptr);
+    else
+        k_trace<false, false><<<s->trace_blocks_closest, kTraceThreads, 0, st>>>(s->dev, rays, n_static, n_dev, hits, occ, w, nullptr);
+    BG_CUDA(cudaGetLastError());
+    return BG_OK;
+}
+
+// ------------------------------------------------------------ commit
+static bool is_identity(const float* m) {
+    for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j)
+            if (m[4 * i + j] != (i == j ? 1.f : 0.f)) return false;
+    return true;
+}
+
+static int commit_scene(bg_scene* s, const bg_build_opts* opts) {
+    auto t0 = std::chrono::steady_clock::now();
+    const int nm = int(s->meshes.size());
+    if (nm == 0) return set_error(BG_ERR_STATE, "bg_scene_commit: the scene has no meshes");
+    int64_t ntris = 0;
+    std::vector<int64_t> start(nm);
+    for (int i = 0; i < nm; ++i) { start[i] = ntris; ntris += s->meshes[i].nfaces; }
+    if (ntris == 0) return set_error(BG_ERR_STATE, "bg_scene_commit: the scene has no triangles");
+    if (ntris > int64_t(kMaxLeafStart)) return set_error(BG_ERR_UNSUPPORTED, "bg_scene_commit: %lld triangles exceed %d", (long long)ntris, kMaxLeafStart);
+    const int nmat = int(s->mats.size());
+    // validate materials per face and lights (AreaLight ctor, light/arealight.cpp:15-19)
+    for (int i = 0; i < nm; ++i)
+        for (int f = 0; f < s->meshes[i].nfaces; ++f)
+            if (s->meshes[i].m[f] < 0 || s->meshes[i].m[f] >= std::max(nmat, 1))
+                if (nmat > 0) return set_error(BG_ERR_INVALID_ARG, "mesh %d face %d: material %d out of range", i, f, s->meshes[i].m[f]);
+    std::vector<BundleRec> bundles(nm);
+    for (int i = 0; i < nm; ++i) {
+        const MeshHost& mh = s->meshes[i];
+        BundleRec& b = bundles[i];
+        memcpy(b.m, mh.xf, sizeof(b.m));
+        memcpy(b.minv, mh.xfinv, sizeof(b.minv));
+        b.identity = is_identity(mh.xf) && is_identity(mh.xfinv);
+        b.arealight = -1;
+        b.nfaces = mh.nfaces;
+        b.pad = 0;
+        b.start = start[i];
+        b.pad2 = 0;
+    }
+    std::vector<LightRec> lights(s->lights.size());
+    for (size_t li = 0; li < s->lights.size(); ++li) {
+        const bg_light_desc& d = s->lights[li];
+        LightRec& L = lights[li];
+        memset(&L, 0, sizeof(L));
+        L.type = d.type;
+        L.mesh = d.mesh;
+        L.face = d.face;
+        L.matidx = -1;
+        if (d.type == BG_LIGHT_AREA) {
+            if (d.mesh < 0 || d.mesh >= nm || d.face < 0 || d.face >= s->meshes[d.mesh].nfaces)
+                return set_error(BG_ERR_INVALID_ARG, "light %zu: mesh/face out of range", li);
+            int mi = s->meshes[d.mesh].m[d.face];
+            if (mi < 0 || mi >= nmat || s->mats[mi].type != BG_MAT_EMISSIVE)
+                return set_error(BG_ERR_INVALID_ARG, "AreaLight: The material passed is not an emissive one (light %zu)", li);
+            L.matidx = mi;
+            for (int k = 0; k < 3; ++k) L.e[k] = s->mats[mi].e[k];
+            bundles[d.mesh].arealight = int(li);   // last one wins, light/arealight.cpp:22
+        } else if (d.type == BG_LIGHT_DIRECTIONAL) {
+            v3 n = normalize(mk(d.d[0], d.d[1], d.d[2]));
+            L.dir[0] = n.x; L.dir[1] = n.y; L.dir[2] = n.z;
+            for (int k = 0; k < 3; ++k) L.e[k] = d.e[k];
+        } else if (d.type == BG_LIGHT_ENVIRONMENT) {
+            // scale * pow(texel, 1/gamma) with the double ::pow of environment_light.cpp:27,48
+            float invgamma = 1.f / d.gamma;
+            for (int k = 0; k < 3; ++k) L.env[k] = float(std::pow(double(d.e[k]), double(invgamma))) * d.scale;
+        } else {
+            return set_error(BG_ERR_INVALID_ARG, "light %zu: unknown type %d", li, d.type);
+        }
+    }
+    std::vector<MatRec> mats(std::max(nmat, 1));
+    for (int i = 0; i < nmat; ++i) {
+        const bg_material_desc& d = s->mats[i];
+        if (d.type < BG_MAT_LAMBERT || d.type > BG_MAT_EMISSIVE)
+            return set_error(BG_ERR_INVALID_ARG, "material %d: unknown type %d", i, d.type);
+        MatRec& m = mats[i];
+        m.type = d.type;
+        for (int k = 0; k < 3; ++k) { m.kd[k] = d.kd[k]; m.ks[k] = d.ks[k]; m.e[k] = d.e[k]; }
+        m.eta = d.eta;
+        m.a = d.roughness;
+    }
+    // world-space triangle bounds (Mesh::GetShapeWorldBounds, primitive/mesh.cpp:263-283)
+    std::vector<float> lo(3 * size_t(ntris)), hi(3 * size_t(ntris));
+    for (int i = 0; i < nm; ++i) {
+        const MeshHost& mh = s->meshes[i];
+        const float* M = mh.xf;
+        float m12[12] = {M[0], M[1], M[2], M[3], M[4], M[5], M[6], M[7], M[8], M[9], M[10], M[11]};
+        for (int f = 0; f < mh.nfaces; ++f) {
+            v3 p[3];
+            for (int k = 0; k < 3; ++k) p[k] = xf_point(m12, mh.verts[mh.vi[3 * f + k]]);
+            size_t t = size_t(start[i] + f);
+            lo[3 * t] = std::min(p[0].x, std::min(p[1].x, p[2].x));
+            lo[3 * t + 1] = std::min(p[0].y, std::min(p[1].y, p[2].y));
+            lo[3 * t + 2] = std::min(p[0].z, std::min(p[1].z, p[2].z));
+            hi[3 * t] = std::max(p[0].x, std::max(p[1].x, p[2].x));
+            hi[3 * t + 1] = std::max(p[0].y, std::max(p[1].y, p[2].y));
+            hi[3 * t + 2] = std::max(p[0].z, std::max(p[1].z, p[2].z));
+        }
+    }
+    BuildParams bp;
+    if (opts) {
+        if (opts->node_width != 0 && opts->node_width != 4)
+            return set_error(BG_ERR_UNSUPPORTED, "node_width %d: this build supports 4-wide nodes", opts->node_width);
+        if (opts->max_leaf_size) bp.max_leaf = opts->max_leaf_size;
+        if (opts->sah_bins) bp.bins = opts->sah_bins;
+    }
+    if (bp.max_leaf < 1 || bp.max_leaf > 16 || bp.bins < 2 || bp.bins > 256)
+        return set_error(BG_ERR_INVALID_ARG, "build options out of range (leaf 1..16, bins 2..256)");
+    BuildResult br = build_wide_bvh(lo.data(), hi.data(), ntris, bp);
+    if (br.max_stack > kStackSize)
+        return set_error(BG_ERR_UNSUPPORTED, "BVH needs a %d-entry traversal stack (> %d)", br.max_stack, kStackSize);
+    // per-triangle records
+    std::vector<int> tri_bundle(static_cast<size_t>(ntris));
+    for (int i = 0; i < nm; ++i)
+        for (int f = 0; f < s->meshes[i].nfaces; ++f) tri_bundle[size_t(start[i] + f)] = i;
+    std::vector<TriRec> tris(static_cast<size_t>(ntris));
+    for (int64_t k = 0; k < ntris; ++k) {
+        int32_t t = br.order[size_t(k)];
+        int b = tri_bundle[size_t(t)];
+        const MeshHost& mh = s->meshes[b];
+        int f = int(t - start[b]);
+        v3 p1 = mh.verts[mh.vi[3 * f]], p2 = mh.verts[mh.vi[3 * f + 1]], p3 = mh.verts[mh.vi[3 * f + 2]];
+        v3 e1 = sub(p2, p1), e2 = sub(p3, p1);
+        TriRec& r = tris[size_t(k)];
+        int bcode = bundles[b].identity ? -1 : b;
+        r.v0 = make_float4(p1.x, p1.y, p1.z, i2f(bcode));
+        r.e1 = make_float4(e1.x, e1.y, e1.z, i2f(t));
+        r.e2 = make_float4(e2.x, e2.y, e2.z, 0.f);
+    }
+    std::vector<ShadeRec> shade(static_cast<size_t>(ntris));
+    for (int b = 0; b < nm; ++b) {
+        const MeshHost& mh = s->meshes[b];
+        for (int f = 0; f < mh.nfaces; ++f) {
+            ShadeRec& r = shade[size_t(start[b] + f)];
+            v3 p1 = mh.verts[mh.vi[3 * f]], p2 = mh.verts[mh.vi[3 * f + 1]], p3 = mh.verts[mh.vi[3 * f + 2]];
+            v3 n1 = mh.normals[mh.ni[3 * f]], n2 = mh.normals[mh.ni[3 * f + 1]], n3 = mh.normals[mh.ni[3 * f + 2]];
+            const float* t1 = &mh.uvs[2 * size_t(mh.ti[3 * f])];
+            const float* t2 = &mh.uvs[2 * size_t(mh.ti[3 * f + 1])];
+            const float* t3 = &mh.uvs[2 * size_t(mh.ti[3 * f + 2])];
+            r.a = make_float4(p1.x, p1.y, p1.z, i2f(b));
+            r.b = make_float4(p2.x, p2.y, p2.z, i2f(mh.m[f]));
+            r.c = make_float4(p3.x, p3.y, p3.z, t1[0]);
+            r.d = make_float4(n1.x, n1.y, n1.z, t1[1]);
+            r.e = make_float4(n2.x, n2.y, n2.z, t2[0]);
+            r.f = make_float4(n3.x, n3.y, n3.z, t2[1]);
+            r.g = make_float4(t3[0], t3[1], 0.f, 0.f);
+        }
+    }
+    int rc;
+    if ((rc = s->nodes.ensure(br.nodes.size() * sizeof(WideNode4))) ||
+        (rc = s->tris.ensure(tris.size() * sizeof(TriRec))) ||
+        (rc = s->shade.ensure(shade.size() * sizeof(ShadeRec))) ||
+        (rc = s->bundles.ensure(bundles.size() * sizeof(BundleRec))) ||
+        (rc = s->mats_d.ensure(mats.size() * sizeof(MatRec))) ||
+        (rc = s->lights_d.ensure(std::max<size_t>(1, lights.size()) * sizeof(LightRec))) ||
+        (rc = s->err.ensure(sizeof(unsigned))) ||
+        (rc = s->work.ensure(kWorkSlots * sizeof(unsigned long long))))
+        return rc;
+    BG_CUDA(cudaMemcpy(s->nodes.ptr, br.nodes.data(), br.nodes.size() * sizeof(WideNode4), cudaMemcpyHostToDevice));
+    BG_CUDA(cudaMemcpy(s->tris.ptr, tris.data(), tris.size() * sizeof(TriRec), cudaMemcpyHostToDevice));
+    BG_CUDA(cudaMemcpy(s->shade.ptr, shade.data(), shade.size() * sizeof(ShadeRec), cudaMemcpyHostToDevice));
+    BG_CUDA(cudaMemcpy(s->bundles.ptr, bundles.data(), bundles.size() * sizeof(BundleRec), cudaMemcpyHostToDevice));
+    BG_CUDA(cudaMemcpy(s->mats_d.ptr, mats.data(), mats.size() * sizeof(MatRec), cudaMemcpyHostToDevice));
+    if (!lights.empty())
+        BG_CUDA(cudaMemcpy(s->lights_d.ptr, lights.data(), lights.size() * sizeof(LightRec), cudaMemcpyHostToDevice));
+    BG_CUDA(cudaMemset(s->err.ptr, 0, sizeof(unsigned)));
+    BG_CUDA(cudaMemset(s->work.ptr, 0, kWorkSlots * sizeof(unsigned long long)));
+    DevScene& d = s->dev;
+    d.nodes = s->nodes.as<WideNode4>();
+    d.tris = s->tris.as<TriRec>();
+    d.shade = s->shade.as<ShadeRec>();
+    d.bundles = s->bundles.as<BundleRec>();
+    d.mats = s->mats_d.as<MatRec>();
+    d.lights = s->lights_d.as<LightRec>();
+    d.errflags = s->err.as<unsigned>();
+    d.ntris = ntris;
+    d.nbundles = nm;
+    d.nmats = nmat;
+    d.nlights = int(lights.size());
+    d.bg[0] = s->bg[0]; d.bg[1] = s->bg[1]; d.bg[2] = s->bg[2];
+    s->trace_blocks_closest = trace_blocks<false, false>(s);
+    s->trace_blocks_any = trace_blocks<true, false>(s);
+    s->trace_blocks_count = trace_blocks<false, true>(s);
+    auto t1 = std::chrono::steady_clock::now();
+    bg_scene_info& info = s->info;
+    info.ntriangles = ntris;
+    info.nnodes = int64_t(br.nodes.size());
+    info.node_bytes = int64_t(br.nodes.size() * sizeof(WideNode4));
+    info.tri_bytes = int64_t(tris.size() * sizeof(TriRec));
+    info.shade_bytes = int64_t(shade.size() * sizeof(ShadeRec));
+    info.node_stride = int32_t(sizeof(WideNode4));
+    info.max_depth = br.max_depth;
+    info.max_stack = br.max_stack;
+    info.nmeshes = nm;
+    info.nmaterials = nmat;
+    info.nlights = int(lights.size());
+    info.build_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    s->committed = true;
+    return BG_OK;
+}
+
+static int check_scene(bg_scene* s) {
+    if (!s) return set_error(BG_ERR_INVALID_ARG, "scene is NULL");
+    if (!s->committed) return set_error(BG_ERR_STATE, "scene not committed (call bg_scene_commit first)");
+    return BG_OK;
+}
+
+static int check_rays(const void* rays, const void* out, int64_t n) {
+    if (n < 0) return set_error(BG_ERR_INVALID_ARG, "negative ray count");
+    if (n > 0 && (!rays || !out)) return set_error(BG_ERR_INVALID_ARG, "NULL ray or output pointer");
+    if (n > 0 && (reinterpret_cast<uintptr_t>(rays) & 15u)) return set_error(BG_ERR_INVALID_ARG, "ray array must be 16-byte aligned");
+    if (n > (int64_t(1) << 40)) return set_error(BG_ERR_INVALID_ARG, "ray count too large");
+    return BG_OK;
+}
+
+}  // namespace bg
+
+using namespace bg;
+
+extern "C" {
+
+const char* bg_last_error(void) { return g_error.c_str(); }
+
+int bg_version(int32_t* major, int32_t* minor) {
+    if (major) *major = 1;
+    if (minor) *minor = 0;
+    return BG_OK;
+}
+
+int bg_ctx_create(int32_t device, bg_ctx** out) {
+    if (!out) return set_error(BG_ERR_INVALID_ARG, "out is NULL");
+    *out = nullptr;
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return set_error(BG_ERR_NO_DEVICE, "no CUDA device available (%s)", cudaGetErrorString(e));
+    }
+    if (device < 0 || device >= n) return set_error(BG_ERR_INVALID_ARG, "device %d out of range (%d devices)", device, n);
+    BG_CUDA(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    BG_CUDA(cudaGetDeviceProperties(&prop, device));
+    if (prop.major < 10) return set_error(BG_ERR_NO_DEVICE, "device %d is sm_%d%d; this library is built for sm_100a", device, prop.major, prop.minor);
+    bg_ctx* c = new (std::nothrow) bg_ctx();
+    if (!c) return set_error(BG_ERR_OOM, "host allocation failed");
+    c->device = device;
+    c->num_sms = prop.multiProcessorCount;
+    c->l2_bytes = size_t(prop.l2CacheSize);
+    *out = c;
+    return BG_OK;
+}
+
+int bg_ctx_destroy(bg_ctx* ctx) {
+    delete ctx;
+    return BG_OK;
+}
+
+int bg_ctx_sync(bg_ctx* ctx) {
+    if (!ctx) return set_error(BG_ERR_INVALID_ARG, "ctx is NULL");
+    BG_CUDA(cudaSetDevice(ctx->device));
+    BG_CUDA(cudaDeviceSynchronize());
+    return BG_OK;
+}
+
+int bg_scene_create(bg_ctx* ctx, bg_scene** out) {
+    if (!ctx || !out) return set_error(BG_ERR_INVALID_ARG, "NULL argument");
+    bg_scene* s = new (std::nothrow) bg_scene();
+    if (!s) return set_error(BG_ERR_OOM, "host allocation failed");
+    s->ctx = ctx;
+    *out = s;
+    return BG_OK;
+}
+
+int bg_scene_destroy(bg_scene* s) {
+    if (!s) return BG_OK;
+    cudaSetDevice(s->ctx->device);
+    cudaDeviceSynchronize();
+    for (DevBuf* b : {&s->nodes, &s->tris, &s->shade, &s->bundles, &s->mats_d, &s->lights_d, &s->err, &s->work,
+                      &s->host_rays, &s->host_out})
+        b->release();
+    if (s->render) render_state_free(s->render);
+    delete s;
+    return BG_OK;
+}
+
+// Mesh::Mesh, primitive/mesh.cpp:126-214 (strided reads; mstride not defaulted)
+int bg_scene_add_mesh(bg_scene* s, const bg_mesh_desc* d, int32_t* index) {
+    if (!s || !d) return set_error(BG_ERR_INVALID_ARG, "NULL argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->committed) return set_error(BG_ERR_STATE, "scene already committed");
+    if (d->nfaces < 0 || d->nvertices < 0 || d->nnormals < 0 || d->nuvs < 0)
+        return set_error(BG_ERR_INVALID_ARG, "negative count in mesh descriptor");
+    if (d->nfaces > 0 && (!d->vertices || !d->normals || !d->vidx || !d->nidx || !d->materials))
+        return set_error(BG_ERR_INVALID_ARG, "mesh descriptor has NULL arrays");
+    MeshHost mh;
+    const int vs = d->vstride ? d->vstride : int(3 * sizeof(float));
+    const int ns = d->nstride ? d->nstride : int(3 * sizeof(float));
+    mh.verts.resize(size_t(d->nvertices));
+    for (int i = 0; i < d->nvertices; ++i) {
+        const float* c = reinterpret_cast<const float*>(reinterpret_cast<const char*>(d->vertices) + size_t(i) * vs);
+        mh.verts[i] = mk(c[0], c[1], c[2]);
+    }
+    mh.normals.resize(size_t(d->nnormals));
+    for (int i = 0; i < d->nnormals; ++i) {
+        const float* c = reinterpret_cast<const float*>(reinterpret_cast<const char*>(d->normals) + size_t(i) * ns);
+        mh.normals[i] = mk(c[0], c[1], c[2]);
+    }
+    const bool hasuv = d->uvs && d->nuvs > 0;
+    if (hasuv) {
+        const int us = d->ustride ? d->ustride : int(2 * sizeof(float));
+        mh.uvs.resize(2 * size_t(d->nuvs));
+        for (int i = 0; i < d->nuvs; ++i) {
+            const float* c = reinterpret_cast<const float*>(reinterpret_cast<const char*>(d->uvs) + size_t(i) * us);
+            mh.uvs[2 * i] = c[0];
+            mh.uvs[2 * i + 1] = c[1];
+        }
+    } else {
+        mh.uvs.assign(2, 0.f);
+    }
+    const int vis = d->vistride ? d->vistride : int(sizeof(int));
+    const int nis = d->nistride ? d->nistride : int(sizeof(int));
+    const int uis = d->uistride ? d->uistride : int(sizeof(int));
+    auto rd = [](const int32_t* p, size_t k, int stride) {
+        return *reinterpret_cast<const int32_t*>(reinterpret_cast<const char*>(p) + k * size_t(stride));
+    };
+    const int nuv = hasuv ? d->nuvs : 1;
+    mh.nfaces = d->nfaces;
+    mh.vi.resize(3 * size_t(d->nfaces));
+    mh.ni.resize(3 * size_t(d->nfaces));
+    mh.ti.resize(3 * size_t(d->nfaces));
+    mh.m.resize(size_t(d->nfaces));
+    for (int f = 0; f < d->nfaces; ++f) {
+        for (int k = 0; k < 3; ++k) {
+            int v = rd(d->vidx, 3 * size_t(f) + k, vis);
+            int nn = rd(d->nidx, 3 * size_t(f) + k, nis);
+            int t = hasuv ? rd(d->uidx, 3 * size_t(f) + k, uis) : 0;
+            if (v < 0 || v >= d->nvertices || nn < 0 || nn >= d->nnormals || t < 0 || t >= nuv)
+                return set_error(BG_ERR_INVALID_ARG, "face %d: index out of range", f);
+            mh.vi[3 * f + k] = v;
+            mh.ni[3 * f + k] = nn;
+            mh.ti[3 * f + k] = t;
+        }
+        mh.m[f] = rd(d->materials, size_t(f), d->mstride);
+    }
+    memcpy(mh.xf, d->m, sizeof(mh.xf));
+    memcpy(mh.xfinv, d->minv, sizeof(mh.xfinv));
+    s->meshes.push_back(std::move(mh));
+    if (index) *index = int32_t(s->meshes.size() - 1);
+    return BG_OK;
+}
+
+int bg_scene_add_material(bg_scene* s, const bg_material_desc* m, int32_t* index) {
+    if (!s || !m) return set_error(BG_ERR_INVALID_ARG, "NULL argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->committed) return set_error(BG_ERR_STATE, "scene already committed");
+    s->mats.push_back(*m);
+    if (index) *index = int32_t(s->mats.size() - 1);
+    return BG_OK;
+}
+
+int bg_scene_add_light(bg_scene* s, const bg_light_desc* l, int32_t* index) {
+    if (!s || !l) return set_error(BG_ERR_INVALID_ARG, "NULL argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->committed) return set_error(BG_ERR_STATE, "scene already committed");
+    s->lights.push_back(*l);
+    if (index) *index = int32_t(s->lights.size() - 1);
+    return BG_OK;
+}
+
+int bg_scene_set_background(bg_scene* s, const float rgb[3]) {
+    if (!s || !rgb) return set_error(BG_ERR_INVALID_ARG, "NULL argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->bg[0] = rgb[0]; s->bg[1] = rgb[1]; s->bg[2] = rgb[2];
+    s->dev.bg[0] = rgb[0]; s->dev.bg[1] = rgb[1]; s->dev.bg[2] = rgb[2];
+    return BG_OK;
+}
+
+int bg_scene_commit(bg_scene* s, const bg_build_opts* opts) {
+    if (!s) return set_error(BG_ERR_INVALID_ARG, "scene is NULL");
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->committed) return set_error(BG_ERR_STATE, "scene already committed");
+    BG_CUDA(cudaSetDevice(s->ctx->device));
+    return commit_scene(s, opts);
+}
+
+int bg_scene_info_get(bg_scene* s, bg_scene_info* info) {
+    int rc = check_scene(s);
+    if (rc) return rc;
+    if (!info) return set_error(BG_ERR_INVALID_ARG, "info is NULL");
+    *info = s->info;
+    return BG_OK;
+}
+
+int bg_scene_error_flags(bg_scene* s, uint32_t* flags, int32_t clear) {
+    int rc = check_scene(s);
+    if (rc) return rc;
+    if (!flags) return set_error(BG_ERR_INVALID_ARG, "flags is NULL");
+    unsigned v = 0;
+    BG_CUDA(cudaMemcpy(&v, s->err.ptr, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    if (clear) BG_CUDA(cudaMemset(s->err.ptr, 0, sizeof(unsigned)));
+    *flags = v;
+    return BG_OK;
+}
+
+int bg_intersect_closest(bg_scene* s, const bg_ray* rays, bg_hit* hits, int64_t n, void* stream) {
+    int rc;
+    if ((rc = check_scene(s)) || (rc = check_rays(rays, hits, n))) return rc;
+    if (n == 0) return BG_OK;
+    if (reinterpret_cast<uintptr_t>(hits) & 15u) return set_error(BG_ERR_INVALID_ARG, "hit array must be 16-byte aligned");
+    return launch_trace(s, false, reinterpret_cast<const float4*>(rays), n, nullptr, hits, nullptr,
+                        static_cast<cudaStream_t>(stream));
+}
+
+int bg_intersect_any(bg_scene* s, const bg_ray* rays, uint8_t* occ, int64_t n, void* stream) {
+    int rc;
+    if ((rc = check_scene(s)) || (rc = check_rays(rays, occ, n))) return rc;
+    if (n == 0) return BG_OK;
+    return launch_trace(s, true, reinterpret_cast<const float4*>(rays), n, nullptr, nullptr, occ,
+                        static_cast<cudaStream_t>(stream));
+}
+
+static int host_cast(bg_scene* s, const bg_ray* rays, void* out, int64_t n, bool any) {
+    int rc;
+    if ((rc = check_scene(s)) || (rc = check_rays(rays, out, n))) return rc;
+    if (n == 0) return BG_OK;
+    std::lock_guard<std::mutex> lk(s->mu);
+    BG_CUDA(cudaSetDevice(s->ctx->device));
+    const size_t rb = size_t(n) * sizeof(bg_ray), ob = size_t(n) * (any ? 1 : sizeof(bg_hit));
+    if ((rc = s->host_rays.ensure(rb)) || (rc = s->host_out.ensure(ob))) return rc;
+    BG_CUDA(cudaMemcpy(s->host_rays.ptr, rays, rb, cudaMemcpyHostToDevice));
+    rc = launch_trace(s, any, s->host_rays.as<float4>(), n, nullptr, any ? nullptr : s->host_out.as<bg_hit>(),
+                      any ? s->host_out.as<uint8_t>() : nullptr, 0);
+    if (rc) return rc;
+    BG_CUDA(cudaMemcpy(out, s->host_out.ptr, ob, cudaMemcpyDeviceToHost));
+    unsigned flags = 0;
+    BG_CUDA(cudaMemcpy(&flags, s->err.ptr, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    if (flags & BG_FLAG_STACK_OVERFLOW) return set_error(BG_ERR_OVERFLOW, "traversal stack overflow");
+    return BG_OK;
+}
+
+int bg_intersect_closest_host(bg_scene* s, const bg_ray* rays, bg_hit* hits, int64_t n) {
+    return host_cast(s, rays, hits, n, false);
+}
+
+int bg_intersect_any_host(bg_scene* s, const bg_ray* rays, uint8_t* occ, int64_t n) {
+    return host_cast(s, rays, occ, n, true);
+}
+
+int bg_traversal_counts(bg_scene* s, const bg_ray* rays, int64_t n, int32_t any_hit, uint64_t* nodes,
+                        uint64_t* triangles, void* stream) {
+    int rc;
+    if ((rc = check_scene(s)) || (rc = check_rays(rays, nodes, n))) return rc;
+    if (!triangles) return set_error(BG_ERR_INVALID_ARG, "triangles is NULL");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    DevBuf tmp;
+    if ((rc = tmp.ensure(2 * sizeof(unsigned long long) + (any_hit ? size_t(n) : size_t(n) * sizeof(bg_hit))))) return rc;
+    unsigned long long* cnt = tmp.as<unsigned long long>();
+    cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned long long), st);
+    unsigned long long* w = next_work_counter(s);
+    cudaMemsetAsync(w, 0, sizeof(unsigned long long), st);
+    bg_hit* hits = reinterpret_cast<bg_hit*>(reinterpret_cast<char*>(tmp.ptr) + 16);
+    uint8_t* occ = reinterpret_cast<uint8_t*>(tmp.ptr) + 16;
+    if (n > 0) {
+        if (any_hit)
+            k_trace<true, true><<<s->trace_blocks_count, kTraceThreads, 0, st>>>(s->dev, reinterpret_cast<const float4*>(rays), n, nullptr, nullptr, occ, w, cnt);
+        else
+            k_trace<false, true><<<s->trace_blocks_count, kTraceThreads, 0, st>>>(s->dev, reinterpret_cast<const float4*>(rays), n, nullptr, hits, nullptr, w, cnt);
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) { tmp.release(); return set_error(BG_ERR_CUDA, "count kernel: %s", cudaGetErrorString(e)); }
+    unsigned long long h[2];
+    e = cudaMemcpyAsync(h, cnt, sizeof(h), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    tmp.release();
+    if (e != cudaSuccess) return set_error(BG_ERR_CUDA, "count readback: %s", cudaGetErrorString(e));
+    *nodes = h[0];
+    *triangles = h[1];
+    return BG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,83 @@
+// Host-side library internals shared by the API and render translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdarg>
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/banshee_gpu.h"
+#include "device_common.cuh"
+#include "scene_types.h"
+
+namespace bg {
+
+int set_error(int code, const char* fmt, ...);
+
+#define BG_CUDA(call)                                                                    \
+    do {                                                                                 \
+        cudaError_t e_ = (call);                                                         \
+        if (e_ != cudaSuccess)                                                           \
+            return ::bg::set_error(e_ == cudaErrorMemoryAllocation ? BG_ERR_OOM : BG_ERR_CUDA, \
+                                   "%s failed: %s", #call, cudaGetErrorString(e_));      \
+    } while (0)
+
+struct MeshHost {
+    std::vector<v3> verts, normals;
+    std::vector<float> uvs;              // 2 per uv
+    std::vector<int32_t> vi, ni, ti, m;  // 3, 3, 3, 1 per face
+    float xf[16], xfinv[16];
+    int nfaces = 0;
+};
+
+// Device buffer that grows on demand (never shrinks until freed).
+struct DevBuf {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    int ensure(size_t need);
+    void release();
+    template <class T> T* as() const { return static_cast<T*>(ptr); }
+};
+
+struct RenderState;   // render.cu
+void render_state_free(RenderState* rs);
+
+}  // namespace bg
+
+struct bg_ctx {
+    int device = 0;
+    int num_sms = 0;
+    size_t l2_bytes = 0;
+};
+
+struct bg_scene {
+    bg_ctx* ctx = nullptr;
+    std::mutex mu;
+    std::vector<bg::MeshHost> meshes;
+    std::vector<bg_material_desc> mats;
+    std::vector<bg_light_desc> lights;
+    float bg[3] = {0.f, 0.f, 0.f};
+    bool committed = false;
+
+    bg::DevBuf nodes, tris, shade, bundles, mats_d, lights_d, err;
+    bg::DevBuf work;          // persistent-kernel work counters (scratch)
+    std::atomic<unsigned> work_slot{0};
+    bg::DevBuf host_rays, host_out;   // staging for the *_host entry points
+    bg::DevScene dev{};
+    bg_scene_info info{};
+    bg::RenderState* render = nullptr;
+    int trace_blocks_closest = 0, trace_blocks_any = 0, trace_blocks_count = 0;
+};
+
+namespace bg {
+// Launch helpers (api.cu)
+constexpr int kTraceThreads = 128;
+constexpr int kWorkSlots = 256;
+unsigned long long* next_work_counter(bg_scene* s);
+int launch_trace(bg_scene* s, bool any_hit, const float4* rays, int64_t n_static, const int* n_dev,
+                 bg_hit* hits, uint8_t* occ, cudaStream_t st);
+}  // namespace bg

@@ -1,0 +1,205 @@
+// Closest-hit / any-hit traversal of the 4-wide BVH.
+//
+// Replaces Bvh::Intersect(ray, Hit&) and Bvh::Intersect(ray)
+// (accelerator/bvh.cpp:499-647) together with Mesh::IntersectShape /
+// IntersectFace (primitive/mesh.cpp:7-45, 216-261):
+//   * a triangle is accepted when its Moller-Trumbore t is in (tmin, best],
+//     computed with the reference's exact operation order in the bundle's
+//     object space (ray transformed by minv as transform_ray does,
+//     math/mathutils.h:154-157; skipped for identity bundles, where it is exact);
+//   * the box test is this project's own: a slab test with a relative slack of
+//     4e-7 on the exit distance (more than the 2*gamma(3) rounding bound of
+//     (lo - o) * (1/d)), so no box that holds an accepted triangle is culled.
+// Children are visited nearest-first; stack entries keep their entry distance
+// and are culled against the current closest hit when popped.
+#pragma once
+
+#include "device_common.cuh"
+#include "scene_types.h"
+#include "../../include/banshee_gpu.h"
+
+namespace bg {
+
+constexpr int kStackSize = 64;     // entries per ray; the builder checks max_stack against it
+constexpr int kRefillSteps = 24;   // traversal steps between warp refill points
+constexpr float kBoxSlack = 4e-7f;
+
+struct Ray {
+    v3 o, d, inv;
+    float tmin, tmax;
+    uint32_t oct;    // bit k set: direction component k is negative (sign of 1/d)
+};
+
+__device__ __forceinline__ Ray make_ray(float4 a, float4 b) {
+    Ray r;
+    r.o = mk(a.x, a.y, a.z); r.tmin = a.w;
+    r.d = mk(b.x, b.y, b.z); r.tmax = b.w;
+    r.inv = mk(1.f / r.d.x, 1.f / r.d.y, 1.f / r.d.z);
+    r.oct = (signbit(r.inv.x) ? 1u : 0u) | (signbit(r.inv.y) ? 2u : 0u) | (signbit(r.inv.z) ? 4u : 0u);
+    return r;
+}
+
+// Mesh::IntersectFace (primitive/mesh.cpp:7-45), bit-exact.
+__device__ __forceinline__ bool mt_test(v3 o, v3 d, v3 p1, v3 e1, v3 e2, float tmin, float tmax,
+                                        float& t, float& a, float& b) {
+    v3 s1 = cross(d, e2);
+    float invd = 1.f / dot(s1, e1);
+    v3 dd = sub(o, p1);
+    float b1 = dot(dd, s1) * invd;
+    if (b1 < 0.f || b1 > 1.f) return false;
+    v3 s2 = cross(dd, e1);
+    float b2 = dot(d, s2) * invd;
+    if (b2 < 0.f || b1 + b2 > 1.f) return false;
+    float tmp = dot(e2, s2) * invd;
+    if (tmp > tmin && tmp <= tmax) {
+        t = tmp; a = b1; b = b2;
+        return true;
+    }
+    return false;
+}
+
+struct ObjRay {          // ray in the object space of bundle `bundle`
+    int bundle;
+    v3 o, d;
+};
+
+__device__ __forceinline__ void obj_ray(const DevScene& S, const Ray& r, int b, ObjRay& c) {
+    if (b == c.bundle) return;
+    c.bundle = b;
+    if (b < 0) { c.o = r.o; c.d = r.d; return; }
+    const float* mi = S.bundles[b].minv;
+    float m[12];
+#pragma unroll
+    for (int k = 0; k < 12; ++k) m[k] = __ldg(mi + k);
+    c.o = xf_point(m, r.o);
+    c.d = xf_vector(m, r.d);
+}
+
+// Test the 4 children of node `ni`; returns a hit mask and entry distances.
+__device__ __forceinline__ uint32_t box4(const WideNode4* __restrict__ nodes, int ni, const Ray& r, float best,
+                                         float tn[4], int32_t ch[4]) {
+    const float4* p = reinterpret_cast<const float4*>(nodes + ni);
+    float4 lx = __ldg(p + 0), hx = __ldg(p + 1), ly = __ldg(p + 2), hy = __ldg(p + 3);
+    float4 lz = __ldg(p + 4), hz = __ldg(p + 5);
+    int4 c = __ldg(reinterpret_cast<const int4*>(p + 6));
+    const bool nx = r.oct & 1u, ny = r.oct & 2u, nz = r.oct & 4u;
+    float lxa[4] = {lx.x, lx.y, lx.z, lx.w}, hxa[4] = {hx.x, hx.y, hx.z, hx.w};
+    float lya[4] = {ly.x, ly.y, ly.z, ly.w}, hya[4] = {hy.x, hy.y, hy.z, hy.w};
+    float lza[4] = {lz.x, lz.y, lz.z, lz.w}, hza[4] = {hz.x, hz.y, hz.z, hz.w};
+    ch[0] = c.x; ch[1] = c.y; ch[2] = c.z; ch[3] = c.w;
+    uint32_t mask = 0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        float ax = ((nx ? hxa[i] : lxa[i]) - r.o.x) * r.inv.x;
+        float bx = ((nx ? lxa[i] : hxa[i]) - r.o.x) * r.inv.x;
+        float ay = ((ny ? hya[i] : lya[i]) - r.o.y) * r.inv.y;
+        float by = ((ny ? lya[i] : hya[i]) - r.o.y) * r.inv.y;
+        float az = ((nz ? hza[i] : lza[i]) - r.o.z) * r.inv.z;
+        float bz = ((nz ? lza[i] : hza[i]) - r.o.z) * r.inv.z;
+        float t0 = fmaxf(fmaxf(ax, ay), fmaxf(az, r.tmin));
+        float t1 = fminf(fminf(bx, by), fminf(bz, best));
+        t1 = t1 + fabsf(t1) * kBoxSlack;
+        tn[i] = t0;
+        if (t0 <= t1) mask |= 1u << i;
+    }
+    return mask;
+}
+
+struct Counters {
+    unsigned long long nodes, tris;
+};
+
+// Per-lane traversal state kept across refill points.
+struct TravState {
+    Ray r;
+    ObjRay cache;
+    float best, u, v;
+    int prim;
+    int item;       // current node / leaf code; kNone when the stack must be popped
+    int sp;
+};
+constexpr int kNone = 0x7fffffff;   // == kEmptyChild
+
+__device__ __forceinline__ void trav_init(TravState& s, float4 a, float4 b) {
+    s.r = make_ray(a, b);
+    s.cache.bundle = -2;
+    s.best = s.r.tmax;
+    s.prim = -1;
+    s.u = s.v = 0.f;
+    s.item = 0;      // root
+    s.sp = 0;
+}
+
+// Runs at most `steps` node / leaf visits.  Returns true when the ray is done.
+template <bool ANY, bool COUNT>
+__device__ __forceinline__ bool trav_steps(const DevScene& S, TravState& s, int2* stack, int steps, Counters& cnt) {
+    for (int it = 0; it < steps; ++it) {
+        int item = s.item;
+        if (item == kNone) {
+            // pop, culling entries that start beyond the closest hit
+            bool found = false;
+            while (s.sp > 0) {
+                int2 e = stack[--s.sp];
+                if (!ANY && __int_as_float(e.y) > s.best) continue;
+                item = e.x;
+                found = true;
+                break;
+            }
+            if (!found) return true;
+        }
+        if (item >= 0) {
+            float tn[4];
+            int32_t ch[4];
+            if (COUNT) ++cnt.nodes;
+            uint32_t mask = box4(S.nodes, item, s.r, s.best, tn, ch);
+            // sort hit children by entry distance (at most 4)
+            int hc[4];
+            float ht[4];
+            int nh = 0;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                if (mask & (1u << i)) { hc[nh] = ch[i]; ht[nh] = tn[i]; ++nh; }
+            }
+            if (nh == 0) { s.item = kNone; continue; }
+#pragma unroll
+            for (int i = 1; i < 4; ++i) {
+                if (i < nh) {
+                    float kt = ht[i];
+                    int kc = hc[i];
+                    int j = i - 1;
+                    while (j >= 0 && ht[j] > kt) { ht[j + 1] = ht[j]; hc[j + 1] = hc[j]; --j; }
+                    ht[j + 1] = kt; hc[j + 1] = kc;
+                }
+            }
+            // push the farther ones (farthest first), continue with the nearest
+            if (s.sp + nh - 1 > kStackSize) {
+                atomicOr(S.errflags, BG_FLAG_STACK_OVERFLOW);
+                return true;
+            }
+            for (int i = nh - 1; i >= 1; --i) stack[s.sp++] = make_int2(hc[i], __float_as_int(ht[i]));
+            s.item = hc[0];
+        } else {
+            // leaf: bit 31 set, count-1 in bits 27..30, first triangle in bits 0..26
+            uint32_t code = uint32_t(item);
+            int count = int((code >> kLeafStartBits) & 15u) + 1;
+            int start = int(code & uint32_t(kMaxLeafStart));
+            for (int k = 0; k < count; ++k) {
+                const float4* tp = reinterpret_cast<const float4*>(S.tris + start + k);
+                float4 v0 = __ldg(tp), e1 = __ldg(tp + 1), e2 = __ldg(tp + 2);
+                if (COUNT) ++cnt.tris;
+                obj_ray(S, s.r, __float_as_int(v0.w), s.cache);
+                float t, a, b;
+                if (mt_test(s.cache.o, s.cache.d, mk(v0.x, v0.y, v0.z), mk(e1.x, e1.y, e1.z), mk(e2.x, e2.y, e2.z),
+                            s.r.tmin, ANY ? s.r.tmax : s.best, t, a, b)) {
+                    s.prim = __float_as_int(e1.w);
+                    if (ANY) return true;
+                    s.best = t; s.u = a; s.v = b;
+                }
+            }
+            s.item = kNone;
+        }
+    }
+    return false;
+}
+
+}  // namespace bg
