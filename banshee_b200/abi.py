@@ -67,8 +67,12 @@ class SceneInfo(C.Structure):
                 ("nmaterials", C.c_int32), ("nlights", C.c_int32), ("build_ms", C.c_double)]
 
 
+BG_RENDER_TIME_PHASES = 0x1
+BG_RENDER_COUNT_TRAVERSAL = 0x2
+
+
 class TracerDesc(C.Structure):
-    _fields_ = [("kind", C.c_int32), ("maxdepth", C.c_int32)]
+    _fields_ = [("kind", C.c_int32), ("maxdepth", C.c_int32), ("flags", C.c_int32), ("reserved", C.c_int32)]
 
 
 class SamplerDesc(C.Structure):
@@ -77,9 +81,14 @@ class SamplerDesc(C.Structure):
 
 
 class RenderStats(C.Structure):
-    _fields_ = [("camera_samples", C.c_int64), ("rays_closest", C.c_int64), ("rays_any", C.c_int64),
-                ("ms_total", C.c_float), ("ms_extend", C.c_float), ("ms_shadow", C.c_float),
-                ("ms_shade", C.c_float)]
+    _fields_ = [("camera_samples", C.c_int64), ("rays_extension", C.c_int64), ("rays_closest", C.c_int64),
+                ("rays_any", C.c_int64), ("kernel_launches", C.c_int64),
+                ("ms_total", C.c_float), ("ms_extend", C.c_float), ("ms_mis", C.c_float), ("ms_shadow", C.c_float),
+                ("ms_shade", C.c_float), ("launches_extend", C.c_int32),
+                ("sub_rays_extension", C.c_int64), ("sub_nodes_extension", C.c_int64),
+                ("sub_tris_extension", C.c_int64),
+                ("sub_rays_any", C.c_int64), ("sub_nodes_any", C.c_int64), ("sub_tris_any", C.c_int64),
+                ("sub_rays_mis", C.c_int64), ("sub_nodes_mis", C.c_int64), ("sub_tris_mis", C.c_int64)]
 
 
 def fptr(a):

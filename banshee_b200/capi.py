@@ -164,25 +164,28 @@ class GpuScene:
         return a.value, b.value
 
     def render(self, accum_dev, width, height, spp, seed=1, sample_offset=0, tracer=abi.BG_TRACER_GI,
-               maxdepth=5, camera=None, stream=None):
+               maxdepth=5, camera=None, stream=None, flags=0, stats=True):
+        """Asynchronous on `stream` unless stats=True (statistics synchronize)."""
         cam = self.scene.camera_desc() if camera is None else camera
-        tr = abi.TracerDesc(tracer, maxdepth)
+        tr = abi.TracerDesc(tracer, maxdepth, flags, 0)
         sm = abi.SamplerDesc(0, spp, seed, sample_offset, 0)
         st = abi.RenderStats()
         check(lib().bg_render(self.h, C.byref(cam), C.byref(tr), C.byref(sm), int(width), int(height),
-                              accum_dev, C.byref(st), _stream_handle(stream)))
-        return {k: getattr(st, k) for k, _ in abi.RenderStats._fields_}
+                              accum_dev, C.byref(st) if stats else None, _stream_handle(stream)))
+        return {k: getattr(st, k) for k, _ in abi.RenderStats._fields_} if stats else None
 
     def render_host(self, width, height, spp, seed=1, sample_offset=0, tracer=abi.BG_TRACER_GI, maxdepth=5,
-                    camera=None, accum=None):
+                    camera=None, accum=None, stats=None, flags=0):
         cam = self.scene.camera_desc() if camera is None else camera
         if accum is None:
             accum = np.zeros((height, width, 4), dtype=np.float32)
-        tr = abi.TracerDesc(tracer, maxdepth)
+        tr = abi.TracerDesc(tracer, maxdepth, flags, 0)
         sm = abi.SamplerDesc(0, spp, seed, sample_offset, 0)
         st = abi.RenderStats()
         check(lib().bg_render_host(self.h, C.byref(cam), C.byref(tr), C.byref(sm), int(width), int(height),
                                    accum.ctypes.data, C.byref(st)))
+        if stats is not None:
+            stats.update({k: getattr(st, k) for k, _ in abi.RenderStats._fields_})
         return accum
 
     def close(self):

@@ -60,12 +60,14 @@ template <bool ANY, bool COUNT>
 __global__ void __launch_bounds__(kTraceThreads)
 k_trace(DevScene S, const float4* __restrict__ rays, int64_t n_static, const int* __restrict__ n_dev,
         bg_hit* __restrict__ hits, uint8_t* __restrict__ occ, unsigned long long* __restrict__ work,
-        unsigned long long* __restrict__ counters) {
-    const int64_t n = n_dev ? int64_t(*n_dev) : n_static;
+        unsigned long long* __restrict__ counters, int stride) {
+    // COUNT: instrumented replay of rays 0, stride, 2*stride, ... (outputs compacted)
+    const int64_t n_all = n_dev ? int64_t(*n_dev) : n_static;
+    const int64_t n = COUNT ? (n_all + stride - 1) / stride : n_all;
     const unsigned lane = threadIdx.x & 31u;
     int2 stack[kStackSize];
     TravState s;
-    Counters cnt{0ull, 0ull};
+    Counters cnt{0ull, 0ull, 0ull};
     int64_t ridx = -1;
     bool active = false, exhausted = false;
     for (;;) {
@@ -82,8 +84,10 @@ k_trace(DevScene S, const float4* __restrict__ rays, int64_t n_static, const int
                     int64_t my = int64_t(base) + __popc(need & ((1u << lane) - 1u));
                     if (my < n) {
                         ridx = my;
-                        float4 a = __ldg(rays + 2 * my), b = __ldg(rays + 2 * my + 1);
+                        const int64_t src = COUNT ? my * stride : my;
+                        float4 a = __ldg(rays + 2 * src), b = __ldg(rays + 2 * src + 1);
                         trav_init(s, a, b);
+                        if (COUNT) ++cnt.rays;
                         active = true;
                     }
                 }
@@ -108,12 +112,14 @@ k_trace(DevScene S, const float4* __restrict__ rays, int64_t n_static, const int
     }
     if (COUNT) {
         for (int off = 16; off > 0; off >>= 1) {
+            cnt.rays += __shfl_down_sync(0xffffffffu, cnt.rays, off);
             cnt.nodes += __shfl_down_sync(0xffffffffu, cnt.nodes, off);
             cnt.tris += __shfl_down_sync(0xffffffffu, cnt.tris, off);
         }
         if (lane == 0) {
-            atomicAdd(counters, cnt.nodes);
-            atomicAdd(counters + 1, cnt.tris);
+            atomicAdd(counters, cnt.rays);
+            atomicAdd(counters + 1, cnt.nodes);
+            atomicAdd(counters + 2, cnt.tris);
         }
     }
 }
@@ -132,13 +138,19 @@ unsigned long long* next_work_counter(bg_scene* s) {
 }
 
 int launch_trace(bg_scene* s, bool any_hit, const float4* rays, int64_t n_static, const int* n_dev,
-                 bg_hit* hits, uint8_t* occ, cudaStream_t st) {
+                 bg_hit* hits, uint8_t* occ, cudaStream_t st, unsigned long long* counters, int stride) {
     unsigned long long* w = next_work_counter(s);
     BG_CUDA(cudaMemsetAsync(w, 0, sizeof(unsigned long long), st));
-    if (any_hit)
-        k_trace<true, false><<<s->trace_blocks_any, kTraceThreads, 0, st>>>(s->dev, rays, n_static, n_dev, hits, occ, w, nullptr);
-    else
-        k_trace<false, false><<<s->trace_blocks_closest, kTraceThreads, 0, st>>>(s->dev, rays, n_static, n_dev, hits, occ, w, nullptr);
+    if (counters) {
+        if (any_hit)
+            k_trace<true, true><<<s->trace_blocks_count, kTraceThreads, 0, st>>>(s->dev, rays, n_static, n_dev, hits, occ, w, counters, stride);
+        else
+            k_trace<false, true><<<s->trace_blocks_count, kTraceThreads, 0, st>>>(s->dev, rays, n_static, n_dev, hits, occ, w, counters, stride);
+    } else if (any_hit) {
+        k_trace<true, false><<<s->trace_blocks_any, kTraceThreads, 0, st>>>(s->dev, rays, n_static, n_dev, hits, occ, w, nullptr, 1);
+    } else {
+        k_trace<false, false><<<s->trace_blocks_closest, kTraceThreads, 0, st>>>(s->dev, rays, n_static, n_dev, hits, occ, w, nullptr, 1);
+    }
     BG_CUDA(cudaGetLastError());
     return BG_OK;
 }
@@ -196,6 +208,14 @@ static int commit_scene(bg_scene* s, const bg_build_opts* opts) {
                 return set_error(BG_ERR_INVALID_ARG, "AreaLight: The material passed is not an emissive one (light %zu)", li);
             L.matidx = mi;
             for (int k = 0; k < 3; ++k) L.e[k] = s->mats[mi].e[k];
+            const MeshHost& mh = s->meshes[d.mesh];
+            const int f = d.face;
+            v3 p1 = mh.verts[mh.vi[3 * f]], p2 = mh.verts[mh.vi[3 * f + 1]], p3 = mh.verts[mh.vi[3 * f + 2]];
+            L.pdf_obj = 1.f / (sqrtf(fabsf(sqnorm(cross(sub(p3, p1), sub(p3, p2))))) * 0.5f);
+            float m12[12];
+            memcpy(m12, mh.xf, sizeof(m12));
+            v3 w1 = xf_point(m12, p1), w2 = xf_point(m12, p2), w3 = xf_point(m12, p3);
+            L.area_world = sqrtf(fabsf(sqnorm(cross(sub(w3, w1), sub(w3, w2))))) * 0.5f;
             bundles[d.mesh].arealight = int(li);   // last one wins, light/arealight.cpp:22
         } else if (d.type == BG_LIGHT_DIRECTIONAL) {
             v3 n = normalize(mk(d.d[0], d.d[1], d.d[2]));
@@ -594,28 +614,22 @@ int bg_traversal_counts(bg_scene* s, const bg_ray* rays, int64_t n, int32_t any_
     if (!triangles) return set_error(BG_ERR_INVALID_ARG, "triangles is NULL");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     DevBuf tmp;
-    if ((rc = tmp.ensure(2 * sizeof(unsigned long long) + (any_hit ? size_t(n) : size_t(n) * sizeof(bg_hit))))) return rc;
+    if ((rc = tmp.ensure(256 + (any_hit ? size_t(n) : size_t(n) * sizeof(bg_hit))))) return rc;
     unsigned long long* cnt = tmp.as<unsigned long long>();
-    cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned long long), st);
-    unsigned long long* w = next_work_counter(s);
-    cudaMemsetAsync(w, 0, sizeof(unsigned long long), st);
-    bg_hit* hits = reinterpret_cast<bg_hit*>(reinterpret_cast<char*>(tmp.ptr) + 16);
-    uint8_t* occ = reinterpret_cast<uint8_t*>(tmp.ptr) + 16;
-    if (n > 0) {
-        if (any_hit)
-            k_trace<true, true><<<s->trace_blocks_count, kTraceThreads, 0, st>>>(s->dev, reinterpret_cast<const float4*>(rays), n, nullptr, nullptr, occ, w, cnt);
-        else
-            k_trace<false, true><<<s->trace_blocks_count, kTraceThreads, 0, st>>>(s->dev, reinterpret_cast<const float4*>(rays), n, nullptr, hits, nullptr, w, cnt);
+    bg_hit* hits = reinterpret_cast<bg_hit*>(tmp.as<char>() + 256);
+    uint8_t* occ = tmp.as<uint8_t>() + 256;
+    cudaError_t e = cudaMemsetAsync(cnt, 0, 3 * sizeof(unsigned long long), st);
+    if (e == cudaSuccess && n > 0) {
+        rc = launch_trace(s, any_hit != 0, reinterpret_cast<const float4*>(rays), n, nullptr, hits, occ, st, cnt, 1);
+        if (rc) { tmp.release(); return rc; }
     }
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) { tmp.release(); return set_error(BG_ERR_CUDA, "count kernel: %s", cudaGetErrorString(e)); }
-    unsigned long long h[2];
-    e = cudaMemcpyAsync(h, cnt, sizeof(h), cudaMemcpyDeviceToHost, st);
+    unsigned long long h[3] = {0, 0, 0};
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h, cnt, sizeof(h), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     tmp.release();
-    if (e != cudaSuccess) return set_error(BG_ERR_CUDA, "count readback: %s", cudaGetErrorString(e));
-    *nodes = h[0];
-    *triangles = h[1];
+    if (e != cudaSuccess) return set_error(BG_ERR_CUDA, "traversal counts: %s", cudaGetErrorString(e));
+    *nodes = h[1];
+    *triangles = h[2];
     return BG_OK;
 }
 

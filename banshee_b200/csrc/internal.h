@@ -79,5 +79,6 @@ constexpr int kTraceThreads = 128;
 constexpr int kWorkSlots = 256;
 unsigned long long* next_work_counter(bg_scene* s);
 int launch_trace(bg_scene* s, bool any_hit, const float4* rays, int64_t n_static, const int* n_dev,
-                 bg_hit* hits, uint8_t* occ, cudaStream_t st);
+                 bg_hit* hits, uint8_t* occ, cudaStream_t st, unsigned long long* counters = nullptr,
+                 int stride = 1);
 }  // namespace bg

@@ -1,16 +1,661 @@
-// Wavefront GI / DI renderer (filled in below).
+// Wavefront GI / DI renderer: Renderer::Render + GiTracer / DiTracer on the GPU.
+//
+// The recursive per-sample GiTracer::GetLi (tracer/gitracer.cpp:13-140) and
+// DiTracer::GetDi (tracer/ditracer.cpp:57-239) become one wave of paths per
+// bounce:
+//   generate  camera rays + per-sample samplers           (renderer/imagerenderer.cpp:25-38)
+//   extend    closest hit of the extension rays           (persistent k_trace)
+//   shade     gather last bounce's direct light, FillHit, light sampling and
+//             BSDF sampling for MIS, BSDF continuation, Russian roulette;
+//             pushes shadow / MIS / extension rays through warp-aggregated
+//             atomics (ballot + prefix count, one atomic per warp)
+//   shadow    any hit of light-sample and environment-MIS rays
+//   mis       closest hit of BSDF-sampled rays towards area lights
+//   resolve   write each visible contribution to its path's fixed DI slot
+//   finalize  gather pending slots, clamp (gitracer.cpp:139), per-sample radiance
+//   accumulate per pixel, samples in order: FileImagePlane::WriteSample
+//             (imageplane/fileimageplane.cpp:29-34), rows flipped
+// Each path owns 2 * nlights DI slots (light-sample and BSDF-sample term per
+// light), summed in light order like GetDi, so images are deterministic.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
 #include "internal.h"
+#include "shading.cuh"
 
 namespace bg {
-struct RenderState {};
-void render_state_free(RenderState* rs) { delete rs; }
+
+constexpr int kShadeThreads = 128;
+
+struct CamDev {        // PerscpectiveCamera frame, computed on the host (perspective_camera.cpp:5-23)
+    float fwd[3], right[3], up[3], p[3];
+    float znear, zfar, dimx, dimy;
+};
+
+struct RenderState {
+    int64_t cap = 0;   // paths per pass
+    int kmax = 0;      // DI slots per path
+    int nlights = 0;
+    DevBuf ext_rays[2], ext_path[2], ext_hits;
+    DevBuf sh_rays, sh_contrib, sh_slot, sh_occ;
+    DevBuf mis_rays, mis_a, mis_b, mis_c, mis_hits;
+    DevBuf end_path;
+    DevBuf counts;     // int: ext[0], ext[1], sh, mis, end ; u64 totals at +64 bytes
+    DevBuf st_key, st_cnt, st_rng, st_bs, st_thr, st_rad, st_dithr, st_flags;
+    DevBuf slots, sample_rad;
+    DevBuf cnt_out;    // outputs of the instrumented 1/64 replays
+    int blocks = 0;
+};
+
+void render_state_free(RenderState* rs) {
+    for (DevBuf* b : {&rs->ext_rays[0], &rs->ext_rays[1], &rs->ext_path[0], &rs->ext_path[1], &rs->ext_hits,
+                      &rs->sh_rays, &rs->sh_contrib, &rs->sh_slot, &rs->sh_occ, &rs->mis_rays, &rs->mis_a, &rs->mis_b,
+                      &rs->mis_c, &rs->mis_hits, &rs->end_path, &rs->counts, &rs->st_key, &rs->st_cnt, &rs->st_rng,
+                      &rs->st_bs, &rs->st_thr, &rs->st_rad, &rs->st_dithr, &rs->st_flags, &rs->slots,
+                      &rs->sample_rad, &rs->cnt_out})
+        b->release();
+    delete rs;
+}
+
+enum : int { kCntExt0 = 0, kCntExt1 = 1, kCntSh = 2, kCntMis = 3, kCntEnd = 4 };
+enum : unsigned { kFlagNoClamp = 1u };
+
+struct PathState {
+    unsigned long long* key;
+    unsigned* cnt;
+    uint4* rng;        // light McRng (z,w), BSDF McRng (z,w)
+    float2* bs;        // GiTracer's BSDF sample, reused at every bounce (gitracer.cpp:36-41,88)
+    float4* thr;       // throughput
+    float4* rad;       // radiance; w = pending DI slots (int bits)
+    float4* dithr;     // throughput of the bounce whose DI is pending; w = light-count multiplier
+    unsigned* flags;
+    float4* slots;     // cap * kmax
+    float4* sample_rad;
+};
+
+struct Queues {
+    float4* ext_rays_in; int* ext_path_in; bg_hit* ext_hits;
+    float4* ext_rays_out; int* ext_path_out;
+    float4* sh_rays; float4* sh_contrib; int* sh_slot; uint8_t* sh_occ;
+    float4* mis_rays; float4* mis_a; float4* mis_b; int4* mis_c; bg_hit* mis_hits;
+    int* end_path;
+    int* n_ext_in; int* n_ext_out; int* n_sh; int* n_mis; int* n_end;
+    unsigned long long* totals;   // [0] closest rays, [1] any rays
+};
+
+// Warp-aggregated slot allocation: one atomicAdd per converged group of lanes.
+__device__ __forceinline__ int warp_push(int* counter) {
+    unsigned m = __activemask();
+    int leader = __ffs(m) - 1;
+    unsigned lane = threadIdx.x & 31u;
+    int base = 0;
+    if (lane == unsigned(leader)) base = atomicAdd(counter, __popc(m));
+    base = __shfl_sync(m, base, leader);
+    return base + __popc(m & ((1u << lane) - 1u));
+}
+
+__device__ __forceinline__ void put_ray(float4* rays, int i, v3 o, float tmin, v3 d, float tmax) {
+    rays[2 * i] = make_float4(o.x, o.y, o.z, tmin);
+    rays[2 * i + 1] = make_float4(d.x, d.y, d.z, tmax);
+}
+
+// ------------------------------------------------------------- generate
+__global__ void __launch_bounds__(kShadeThreads)
+k_generate(CamDev cam, int np, int ns, int p0, int s0, int W, int H, uint64_t seed, PathState P, Queues Q, int total) {
+    const int nthreads = gridDim.x * blockDim.x;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += nthreads) {
+        const int sl = i / np;
+        const int pix = p0 + (i - sl * np);
+        const uint32_t s = uint32_t(s0 + sl);
+        const uint64_t key = keyed_key(seed, uint32_t(pix), s);
+        McRng img{keyed_rand(key, 0), keyed_rand(key, 1)};
+        McRng lr{keyed_rand(key, 2), keyed_rand(key, 3)};
+        McRng br{keyed_rand(key, 4), keyed_rand(key, 5)};
+        float sx, sy;
+        sample2d(img, sx, sy);
+        const int x = pix % W, y = pix / W;
+        float ix = (float)x / W + (1.f / W) * sx;
+        float iy = (float)y / H + (1.f / H) * sy;
+        // PerscpectiveCamera::GenerateRay (perspective_camera.cpp:25-38)
+        float cx = (ix - 0.5f) * cam.dimx, cy = (iy - 0.5f) * cam.dimy;
+        v3 d = normalize(add(add(muls(mk(cam.fwd[0], cam.fwd[1], cam.fwd[2]), cam.znear),
+                                 muls(mk(cam.right[0], cam.right[1], cam.right[2]), cx)),
+                             muls(mk(cam.up[0], cam.up[1], cam.up[2]), cy)));
+        put_ray(Q.ext_rays_in, i, mk(cam.p[0], cam.p[1], cam.p[2]), cam.znear, d, cam.zfar);
+        Q.ext_path_in[i] = i;
+        P.key[i] = key;
+        P.cnt[i] = 6u;
+        P.rng[i] = make_uint4(lr.z, lr.w, br.z, br.w);
+        P.thr[i] = make_float4(1.f, 1.f, 1.f, 0.f);
+        P.rad[i] = make_float4(0.f, 0.f, 0.f, __int_as_float(0));
+        P.flags[i] = 0u;
+        P.sample_rad[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) *Q.n_ext_in = total;
+}
+
+// Adds the pending direct-light slots of path `path` into its radiance in light
+// order: di = ls + bs per light (GetDi), radiance += (throughput * di) * mult.
+__device__ __forceinline__ v3 gather_pending(const PathState& P, int kmax, int path, v3 rad, int pending) {
+    if (pending == 0) return rad;
+    float4 dt = P.dithr[path];
+    v3 thr = mk(dt.x, dt.y, dt.z);
+    const float4* sl = P.slots + size_t(path) * kmax;
+    for (int j = 0; j < pending; j += 2) {
+        float4 a = sl[j], b = sl[j + 1];
+        v3 di = add(mk(a.x, a.y, a.z), mk(b.x, b.y, b.z));
+        rad = add(rad, muls(mulv(thr, di), dt.w));
+    }
+    return rad;
+}
+
+struct ShadeArgs {
+    int bounce, maxdepth, kind, kmax, nlights;
+};
+
+// One light's DirectIllumination terms (DiTracer::GetDi, ditracer.cpp:57-239, n = 1).
+__device__ __forceinline__ void emit_di(const DevScene& S, const Queues& Q, int li, const SHit& h, const MatRec& M, v3 wo,
+                                        McRng& lr, McRng& br, int slot0, int path) {
+    const LightRec L = load_light(S, li);
+    float lx, ly, bx, by;
+    sample2d(lr, lx, ly);
+    sample2d(br, bx, by);
+    const bool singular = light_singular(L);
+    float lightpdf = 0.f, bsdfpdf = 0.f;
+    v3 ldir;
+    v3 le = light_getsample(S, L, h, lx, ly, ldir, lightpdf);
+    if (lightpdf > BG_MINPDF && sqnorm(le) > 0.f) {
+        v3 wi = normalize(ldir);
+        float dist = sqrtf(sqnorm(ldir));
+        v3 bsdf = mat_eval(M, h, wi, wo);
+        float c = fabsf(dot(h.n, wi));
+        v3 ls;
+        if (singular) {
+            ls = muls(muls(mulv(le, bsdf), c), (1.f / lightpdf));
+        } else {
+            bsdfpdf = mat_pdf(M, h, wi, wo);
+            float w = power_heuristic(lightpdf, bsdfpdf);
+            ls = muls(muls(muls(mulv(le, bsdf), c), w), (1.f / lightpdf));
+        }
+        if (sqnorm(ls) > 0.f) {
+            int e = warp_push(Q.n_sh);
+            put_ray(Q.sh_rays, e, h.p, 0.01f, wi, dist - 0.01f);
+            Q.sh_contrib[e] = make_float4(ls.x, ls.y, ls.z, 0.f);
+            Q.sh_slot[e] = slot0;
+        }
+    }
+    if (!singular) {
+        int type = 0;
+        v3 wi;
+        v3 f = mat_sample(M, h, bx, by, wo, wi, bsdfpdf, type);
+        wi = normalize(wi);
+        if (sqnorm(f) > 0.f && bsdfpdf > BG_MINPDF) {
+            float w = 1.f;
+            bool skip = false;
+            if (!(type & kBsdfSpecular)) {
+                float lp = light_getpdf(S, L, h, wi);
+                if (lp < BG_MINPDF) skip = true;
+                else w = power_heuristic(bsdfpdf, lp);
+            }
+            if (!skip) {
+                float c = fabsf(dot(h.n, wi));
+                if (L.type == BG_LIGHT_ENVIRONMENT) {
+                    // a hit anywhere gives 0 (no bundle points at this light); a miss gives GetLe
+                    v3 lev = mk(L.env[0], L.env[1], L.env[2]);
+                    v3 bs = muls(muls(muls(mulv(lev, f), c), w), (1.f / bsdfpdf));
+                    if (sqnorm(bs) > 0.f) {
+                        int e = warp_push(Q.n_sh);
+                        put_ray(Q.sh_rays, e, h.p, 0.01f, wi, 10000000.f);
+                        Q.sh_contrib[e] = make_float4(bs.x, bs.y, bs.z, 0.f);
+                        Q.sh_slot[e] = slot0 + 1;
+                    }
+                } else {
+                    int e = warp_push(Q.n_mis);
+                    put_ray(Q.mis_rays, e, h.p, 0.01f, wi, 10000000.f);
+                    Q.mis_a[e] = make_float4(f.x, f.y, f.z, c);
+                    Q.mis_b[e] = make_float4(h.p.x, h.p.y, h.p.z, w);
+                    Q.mis_c[e] = make_int4(path, slot0 + 1, li, __float_as_int(1.f / bsdfpdf));
+                }
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kShadeThreads)
+k_shade(DevScene S, ShadeArgs A, PathState P, Queues Q) {
+    const int n = *Q.n_ext_in;
+    const int nthreads = gridDim.x * blockDim.x;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += nthreads) {
+        const int path = Q.ext_path_in[e];
+        const bg_hit hit = Q.ext_hits[e];
+        const float4 rd = Q.ext_rays_in[2 * e + 1];
+        const v3 d = mk(rd.x, rd.y, rd.z);
+        float4 r4 = P.rad[path];
+        v3 rad = mk(r4.x, r4.y, r4.z);
+        rad = gather_pending(P, A.kmax, path, rad, __float_as_int(r4.w));
+        unsigned flags = 0u;
+        int pending = 0;
+        bool end = false;
+        if (hit.primid < 0) {
+            if (A.bounce == 0) {        // primary miss: bgcolor + sum of GetLe, unclamped (gitracer.cpp:22-33)
+                rad = add(rad, mk(S.bg[0], S.bg[1], S.bg[2]));
+                for (int i = 0; i < S.nlights; ++i) {
+                    LightRec L = load_light(S, i);
+                    if (L.type == BG_LIGHT_ENVIRONMENT) rad = add(rad, mk(L.env[0], L.env[1], L.env[2]));
+                }
+                flags |= kFlagNoClamp;
+            }
+            end = true;
+        } else {
+            SHit h;
+            fill_hit(S, hit.primid, hit.u, hit.v, h);
+            uint4 rg = P.rng[path];
+            McRng lr{rg.x, rg.y}, br{rg.z, rg.w};
+            float2 bs;
+            if (A.bounce == 0 && A.kind == BG_TRACER_GI) {
+                sample2d(br, bs.x, bs.y);
+                P.bs[path] = bs;
+            } else {
+                bs = P.bs[path];
+            }
+            const MatRec M = load_mat(S, h.m);
+            const v3 wo = neg(d);
+            float4 t4 = P.thr[path];
+            v3 thr = mk(t4.x, t4.y, t4.z);
+            if (A.bounce == 0 && M.type == BG_MAT_EMISSIVE) {
+                if (A.kind == BG_TRACER_GI) rad = add(rad, emissive_le(M, h.n, wo));   // gitracer.cpp:61-68
+                if (A.kind == BG_TRACER_DI) flags |= kFlagNoClamp;                    // ditracer.cpp:29-32
+                end = true;
+            } else {
+                unsigned cnt = P.cnt[path];
+                const int base = path * A.kmax;
+                float mult = 1.f;
+                if (A.bounce == 0) {
+                    pending = 2 * A.nlights;
+                    for (int j = 0; j < pending; ++j) P.slots[size_t(base) + j] = make_float4(0.f, 0.f, 0.f, 0.f);
+                    for (int i = 0; i < A.nlights; ++i) emit_di(S, Q, i, h, M, wo, lr, br, base + 2 * i, path);
+                } else {
+                    int idx = int(keyed_rand(P.key[path], cnt++) % unsigned(A.nlights));   // gitracer.cpp:74-76
+                    pending = 2;
+                    P.slots[size_t(base)] = make_float4(0.f, 0.f, 0.f, 0.f);
+                    P.slots[size_t(base) + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
+                    emit_di(S, Q, idx, h, M, wo, lr, br, base, path);
+                    mult = (float)A.nlights;
+                }
+                P.dithr[path] = make_float4(thr.x, thr.y, thr.z, mult);
+                if (A.kind == BG_TRACER_DI) {
+                    flags |= kFlagNoClamp;
+                    end = true;
+                } else {
+                    // continue the path with the reused BSDF sample (gitracer.cpp:87-134)
+                    int type = 0;
+                    float pdf = 0.f;
+                    v3 wi;
+                    v3 f = mat_sample(M, h, bs.x, bs.y, wo, wi, pdf, type);
+                    if (sqnorm(f) == 0.f || pdf < BG_MINPDF) {
+                        end = true;
+                    } else {
+                        v3 nd = normalize(wi);
+                        thr = mulv(thr, muls(f, (fabsf(dot(h.n, wi)) / pdf)));
+                        if (A.bounce > 3) {
+                            float rnd = rand_float(keyed_rand(P.key[path], cnt++));
+                            float lum = 0.2126f * thr.x + 0.7152f * thr.y + 0.0722f * thr.z;
+                            float q = fmin_std(0.5f, lum);
+                            if (rnd > q) end = true;
+                            else thr = muls(thr, (1.f / q));
+                        }
+                        if (!end && A.bounce + 1 >= A.maxdepth) end = true;   // loop ends before the next hit is used
+                        if (!end) {
+                            int k = warp_push(Q.n_ext_out);
+                            put_ray(Q.ext_rays_out, k, h.p, 0.01f, nd, 1000000.f);
+                            Q.ext_path_out[k] = path;
+                        }
+                        P.thr[path] = make_float4(thr.x, thr.y, thr.z, 0.f);
+                    }
+                }
+                P.cnt[path] = cnt;
+                P.rng[path] = make_uint4(lr.z, lr.w, br.z, br.w);
+            }
+        }
+        P.rad[path] = make_float4(rad.x, rad.y, rad.z, __int_as_float(pending));
+        if (end) {
+            P.flags[path] = flags;
+            int k = warp_push(Q.n_end);
+            Q.end_path[k] = path;
+        }
+    }
+}
+
+// Visible light-sample / environment terms land in their slot.
+__global__ void __launch_bounds__(kShadeThreads)
+k_resolve_shadow(PathState P, Queues Q) {
+    const int n = *Q.n_sh;
+    const int nthreads = gridDim.x * blockDim.x;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += nthreads)
+        if (!Q.sh_occ[e]) P.slots[Q.sh_slot[e]] = Q.sh_contrib[e];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        Q.totals[0] += (unsigned long long)*Q.n_ext_in;
+        Q.totals[1] += (unsigned long long)n;
+        Q.totals[2] += (unsigned long long)*Q.n_mis;
+    }
+}
+
+// BSDF-sampled rays towards area lights: the closest hit must be on a bundle
+// whose (last registered) area light is this one, front facing
+// (ditracer.cpp:199-220).
+__global__ void __launch_bounds__(kShadeThreads)
+k_resolve_mis(DevScene S, PathState P, Queues Q) {
+    const int n = *Q.n_mis;
+    const int nthreads = gridDim.x * blockDim.x;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += nthreads) {
+        const bg_hit hit = Q.mis_hits[e];
+        if (hit.primid < 0) continue;   // area lights emit nothing on a miss
+        const int4 c = Q.mis_c[e];
+        const int bundle = __float_as_int(__ldg(&S.shade[hit.primid].a.w));
+        if (__ldg(&S.bundles[bundle].arealight) != c.z) continue;
+        SHit h;
+        fill_hit(S, hit.primid, hit.u, hit.v, h);
+        const float4 rd = Q.mis_rays[2 * e + 1];
+        const v3 wi = mk(rd.x, rd.y, rd.z);
+        const float4 a = Q.mis_a[e], b = Q.mis_b[e];
+        v3 dd = sub(h.p, mk(b.x, b.y, b.z));
+        if (!(dot(h.n, neg(wi)) > 0.f)) continue;
+        float d2inv = 1.f / sqnorm(dd);
+        const MatRec M = load_mat(S, h.m);
+        if (M.type != BG_MAT_EMISSIVE) continue;
+        v3 le = muls(emissive_le(M, h.n, neg(wi)), d2inv);
+        if (!(sqnorm(le) > 0.f)) continue;
+        v3 bs = muls(muls(muls(mulv(le, mk(a.x, a.y, a.z)), a.w), b.w), __int_as_float(c.w));
+        P.slots[c.y] = make_float4(bs.x, bs.y, bs.z, 0.f);
+    }
+}
+
+__global__ void __launch_bounds__(kShadeThreads)
+k_finalize(PathState P, Queues Q, int kmax) {
+    const int n = *Q.n_end;
+    const int nthreads = gridDim.x * blockDim.x;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += nthreads) {
+        const int path = Q.end_path[e];
+        float4 r4 = P.rad[path];
+        v3 rad = gather_pending(P, kmax, path, mk(r4.x, r4.y, r4.z), __float_as_int(r4.w));
+        if (!(P.flags[path] & kFlagNoClamp)) {
+            v3 r = muls(rad, (1.f / 1));
+            rad = mk(clamp_ref(r.x, 0.f, BG_MAXRADIANCE), clamp_ref(r.y, 0.f, BG_MAXRADIANCE), clamp_ref(r.z, 0.f, BG_MAXRADIANCE));
+        }
+        P.sample_rad[path] = make_float4(rad.x, rad.y, rad.z, 1.f);
+    }
+}
+
+// FileImagePlane::WriteSample per pixel, samples in order (rows flipped).
+__global__ void __launch_bounds__(kShadeThreads)
+k_accumulate(PathState P, int np, int ns, int p0, int W, int H, float4* accum) {
+    const int nthreads = gridDim.x * blockDim.x;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np; i += nthreads) {
+        const int pix = p0 + i;
+        const int x = pix % W, y = pix / W;
+        float4* px = accum + size_t(W) * size_t(H - 1 - y) + x;
+        float4 acc = *px;
+        for (int s = 0; s < ns; ++s) {
+            float4 v = P.sample_rad[size_t(s) * np + i];
+            acc.x += v.x; acc.y += v.y; acc.z += v.z; acc.w += 1.f;
+        }
+        *px = acc;
+    }
+}
+
+static CamDev make_camera(const bg_camera_desc* c) {
+    CamDev k;
+    v3 eye = mk(c->eye[0], c->eye[1], c->eye[2]), at = mk(c->at[0], c->at[1], c->at[2]), up = mk(c->up[0], c->up[1], c->up[2]);
+    v3 fwd = normalize(sub(at, eye));
+    v3 right = cross(fwd, normalize(up));
+    v3 u = cross(right, fwd);
+    k.fwd[0] = fwd.x; k.fwd[1] = fwd.y; k.fwd[2] = fwd.z;
+    k.right[0] = right.x; k.right[1] = right.y; k.right[2] = right.z;
+    k.up[0] = u.x; k.up[1] = u.y; k.up[2] = u.z;
+    k.p[0] = eye.x; k.p[1] = eye.y; k.p[2] = eye.z;
+    k.znear = c->znear;
+    k.zfar = c->zfar;
+    k.dimx = 2 * tanf(c->fovy * 0.5f) * c->znear;
+    k.dimy = k.dimx / c->aspect;
+    return k;
+}
+
+static int ensure_state(bg_scene* s, int64_t cap) {
+    RenderState* rs = s->render;
+    const int L = std::max(1, s->dev.nlights);
+    if (rs && rs->cap >= cap && rs->nlights == L) return BG_OK;
+    if (rs) render_state_free(rs);
+    rs = s->render = new RenderState();
+    rs->cap = cap;
+    rs->nlights = L;
+    rs->kmax = 2 * L;
+    const size_t C = size_t(cap);
+    int rc;
+    for (int k = 0; k < 2; ++k) {
+        if ((rc = rs->ext_rays[k].ensure(C * 32)) || (rc = rs->ext_path[k].ensure(C * 4))) return rc;
+    }
+    if ((rc = rs->ext_hits.ensure(C * 16)) ||
+        (rc = rs->sh_rays.ensure(C * 2 * L * 32)) || (rc = rs->sh_contrib.ensure(C * 2 * L * 16)) ||
+        (rc = rs->sh_slot.ensure(C * 2 * L * 4)) || (rc = rs->sh_occ.ensure(C * 2 * L)) ||
+        (rc = rs->mis_rays.ensure(C * L * 32)) || (rc = rs->mis_a.ensure(C * L * 16)) ||
+        (rc = rs->mis_b.ensure(C * L * 16)) || (rc = rs->mis_c.ensure(C * L * 16)) ||
+        (rc = rs->mis_hits.ensure(C * L * 16)) || (rc = rs->end_path.ensure(C * 4)) ||
+        (rc = rs->counts.ensure(256)) ||
+        (rc = rs->st_key.ensure(C * 8)) || (rc = rs->st_cnt.ensure(C * 4)) || (rc = rs->st_rng.ensure(C * 16)) ||
+        (rc = rs->st_bs.ensure(C * 8)) || (rc = rs->st_thr.ensure(C * 16)) || (rc = rs->st_rad.ensure(C * 16)) ||
+        (rc = rs->st_dithr.ensure(C * 16)) || (rc = rs->st_flags.ensure(C * 4)) ||
+        (rc = rs->slots.ensure(C * rs->kmax * 16)) || (rc = rs->sample_rad.ensure(C * 16)) ||
+        (rc = rs->cnt_out.ensure((C * 2 * L / 64 + 64) * 16)))
+        return rc;
+    int nb = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_shade, kShadeThreads, 0);
+    rs->blocks = std::max(1, nb) * s->ctx->num_sms;
+    return BG_OK;
+}
+
+static int render_impl(bg_scene* s, const bg_camera_desc* cam, const bg_tracer_desc* tr, const bg_sampler_desc* sm,
+                       int W, int H, float4* accum, bg_render_stats* stats, cudaStream_t st) {
+    if (!s) return set_error(BG_ERR_INVALID_ARG, "scene is NULL");
+    if (!s->committed) return set_error(BG_ERR_STATE, "scene not committed");
+    if (!cam || !tr || !sm || !accum) return set_error(BG_ERR_INVALID_ARG, "NULL argument");
+    if (W <= 0 || H <= 0 || int64_t(W) * H > (int64_t(1) << 28)) return set_error(BG_ERR_INVALID_ARG, "bad resolution %dx%d", W, H);
+    if (sm->kind != 0) return set_error(BG_ERR_UNSUPPORTED, "sampler kind %d", sm->kind);
+    if (sm->spp < 0 || sm->sample_offset < 0) return set_error(BG_ERR_INVALID_ARG, "negative spp / sample offset");
+    if (tr->kind != BG_TRACER_GI && tr->kind != BG_TRACER_DI) return set_error(BG_ERR_UNSUPPORTED, "tracer kind %d", tr->kind);
+    if (tr->kind == BG_TRACER_GI && (tr->maxdepth < 0 || tr->maxdepth > 1024)) return set_error(BG_ERR_INVALID_ARG, "maxdepth %d", tr->maxdepth);
+    if (s->dev.nlights == 0) return set_error(BG_ERR_UNSUPPORTED, "a scene without lights (GiTracer divides by the light count)");
+    if (reinterpret_cast<uintptr_t>(accum) & 15u) return set_error(BG_ERR_INVALID_ARG, "accumulation buffer must be 16-byte aligned");
+    const int64_t npix = int64_t(W) * H;
+    const int64_t target = int64_t(1) << 21;   // paths per pass
+    int64_t cap = std::min<int64_t>(std::max<int64_t>(npix, 1), target);
+    if (npix < target) cap = std::min<int64_t>(target, npix * std::max(1, sm->spp));
+    cap = std::max<int64_t>(cap, 1);
+    int rc = ensure_state(s, cap);
+    if (rc) return rc;
+    RenderState* rs = s->render;
+    const CamDev camd = make_camera(cam);
+    PathState P;
+    P.key = rs->st_key.as<unsigned long long>();
+    P.cnt = rs->st_cnt.as<unsigned>();
+    P.rng = rs->st_rng.as<uint4>();
+    P.bs = rs->st_bs.as<float2>();
+    P.thr = rs->st_thr.as<float4>();
+    P.rad = rs->st_rad.as<float4>();
+    P.dithr = rs->st_dithr.as<float4>();
+    P.flags = rs->st_flags.as<unsigned>();
+    P.slots = rs->slots.as<float4>();
+    P.sample_rad = rs->sample_rad.as<float4>();
+    int* cnt = rs->counts.as<int>();
+    unsigned long long* totals = reinterpret_cast<unsigned long long*>(rs->counts.as<char>() + 64);
+    // totals: [0] extension rays, [1] any rays, [2] MIS rays, replays (rays, nodes, tris):
+    // [3..5] extension, [6..8] any, [9..11] MIS
+    BG_CUDA(cudaMemsetAsync(totals, 0, 12 * sizeof(unsigned long long), st));
+    const bool time_phases = stats && (tr->flags & BG_RENDER_TIME_PHASES);
+    const bool count_trav = stats && (tr->flags & BG_RENDER_COUNT_TRAVERSAL);
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::vector<cudaEvent_t> evs;   // begin/end pairs: phase tag in evtag
+    std::vector<int> evtag;
+    auto mark = [&](int tag) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        cudaEventRecord(e, st);
+        evs.push_back(e);
+        evtag.push_back(tag);
+    };
+    int64_t launches = 0;
+    int launches_extend = 0;
+    if (stats) {
+        cudaEventCreate(&ev0);
+        cudaEventCreate(&ev1);
+        cudaEventRecord(ev0, st);
+    }
+    const int maxdepth = tr->kind == BG_TRACER_DI ? 1 : tr->maxdepth;
+    const int nb = rs->blocks;
+    int64_t done_samples = 0;
+    for (int64_t p0 = 0; p0 < npix; p0 += cap) {
+        const int np = int(std::min<int64_t>(cap, npix - p0));
+        for (int s0 = 0; s0 < sm->spp;) {
+            const int ns = int(std::max<int64_t>(1, std::min<int64_t>(sm->spp - s0, cap / np)));
+            const int total = np * ns;
+            int cur = 0;
+            Queues Q;
+            Q.ext_hits = rs->ext_hits.as<bg_hit>();
+            Q.sh_rays = rs->sh_rays.as<float4>(); Q.sh_contrib = rs->sh_contrib.as<float4>();
+            Q.sh_slot = rs->sh_slot.as<int>(); Q.sh_occ = rs->sh_occ.as<uint8_t>();
+            Q.mis_rays = rs->mis_rays.as<float4>(); Q.mis_a = rs->mis_a.as<float4>(); Q.mis_b = rs->mis_b.as<float4>();
+            Q.mis_c = rs->mis_c.as<int4>(); Q.mis_hits = rs->mis_hits.as<bg_hit>();
+            Q.end_path = rs->end_path.as<int>();
+            Q.n_sh = cnt + kCntSh; Q.n_mis = cnt + kCntMis; Q.n_end = cnt + kCntEnd;
+            Q.totals = totals;
+            auto setq = [&](int c) {
+                Q.ext_rays_in = rs->ext_rays[c].as<float4>(); Q.ext_path_in = rs->ext_path[c].as<int>();
+                Q.ext_rays_out = rs->ext_rays[1 - c].as<float4>(); Q.ext_path_out = rs->ext_path[1 - c].as<int>();
+                Q.n_ext_in = cnt + (c ? kCntExt1 : kCntExt0);
+                Q.n_ext_out = cnt + (c ? kCntExt0 : kCntExt1);
+            };
+            setq(cur);
+            k_generate<<<nb, kShadeThreads, 0, st>>>(camd, np, ns, int(p0), sm->sample_offset + s0, W, H, sm->seed, P, Q, total);
+            ++launches;
+            bg_hit* cnt_hits = rs->cnt_out.as<bg_hit>();
+            uint8_t* cnt_occ = rs->cnt_out.as<uint8_t>();
+            for (int b = 0; b < std::max(1, maxdepth); ++b) {
+                // zero the counters this bounce produces
+                BG_CUDA(cudaMemsetAsync(Q.n_ext_out, 0, sizeof(int), st));
+                BG_CUDA(cudaMemsetAsync(cnt + kCntSh, 0, 3 * sizeof(int), st));
+                if (time_phases) mark(0);
+                rc = launch_trace(s, false, Q.ext_rays_in, 0, Q.n_ext_in, Q.ext_hits, nullptr, st);
+                if (rc) return rc;
+                if (time_phases) mark(0);
+                ++launches; ++launches_extend;
+                if (count_trav) {
+                    rc = launch_trace(s, false, Q.ext_rays_in, 0, Q.n_ext_in, cnt_hits, nullptr, st, totals + 3, 64);
+                    if (rc) return rc;
+                    ++launches;
+                }
+                ShadeArgs A{b, maxdepth, tr->kind, rs->kmax, s->dev.nlights};
+                k_shade<<<nb, kShadeThreads, 0, st>>>(s->dev, A, P, Q);
+                ++launches;
+                if (time_phases) mark(1);
+                rc = launch_trace(s, true, Q.sh_rays, 0, Q.n_sh, nullptr, Q.sh_occ, st);
+                if (rc) return rc;
+                if (time_phases) mark(1);
+                if (time_phases) mark(2);
+                rc = launch_trace(s, false, Q.mis_rays, 0, Q.n_mis, Q.mis_hits, nullptr, st);
+                if (rc) return rc;
+                if (time_phases) mark(2);
+                launches += 2;
+                if (count_trav) {
+                    rc = launch_trace(s, true, Q.sh_rays, 0, Q.n_sh, nullptr, cnt_occ, st, totals + 6, 64);
+                    if (rc) return rc;
+                    rc = launch_trace(s, false, Q.mis_rays, 0, Q.n_mis, cnt_hits, nullptr, st, totals + 9, 64);
+                    if (rc) return rc;
+                    launches += 2;
+                }
+                k_resolve_shadow<<<nb, kShadeThreads, 0, st>>>(P, Q);
+                k_resolve_mis<<<nb, kShadeThreads, 0, st>>>(s->dev, P, Q);
+                k_finalize<<<nb, kShadeThreads, 0, st>>>(P, Q, rs->kmax);
+                launches += 3;
+                cur = 1 - cur;
+                setq(cur);
+            }
+            k_accumulate<<<nb, kShadeThreads, 0, st>>>(P, np, ns, int(p0), W, H, accum);
+            ++launches;
+            BG_CUDA(cudaGetLastError());
+            done_samples += total;
+            s0 += ns;
+        }
+    }
+    if (stats) {
+        cudaEventRecord(ev1, st);
+        BG_CUDA(cudaEventSynchronize(ev1));
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ev0, ev1);
+        unsigned long long t[12];
+        BG_CUDA(cudaMemcpy(t, totals, sizeof(t), cudaMemcpyDeviceToHost));
+        memset(stats, 0, sizeof(*stats));
+        stats->camera_samples = done_samples;
+        stats->rays_extension = int64_t(t[0]);
+        stats->rays_closest = int64_t(t[0] + t[2]);
+        stats->rays_any = int64_t(t[1]);
+        stats->kernel_launches = launches;
+        stats->launches_extend = launches_extend;
+        stats->ms_total = ms;
+        float phase[3] = {0.f, 0.f, 0.f};
+        for (size_t i = 0; i + 1 < evs.size(); i += 2) {
+            float m = 0.f;
+            cudaEventElapsedTime(&m, evs[i], evs[i + 1]);
+            phase[evtag[i]] += m;
+        }
+        for (cudaEvent_t e : evs) cudaEventDestroy(e);
+        stats->ms_extend = phase[0];
+        stats->ms_shadow = phase[1];
+        stats->ms_mis = phase[2];
+        stats->ms_shade = time_phases ? ms - phase[0] - phase[1] - phase[2] : 0.f;
+        stats->sub_rays_extension = int64_t(t[3]);
+        stats->sub_nodes_extension = int64_t(t[4]);
+        stats->sub_tris_extension = int64_t(t[5]);
+        stats->sub_rays_any = int64_t(t[6]);
+        stats->sub_nodes_any = int64_t(t[7]);
+        stats->sub_tris_any = int64_t(t[8]);
+        stats->sub_rays_mis = int64_t(t[9]);
+        stats->sub_nodes_mis = int64_t(t[10]);
+        stats->sub_tris_mis = int64_t(t[11]);
+        cudaEventDestroy(ev0);
+        cudaEventDestroy(ev1);
+    }
+    return BG_OK;
+}
+
 }  // namespace bg
 
-extern "C" int bg_render(bg_scene*, const bg_camera_desc*, const bg_tracer_desc*, const bg_sampler_desc*, int32_t,
-                         int32_t, float*, bg_render_stats*, void*) {
-    return bg::set_error(BG_ERR_UNSUPPORTED, "not built yet");
+using namespace bg;
+
+extern "C" int bg_render(bg_scene* s, const bg_camera_desc* cam, const bg_tracer_desc* tr, const bg_sampler_desc* sm,
+                         int32_t W, int32_t H, float* accum, bg_render_stats* stats, void* stream) {
+    if (!s) return set_error(BG_ERR_INVALID_ARG, "scene is NULL");
+    std::lock_guard<std::mutex> lk(s->mu);
+    return render_impl(s, cam, tr, sm, W, H, reinterpret_cast<float4*>(accum), stats, static_cast<cudaStream_t>(stream));
 }
-extern "C" int bg_render_host(bg_scene*, const bg_camera_desc*, const bg_tracer_desc*, const bg_sampler_desc*,
-                              int32_t, int32_t, float*, bg_render_stats*) {
-    return bg::set_error(BG_ERR_UNSUPPORTED, "not built yet");
+
+extern "C" int bg_render_host(bg_scene* s, const bg_camera_desc* cam, const bg_tracer_desc* tr, const bg_sampler_desc* sm,
+                              int32_t W, int32_t H, float* accum, bg_render_stats* stats) {
+    if (!s) return set_error(BG_ERR_INVALID_ARG, "scene is NULL");
+    if (!accum) return set_error(BG_ERR_INVALID_ARG, "accum is NULL");
+    if (W <= 0 || H <= 0) return set_error(BG_ERR_INVALID_ARG, "bad resolution");
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (!s->committed) return set_error(BG_ERR_STATE, "scene not committed");
+    const size_t bytes = size_t(W) * H * 16;
+    int rc = s->host_out.ensure(bytes);   // staging shared with the host ray casts (both hold the scene lock)
+    if (rc) return rc;
+    float4* d = s->host_out.as<float4>();
+    BG_CUDA(cudaMemcpy(d, accum, bytes, cudaMemcpyHostToDevice));
+    rc = render_impl(s, cam, tr, sm, W, H, d, stats, 0);
+    if (rc) return rc;
+    BG_CUDA(cudaMemcpy(accum, d, bytes, cudaMemcpyDeviceToHost));
+    unsigned flags = 0;
+    BG_CUDA(cudaMemcpy(&flags, s->err.ptr, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    if (flags & BG_FLAG_STACK_OVERFLOW) return set_error(BG_ERR_OVERFLOW, "traversal stack overflow");
+    return BG_OK;
 }

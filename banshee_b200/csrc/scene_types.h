@@ -57,6 +57,8 @@ struct LightRec {
     float dir[3];       // directional: normalize(d) (light/directional_light.h:44)
     float e[3];         // directional radiance / area: emission of the material
     float env[3];       // environment: scale * pow(texel, 1/gamma), precomputed on the host
+    float area_world;   // area: Mesh::GetShapeSurfaceArea (world space, mesh.cpp:304-321)
+    float pdf_obj;      // area: FillSample's 1 / area in object space (mesh.cpp:121)
     float pad;
 };
 

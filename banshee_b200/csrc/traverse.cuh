@@ -106,7 +106,7 @@ __device__ __forceinline__ uint32_t box4(const WideNode4* __restrict__ nodes, in
 }
 
 struct Counters {
-    unsigned long long nodes, tris;
+    unsigned long long rays, nodes, tris;
 };
 
 // Per-lane traversal state kept across refill points.

@@ -142,8 +142,8 @@ typedef struct bg_camera_desc {
 } bg_camera_desc;
 
 typedef struct bg_build_opts {
-    int32_t node_width;     /* BVH fan-out: 4 or 8 (0 = default 8)      */
-    int32_t max_leaf_size;  /* triangles per leaf, 1..8 (0 = default 4) */
+    int32_t node_width;     /* BVH fan-out: 4 (0 = default 4)           */
+    int32_t max_leaf_size;  /* triangles per leaf, 1..16 (0 = default 4)*/
     int32_t sah_bins;       /* binned-SAH bins (0 = default 32)         */
     int32_t reserved;
 } bg_build_opts;
@@ -169,9 +169,14 @@ enum {
     BG_TRACER_DI = 1        /* DiTracer, tracer/ditracer.cpp:19-55        */
 };
 
+#define BG_RENDER_TIME_PHASES   0x1  /* per-phase CUDA-event timing into bg_render_stats */
+#define BG_RENDER_COUNT_TRAVERSAL 0x2 /* instrumented replay of every 64th traced ray    */
+
 typedef struct bg_tracer_desc {
     int32_t kind;
     int32_t maxdepth;
+    int32_t flags;          /* BG_RENDER_* instrumentation bits (0 = none)   */
+    int32_t reserved;
 } bg_tracer_desc;
 
 /* Sampler plugin: every camera sample (pixel p, sample index s) gets fresh
@@ -193,12 +198,21 @@ typedef struct bg_sampler_desc {
 
 typedef struct bg_render_stats {
     int64_t camera_samples;
+    int64_t rays_extension; /* extension (camera + bounce) closest-hit rays */
     int64_t rays_closest;   /* extension + MIS closest-hit rays           */
     int64_t rays_any;       /* shadow rays                                */
+    int64_t kernel_launches;/* library kernels launched by the call       */
     float   ms_total;
-    float   ms_extend;      /* closest-hit traversal                      */
+    float   ms_extend;      /* extension closest-hit traversal            */
+    float   ms_mis;         /* MIS closest-hit traversal                  */
     float   ms_shadow;      /* any-hit traversal                          */
     float   ms_shade;       /* generate + shade + resolve + accumulate    */
+    int32_t launches_extend;/* extension traversal launches               */
+    /* BG_RENDER_COUNT_TRAVERSAL: replay of every 64th ray of each queue:
+     * rays replayed, nodes fetched, triangles tested                      */
+    int64_t sub_rays_extension, sub_nodes_extension, sub_tris_extension;
+    int64_t sub_rays_any, sub_nodes_any, sub_tris_any;
+    int64_t sub_rays_mis, sub_nodes_mis, sub_tris_mis;
 } bg_render_stats;
 
 /* ------------------------------------------------------------------- API */
