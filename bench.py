@@ -70,7 +70,12 @@ class ClockSampler:
         for line in self.proc.stdout:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) >= 4:
-                self.samples.append(parts)
+                self.samples.append((time.perf_counter(), parts))
+
+    def window(self, t0, t1):
+        """Keep only the samples taken inside [t0, t1] (the timed region)."""
+        inside = [s for s in self.samples if t0 <= s[0] <= t1]
+        self.samples = inside if inside else self.samples[-1:]
 
     def stop(self):
         if self.proc:
@@ -85,7 +90,7 @@ class ClockSampler:
                  0x10: "sync_boost", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown",
                  0x80: "hw_power_brake_slowdown", 0x100: "display_clock_setting"}
         sm, mx, reasons = [], None, set()
-        for s in self.samples:
+        for _, s in self.samples:
             try:
                 sm.append(float(s[0]))
                 mx = float(s[1])
@@ -162,7 +167,7 @@ def run_reference_arm(args, rank):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=150)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="bounded CPU-baseline sample (seconds)")
@@ -220,16 +225,20 @@ def main():
         dist.barrier()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    w0 = time.perf_counter()
     e0.record(stream)
     for i in range(args.steps):
         step(args.warmup + i)
         exchange()
     e1.record(stream)
     torch.cuda.synchronize()
+    w1 = time.perf_counter()
     if dist is not None:
         dist.barrier()
     ms = e0.elapsed_time(e1)
+    time.sleep(0.25)
     clocks.stop()
+    clocks.window(w0, w1 + 0.05)
     if dist is not None:
         t = torch.tensor([ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
