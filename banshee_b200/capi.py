@@ -53,6 +53,8 @@ def lib():
             "bg_intersect_closest_host": [_vp, _vp, _vp, _i64],
             "bg_intersect_any_host": [_vp, _vp, _vp, _i64],
             "bg_traversal_counts": [_vp, _vp, _i64, _i32, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), _vp],
+            "bg_traversal_counts_noalloc": [_vp, _vp, _i64, _i32, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
+                                            _vp],
             "bg_render": [_vp, C.POINTER(abi.CameraDesc), C.POINTER(abi.TracerDesc), C.POINTER(abi.SamplerDesc),
                           _i32, _i32, _vp, C.POINTER(abi.RenderStats), _vp],
             "bg_render_host": [_vp, C.POINTER(abi.CameraDesc), C.POINTER(abi.TracerDesc),
@@ -161,6 +163,13 @@ class GpuScene:
         a, b = C.c_uint64(), C.c_uint64()
         check(lib().bg_traversal_counts(self.h, rays_dev, int(n), int(any_hit), C.byref(a), C.byref(b),
                                         _stream_handle(stream)))
+        return a.value, b.value
+
+    def traversal_counts_noalloc(self, rays_dev, n, any_hit=False, stream=None):
+        """bg_traversal_counts_noalloc: the same counts with the library's static scratch."""
+        a, b = C.c_uint64(), C.c_uint64()
+        check(lib().bg_traversal_counts_noalloc(self.h, rays_dev, int(n), int(any_hit), C.byref(a), C.byref(b),
+                                                _stream_handle(stream)))
         return a.value, b.value
 
     def render(self, accum_dev, width, height, spp, seed=1, sample_offset=0, tracer=abi.BG_TRACER_GI,

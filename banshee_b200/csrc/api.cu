@@ -634,3 +634,90 @@ int bg_traversal_counts(bg_scene* s, const bg_ray* rays, int64_t n, int32_t any_
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------------
+// Allocation-free traversal counts.
+//
+// bg_traversal_counts() allocates a temporary device buffer on every call (for
+// the counters and for the hits the replay writes and throws away).  Some
+// callers cannot let a library allocate: an application that reserves all of
+// the device's memory up front for its own pool, where a cudaMalloc at run time
+// may fail or fragment that pool; and a profiling harness, where cudaFree's
+// implicit device synchronisation would disturb the timing it is measuring.
+// bg_traversal_counts_noalloc() does the same replay with its scratch in the
+// fixed-size array below, so it calls no cudaMalloc, cudaFree or allocating
+// library routine.
+//
+// The array lives in every CUDA context that loads this library, from module
+// load until exit.  Its device address is looked up once per device with
+// cudaGetSymbolAddress, by the first call on that device, with that device
+// current; make that first call before any stream capture.  All calls share the
+// array and it keeps the last call's contents: each call clears the counters it
+// uses, and calls whose work overlaps on the GPU (different streams, or
+// different host threads) race on the same memory.
+namespace bg {
+constexpr size_t kNoAllocScratchBytes = size_t(16) << 20;   // 16 MiB
+constexpr size_t kNoAllocHeader = 256;                       // counters + work counter
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+static std::mutex g_noalloc_mu;
+static void* g_noalloc_ptr[64] = {nullptr};
+
+static int noalloc_scratch(int device, unsigned char** out) {
+    if (device < 0 || device >= 64) return set_error(BG_ERR_INVALID_ARG, "device %d out of range for the static scratch", device);
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[device]) {
+        int cur = -1;
+        cudaError_t e = cudaGetDevice(&cur);
+        if (e == cudaSuccess && cur != device) e = cudaSetDevice(device);
+        void* p = nullptr;
+        if (e == cudaSuccess) e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return set_error(BG_ERR_CUDA, "cudaGetSymbolAddress(static scratch) failed: %s", cudaGetErrorString(e));
+        }
+        g_noalloc_ptr[device] = p;
+    }
+    *out = static_cast<unsigned char*>(g_noalloc_ptr[device]);
+    return BG_OK;
+}
+}  // namespace bg
+
+extern "C" int bg_traversal_counts_noalloc(bg_scene* s, const bg_ray* rays, int64_t n, int32_t any_hit,
+                                           uint64_t* nodes, uint64_t* triangles, void* stream) {
+    using namespace bg;
+    int rc;
+    if ((rc = check_scene(s)) || (rc = check_rays(rays, nodes, n))) return rc;
+    if (!triangles) return set_error(BG_ERR_INVALID_ARG, "triangles is NULL");
+    const size_t per_ray = any_hit ? 1 : sizeof(bg_hit);
+    const int64_t max_rays = int64_t((kNoAllocScratchBytes - kNoAllocHeader) / per_ray);
+    if (n > max_rays)
+        return set_error(BG_ERR_INVALID_ARG,
+                         "bg_traversal_counts_noalloc: %lld rays exceed the %lld-ray limit of its %zu-byte static "
+                         "scratch (%s); split the rays or use bg_traversal_counts",
+                         (long long)n, (long long)max_rays, kNoAllocScratchBytes, any_hit ? "any hit" : "closest hit");
+    unsigned char* base = nullptr;
+    if ((rc = noalloc_scratch(s->ctx->device, &base))) return rc;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    unsigned long long* cnt = reinterpret_cast<unsigned long long*>(base);        // rays, nodes, triangles
+    unsigned long long* work = cnt + 4;                                            // persistent-kernel work counter
+    bg_hit* hits = reinterpret_cast<bg_hit*>(base + kNoAllocHeader);
+    uint8_t* occ = base + kNoAllocHeader;
+    cudaError_t e = cudaMemsetAsync(base, 0, kNoAllocHeader, st);   // counters and work counter start at zero
+    if (e == cudaSuccess && n > 0) {
+        if (any_hit)
+            k_trace<true, true><<<s->trace_blocks_count, kTraceThreads, 0, st>>>(
+                s->dev, reinterpret_cast<const float4*>(rays), n, nullptr, nullptr, occ, work, cnt, 1);
+        else
+            k_trace<false, true><<<s->trace_blocks_count, kTraceThreads, 0, st>>>(
+                s->dev, reinterpret_cast<const float4*>(rays), n, nullptr, hits, nullptr, work, cnt, 1);
+        e = cudaGetLastError();
+    }
+    unsigned long long h[3] = {0, 0, 0};
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h, cnt, sizeof(h), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return set_error(BG_ERR_CUDA, "bg_traversal_counts_noalloc: %s", cudaGetErrorString(e));
+    *nodes = h[1];
+    *triangles = h[2];
+    return BG_OK;
+}

@@ -252,6 +252,18 @@ int bg_intersect_any_host(bg_scene* scene, const bg_ray* rays, uint8_t* occluded
  * triangles tested over the n rays (the per-ray byte model of the roofline). */
 int bg_traversal_counts(bg_scene* scene, const bg_ray* rays_dev, int64_t n, int32_t any_hit,
                         uint64_t* nodes, uint64_t* triangles, void* stream);
+/* Same counts as bg_traversal_counts, for callers that cannot let the library
+ * allocate device memory (an application that reserves the device's memory for
+ * its own pool; a profiling harness that cudaFree's implicit synchronisation
+ * would disturb).  No counterpart in the reference.  Allocates nothing: its
+ * scratch is a 16 MiB static device array, held by every GPU that loads the
+ * library until exit, so n is limited to 1,048,560 rays for closest hit and
+ * 16,776,960 for any hit (larger n returns BG_ERR_INVALID_ARG).  The first
+ * call on a device looks up the array's address; make it before any stream
+ * capture.  Calls share the array: calls that overlap on the GPU race.
+ * Synchronous on `stream`. */
+int bg_traversal_counts_noalloc(bg_scene* scene, const bg_ray* rays_dev, int64_t n, int32_t any_hit,
+                                uint64_t* nodes, uint64_t* triangles, void* stream);
 
 /* Renderer::Render for ImageRenderer/MtImageRenderer + the tracer plugin
  * (renderer/imagerenderer.cpp:9-59).  Adds spp samples per pixel into
