@@ -192,7 +192,7 @@ class GpuScene:
         sm = abi.SamplerDesc(0, spp, seed, sample_offset, 0)
         st = abi.RenderStats()
         check(lib().bg_render_host(self.h, C.byref(cam), C.byref(tr), C.byref(sm), int(width), int(height),
-                                   accum.ctypes.data, C.byref(st)))
+                                   accum.ctypes.data, C.byref(st) if stats is not None else None))
         if stats is not None:
             stats.update({k: getattr(st, k) for k, _ in abi.RenderStats._fields_})
         return accum

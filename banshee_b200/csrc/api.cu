@@ -57,7 +57,7 @@ void DevBuf::release() {
 // atomicAdd, every kRefillSteps traversal steps.  Termination: the counter is
 // monotone and every ray finishes after at most one visit per node.
 template <bool ANY, bool COUNT>
-__global__ void __launch_bounds__(kTraceThreads)
+__global__ void __launch_bounds__(kTraceThreads, 8)
 k_trace(DevScene S, const float4* __restrict__ rays, int64_t n_static, const int* __restrict__ n_dev,
         bg_hit* __restrict__ hits, uint8_t* __restrict__ occ, unsigned long long* __restrict__ work,
         unsigned long long* __restrict__ counters, int stride) {
@@ -138,8 +138,9 @@ unsigned long long* next_work_counter(bg_scene* s) {
 }
 
 int launch_trace(bg_scene* s, bool any_hit, const float4* rays, int64_t n_static, const int* n_dev,
-                 bg_hit* hits, uint8_t* occ, cudaStream_t st, unsigned long long* counters, int stride) {
-    unsigned long long* w = next_work_counter(s);
+                 bg_hit* hits, uint8_t* occ, cudaStream_t st, unsigned long long* counters, int stride,
+                 unsigned long long* work) {
+    unsigned long long* w = work ? work : next_work_counter(s);
     BG_CUDA(cudaMemsetAsync(w, 0, sizeof(unsigned long long), st));
     if (counters) {
         if (any_hit)

@@ -80,5 +80,5 @@ constexpr int kWorkSlots = 256;
 unsigned long long* next_work_counter(bg_scene* s);
 int launch_trace(bg_scene* s, bool any_hit, const float4* rays, int64_t n_static, const int* n_dev,
                  bg_hit* hits, uint8_t* occ, cudaStream_t st, unsigned long long* counters = nullptr,
-                 int stride = 1);
+                 int stride = 1, unsigned long long* work = nullptr);
 }  // namespace bg

@@ -28,6 +28,7 @@
 namespace bg {
 
 constexpr int kShadeThreads = 128;
+constexpr int kMaxBounceCounters = 6 * 1024;   // 6 work counters per bounce, maxdepth <= 1024
 
 struct CamDev {        // PerscpectiveCamera frame, computed on the host (perspective_camera.cpp:5-23)
     float fwd[3], right[3], up[3], p[3];
@@ -46,15 +47,28 @@ struct RenderState {
     DevBuf st_key, st_cnt, st_rng, st_bs, st_thr, st_rad, st_dithr, st_flags;
     DevBuf slots, sample_rad;
     DevBuf cnt_out;    // outputs of the instrumented 1/64 replays
+    DevBuf work;       // persistent-kernel work counters of the pass (6 per bounce)
     int blocks = 0;
+    // CUDA graph of one pass, replayed on an internal stream
+    cudaStream_t gstream = nullptr;
+    cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaGraphNode_t gen_node = nullptr, acc_node = nullptr;
+    int64_t graph_key[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 };
 
 void render_state_free(RenderState* rs) {
+    if (rs->exec) cudaGraphExecDestroy(rs->exec);
+    if (rs->graph) cudaGraphDestroy(rs->graph);
+    if (rs->ev_in) cudaEventDestroy(rs->ev_in);
+    if (rs->ev_out) cudaEventDestroy(rs->ev_out);
+    if (rs->gstream) cudaStreamDestroy(rs->gstream);
     for (DevBuf* b : {&rs->ext_rays[0], &rs->ext_rays[1], &rs->ext_path[0], &rs->ext_path[1], &rs->ext_hits,
                       &rs->sh_rays, &rs->sh_contrib, &rs->sh_slot, &rs->sh_occ, &rs->mis_rays, &rs->mis_a, &rs->mis_b,
                       &rs->mis_c, &rs->mis_hits, &rs->end_path, &rs->counts, &rs->st_key, &rs->st_cnt, &rs->st_rng,
                       &rs->st_bs, &rs->st_thr, &rs->st_rad, &rs->st_dithr, &rs->st_flags, &rs->slots,
-                      &rs->sample_rad, &rs->cnt_out})
+                      &rs->sample_rad, &rs->cnt_out, &rs->work})
         b->release();
     delete rs;
 }
@@ -156,7 +170,7 @@ struct ShadeArgs {
 };
 
 // One light's DirectIllumination terms (DiTracer::GetDi, ditracer.cpp:57-239, n = 1).
-__device__ __forceinline__ void emit_di(const DevScene& S, const Queues& Q, int li, const SHit& h, const MatRec& M, v3 wo,
+__device__ __noinline__ void emit_di(const DevScene& S, const Queues& Q, int li, const SHit& h, const MatRec& M, v3 wo,
                                         McRng& lr, McRng& br, int slot0, int path) {
     const LightRec L = load_light(S, li);
     float lx, ly, bx, by;
@@ -223,7 +237,7 @@ __device__ __forceinline__ void emit_di(const DevScene& S, const Queues& Q, int 
     }
 }
 
-__global__ void __launch_bounds__(kShadeThreads)
+__global__ void __launch_bounds__(kShadeThreads, 3)
 k_shade(DevScene S, ShadeArgs A, PathState P, Queues Q) {
     const int n = *Q.n_ext_in;
     const int nthreads = gridDim.x * blockDim.x;
@@ -271,19 +285,18 @@ k_shade(DevScene S, ShadeArgs A, PathState P, Queues Q) {
             } else {
                 unsigned cnt = P.cnt[path];
                 const int base = path * A.kmax;
+                // bounce 0: every light, weight 1; later: one light picked by rand(), weight L
+                // (gitracer.cpp:72-84)
+                int first = 0, nl = A.nlights;
                 float mult = 1.f;
-                if (A.bounce == 0) {
-                    pending = 2 * A.nlights;
-                    for (int j = 0; j < pending; ++j) P.slots[size_t(base) + j] = make_float4(0.f, 0.f, 0.f, 0.f);
-                    for (int i = 0; i < A.nlights; ++i) emit_di(S, Q, i, h, M, wo, lr, br, base + 2 * i, path);
-                } else {
-                    int idx = int(keyed_rand(P.key[path], cnt++) % unsigned(A.nlights));   // gitracer.cpp:74-76
-                    pending = 2;
-                    P.slots[size_t(base)] = make_float4(0.f, 0.f, 0.f, 0.f);
-                    P.slots[size_t(base) + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
-                    emit_di(S, Q, idx, h, M, wo, lr, br, base, path);
+                if (A.bounce != 0) {
+                    first = int(keyed_rand(P.key[path], cnt++) % unsigned(A.nlights));
+                    nl = 1;
                     mult = (float)A.nlights;
                 }
+                pending = 2 * nl;
+                for (int j = 0; j < pending; ++j) P.slots[size_t(base) + j] = make_float4(0.f, 0.f, 0.f, 0.f);
+                for (int i = 0; i < nl; ++i) emit_di(S, Q, first + i, h, M, wo, lr, br, base + 2 * i, path);
                 P.dithr[path] = make_float4(thr.x, thr.y, thr.z, mult);
                 if (A.kind == BG_TRACER_DI) {
                     flags |= kFlagNoClamp;
@@ -447,11 +460,181 @@ static int ensure_state(bg_scene* s, int64_t cap) {
         (rc = rs->st_bs.ensure(C * 8)) || (rc = rs->st_thr.ensure(C * 16)) || (rc = rs->st_rad.ensure(C * 16)) ||
         (rc = rs->st_dithr.ensure(C * 16)) || (rc = rs->st_flags.ensure(C * 4)) ||
         (rc = rs->slots.ensure(C * rs->kmax * 16)) || (rc = rs->sample_rad.ensure(C * 16)) ||
-        (rc = rs->cnt_out.ensure((C * 2 * L / 64 + 64) * 16)))
+        (rc = rs->cnt_out.ensure((C * 2 * L / 64 + 64) * 16)) ||
+        (rc = rs->work.ensure(size_t(kMaxBounceCounters) * 8)))
         return rc;
     int nb = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_shade, kShadeThreads, 0);
     rs->blocks = std::max(1, nb) * s->ctx->num_sms;
+    BG_CUDA(cudaStreamCreateWithFlags(&rs->gstream, cudaStreamNonBlocking));
+    BG_CUDA(cudaEventCreateWithFlags(&rs->ev_in, cudaEventDisableTiming));
+    BG_CUDA(cudaEventCreateWithFlags(&rs->ev_out, cudaEventDisableTiming));
+    return BG_OK;
+}
+
+struct Instr {
+    bool time_phases = false, count_trav = false;
+    cudaStream_t st = nullptr;
+    std::vector<cudaEvent_t> evs;   // begin/end pairs; phase tag in tags
+    std::vector<int> tags;
+    int64_t launches = 0;
+    int launches_extend = 0;
+    void mark(int tag) {
+        if (!time_phases) return;
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        cudaEventRecord(e, st);
+        evs.push_back(e);
+        tags.push_back(tag);
+    }
+};
+
+struct PassCfg {
+    int np, ns, p0, s0, W, H, maxdepth, kind;
+    uint64_t seed;
+    float4* accum;
+};
+
+static void pass_queues(RenderState* rs, int c, Queues& Q) {
+    int* cnt = rs->counts.as<int>();
+    Q.ext_hits = rs->ext_hits.as<bg_hit>();
+    Q.sh_rays = rs->sh_rays.as<float4>(); Q.sh_contrib = rs->sh_contrib.as<float4>();
+    Q.sh_slot = rs->sh_slot.as<int>(); Q.sh_occ = rs->sh_occ.as<uint8_t>();
+    Q.mis_rays = rs->mis_rays.as<float4>(); Q.mis_a = rs->mis_a.as<float4>(); Q.mis_b = rs->mis_b.as<float4>();
+    Q.mis_c = rs->mis_c.as<int4>(); Q.mis_hits = rs->mis_hits.as<bg_hit>();
+    Q.end_path = rs->end_path.as<int>();
+    Q.n_sh = cnt + kCntSh; Q.n_mis = cnt + kCntMis; Q.n_end = cnt + kCntEnd;
+    Q.totals = reinterpret_cast<unsigned long long*>(rs->counts.as<char>() + 64);
+    Q.ext_rays_in = rs->ext_rays[c].as<float4>(); Q.ext_path_in = rs->ext_path[c].as<int>();
+    Q.ext_rays_out = rs->ext_rays[1 - c].as<float4>(); Q.ext_path_out = rs->ext_path[1 - c].as<int>();
+    Q.n_ext_in = cnt + (c ? kCntExt1 : kCntExt0);
+    Q.n_ext_out = cnt + (c ? kCntExt0 : kCntExt1);
+}
+
+static PathState path_state(RenderState* rs) {
+    PathState P;
+    P.key = rs->st_key.as<unsigned long long>();
+    P.cnt = rs->st_cnt.as<unsigned>();
+    P.rng = rs->st_rng.as<uint4>();
+    P.bs = rs->st_bs.as<float2>();
+    P.thr = rs->st_thr.as<float4>();
+    P.rad = rs->st_rad.as<float4>();
+    P.dithr = rs->st_dithr.as<float4>();
+    P.flags = rs->st_flags.as<unsigned>();
+    P.slots = rs->slots.as<float4>();
+    P.sample_rad = rs->sample_rad.as<float4>();
+    return P;
+}
+
+// Enqueues one pass (np pixels x ns samples) on `st`: generate, maxdepth bounces
+// of extend / shade / shadow / MIS / resolve / finalize, accumulate.
+static int enqueue_pass(bg_scene* s, RenderState* rs, cudaStream_t st, const CamDev& cam, const PassCfg& c, Instr* ins) {
+    const int nb = rs->blocks;
+    const int total = c.np * c.ns;
+    PathState P = path_state(rs);
+    Queues Q;
+    int cur = 0;
+    pass_queues(rs, cur, Q);
+    int* cnt = rs->counts.as<int>();
+    int rc;
+    k_generate<<<nb, kShadeThreads, 0, st>>>(cam, c.np, c.ns, c.p0, c.s0, c.W, c.H, c.seed, P, Q, total);
+    if (ins) ++ins->launches;
+    bg_hit* cnt_hits = rs->cnt_out.as<bg_hit>();
+    uint8_t* cnt_occ = rs->cnt_out.as<uint8_t>();
+    for (int b = 0; b < std::max(1, c.maxdepth); ++b) {
+        unsigned long long* wk = rs->work.as<unsigned long long>() + 6 * b;
+        BG_CUDA(cudaMemsetAsync(Q.n_ext_out, 0, sizeof(int), st));
+        BG_CUDA(cudaMemsetAsync(cnt + kCntSh, 0, 3 * sizeof(int), st));
+        if (ins) ins->mark(0);
+        if ((rc = launch_trace(s, false, Q.ext_rays_in, 0, Q.n_ext_in, Q.ext_hits, nullptr, st, nullptr, 1, wk))) return rc;
+        if (ins) { ins->mark(0); ++ins->launches; ++ins->launches_extend; }
+        if (ins && ins->count_trav) {
+            if ((rc = launch_trace(s, false, Q.ext_rays_in, 0, Q.n_ext_in, cnt_hits, nullptr, st, Q.totals + 3, 64, wk + 1))) return rc;
+            ++ins->launches;
+        }
+        ShadeArgs A{b, c.maxdepth, c.kind, rs->kmax, s->dev.nlights};
+        k_shade<<<nb, kShadeThreads, 0, st>>>(s->dev, A, P, Q);
+        if (ins) { ++ins->launches; ins->mark(1); }
+        if ((rc = launch_trace(s, true, Q.sh_rays, 0, Q.n_sh, nullptr, Q.sh_occ, st, nullptr, 1, wk + 2))) return rc;
+        if (ins) { ins->mark(1); ins->mark(2); }
+        if ((rc = launch_trace(s, false, Q.mis_rays, 0, Q.n_mis, Q.mis_hits, nullptr, st, nullptr, 1, wk + 3))) return rc;
+        if (ins) { ins->mark(2); ins->launches += 2; }
+        if (ins && ins->count_trav) {
+            if ((rc = launch_trace(s, true, Q.sh_rays, 0, Q.n_sh, nullptr, cnt_occ, st, Q.totals + 6, 64, wk + 4))) return rc;
+            if ((rc = launch_trace(s, false, Q.mis_rays, 0, Q.n_mis, cnt_hits, nullptr, st, Q.totals + 9, 64, wk + 5))) return rc;
+            ins->launches += 2;
+        }
+        k_resolve_shadow<<<nb, kShadeThreads, 0, st>>>(P, Q);
+        k_resolve_mis<<<nb, kShadeThreads, 0, st>>>(s->dev, P, Q);
+        k_finalize<<<nb, kShadeThreads, 0, st>>>(P, Q, rs->kmax);
+        if (ins) ins->launches += 3;
+        cur = 1 - cur;
+        pass_queues(rs, cur, Q);
+    }
+    k_accumulate<<<nb, kShadeThreads, 0, st>>>(P, c.np, c.ns, c.p0, c.W, c.H, c.accum);
+    if (ins) ++ins->launches;
+    BG_CUDA(cudaGetLastError());
+    return BG_OK;
+}
+
+// Captures one pass into a CUDA graph (once per pass shape) and finds the two
+// kernel nodes whose arguments change from pass to pass.
+static int pass_graph(bg_scene* s, RenderState* rs, const CamDev& cam, const PassCfg& c) {
+    const int64_t key[8] = {c.np, c.ns, c.W, c.H, c.maxdepth, c.kind, int64_t(reinterpret_cast<uintptr_t>(c.accum)),
+                            s->dev.nlights};
+    if (rs->exec && memcmp(key, rs->graph_key, sizeof(key)) == 0) return BG_OK;
+    if (rs->exec) { cudaGraphExecDestroy(rs->exec); rs->exec = nullptr; }
+    if (rs->graph) { cudaGraphDestroy(rs->graph); rs->graph = nullptr; }
+    BG_CUDA(cudaStreamBeginCapture(rs->gstream, cudaStreamCaptureModeThreadLocal));
+    int rc = enqueue_pass(s, rs, rs->gstream, cam, c, nullptr);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(rs->gstream, &g);
+    if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+    if (e != cudaSuccess) return set_error(BG_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
+    rs->graph = g;
+    size_t nn = 0;
+    BG_CUDA(cudaGraphGetNodes(g, nullptr, &nn));
+    std::vector<cudaGraphNode_t> nodes(nn);
+    BG_CUDA(cudaGraphGetNodes(g, nodes.data(), &nn));
+    rs->gen_node = rs->acc_node = nullptr;
+    for (cudaGraphNode_t n : nodes) {
+        cudaGraphNodeType t;
+        BG_CUDA(cudaGraphNodeGetType(n, &t));
+        if (t != cudaGraphNodeTypeKernel) continue;
+        cudaKernelNodeParams kp;
+        BG_CUDA(cudaGraphKernelNodeGetParams(n, &kp));
+        if (kp.func == reinterpret_cast<void*>(k_generate)) rs->gen_node = n;
+        if (kp.func == reinterpret_cast<void*>(k_accumulate)) rs->acc_node = n;
+    }
+    if (!rs->gen_node || !rs->acc_node) return set_error(BG_ERR_STATE, "pass graph: kernel nodes not found");
+    BG_CUDA(cudaGraphInstantiate(&rs->exec, g, 0));
+    memcpy(rs->graph_key, key, sizeof(key));
+    return BG_OK;
+}
+
+static int launch_pass_graph(bg_scene* s, RenderState* rs, const CamDev& cam, const PassCfg& c) {
+    int rc = pass_graph(s, rs, cam, c);
+    if (rc) return rc;
+    PathState P = path_state(rs);
+    Queues Q;
+    pass_queues(rs, 0, Q);
+    int total = c.np * c.ns;
+    CamDev camv = cam;
+    int np = c.np, ns = c.ns, p0 = c.p0, s0 = c.s0, W = c.W, H = c.H;
+    uint64_t seed = c.seed;
+    void* gargs[] = {&camv, &np, &ns, &p0, &s0, &W, &H, &seed, &P, &Q, &total};
+    cudaKernelNodeParams kp;
+    BG_CUDA(cudaGraphKernelNodeGetParams(rs->gen_node, &kp));
+    kp.kernelParams = gargs;
+    kp.extra = nullptr;
+    BG_CUDA(cudaGraphExecKernelNodeSetParams(rs->exec, rs->gen_node, &kp));
+    float4* accum = c.accum;
+    void* aargs[] = {&P, &np, &ns, &p0, &W, &H, &accum};
+    BG_CUDA(cudaGraphKernelNodeGetParams(rs->acc_node, &kp));
+    kp.kernelParams = aargs;
+    kp.extra = nullptr;
+    BG_CUDA(cudaGraphExecKernelNodeSetParams(rs->exec, rs->acc_node, &kp));
+    BG_CUDA(cudaGraphLaunch(rs->exec, rs->gstream));
     return BG_OK;
 }
 
@@ -476,116 +659,45 @@ static int render_impl(bg_scene* s, const bg_camera_desc* cam, const bg_tracer_d
     if (rc) return rc;
     RenderState* rs = s->render;
     const CamDev camd = make_camera(cam);
-    PathState P;
-    P.key = rs->st_key.as<unsigned long long>();
-    P.cnt = rs->st_cnt.as<unsigned>();
-    P.rng = rs->st_rng.as<uint4>();
-    P.bs = rs->st_bs.as<float2>();
-    P.thr = rs->st_thr.as<float4>();
-    P.rad = rs->st_rad.as<float4>();
-    P.dithr = rs->st_dithr.as<float4>();
-    P.flags = rs->st_flags.as<unsigned>();
-    P.slots = rs->slots.as<float4>();
-    P.sample_rad = rs->sample_rad.as<float4>();
-    int* cnt = rs->counts.as<int>();
+    const int maxdepth = tr->kind == BG_TRACER_DI ? 1 : tr->maxdepth;
     unsigned long long* totals = reinterpret_cast<unsigned long long*>(rs->counts.as<char>() + 64);
-    // totals: [0] extension rays, [1] any rays, [2] MIS rays, replays (rays, nodes, tris):
-    // [3..5] extension, [6..8] any, [9..11] MIS
-    BG_CUDA(cudaMemsetAsync(totals, 0, 12 * sizeof(unsigned long long), st));
-    const bool time_phases = stats && (tr->flags & BG_RENDER_TIME_PHASES);
-    const bool count_trav = stats && (tr->flags & BG_RENDER_COUNT_TRAVERSAL);
+
+    // Graph replay unless statistics were asked for or the caller's stream is capturing.
+    cudaStreamCaptureStatus cap_st = cudaStreamCaptureStatusNone;
+    BG_CUDA(cudaStreamIsCapturing(st, &cap_st));
+    const bool use_graph = !stats && cap_st == cudaStreamCaptureStatusNone;
+    Instr ins;
+    ins.st = st;
+    ins.time_phases = stats && (tr->flags & BG_RENDER_TIME_PHASES);
+    ins.count_trav = stats && (tr->flags & BG_RENDER_COUNT_TRAVERSAL);
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    std::vector<cudaEvent_t> evs;   // begin/end pairs: phase tag in evtag
-    std::vector<int> evtag;
-    auto mark = [&](int tag) {
-        cudaEvent_t e;
-        cudaEventCreate(&e);
-        cudaEventRecord(e, st);
-        evs.push_back(e);
-        evtag.push_back(tag);
-    };
-    int64_t launches = 0;
-    int launches_extend = 0;
     if (stats) {
+        // totals: [0] extension rays, [1] any rays, [2] MIS rays, replays (rays, nodes, tris):
+        // [3..5] extension, [6..8] any, [9..11] MIS
+        BG_CUDA(cudaMemsetAsync(totals, 0, 12 * sizeof(unsigned long long), st));
         cudaEventCreate(&ev0);
         cudaEventCreate(&ev1);
         cudaEventRecord(ev0, st);
     }
-    const int maxdepth = tr->kind == BG_TRACER_DI ? 1 : tr->maxdepth;
-    const int nb = rs->blocks;
+    if (use_graph) {
+        BG_CUDA(cudaEventRecord(rs->ev_in, st));
+        BG_CUDA(cudaStreamWaitEvent(rs->gstream, rs->ev_in, 0));
+    }
     int64_t done_samples = 0;
     for (int64_t p0 = 0; p0 < npix; p0 += cap) {
         const int np = int(std::min<int64_t>(cap, npix - p0));
         for (int s0 = 0; s0 < sm->spp;) {
             const int ns = int(std::max<int64_t>(1, std::min<int64_t>(sm->spp - s0, cap / np)));
-            const int total = np * ns;
-            int cur = 0;
-            Queues Q;
-            Q.ext_hits = rs->ext_hits.as<bg_hit>();
-            Q.sh_rays = rs->sh_rays.as<float4>(); Q.sh_contrib = rs->sh_contrib.as<float4>();
-            Q.sh_slot = rs->sh_slot.as<int>(); Q.sh_occ = rs->sh_occ.as<uint8_t>();
-            Q.mis_rays = rs->mis_rays.as<float4>(); Q.mis_a = rs->mis_a.as<float4>(); Q.mis_b = rs->mis_b.as<float4>();
-            Q.mis_c = rs->mis_c.as<int4>(); Q.mis_hits = rs->mis_hits.as<bg_hit>();
-            Q.end_path = rs->end_path.as<int>();
-            Q.n_sh = cnt + kCntSh; Q.n_mis = cnt + kCntMis; Q.n_end = cnt + kCntEnd;
-            Q.totals = totals;
-            auto setq = [&](int c) {
-                Q.ext_rays_in = rs->ext_rays[c].as<float4>(); Q.ext_path_in = rs->ext_path[c].as<int>();
-                Q.ext_rays_out = rs->ext_rays[1 - c].as<float4>(); Q.ext_path_out = rs->ext_path[1 - c].as<int>();
-                Q.n_ext_in = cnt + (c ? kCntExt1 : kCntExt0);
-                Q.n_ext_out = cnt + (c ? kCntExt0 : kCntExt1);
-            };
-            setq(cur);
-            k_generate<<<nb, kShadeThreads, 0, st>>>(camd, np, ns, int(p0), sm->sample_offset + s0, W, H, sm->seed, P, Q, total);
-            ++launches;
-            bg_hit* cnt_hits = rs->cnt_out.as<bg_hit>();
-            uint8_t* cnt_occ = rs->cnt_out.as<uint8_t>();
-            for (int b = 0; b < std::max(1, maxdepth); ++b) {
-                // zero the counters this bounce produces
-                BG_CUDA(cudaMemsetAsync(Q.n_ext_out, 0, sizeof(int), st));
-                BG_CUDA(cudaMemsetAsync(cnt + kCntSh, 0, 3 * sizeof(int), st));
-                if (time_phases) mark(0);
-                rc = launch_trace(s, false, Q.ext_rays_in, 0, Q.n_ext_in, Q.ext_hits, nullptr, st);
-                if (rc) return rc;
-                if (time_phases) mark(0);
-                ++launches; ++launches_extend;
-                if (count_trav) {
-                    rc = launch_trace(s, false, Q.ext_rays_in, 0, Q.n_ext_in, cnt_hits, nullptr, st, totals + 3, 64);
-                    if (rc) return rc;
-                    ++launches;
-                }
-                ShadeArgs A{b, maxdepth, tr->kind, rs->kmax, s->dev.nlights};
-                k_shade<<<nb, kShadeThreads, 0, st>>>(s->dev, A, P, Q);
-                ++launches;
-                if (time_phases) mark(1);
-                rc = launch_trace(s, true, Q.sh_rays, 0, Q.n_sh, nullptr, Q.sh_occ, st);
-                if (rc) return rc;
-                if (time_phases) mark(1);
-                if (time_phases) mark(2);
-                rc = launch_trace(s, false, Q.mis_rays, 0, Q.n_mis, Q.mis_hits, nullptr, st);
-                if (rc) return rc;
-                if (time_phases) mark(2);
-                launches += 2;
-                if (count_trav) {
-                    rc = launch_trace(s, true, Q.sh_rays, 0, Q.n_sh, nullptr, cnt_occ, st, totals + 6, 64);
-                    if (rc) return rc;
-                    rc = launch_trace(s, false, Q.mis_rays, 0, Q.n_mis, cnt_hits, nullptr, st, totals + 9, 64);
-                    if (rc) return rc;
-                    launches += 2;
-                }
-                k_resolve_shadow<<<nb, kShadeThreads, 0, st>>>(P, Q);
-                k_resolve_mis<<<nb, kShadeThreads, 0, st>>>(s->dev, P, Q);
-                k_finalize<<<nb, kShadeThreads, 0, st>>>(P, Q, rs->kmax);
-                launches += 3;
-                cur = 1 - cur;
-                setq(cur);
-            }
-            k_accumulate<<<nb, kShadeThreads, 0, st>>>(P, np, ns, int(p0), W, H, accum);
-            ++launches;
-            BG_CUDA(cudaGetLastError());
-            done_samples += total;
+            PassCfg c{np, ns, int(p0), sm->sample_offset + s0, W, H, maxdepth, tr->kind, sm->seed, accum};
+            rc = use_graph ? launch_pass_graph(s, rs, camd, c) : enqueue_pass(s, rs, st, camd, c, &ins);
+            if (rc) return rc;
+            done_samples += int64_t(np) * ns;
             s0 += ns;
         }
+    }
+    if (use_graph) {
+        BG_CUDA(cudaEventRecord(rs->ev_out, rs->gstream));
+        BG_CUDA(cudaStreamWaitEvent(st, rs->ev_out, 0));
     }
     if (stats) {
         cudaEventRecord(ev1, st);
@@ -599,20 +711,20 @@ static int render_impl(bg_scene* s, const bg_camera_desc* cam, const bg_tracer_d
         stats->rays_extension = int64_t(t[0]);
         stats->rays_closest = int64_t(t[0] + t[2]);
         stats->rays_any = int64_t(t[1]);
-        stats->kernel_launches = launches;
-        stats->launches_extend = launches_extend;
+        stats->kernel_launches = ins.launches;
+        stats->launches_extend = ins.launches_extend;
         stats->ms_total = ms;
         float phase[3] = {0.f, 0.f, 0.f};
-        for (size_t i = 0; i + 1 < evs.size(); i += 2) {
+        for (size_t i = 0; i + 1 < ins.evs.size(); i += 2) {
             float m = 0.f;
-            cudaEventElapsedTime(&m, evs[i], evs[i + 1]);
-            phase[evtag[i]] += m;
+            cudaEventElapsedTime(&m, ins.evs[i], ins.evs[i + 1]);
+            phase[ins.tags[i]] += m;
         }
-        for (cudaEvent_t e : evs) cudaEventDestroy(e);
+        for (cudaEvent_t e : ins.evs) cudaEventDestroy(e);
         stats->ms_extend = phase[0];
         stats->ms_shadow = phase[1];
         stats->ms_mis = phase[2];
-        stats->ms_shade = time_phases ? ms - phase[0] - phase[1] - phase[2] : 0.f;
+        stats->ms_shade = ins.time_phases ? ms - phase[0] - phase[1] - phase[2] : 0.f;
         stats->sub_rays_extension = int64_t(t[3]);
         stats->sub_nodes_extension = int64_t(t[4]);
         stats->sub_tris_extension = int64_t(t[5]);

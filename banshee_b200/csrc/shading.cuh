@@ -11,6 +11,10 @@
 //                                        light/arealight.cpp, directional_light.cpp,
 //                                        environment_light.cpp
 //   map_to_hemisphere / orthovector / PowerHeuristic   math/mathutils.h:214-296
+//
+// The larger functions are __noinline__: k_shade calls them from several places,
+// and one shared copy keeps the shading kernel inside the instruction cache
+// (measured: the fully inlined kernel stalled on instruction fetch).
 #pragma once
 
 #include "device_common.cuh"
@@ -52,7 +56,7 @@ __device__ __forceinline__ v3 orthovector(v3 n) {
 }
 
 // Mesh::FillHit, primitive/mesh.cpp:47-97
-__device__ __forceinline__ void fill_hit(const DevScene& S, int prim, float a, float b, SHit& h) {
+__device__ __noinline__ void fill_hit(const DevScene& S, int prim, float a, float b, SHit& h) {
     const float4* sr = reinterpret_cast<const float4*>(S.shade + prim);
     float4 ra = __ldg(sr), rb = __ldg(sr + 1), rc = __ldg(sr + 2), rd = __ldg(sr + 3);
     float4 re = __ldg(sr + 4), rf = __ldg(sr + 5), rg = __ldg(sr + 6);
@@ -91,7 +95,7 @@ __device__ __forceinline__ void fill_hit(const DevScene& S, int prim, float a, f
 }
 
 // map_to_hemisphere(n, s, e), math/mathutils.h:230-244
-__device__ __forceinline__ v3 map_to_hemisphere(v3 n, float sx, float sy, float e) {
+__device__ __noinline__ v3 map_to_hemisphere(v3 n, float sx, float sy, float e) {
     v3 u = orthovector(n);
     v3 v = cross(u, n);
     u = cross(n, v);
@@ -142,7 +146,7 @@ __device__ __forceinline__ float fresnel_dielectric(float etai, float etat, floa
     float rperp = ((ei * ndotwi) - (et * ndotwt)) / ((ei * ndotwi) + (et * ndotwt));
     return (rparl * rparl + rperp * rperp) * 0.5f;
 }
-__device__ __forceinline__ v3 microfacet_eval(const MatRec& M, const SHit& h, v3 wi, v3 wo) {
+__device__ __noinline__ v3 microfacet_eval(const MatRec& M, const SHit& h, v3 wi, v3 wo) {
     float sameside = dot(wi, h.n) * dot(wo, h.n);
     if (sameside < 0.f) return mk(0.f, 0.f, 0.f);
     v3 n = dot(h.n, wi) < 0.f ? neg(h.n) : h.n;
@@ -154,7 +158,7 @@ __device__ __forceinline__ v3 microfacet_eval(const MatRec& M, const SHit& h, v3
     float G = ggx_G1(M.a, wi, wh, n) * ggx_G1(M.a, wo, wh, n);
     return muls(mk(M.ks[0], M.ks[1], M.ks[2]), (ggx_D(M.a, wh, n) * G * F / (4.f * cos_i * cos_o)));
 }
-__device__ __forceinline__ v3 microfacet_sample(const MatRec& M, const SHit& h, float sx, float sy, v3 wi, v3& wo, float& pdf) {
+__device__ __noinline__ v3 microfacet_sample(const MatRec& M, const SHit& h, float sx, float sy, v3 wi, v3& wo, float& pdf) {
     v3 n = h.n, du = h.dpdu, dv = h.dpdv;
     if (dot(h.n, wi) < 0.f) { n = neg(n); du = neg(du); dv = neg(dv); }
     float temp = atanf(M.a * sqrtf(sx) / sqrtf(1.f - sx));
@@ -168,13 +172,13 @@ __device__ __forceinline__ v3 microfacet_sample(const MatRec& M, const SHit& h, 
     pdf = ggx_pdf(M.a, n, wi, wo);
     return microfacet_eval(M, h, wi, wo);
 }
-__device__ __forceinline__ float microfacet_pdf(const MatRec& M, const SHit& h, v3 wi, v3 wo) {
+__device__ __noinline__ float microfacet_pdf(const MatRec& M, const SHit& h, v3 wi, v3 wo) {
     float sameside = dot(wi, h.n) * dot(wo, h.n);
     if (sameside < 0.f) return 0.f;
     v3 n = dot(h.n, wi) < 0 ? neg(h.n) : h.n;
     return ggx_pdf(M.a, n, wi, wo);
 }
-__device__ __forceinline__ v3 lambert_sample(const MatRec& M, const SHit& h, float sx, float sy, v3 wi, v3& wo, float& pdf) {
+__device__ __noinline__ v3 lambert_sample(const MatRec& M, const SHit& h, float sx, float sy, v3 wi, v3& wo, float& pdf) {
     v3 n = dot(wi, h.ng) >= 0.f ? h.n : neg(h.n);
     wo = map_to_hemisphere(n, sx, sy, 1.f);
     float invpi = 1.f / BG_PI;
@@ -248,7 +252,7 @@ __device__ __forceinline__ LightRec load_light(const DevScene& S, int i) {
 // AreaLight::GetSample (light/arealight.cpp:25-51) with Mesh::GetSampleOnShape /
 // FillSample (primitive/mesh.cpp:99-123,323-336); the area pdf 1/area in object
 // space is precomputed on the host (same float ops).
-__device__ __forceinline__ v3 area_getsample(const DevScene& S, const LightRec& L, v3 hp, float ux, float uy, v3& d, float& pdf) {
+__device__ __noinline__ v3 area_getsample(const DevScene& S, const LightRec& L, v3 hp, float ux, float uy, v3& d, float& pdf) {
     const int prim = int(__ldg(&S.bundles[L.mesh].start)) + L.face;
     const float4* sr = reinterpret_cast<const float4*>(S.shade + prim);
     float4 ra = __ldg(sr), rb = __ldg(sr + 1), rc = __ldg(sr + 2), rd = __ldg(sr + 3), re = __ldg(sr + 4), rf = __ldg(sr + 5);
@@ -276,7 +280,7 @@ __device__ __forceinline__ v3 area_getsample(const DevScene& S, const LightRec& 
 
 // AreaLight::GetPdf -> Mesh::GetPdfOnShape (primitive/mesh.cpp:354-378): intersect the
 // light's own triangle from p along w with t in (0.001, 1e5].
-__device__ __forceinline__ float area_getpdf(const DevScene& S, const LightRec& L, v3 hp, v3 w) {
+__device__ __noinline__ float area_getpdf(const DevScene& S, const LightRec& L, v3 hp, v3 w) {
     const int prim = int(__ldg(&S.bundles[L.mesh].start)) + L.face;
     const float4* sr = reinterpret_cast<const float4*>(S.shade + prim);
     float4 ra = __ldg(sr), rb = __ldg(sr + 1), rc = __ldg(sr + 2);
