@@ -59,6 +59,15 @@ def lib():
                           _i32, _i32, _vp, C.POINTER(abi.RenderStats), _vp],
             "bg_render_host": [_vp, C.POINTER(abi.CameraDesc), C.POINTER(abi.TracerDesc),
                                C.POINTER(abi.SamplerDesc), _i32, _i32, _vp, C.POINTER(abi.RenderStats)],
+            "bg_cache_create": [_vp, C.POINTER(abi.CacheDesc), C.POINTER(_vp)],
+            "bg_cache_destroy": [_vp],
+            "bg_cache_info": [_vp, C.POINTER(_i32), C.POINTER(_i64), C.POINTER(_i32), C.POINTER(C.c_float)],
+            "bg_cache_query": [_vp, _vp, _vp, _i64, _vp],
+            "bg_cache_train": [_vp, _vp, _vp, _i64, _i32, C.POINTER(C.c_float), _vp],
+            "bg_cache_params": [_vp, _vp, _vp, _vp, _vp],
+            "bg_cache_set_params": [_vp, _vp, _vp],
+            "bg_render_cached": [_vp, _vp, C.POINTER(abi.CameraDesc), C.POINTER(abi.TracerDesc),
+                                 C.POINTER(abi.SamplerDesc), _i32, _i32, _vp, C.POINTER(abi.RenderStats), _vp],
         }
         for name, args in sig.items():
             fn = getattr(L, name)
@@ -200,6 +209,84 @@ class GpuScene:
     def close(self):
         if self.h:
             lib().bg_scene_destroy(self.h)
+            self.h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class RadianceCache:
+    """bg_cache: the online-trained neural radiance cache of a committed scene."""
+
+    def __init__(self, gscene, log2_table_size=19, base_resolution=16, max_resolution=2048, train_paths=65536,
+                 cache_depth=2, train_batch=16384, train_steps=4, learning_rate=1e-2, bbox=None, seed=1):
+        d = abi.CacheDesc()
+        d.levels = 16
+        d.log2_table_size = log2_table_size
+        d.base_resolution = base_resolution
+        d.max_resolution = max_resolution
+        d.train_paths = train_paths
+        d.cache_depth = cache_depth
+        d.train_batch = train_batch
+        d.train_steps = train_steps
+        d.learning_rate = learning_rate
+        if bbox is not None:
+            d.bbox_min[:] = list(bbox[0])
+            d.bbox_max[:] = list(bbox[1])
+        d.seed = seed
+        self.gs = gscene
+        self.h = _vp()
+        check(lib().bg_cache_create(gscene.h, C.byref(d), C.byref(self.h)))
+        self.log2_table_size = log2_table_size
+
+    def info(self):
+        nm, ng = _i32(), _i64()
+        res = (_i32 * 16)()
+        norm = (C.c_float * 6)()
+        check(lib().bg_cache_info(self.h, C.byref(nm), C.byref(ng), res, norm))
+        return {"mlp_params": nm.value, "grid_params": ng.value, "resolutions": list(res),
+                "bmin": np.array(norm[:3], dtype=np.float32), "bscale": np.array(norm[3:], dtype=np.float32)}
+
+    def query(self, feat_dev, out_dev, n, stream=None):
+        check(lib().bg_cache_query(self.h, feat_dev, out_dev, int(n), _stream_handle(stream)))
+
+    def train(self, feat_dev, target_dev, n, apply=True, want_loss=True, stream=None):
+        loss = C.c_float()
+        check(lib().bg_cache_train(self.h, feat_dev, target_dev, int(n), int(apply),
+                                   C.byref(loss) if want_loss else None, _stream_handle(stream)))
+        return loss.value if want_loss else None
+
+    def params(self):
+        inf = self.info()
+        mlp = np.zeros(inf["mlp_params"], np.float32)
+        grid = np.zeros(inf["grid_params"], np.float32)
+        gm = np.zeros_like(mlp)
+        gg = np.zeros_like(grid)
+        check(lib().bg_cache_params(self.h, mlp.ctypes.data, grid.ctypes.data, gm.ctypes.data, gg.ctypes.data))
+        return mlp, grid, gm, gg
+
+    def set_params(self, mlp=None, grid=None):
+        m = None if mlp is None else np.ascontiguousarray(mlp, np.float32)
+        g = None if grid is None else np.ascontiguousarray(grid, np.float32)
+        check(lib().bg_cache_set_params(self.h, None if m is None else m.ctypes.data, None if g is None else g.ctypes.data))
+
+    def render(self, accum_dev, width, height, spp, seed=1, sample_offset=0, maxdepth=8, camera=None, stream=None,
+               flags=0, stats=False):
+        sc = self.gs.scene
+        cam = sc.camera_desc() if camera is None else camera
+        tr = abi.TracerDesc(abi.BG_TRACER_GI, maxdepth, flags, 0)
+        sm = abi.SamplerDesc(0, spp, seed, sample_offset, 0)
+        st = abi.RenderStats()
+        check(lib().bg_render_cached(self.gs.h, self.h, C.byref(cam), C.byref(tr), C.byref(sm), int(width), int(height),
+                                     accum_dev, C.byref(st) if stats else None, _stream_handle(stream)))
+        return {k: getattr(st, k) for k, _ in abi.RenderStats._fields_} if stats else None
+
+    def close(self):
+        if self.h:
+            lib().bg_cache_destroy(self.h)
             self.h = _vp()
 
     def __del__(self):

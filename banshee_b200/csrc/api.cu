@@ -1,5 +1,6 @@
 // C ABI (include/banshee_gpu.h): context, scene assembly and commit, ray casts.
 #include <algorithm>
+#include <cfloat>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -259,6 +260,12 @@ static int commit_scene(bg_scene* s, const bg_build_opts* opts) {
             hi[3 * t + 2] = std::max(p[0].z, std::max(p[1].z, p[2].z));
         }
     }
+    for (int k = 0; k < 3; ++k) { s->bbox_lo[k] = FLT_MAX; s->bbox_hi[k] = -FLT_MAX; }
+    for (int64_t t = 0; t < ntris; ++t)
+        for (int k = 0; k < 3; ++k) {
+            if (std::isfinite(lo[3 * size_t(t) + k])) s->bbox_lo[k] = std::min(s->bbox_lo[k], lo[3 * size_t(t) + k]);
+            if (std::isfinite(hi[3 * size_t(t) + k])) s->bbox_hi[k] = std::max(s->bbox_hi[k], hi[3 * size_t(t) + k]);
+        }
     BuildParams bp;
     if (opts) {
         if (opts->node_width != 0 && opts->node_width != 4)

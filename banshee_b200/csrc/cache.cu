@@ -1,0 +1,724 @@
+// Neural radiance cache (see cache.h): encoding, fused BF16 tensor-core MLP
+// inference and training, hash-grid backward, Adam, and its C ABI.
+//
+// The MLP kernels keep a warp's 16 rows in registers through all six layers:
+// the fp32 accumulator fragment of mma.m16n8k16 for output columns 16j..16j+15
+// is, after ReLU and bf16 packing, exactly the A fragment of k-tile j of the
+// next layer, so activations never leave the register file.  Weights live in
+// shared memory with rows padded by 8 elements (conflict-free fragment loads);
+// the backward pass uses a transposed copy.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "cache.h"
+#include "internal.h"
+
+namespace bg {
+
+// ------------------------------------------------------------- helpers
+__device__ __forceinline__ void mma16816(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+__device__ __forceinline__ uint32_t pack2(float lo, float hi) {
+    __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<uint32_t*>(&v);
+}
+__device__ __forceinline__ float lo_f(uint32_t v) { return __uint_as_float(v << 16); }
+__device__ __forceinline__ float hi_f(uint32_t v) { return __uint_as_float(v & 0xffff0000u); }
+
+// shared-memory layouts (bf16 elements): forward W[out][in], backward W^T[in][out]
+constexpr int kS0 = 136, kS1 = 72, kS5 = 72;           // forward row strides
+constexpr int kFwW0 = 0, kFwW1 = kFwW0 + 64 * kS0, kFwW5 = kFwW1 + 4 * 64 * kS1, kFwTotal = kFwW5 + 16 * kS5;
+constexpr int kT0 = 72, kT1 = 72, kT5 = 24;            // backward row strides
+constexpr int kBwW0 = 0, kBwW1 = kBwW0 + 128 * kT0, kBwW5 = kBwW1 + 4 * 64 * kT1, kBwTotal = kBwW5 + 64 * kT5;
+
+__device__ void load_weights_fwd(const __nv_bfloat16* __restrict__ wb, __nv_bfloat16* s) {
+    for (int i = threadIdx.x; i < kNrcParams; i += blockDim.x) {
+        int off;
+        if (i < kNrcW1) off = kFwW0 + (i / 128) * kS0 + (i % 128);
+        else if (i < kNrcW5) { int j = i - kNrcW1, l = j / 4096, k = j % 4096; off = kFwW1 + l * 64 * kS1 + (k / 64) * kS1 + (k % 64); }
+        else { int j = i - kNrcW5; off = kFwW5 + (j / 64) * kS5 + (j % 64); }
+        s[off] = wb[i];
+    }
+}
+__device__ void load_weights_bwd(const __nv_bfloat16* __restrict__ wb, __nv_bfloat16* s) {
+    for (int i = threadIdx.x; i < kNrcParams; i += blockDim.x) {
+        int off;
+        if (i < kNrcW1) { int o = i / 128, in = i % 128; off = kBwW0 + in * kT0 + o; }
+        else if (i < kNrcW5) { int j = i - kNrcW1, l = j / 4096, k = j % 4096, o = k / 64, in = k % 64; off = kBwW1 + l * 64 * kT1 + in * kT1 + o; }
+        else { int j = i - kNrcW5, o = j / 64, in = j % 64; off = kBwW5 + in * kT5 + o; }
+        s[off] = wb[i];
+    }
+}
+
+// acc[NT] += A[KT] x B, with B[k][n] = W[n][k] (row stride `stride`)
+template <int KT, int NT>
+__device__ __forceinline__ void mlp_layer(const uint32_t (&a)[KT][4], const __nv_bfloat16* W, int stride, float (&acc)[NT][4]) {
+    const int lane = threadIdx.x & 31, r = lane >> 2, c = (lane & 3) * 2;
+#pragma unroll
+    for (int nt = 0; nt < NT; ++nt) acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
+#pragma unroll
+    for (int kt = 0; kt < KT; ++kt) {
+#pragma unroll
+        for (int nt = 0; nt < NT; ++nt) {
+            const __nv_bfloat16* wp = W + (nt * 8 + r) * stride + kt * 16 + c;
+            uint32_t b0 = *reinterpret_cast<const uint32_t*>(wp);
+            uint32_t b1 = *reinterpret_cast<const uint32_t*>(wp + 8);
+            mma16816(acc[nt], a[kt], b0, b1);
+        }
+    }
+}
+
+// accumulator fragments of 2*KT n-tiles -> A fragments of KT k-tiles
+template <int KT>
+__device__ __forceinline__ void to_afrag(const float (&acc)[2 * KT][4], uint32_t (&a)[KT][4], bool relu) {
+#pragma unroll
+    for (int j = 0; j < KT; ++j) {
+        float v[8] = {acc[2 * j][0], acc[2 * j][1], acc[2 * j][2], acc[2 * j][3],
+                      acc[2 * j + 1][0], acc[2 * j + 1][1], acc[2 * j + 1][2], acc[2 * j + 1][3]};
+        if (relu) {
+#pragma unroll
+            for (int e = 0; e < 8; ++e) v[e] = fmaxf(v[e], 0.f);
+        }
+        a[j][0] = pack2(v[0], v[1]);
+        a[j][1] = pack2(v[2], v[3]);
+        a[j][2] = pack2(v[4], v[5]);
+        a[j][3] = pack2(v[6], v[7]);
+    }
+}
+
+// zero the gradient entries whose forward activation (A fragments h) was <= 0
+template <int KT>
+__device__ __forceinline__ void relu_mask(float (&g)[2 * KT][4], const uint32_t (&h)[KT][4]) {
+#pragma unroll
+    for (int nt = 0; nt < 2 * KT; ++nt) {
+        const int j = nt >> 1, q = (nt & 1) ? 2 : 0;
+        if (!(lo_f(h[j][q]) > 0.f)) g[nt][0] = 0.f;
+        if (!(hi_f(h[j][q]) > 0.f)) g[nt][1] = 0.f;
+        if (!(lo_f(h[j][q + 1]) > 0.f)) g[nt][2] = 0.f;
+        if (!(hi_f(h[j][q + 1]) > 0.f)) g[nt][3] = 0.f;
+    }
+}
+
+// store A fragments (16 rows x 16*KT cols) as bf16 rows [row][ld]
+template <int KT>
+__device__ __forceinline__ void store_afrag(const uint32_t (&a)[KT][4], __nv_bfloat16* base, int row0, int nrows, int ld) {
+    const int lane = threadIdx.x & 31, r = lane >> 2, c = (lane & 3) * 2;
+#pragma unroll
+    for (int j = 0; j < KT; ++j) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int row = row0 + r + ((q & 1) ? 8 : 0);
+            const int col = 16 * j + c + ((q & 2) ? 8 : 0);
+            if (row < nrows) *reinterpret_cast<uint32_t*>(base + size_t(row) * ld + col) = a[j][q];
+        }
+    }
+}
+
+__device__ __forceinline__ void load_input(const __nv_bfloat16* X, int row0, int nrows, uint32_t (&a)[8][4]) {
+    const int lane = threadIdx.x & 31, r = lane >> 2, c = (lane & 3) * 2;
+#pragma unroll
+    for (int kt = 0; kt < 8; ++kt) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int row = row0 + r + ((q & 1) ? 8 : 0);
+            const int col = 16 * kt + c + ((q & 2) ? 8 : 0);
+            a[kt][q] = row < nrows ? *reinterpret_cast<const uint32_t*>(X + size_t(row) * kNrcIn + col) : 0u;
+        }
+    }
+}
+
+// forward through all layers; h[l] (l = 0..4) = post-ReLU hidden activations
+__device__ __forceinline__ void mlp_forward(const __nv_bfloat16* sw, const uint32_t (&ain)[8][4], uint32_t (&h)[5][4][4],
+                                            float (&out)[2][4]) {
+    float acc[8][4];
+    mlp_layer<8, 8>(ain, sw + kFwW0, kS0, acc);
+    to_afrag<4>(acc, h[0], true);
+#pragma unroll
+    for (int l = 1; l < 5; ++l) {
+        mlp_layer<4, 8>(h[l - 1], sw + kFwW1 + (l - 1) * 64 * kS1, kS1, acc);
+        to_afrag<4>(acc, h[l], true);
+    }
+    mlp_layer<4, 2>(h[4], sw + kFwW5, kS5, out);
+}
+
+// ------------------------------------------------------------- encoding
+__device__ __forceinline__ uint32_t grid_index(const NrcDev& C, int level, int x, int y, int z) {
+    const uint32_t T = 1u << C.log2_T;
+    const uint32_t n1 = uint32_t(C.res[level]) + 1u;
+    if (uint64_t(n1) * n1 * n1 <= T) return uint32_t(x) + n1 * (uint32_t(y) + n1 * uint32_t(z));
+    return (uint32_t(x) * 1u ^ uint32_t(y) * 2654435761u ^ uint32_t(z) * 805459861u) & (T - 1u);
+}
+
+struct GridCorner {
+    int x0, y0, z0;
+    float fx, fy, fz;
+};
+__device__ __forceinline__ GridCorner grid_cell(const NrcDev& C, int level, const float* u) {
+    GridCorner g;
+    const float N = float(C.res[level]);
+    float x = u[0] * N, y = u[1] * N, z = u[2] * N;
+    float fx0 = fminf(floorf(x), N - 1.f), fy0 = fminf(floorf(y), N - 1.f), fz0 = fminf(floorf(z), N - 1.f);
+    g.x0 = int(fx0); g.y0 = int(fy0); g.z0 = int(fz0);
+    g.fx = x - fx0; g.fy = y - fy0; g.fz = z - fz0;
+    return g;
+}
+
+__device__ __forceinline__ void norm_pos(const NrcDev& C, const float* f, float* u) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) u[k] = fminf(fmaxf((f[k] - C.bmin[k]) * C.bscale[k], 0.f), 1.f);
+}
+
+__device__ __forceinline__ void one_blob(float v, __nv_bfloat16* dst) {
+#pragma unroll
+    for (int b = 0; b < 16; ++b) {
+        float d = v - (b + 0.5f) * (1.f / 16.f);
+        dst[b] = __float2bfloat16_rn(__expf(-d * d * 128.f));
+    }
+}
+
+__device__ __forceinline__ void sph(float x, float y, float z, float& th, float& ph) {
+    th = acosf(fminf(fmaxf(z, -1.f), 1.f)) * (1.f / BG_PI);
+    ph = atan2f(y, x) * (0.5f / BG_PI) + 0.5f;
+}
+
+// raw query records [n][16] -> encoded bf16 rows [n][128]
+__global__ void __launch_bounds__(128) k_nrc_encode(NrcDev C, const float* __restrict__ feat, const int* n_dev, int64_t n_static,
+                                                    int offset, int limit, __nv_bfloat16* __restrict__ X) {
+    int64_t n = n_dev ? int64_t(*n_dev) : n_static;
+    n = n - offset;
+    if (limit > 0 && n > limit) n = limit;
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+        const float* f = feat + (size_t(offset) + size_t(i)) * kNrcFeatFloats;
+        float fr[13];
+#pragma unroll
+        for (int k = 0; k < 13; ++k) fr[k] = f[k];
+        __nv_bfloat16 row[kNrcIn];
+        float u[3];
+        norm_pos(C, fr, u);
+        for (int l = 0; l < kNrcLevels; ++l) {
+            GridCorner g = grid_cell(C, l, u);
+            float a0 = 0.f, a1 = 0.f;
+#pragma unroll
+            for (int cidx = 0; cidx < 8; ++cidx) {
+                const int dx = cidx & 1, dy = (cidx >> 1) & 1, dz = (cidx >> 2) & 1;
+                const float w = (dx ? g.fx : 1.f - g.fx) * (dy ? g.fy : 1.f - g.fy) * (dz ? g.fz : 1.f - g.fz);
+                const uint32_t idx = grid_index(C, l, g.x0 + dx, g.y0 + dy, g.z0 + dz);
+                const float2 v = *reinterpret_cast<const float2*>(C.grid + (size_t(l) << C.log2_T) * 2 + size_t(idx) * 2);
+                a0 += w * v.x;
+                a1 += w * v.y;
+            }
+            row[2 * l] = __float2bfloat16_rn(a0);
+            row[2 * l + 1] = __float2bfloat16_rn(a1);
+        }
+        float th, ph;
+        sph(fr[3], fr[4], fr[5], th, ph);
+        one_blob(th, row + 32);
+        one_blob(ph, row + 48);
+        sph(fr[6], fr[7], fr[8], th, ph);
+        one_blob(th, row + 64);
+        one_blob(ph, row + 80);
+        row[96] = __float2bfloat16_rn(fr[9]);
+        row[97] = __float2bfloat16_rn(fr[10]);
+        row[98] = __float2bfloat16_rn(fr[11]);
+        row[99] = __float2bfloat16_rn(fr[12]);
+        row[100] = __float2bfloat16_rn(1.f);
+        for (int k = 101; k < kNrcIn; ++k) row[k] = __float2bfloat16_rn(0.f);
+        uint4* dst = reinterpret_cast<uint4*>(X + size_t(i) * kNrcIn);
+        const uint4* src = reinterpret_cast<const uint4*>(row);
+#pragma unroll
+        for (int k = 0; k < kNrcIn / 8; ++k) dst[k] = src[k];
+    }
+}
+
+// ------------------------------------------------------------- inference
+// out[i] = (r, g, b, 0) for the n encoded rows
+__global__ void __launch_bounds__(128) k_nrc_infer(NrcDev C, const __nv_bfloat16* __restrict__ X, const int* n_dev,
+                                                   int64_t n_static, float4* __restrict__ out) {
+    extern __shared__ __align__(16) __nv_bfloat16 sw[];
+    load_weights_fwd(C.wb, sw);
+    __syncthreads();
+    const int64_t n = n_dev ? int64_t(*n_dev) : n_static;
+    const int lane = threadIdx.x & 31, r = lane >> 2, q = lane & 3;
+    const int warps = blockDim.x / 32;
+    for (int64_t tile = int64_t(blockIdx.x) * warps + (threadIdx.x >> 5); tile * 16 < n; tile += int64_t(gridDim.x) * warps) {
+        const int row0 = int(tile * 16);
+        uint32_t ain[8][4];
+        load_input(X, row0, int(n), ain);
+        uint32_t h[5][4][4];
+        float o[2][4];
+        mlp_forward(sw, ain, h, o);
+        // columns 0,1 live in lanes with q == 0, column 2 in lanes with q == 1
+        if (q <= 1) {
+            for (int half = 0; half < 2; ++half) {
+                const int row = row0 + r + 8 * half;
+                if (row >= n) continue;
+                float* dst = reinterpret_cast<float*>(out + row);
+                if (q == 0) { dst[0] = o[0][2 * half]; dst[1] = o[0][2 * half + 1]; }
+                else { dst[2] = o[0][2 * half]; dst[3] = 0.f; }
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------- training
+struct TrainBufs {
+    const __nv_bfloat16* X;     // encoded inputs [B][128]
+    const float4* target;       // [B]
+    __nv_bfloat16* H;           // hidden activations h1..h5, [5][B][64]
+    __nv_bfloat16* DZ;          // gradients of layer outputs: dZ0..dZ4 [5][B][64], dZ5 at DZ5
+    __nv_bfloat16* DZ5;         // [B][16]
+    float* dX;                  // [B][32] gradient of the hash-grid features
+    float* loss;                // accumulated sum of the relative L2 terms
+    int B;                      // rows in this step
+};
+
+__global__ void __launch_bounds__(128) k_nrc_train(NrcDev C, TrainBufs T, const int* n_dev, int offset, int limit) {
+    extern __shared__ __align__(16) __nv_bfloat16 smem[];
+    __nv_bfloat16* sw = smem;
+    __nv_bfloat16* st = smem + kFwTotal;
+    load_weights_fwd(C.wb, sw);
+    load_weights_bwd(C.wb, st);
+    __syncthreads();
+    int n = n_dev ? *n_dev - offset : T.B;
+    if (limit > 0 && n > limit) n = limit;
+    const float invn = n > 0 ? 1.f / (3.f * float(n)) : 0.f;
+    const int lane = threadIdx.x & 31, r = lane >> 2, q = lane & 3, c = q * 2;
+    const int warps = blockDim.x / 32;
+    float lsum = 0.f;
+    for (int tile = blockIdx.x * warps + (threadIdx.x >> 5); tile * 16 < n; tile += gridDim.x * warps) {
+        const int row0 = tile * 16;
+        uint32_t ain[8][4];
+        load_input(T.X, row0, n, ain);
+        uint32_t h[5][4][4];
+        float o[2][4];
+        mlp_forward(sw, ain, h, o);
+#pragma unroll
+        for (int l = 0; l < 5; ++l) store_afrag<4>(h[l], T.H + size_t(l) * T.B * 64, row0, n, 64);
+        // relative L2 loss gradient on the 3 used outputs (columns 0..2 of n-tile 0)
+        float g[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const int row = row0 + r + ((e & 2) ? 8 : 0);
+            const int col = c + (e & 1);
+            if (row < n && col < 3) {
+                const float y = reinterpret_cast<const float*>(T.target + row)[col];
+                const float p = o[0][e];
+                const float den = p * p + 0.01f;
+                const float d = p - y;
+                lsum += d * d / den;
+                g[0][e] = 2.f * d / den * invn;
+            }
+        }
+        uint32_t adz[4][4];
+        uint32_t adz5[1][4];
+        to_afrag<1>(g, adz5, false);
+        store_afrag<1>(adz5, T.DZ5, row0, n, 16);
+        float acc[8][4];
+        mlp_layer<1, 8>(adz5, st + kBwW5, kT5, acc);       // dH5 = dZ5 W5
+        relu_mask<4>(acc, h[4]);
+        to_afrag<4>(acc, adz, false);
+        store_afrag<4>(adz, T.DZ + size_t(4) * T.B * 64, row0, n, 64);
+#pragma unroll
+        for (int l = 4; l >= 1; --l) {                      // dH_l = dZ_l W_l, masked by h_{l-1}
+            mlp_layer<4, 8>(adz, st + kBwW1 + (l - 1) * 64 * kT1, kT1, acc);
+            relu_mask<4>(acc, h[l - 1]);
+            to_afrag<4>(acc, adz, false);
+            store_afrag<4>(adz, T.DZ + size_t(l - 1) * T.B * 64, row0, n, 64);
+        }
+        float dx[4][4];                                     // dX (hash-grid columns 0..31) = dZ0 W0
+        mlp_layer<4, 4>(adz, st + kBwW0, kT0, dx);
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) {
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const int row = row0 + r + ((e & 2) ? 8 : 0);
+                const int col = nt * 8 + c + (e & 1);
+                if (row < n) T.dX[size_t(row) * 32 + col] = dx[nt][e];
+            }
+        }
+    }
+    for (int off = 16; off > 0; off >>= 1) lsum += __shfl_down_sync(0xffffffffu, lsum, off);
+    if (lane == 0) atomicAdd(T.loss, lsum);
+}
+
+// dW[o][i] += sum_s dZ[s][o] X[s][i] over this block's sample chunks (split K).
+template <int OUT, int IN>
+__global__ void __launch_bounds__(256) k_nrc_wgrad(const __nv_bfloat16* __restrict__ DZ, const __nv_bfloat16* __restrict__ X,
+                                                   const int* n_dev, int offset, int limit, int Bstatic, float* __restrict__ dW) {
+    constexpr int KC = 64, LD = KC + 8;   // samples per staged chunk (static shared memory <= 48 KB)
+    constexpr int MT = OUT / 16, NTT = IN / 8, PAIRS = MT * NTT, PW = PAIRS / 8;
+    __shared__ __align__(16) __nv_bfloat16 dzT[OUT * LD];
+    __shared__ __align__(16) __nv_bfloat16 xT[IN * LD];
+    int n = n_dev ? *n_dev - offset : Bstatic;
+    if (limit > 0 && n > limit) n = limit;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, r = lane >> 2, c = (lane & 3) * 2;
+    float acc[PW][4];
+#pragma unroll
+    for (int p = 0; p < PW; ++p) acc[p][0] = acc[p][1] = acc[p][2] = acc[p][3] = 0.f;
+    for (int s0 = blockIdx.x * KC; s0 < n; s0 += gridDim.x * KC) {
+        __syncthreads();
+        for (int v = threadIdx.x; v < KC * (OUT / 8); v += blockDim.x) {
+            const int sl = v / (OUT / 8), o0 = (v % (OUT / 8)) * 8;
+            uint4 w = make_uint4(0u, 0u, 0u, 0u);
+            if (s0 + sl < n) w = *reinterpret_cast<const uint4*>(DZ + size_t(s0 + sl) * OUT + o0);
+            const __nv_bfloat16* e = reinterpret_cast<const __nv_bfloat16*>(&w);
+#pragma unroll
+            for (int j = 0; j < 8; ++j) dzT[(o0 + j) * LD + sl] = e[j];
+        }
+        for (int v = threadIdx.x; v < KC * (IN / 8); v += blockDim.x) {
+            const int sl = v / (IN / 8), i0 = (v % (IN / 8)) * 8;
+            uint4 w = make_uint4(0u, 0u, 0u, 0u);
+            if (s0 + sl < n) w = *reinterpret_cast<const uint4*>(X + size_t(s0 + sl) * IN + i0);
+            const __nv_bfloat16* e = reinterpret_cast<const __nv_bfloat16*>(&w);
+#pragma unroll
+            for (int j = 0; j < 8; ++j) xT[(i0 + j) * LD + sl] = e[j];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int p = 0; p < PW; ++p) {
+            const int pair = warp + 8 * p;
+            const int m0 = (pair % MT) * 16, n0 = (pair / MT) * 8;
+#pragma unroll
+            for (int k0 = 0; k0 < KC; k0 += 16) {
+                uint32_t a[4];
+                a[0] = *reinterpret_cast<const uint32_t*>(dzT + (m0 + r) * LD + k0 + c);
+                a[1] = *reinterpret_cast<const uint32_t*>(dzT + (m0 + r + 8) * LD + k0 + c);
+                a[2] = *reinterpret_cast<const uint32_t*>(dzT + (m0 + r) * LD + k0 + c + 8);
+                a[3] = *reinterpret_cast<const uint32_t*>(dzT + (m0 + r + 8) * LD + k0 + c + 8);
+                uint32_t b0 = *reinterpret_cast<const uint32_t*>(xT + (n0 + r) * LD + k0 + c);
+                uint32_t b1 = *reinterpret_cast<const uint32_t*>(xT + (n0 + r) * LD + k0 + c + 8);
+                mma16816(acc[p], a, b0, b1);
+            }
+        }
+    }
+#pragma unroll
+    for (int p = 0; p < PW; ++p) {
+        const int pair = warp + 8 * p;
+        const int m0 = (pair % MT) * 16, n0 = (pair / MT) * 8;
+        atomicAdd(dW + (m0 + r) * IN + n0 + c, acc[p][0]);
+        atomicAdd(dW + (m0 + r) * IN + n0 + c + 1, acc[p][1]);
+        atomicAdd(dW + (m0 + r + 8) * IN + n0 + c, acc[p][2]);
+        atomicAdd(dW + (m0 + r + 8) * IN + n0 + c + 1, acc[p][3]);
+    }
+}
+
+// hash-grid backward: scatter dX through the trilinear weights
+__global__ void __launch_bounds__(128) k_nrc_grid_bwd(NrcDev C, const float* __restrict__ feat, const float* __restrict__ dX,
+                                                      const int* n_dev, int offset, int limit, int Bstatic) {
+    int n = n_dev ? *n_dev - offset : Bstatic;
+    if (limit > 0 && n > limit) n = limit;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float* f = feat + (size_t(offset) + size_t(i)) * kNrcFeatFloats;
+        float fr[3] = {f[0], f[1], f[2]};
+        float u[3];
+        norm_pos(C, fr, u);
+        for (int l = 0; l < kNrcLevels; ++l) {
+            const float g0 = dX[size_t(i) * 32 + 2 * l], g1 = dX[size_t(i) * 32 + 2 * l + 1];
+            if (g0 == 0.f && g1 == 0.f) continue;
+            GridCorner g = grid_cell(C, l, u);
+#pragma unroll
+            for (int cidx = 0; cidx < 8; ++cidx) {
+                const int dx = cidx & 1, dy = (cidx >> 1) & 1, dz = (cidx >> 2) & 1;
+                const float w = (dx ? g.fx : 1.f - g.fx) * (dy ? g.fy : 1.f - g.fy) * (dz ? g.fz : 1.f - g.fz);
+                const uint32_t idx = grid_index(C, l, g.x0 + dx, g.y0 + dy, g.z0 + dz);
+                float* dst = C.grid_grad + (size_t(l) << C.log2_T) * 2 + size_t(idx) * 2;
+                atomicAdd(dst, w * g0);
+                atomicAdd(dst + 1, w * g1);
+            }
+        }
+    }
+}
+
+__global__ void k_nrc_step(int* step) { *step += 1; }
+
+// Adam on fp32 masters; optionally writes a bf16 copy; clears the gradient.
+__global__ void __launch_bounds__(256) k_nrc_adam(float* __restrict__ p, float* __restrict__ g, float* __restrict__ m,
+                                                  float* __restrict__ v, int64_t n, const int* step, float lr, float b1,
+                                                  float b2, float eps, __nv_bfloat16* __restrict__ out) {
+    const int t = *step;
+    const float c1 = 1.f / (1.f - powf(b1, float(t))), c2 = 1.f / (1.f - powf(b2, float(t)));
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+        const float gi = g[i];
+        const float mi = b1 * m[i] + (1.f - b1) * gi;
+        const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        const float pi = p[i] - lr * (mi * c1) / (sqrtf(vi * c2) + eps);
+        p[i] = pi;
+        g[i] = 0.f;
+        if (out) out[i] = __float2bfloat16_rn(pi);
+    }
+}
+
+__global__ void k_nrc_to_bf16(const float* __restrict__ p, __nv_bfloat16* __restrict__ out, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = __float2bfloat16_rn(p[i]);
+}
+
+}  // namespace bg
+
+// ============================================================= host side
+struct bg_cache {
+    bg_scene* scene = nullptr;
+    bg_cache_desc desc{};
+    bg::NrcDev dev{};
+    bg::DevBuf grid, grid_grad, grid_m, grid_v, w, w_grad, w_m, w_v, wb, step;
+    bg::DevBuf X, H, DZ, DZ5, dX, feat, target, out, loss;   // training / query scratch
+    int64_t cap = 0;
+    int sms = 0;
+    int64_t frame = 0;
+};
+
+namespace bg {
+
+static int64_t grid_params(const bg_cache* c) { return int64_t(kNrcLevels) * (int64_t(1) << c->dev.log2_T) * kNrcFeat; }
+
+static int cache_scratch(bg_cache* c, int64_t rows) {
+    if (rows <= c->cap) return BG_OK;
+    int rc;
+    const size_t R = size_t(rows);
+    if ((rc = c->X.ensure(R * kNrcIn * 2)) || (rc = c->H.ensure(5 * R * 64 * 2)) || (rc = c->DZ.ensure(5 * R * 64 * 2)) ||
+        (rc = c->DZ5.ensure(R * 16 * 2)) || (rc = c->dX.ensure(R * 32 * 4)) || (rc = c->out.ensure(R * 16)))
+        return rc;
+    c->cap = rows;
+    return BG_OK;
+}
+
+static uint64_t mix64(uint64_t z) { return splitmix64(z); }
+
+static int cache_init_params(bg_cache* c) {
+    const int64_t gp = grid_params(c);
+    std::vector<float> g(static_cast<size_t>(gp)), w(kNrcParams);
+    uint64_t s = c->desc.seed * 0x9E3779B97F4A7C15ull + 12345u;
+    for (int64_t i = 0; i < gp; ++i) {
+        double u = double(mix64(s + uint64_t(i)) >> 11) * (1.0 / 9007199254740992.0);
+        g[size_t(i)] = float((u * 2.0 - 1.0) * 1e-4);
+    }
+    auto fill = [&](int off, int out, int in, uint64_t salt) {
+        const double lim = std::sqrt(6.0 / double(in + out));
+        for (int i = 0; i < out * in; ++i) {
+            double u = double(mix64(s ^ (salt * 0xD1B54A32D192ED03ull) ^ uint64_t(i)) >> 11) * (1.0 / 9007199254740992.0);
+            w[size_t(off + i)] = float((u * 2.0 - 1.0) * lim);
+        }
+    };
+    fill(kNrcW0, 64, 128, 1);
+    for (int l = 0; l < 4; ++l) fill(kNrcW1 + l * 4096, 64, 64, 2 + l);
+    fill(kNrcW5, 16, 64, 7);
+    BG_CUDA(cudaMemcpy(c->grid.ptr, g.data(), g.size() * 4, cudaMemcpyHostToDevice));
+    BG_CUDA(cudaMemcpy(c->w.ptr, w.data(), w.size() * 4, cudaMemcpyHostToDevice));
+    BG_CUDA(cudaMemset(c->grid_grad.ptr, 0, size_t(gp) * 4));
+    BG_CUDA(cudaMemset(c->grid_m.ptr, 0, size_t(gp) * 4));
+    BG_CUDA(cudaMemset(c->grid_v.ptr, 0, size_t(gp) * 4));
+    BG_CUDA(cudaMemset(c->w_grad.ptr, 0, kNrcParams * 4));
+    BG_CUDA(cudaMemset(c->w_m.ptr, 0, kNrcParams * 4));
+    BG_CUDA(cudaMemset(c->w_v.ptr, 0, kNrcParams * 4));
+    BG_CUDA(cudaMemset(c->step.ptr, 0, 16));
+    k_nrc_to_bf16<<<64, 256>>>(c->w.as<float>(), c->wb.as<__nv_bfloat16>(), kNrcParams);
+    BG_CUDA(cudaGetLastError());
+    BG_CUDA(cudaDeviceSynchronize());
+    return BG_OK;
+}
+
+static constexpr int kInferSmem = kFwTotal * 2;
+static constexpr int kTrainSmem = (kFwTotal + kBwTotal) * 2;
+
+int nrc_encode(bg_cache* c, const float* feat, const int* n_dev, int64_t n_static, int offset, int limit, cudaStream_t st) {
+    k_nrc_encode<<<c->sms * 8, 128, 0, st>>>(c->dev, feat, n_dev, n_static, offset, limit, c->X.as<__nv_bfloat16>());
+    BG_CUDA(cudaGetLastError());
+    return BG_OK;
+}
+
+int nrc_infer(bg_cache* c, const int* n_dev, int64_t n_static, float4* out, cudaStream_t st) {
+    k_nrc_infer<<<c->sms * 4, 128, kInferSmem, st>>>(c->dev, c->X.as<__nv_bfloat16>(), n_dev, n_static, out);
+    BG_CUDA(cudaGetLastError());
+    return BG_OK;
+}
+
+// One Adam step on rows [offset, offset + B) of (feat, target); n from n_dev or B.
+int nrc_train_step(bg_cache* c, const float* feat, const float4* target, const int* n_dev, int offset, int B, bool apply,
+                   cudaStream_t st) {
+    int rc;
+    if ((rc = nrc_encode(c, feat, n_dev, B, offset, B, st))) return rc;
+    TrainBufs T;
+    T.X = c->X.as<__nv_bfloat16>();
+    T.target = target + offset;
+    T.H = c->H.as<__nv_bfloat16>();
+    T.DZ = c->DZ.as<__nv_bfloat16>();
+    T.DZ5 = c->DZ5.as<__nv_bfloat16>();
+    T.dX = c->dX.as<float>();
+    T.loss = c->loss.as<float>();
+    T.B = B;
+    k_nrc_train<<<c->sms * 2, 128, kTrainSmem, st>>>(c->dev, T, n_dev, offset, B);
+    const int wg = c->sms;
+    const __nv_bfloat16* H = c->H.as<__nv_bfloat16>();
+    const __nv_bfloat16* DZ = c->DZ.as<__nv_bfloat16>();
+    float* dW = c->w_grad.as<float>();
+    const size_t L = size_t(B) * 64;
+    k_nrc_wgrad<64, 128><<<wg, 256, 0, st>>>(DZ, T.X, n_dev, offset, B, B, dW + kNrcW0);
+    for (int l = 1; l < 5; ++l)
+        k_nrc_wgrad<64, 64><<<wg, 256, 0, st>>>(DZ + l * L, H + (l - 1) * L, n_dev, offset, B, B, dW + kNrcW1 + (l - 1) * 4096);
+    k_nrc_wgrad<16, 64><<<wg, 256, 0, st>>>(T.DZ5, H + 4 * L, n_dev, offset, B, B, dW + kNrcW5);
+    k_nrc_grid_bwd<<<c->sms * 8, 128, 0, st>>>(c->dev, feat, T.dX, n_dev, offset, B, B);
+    BG_CUDA(cudaGetLastError());
+    if (apply) {
+        k_nrc_step<<<1, 1, 0, st>>>(c->step.as<int>());
+        k_nrc_adam<<<c->sms * 4, 256, 0, st>>>(c->w.as<float>(), dW, c->w_m.as<float>(), c->w_v.as<float>(), kNrcParams,
+                                               c->step.as<int>(), c->dev.lr, c->dev.beta1, c->dev.beta2, c->dev.eps,
+                                               c->wb.as<__nv_bfloat16>());
+        k_nrc_adam<<<c->sms * 8, 256, 0, st>>>(c->grid.as<float>(), c->grid_grad.as<float>(), c->grid_m.as<float>(),
+                                               c->grid_v.as<float>(), grid_params(c), c->step.as<int>(), c->dev.lr,
+                                               c->dev.beta1, c->dev.beta2, c->dev.eps, nullptr);
+        BG_CUDA(cudaGetLastError());
+    }
+    return BG_OK;
+}
+
+int nrc_prepare(bg_cache* c, int64_t rows) { return cache_scratch(c, rows); }
+const bg_cache_desc* nrc_desc(const bg_cache* c) { return &c->desc; }
+int64_t nrc_next_frame(bg_cache* c) { return c->frame++; }
+bg_scene* nrc_scene(const bg_cache* c) { return c->scene; }
+
+}  // namespace bg
+
+using namespace bg;
+
+extern "C" {
+
+int bg_cache_create(bg_scene* s, const bg_cache_desc* d, bg_cache** out) {
+    if (!s || !d || !out) return set_error(BG_ERR_INVALID_ARG, "NULL argument");
+    if (!s->committed) return set_error(BG_ERR_STATE, "scene not committed");
+    if (d->levels != 0 && d->levels != kNrcLevels) return set_error(BG_ERR_UNSUPPORTED, "levels must be %d", kNrcLevels);
+    if (d->log2_table_size < 4 || d->log2_table_size > 24) return set_error(BG_ERR_INVALID_ARG, "log2_table_size out of range 4..24");
+    if (d->base_resolution < 2 || d->max_resolution < d->base_resolution || d->max_resolution > (1 << 20))
+        return set_error(BG_ERR_INVALID_ARG, "bad grid resolutions");
+    *out = nullptr;
+    bg_cache* c = new bg_cache();
+    c->scene = s;
+    c->desc = *d;
+    if (c->desc.train_paths <= 0) c->desc.train_paths = 65536;
+    if (c->desc.train_batch <= 0) c->desc.train_batch = 16384;
+    if (c->desc.train_steps < 0) c->desc.train_steps = 0;
+    if (c->desc.cache_depth < 0) c->desc.cache_depth = 2;
+    c->sms = s->ctx->num_sms;
+    NrcDev& D = c->dev;
+    D.log2_T = d->log2_table_size;
+    const double b = std::exp((std::log(double(d->max_resolution)) - std::log(double(d->base_resolution))) / (kNrcLevels - 1));
+    for (int l = 0; l < kNrcLevels; ++l) D.res[l] = int(std::floor(double(d->base_resolution) * std::pow(b, l)));
+    float lo[3], hi[3];
+    for (int k = 0; k < 3; ++k) {
+        lo[k] = d->bbox_max[k] > d->bbox_min[k] ? d->bbox_min[k] : s->bbox_lo[k];
+        hi[k] = d->bbox_max[k] > d->bbox_min[k] ? d->bbox_max[k] : s->bbox_hi[k];
+        const float ext = std::max(hi[k] - lo[k], 1e-6f);
+        D.bmin[k] = lo[k] - 1e-3f * ext;
+        D.bscale[k] = 1.f / (ext * 1.002f);
+    }
+    D.lr = d->learning_rate > 0.f ? d->learning_rate : 1e-2f;
+    D.beta1 = 0.9f;
+    D.beta2 = 0.99f;
+    D.eps = 1e-15f;
+    const int64_t gp = grid_params(c);
+    int rc;
+    if ((rc = c->grid.ensure(size_t(gp) * 4)) || (rc = c->grid_grad.ensure(size_t(gp) * 4)) ||
+        (rc = c->grid_m.ensure(size_t(gp) * 4)) || (rc = c->grid_v.ensure(size_t(gp) * 4)) ||
+        (rc = c->w.ensure(kNrcParams * 4)) || (rc = c->w_grad.ensure(kNrcParams * 4)) ||
+        (rc = c->w_m.ensure(kNrcParams * 4)) || (rc = c->w_v.ensure(kNrcParams * 4)) ||
+        (rc = c->wb.ensure(kNrcParams * 2)) || (rc = c->step.ensure(16)) || (rc = c->loss.ensure(16))) {
+        bg_cache_destroy(c);
+        return rc;
+    }
+    D.grid = c->grid.as<float>(); D.grid_grad = c->grid_grad.as<float>();
+    D.grid_m = c->grid_m.as<float>(); D.grid_v = c->grid_v.as<float>();
+    D.w = c->w.as<float>(); D.w_grad = c->w_grad.as<float>(); D.w_m = c->w_m.as<float>(); D.w_v = c->w_v.as<float>();
+    D.wb = c->wb.as<__nv_bfloat16>();
+    D.step = c->step.as<int>();
+    cudaFuncSetAttribute(k_nrc_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, kInferSmem);
+    cudaFuncSetAttribute(k_nrc_train, cudaFuncAttributeMaxDynamicSharedMemorySize, kTrainSmem);
+    if ((rc = cache_init_params(c))) { bg_cache_destroy(c); return rc; }
+    *out = c;
+    return BG_OK;
+}
+
+int bg_cache_destroy(bg_cache* c) {
+    if (!c) return BG_OK;
+    cudaDeviceSynchronize();
+    for (DevBuf* b : {&c->grid, &c->grid_grad, &c->grid_m, &c->grid_v, &c->w, &c->w_grad, &c->w_m, &c->w_v, &c->wb,
+                      &c->step, &c->X, &c->H, &c->DZ, &c->DZ5, &c->dX, &c->feat, &c->target, &c->out, &c->loss})
+        b->release();
+    delete c;
+    return BG_OK;
+}
+
+int bg_cache_query(bg_cache* c, const float* feat, float* out_rgba, int64_t n, void* stream) {
+    if (!c || (n > 0 && (!feat || !out_rgba))) return set_error(BG_ERR_INVALID_ARG, "NULL argument");
+    if (n < 0 || n > (int64_t(1) << 30)) return set_error(BG_ERR_INVALID_ARG, "bad query count");
+    if (n == 0) return BG_OK;
+    int rc;
+    if ((rc = cache_scratch(c, n))) return rc;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if ((rc = nrc_encode(c, feat, nullptr, n, 0, 0, st))) return rc;
+    return nrc_infer(c, nullptr, n, reinterpret_cast<float4*>(out_rgba), st);
+}
+
+int bg_cache_train(bg_cache* c, const float* feat, const float* target_rgba, int64_t n, int32_t apply, float* loss,
+                   void* stream) {
+    if (!c || (n > 0 && (!feat || !target_rgba))) return set_error(BG_ERR_INVALID_ARG, "NULL argument");
+    if (n <= 0 || n > (int64_t(1) << 26)) return set_error(BG_ERR_INVALID_ARG, "bad training batch size");
+    int rc;
+    if ((rc = cache_scratch(c, n))) return rc;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    BG_CUDA(cudaMemsetAsync(c->loss.ptr, 0, 4, st));
+    if ((rc = nrc_train_step(c, feat, reinterpret_cast<const float4*>(target_rgba), nullptr, 0, int(n), apply != 0, st)))
+        return rc;
+    if (loss) {
+        float l = 0.f;
+        BG_CUDA(cudaMemcpyAsync(&l, c->loss.ptr, 4, cudaMemcpyDeviceToHost, st));
+        BG_CUDA(cudaStreamSynchronize(st));
+        *loss = l / float(3 * n);
+    }
+    return BG_OK;
+}
+
+int bg_cache_params(bg_cache* c, float* mlp, float* grid, float* mlp_grad, float* grid_grad) {
+    if (!c) return set_error(BG_ERR_INVALID_ARG, "cache is NULL");
+    BG_CUDA(cudaDeviceSynchronize());
+    const size_t gp = size_t(grid_params(c));
+    if (mlp) BG_CUDA(cudaMemcpy(mlp, c->w.ptr, kNrcParams * 4, cudaMemcpyDeviceToHost));
+    if (grid) BG_CUDA(cudaMemcpy(grid, c->grid.ptr, gp * 4, cudaMemcpyDeviceToHost));
+    if (mlp_grad) BG_CUDA(cudaMemcpy(mlp_grad, c->w_grad.ptr, kNrcParams * 4, cudaMemcpyDeviceToHost));
+    if (grid_grad) BG_CUDA(cudaMemcpy(grid_grad, c->grid_grad.ptr, gp * 4, cudaMemcpyDeviceToHost));
+    return BG_OK;
+}
+
+int bg_cache_set_params(bg_cache* c, const float* mlp, const float* grid) {
+    if (!c) return set_error(BG_ERR_INVALID_ARG, "cache is NULL");
+    BG_CUDA(cudaDeviceSynchronize());
+    if (mlp) {
+        BG_CUDA(cudaMemcpy(c->w.ptr, mlp, kNrcParams * 4, cudaMemcpyHostToDevice));
+        k_nrc_to_bf16<<<64, 256>>>(c->w.as<float>(), c->wb.as<__nv_bfloat16>(), kNrcParams);
+        BG_CUDA(cudaGetLastError());
+    }
+    if (grid) BG_CUDA(cudaMemcpy(c->grid.ptr, grid, size_t(grid_params(c)) * 4, cudaMemcpyHostToDevice));
+    BG_CUDA(cudaMemset(c->w_grad.ptr, 0, kNrcParams * 4));
+    BG_CUDA(cudaMemset(c->grid_grad.ptr, 0, size_t(grid_params(c)) * 4));
+    BG_CUDA(cudaDeviceSynchronize());
+    return BG_OK;
+}
+
+int bg_cache_info(bg_cache* c, int32_t* nparams_mlp, int64_t* nparams_grid, int32_t* resolutions, float* norm6) {
+    if (!c) return set_error(BG_ERR_INVALID_ARG, "cache is NULL");
+    if (nparams_mlp) *nparams_mlp = kNrcParams;
+    if (nparams_grid) *nparams_grid = grid_params(c);
+    if (resolutions) memcpy(resolutions, c->dev.res, sizeof(c->dev.res));
+    if (norm6) {
+        memcpy(norm6, c->dev.bmin, 3 * sizeof(float));
+        memcpy(norm6 + 3, c->dev.bscale, 3 * sizeof(float));
+    }
+    return BG_OK;
+}
+
+}  // extern "C"

@@ -61,6 +61,7 @@ struct bg_scene {
     std::vector<bg_material_desc> mats;
     std::vector<bg_light_desc> lights;
     float bg[3] = {0.f, 0.f, 0.f};
+    float bbox_lo[3] = {0.f, 0.f, 0.f}, bbox_hi[3] = {0.f, 0.f, 0.f};   // world bounds of all triangles
     bool committed = false;
 
     bg::DevBuf nodes, tris, shade, bundles, mats_d, lights_d, err;

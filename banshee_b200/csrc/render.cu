@@ -22,10 +22,25 @@
 #include <cstring>
 #include <vector>
 
+#include "cache.h"
 #include "internal.h"
 #include "shading.cuh"
 
 namespace bg {
+
+// cache.cu
+int nrc_prepare(bg_cache* c, int64_t rows);
+int nrc_encode(bg_cache* c, const float* feat, const int* n_dev, int64_t n_static, int offset, int limit, cudaStream_t st);
+int nrc_infer(bg_cache* c, const int* n_dev, int64_t n_static, float4* out, cudaStream_t st);
+int nrc_train_step(bg_cache* c, const float* feat, const float4* target, const int* n_dev, int offset, int B, bool apply,
+                   cudaStream_t st);
+const bg_cache_desc* nrc_desc(const bg_cache* c);
+int64_t nrc_next_frame(bg_cache* c);
+bg_scene* nrc_scene(const bg_cache* c);
+
+__global__ void k_clamp_count(int* n, int cap) {
+    if (*n > cap) *n = cap;
+}
 
 constexpr int kShadeThreads = 128;
 constexpr int kMaxBounceCounters = 6 * 1024;   // 6 work counters per bounce, maxdepth <= 1024
@@ -48,6 +63,9 @@ struct RenderState {
     DevBuf slots, sample_rad;
     DevBuf cnt_out;    // outputs of the instrumented 1/64 replays
     DevBuf work;       // persistent-kernel work counters of the pass (6 per bounce)
+    // radiance-cache mode: cache queries, training-path vertex records, training samples
+    DevBuf q_feat, q_path, q_thr, q_out, rec, tr_feat, tr_target;
+    int64_t q_cap = 0, tr_cap = 0;
     int blocks = 0;
     // CUDA graph of one pass, replayed on an internal stream
     cudaStream_t gstream = nullptr;
@@ -68,13 +86,14 @@ void render_state_free(RenderState* rs) {
                       &rs->sh_rays, &rs->sh_contrib, &rs->sh_slot, &rs->sh_occ, &rs->mis_rays, &rs->mis_a, &rs->mis_b,
                       &rs->mis_c, &rs->mis_hits, &rs->end_path, &rs->counts, &rs->st_key, &rs->st_cnt, &rs->st_rng,
                       &rs->st_bs, &rs->st_thr, &rs->st_rad, &rs->st_dithr, &rs->st_flags, &rs->slots,
-                      &rs->sample_rad, &rs->cnt_out, &rs->work})
+                      &rs->sample_rad, &rs->cnt_out, &rs->work, &rs->q_feat, &rs->q_path, &rs->q_thr,
+                      &rs->q_out, &rs->rec, &rs->tr_feat, &rs->tr_target})
         b->release();
     delete rs;
 }
 
-enum : int { kCntExt0 = 0, kCntExt1 = 1, kCntSh = 2, kCntMis = 3, kCntEnd = 4 };
-enum : unsigned { kFlagNoClamp = 1u };
+enum : int { kCntExt0 = 0, kCntExt1 = 1, kCntSh = 2, kCntMis = 3, kCntEnd = 4, kCntQuery = 5, kCntTrain = 6 };
+enum : unsigned { kFlagNoClamp = 1u, kFlagTrain = 2u };   // bits 8..15: recorded vertices of a training path
 
 struct PathState {
     unsigned long long* key;
@@ -87,6 +106,7 @@ struct PathState {
     unsigned* flags;
     float4* slots;     // cap * kmax
     float4* sample_rad;
+    float4* rec;       // training paths: per vertex feat[4], throughput, radiance before the vertex
 };
 
 struct Queues {
@@ -97,6 +117,8 @@ struct Queues {
     int* end_path;
     int* n_ext_in; int* n_ext_out; int* n_sh; int* n_mis; int* n_end;
     unsigned long long* totals;   // [0] closest rays, [1] any rays
+    float4* q_feat; int* q_path; float4* q_thr; int* n_query;        // cache queries
+    float4* tr_feat; float4* tr_target; int* n_train; int tr_cap;   // training samples
 };
 
 // Warp-aggregated slot allocation: one atomicAdd per converged group of lanes.
@@ -117,7 +139,8 @@ __device__ __forceinline__ void put_ray(float4* rays, int i, v3 o, float tmin, v
 
 // ------------------------------------------------------------- generate
 __global__ void __launch_bounds__(kShadeThreads)
-k_generate(CamDev cam, int np, int ns, int p0, int s0, int W, int H, uint64_t seed, PathState P, Queues Q, int total) {
+k_generate(CamDev cam, int np, int ns, int p0, int s0, int W, int H, uint64_t seed, PathState P, Queues Q, int total,
+           int train_stride, int train_phase) {
     const int nthreads = gridDim.x * blockDim.x;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += nthreads) {
         const int sl = i / np;
@@ -144,7 +167,7 @@ k_generate(CamDev cam, int np, int ns, int p0, int s0, int W, int H, uint64_t se
         P.rng[i] = make_uint4(lr.z, lr.w, br.z, br.w);
         P.thr[i] = make_float4(1.f, 1.f, 1.f, 0.f);
         P.rad[i] = make_float4(0.f, 0.f, 0.f, __int_as_float(0));
-        P.flags[i] = 0u;
+        P.flags[i] = (train_stride > 0 && (i + train_phase) % train_stride == 0) ? kFlagTrain : 0u;
         P.sample_rad[i] = make_float4(0.f, 0.f, 0.f, 0.f);
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) *Q.n_ext_in = total;
@@ -167,7 +190,26 @@ __device__ __forceinline__ v3 gather_pending(const PathState& P, int kmax, int p
 
 struct ShadeArgs {
     int bounce, maxdepth, kind, kmax, nlights;
+    int cache_depth;              // -1: plain tracer
+    int train_stride, train_phase;
 };
+
+// Radiance-cache query record of a surface point: position, outgoing
+// direction, shading normal, roughness, albedo (layout of bg_cache_query).
+__device__ __forceinline__ void cache_features(const SHit& h, v3 wo, const MatRec& M, float4 (&f)[4]) {
+    float rough = 0.f, ar = 0.f, ag = 0.f, ab = 0.f;
+    if (M.type == BG_MAT_LAMBERT) {
+        rough = 1.f; ar = M.kd[0]; ag = M.kd[1]; ab = M.kd[2];
+    } else if (M.type == BG_MAT_MICROFACET_GGX) {
+        float r0 = (M.eta - 1.f) / (M.eta + 1.f);
+        r0 *= r0;
+        rough = M.a; ar = r0 * M.ks[0]; ag = r0 * M.ks[1]; ab = r0 * M.ks[2];
+    }
+    f[0] = make_float4(h.p.x, h.p.y, h.p.z, wo.x);
+    f[1] = make_float4(wo.y, wo.z, h.n.x, h.n.y);
+    f[2] = make_float4(h.n.z, rough, ar, ag);
+    f[3] = make_float4(ab, 0.f, 0.f, 0.f);
+}
 
 // One light's DirectIllumination terms (DiTracer::GetDi, ditracer.cpp:57-239, n = 1).
 __device__ __noinline__ void emit_di(const DevScene& S, const Queues& Q, int li, const SHit& h, const MatRec& M, v3 wo,
@@ -278,11 +320,36 @@ k_shade(DevScene S, ShadeArgs A, PathState P, Queues Q) {
             const v3 wo = neg(d);
             float4 t4 = P.thr[path];
             v3 thr = mk(t4.x, t4.y, t4.z);
+            const unsigned pflags = P.flags[path];
+            const bool train = (pflags & kFlagTrain) != 0;
+            flags = pflags;
             if (A.bounce == 0 && M.type == BG_MAT_EMISSIVE) {
                 if (A.kind == BG_TRACER_GI) rad = add(rad, emissive_le(M, h.n, wo));   // gitracer.cpp:61-68
                 if (A.kind == BG_TRACER_DI) flags |= kFlagNoClamp;                    // ditracer.cpp:29-32
                 end = true;
+            } else if (A.cache_depth >= 0 && !train && A.bounce == A.cache_depth) {
+                // the rendering path ends into the radiance cache at this vertex
+                float4 f[4];
+                cache_features(h, wo, M, f);
+                int q = warp_push(Q.n_query);
+#pragma unroll
+                for (int k = 0; k < 4; ++k) Q.q_feat[4 * q + k] = f[k];
+                Q.q_path[q] = path;
+                Q.q_thr[q] = make_float4(thr.x, thr.y, thr.z, 0.f);
+                end = true;
             } else {
+                if (A.cache_depth >= 0 && train) {
+                    // training path: remember the vertex, its throughput and the radiance so far
+                    const int t = (path + A.train_phase) / A.train_stride;
+                    float4* rr = P.rec + (size_t(t) * A.maxdepth + A.bounce) * 6;
+                    float4 f[4];
+                    cache_features(h, wo, M, f);
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) rr[k] = f[k];
+                    rr[4] = make_float4(thr.x, thr.y, thr.z, 0.f);
+                    rr[5] = make_float4(rad.x, rad.y, rad.z, 0.f);
+                    flags = (flags & ~0xff00u) | (unsigned(A.bounce + 1) << 8);
+                }
                 unsigned cnt = P.cnt[path];
                 const int base = path * A.kmax;
                 // bounce 0: every light, weight 1; later: one light picked by rand(), weight L
@@ -333,8 +400,9 @@ k_shade(DevScene S, ShadeArgs A, PathState P, Queues Q) {
             }
         }
         P.rad[path] = make_float4(rad.x, rad.y, rad.z, __int_as_float(pending));
+        if (hit.primid < 0) flags |= P.flags[path];
+        P.flags[path] = flags;
         if (end) {
-            P.flags[path] = flags;
             int k = warp_push(Q.n_end);
             Q.end_path[k] = path;
         }
@@ -386,18 +454,51 @@ k_resolve_mis(DevScene S, PathState P, Queues Q) {
 }
 
 __global__ void __launch_bounds__(kShadeThreads)
-k_finalize(PathState P, Queues Q, int kmax) {
+k_finalize(PathState P, Queues Q, int kmax, int maxdepth, int train_stride, int train_phase) {
     const int n = *Q.n_end;
     const int nthreads = gridDim.x * blockDim.x;
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += nthreads) {
         const int path = Q.end_path[e];
         float4 r4 = P.rad[path];
         v3 rad = gather_pending(P, kmax, path, mk(r4.x, r4.y, r4.z), __float_as_int(r4.w));
-        if (!(P.flags[path] & kFlagNoClamp)) {
+        const unsigned fl = P.flags[path];
+        const int nv = int((fl >> 8) & 0xffu);
+        if ((fl & kFlagTrain) && nv > 0 && train_stride > 0) {
+            // one training sample per recorded vertex: radiance gathered from that
+            // vertex on, divided by the throughput that reached it
+            const int t = (path + train_phase) / train_stride;
+            for (int k = 0; k < nv; ++k) {
+                const float4* rr = P.rec + (size_t(t) * maxdepth + k) * 6;
+                const float4 tk = rr[4], rb = rr[5];
+                if (!(tk.x > 1e-6f && tk.y > 1e-6f && tk.z > 1e-6f)) continue;
+                int q = warp_push(Q.n_train);
+                if (q >= Q.tr_cap) continue;
+#pragma unroll
+                for (int j = 0; j < 4; ++j) Q.tr_feat[4 * q + j] = rr[j];
+                Q.tr_target[q] = make_float4((rad.x - rb.x) / tk.x, (rad.y - rb.y) / tk.y, (rad.z - rb.z) / tk.z, 0.f);
+            }
+        }
+        if (!(fl & kFlagNoClamp)) {
             v3 r = muls(rad, (1.f / 1));
             rad = mk(clamp_ref(r.x, 0.f, BG_MAXRADIANCE), clamp_ref(r.y, 0.f, BG_MAXRADIANCE), clamp_ref(r.z, 0.f, BG_MAXRADIANCE));
         }
         P.sample_rad[path] = make_float4(rad.x, rad.y, rad.z, 1.f);
+    }
+}
+
+// rendering paths that ended into the cache: radiance += throughput * max(prediction, 0)
+__global__ void __launch_bounds__(kShadeThreads)
+k_cache_resolve(PathState P, Queues Q, const float4* __restrict__ pred) {
+    const int n = *Q.n_query;
+    const int nthreads = gridDim.x * blockDim.x;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += nthreads) {
+        const int path = Q.q_path[q];
+        const float4 p = pred[q], t = Q.q_thr[q];
+        float4 r = P.rad[path];
+        r.x += t.x * fmaxf(p.x, 0.f);
+        r.y += t.y * fmaxf(p.y, 0.f);
+        r.z += t.z * fmaxf(p.z, 0.f);
+        P.rad[path] = r;
     }
 }
 
@@ -493,6 +594,8 @@ struct PassCfg {
     int np, ns, p0, s0, W, H, maxdepth, kind;
     uint64_t seed;
     float4* accum;
+    bg_cache* cache;           // radiance-cache mode when non-null
+    int cache_depth, train_stride, train_phase;
 };
 
 static void pass_queues(RenderState* rs, int c, Queues& Q) {
@@ -509,6 +612,11 @@ static void pass_queues(RenderState* rs, int c, Queues& Q) {
     Q.ext_rays_out = rs->ext_rays[1 - c].as<float4>(); Q.ext_path_out = rs->ext_path[1 - c].as<int>();
     Q.n_ext_in = cnt + (c ? kCntExt1 : kCntExt0);
     Q.n_ext_out = cnt + (c ? kCntExt0 : kCntExt1);
+    Q.q_feat = rs->q_feat.as<float4>(); Q.q_path = rs->q_path.as<int>(); Q.q_thr = rs->q_thr.as<float4>();
+    Q.n_query = cnt + kCntQuery;
+    Q.tr_feat = rs->tr_feat.as<float4>(); Q.tr_target = rs->tr_target.as<float4>();
+    Q.n_train = cnt + kCntTrain;
+    Q.tr_cap = int(rs->tr_cap);
 }
 
 static PathState path_state(RenderState* rs) {
@@ -523,6 +631,7 @@ static PathState path_state(RenderState* rs) {
     P.flags = rs->st_flags.as<unsigned>();
     P.slots = rs->slots.as<float4>();
     P.sample_rad = rs->sample_rad.as<float4>();
+    P.rec = rs->rec.as<float4>();
     return P;
 }
 
@@ -537,7 +646,8 @@ static int enqueue_pass(bg_scene* s, RenderState* rs, cudaStream_t st, const Cam
     pass_queues(rs, cur, Q);
     int* cnt = rs->counts.as<int>();
     int rc;
-    k_generate<<<nb, kShadeThreads, 0, st>>>(cam, c.np, c.ns, c.p0, c.s0, c.W, c.H, c.seed, P, Q, total);
+    k_generate<<<nb, kShadeThreads, 0, st>>>(cam, c.np, c.ns, c.p0, c.s0, c.W, c.H, c.seed, P, Q, total,
+                                             c.cache ? c.train_stride : 0, c.train_phase);
     if (ins) ++ins->launches;
     bg_hit* cnt_hits = rs->cnt_out.as<bg_hit>();
     uint8_t* cnt_occ = rs->cnt_out.as<uint8_t>();
@@ -552,7 +662,9 @@ static int enqueue_pass(bg_scene* s, RenderState* rs, cudaStream_t st, const Cam
             if ((rc = launch_trace(s, false, Q.ext_rays_in, 0, Q.n_ext_in, cnt_hits, nullptr, st, Q.totals + 3, 64, wk + 1))) return rc;
             ++ins->launches;
         }
-        ShadeArgs A{b, c.maxdepth, c.kind, rs->kmax, s->dev.nlights};
+        ShadeArgs A{b, c.maxdepth, c.kind, rs->kmax, s->dev.nlights, c.cache ? c.cache_depth : -1,
+                    c.cache ? c.train_stride : 0, c.train_phase};
+        if (c.cache && b == c.cache_depth) BG_CUDA(cudaMemsetAsync(Q.n_query, 0, sizeof(int), st));
         k_shade<<<nb, kShadeThreads, 0, st>>>(s->dev, A, P, Q);
         if (ins) { ++ins->launches; ins->mark(1); }
         if ((rc = launch_trace(s, true, Q.sh_rays, 0, Q.n_sh, nullptr, Q.sh_occ, st, nullptr, 1, wk + 2))) return rc;
@@ -566,7 +678,15 @@ static int enqueue_pass(bg_scene* s, RenderState* rs, cudaStream_t st, const Cam
         }
         k_resolve_shadow<<<nb, kShadeThreads, 0, st>>>(P, Q);
         k_resolve_mis<<<nb, kShadeThreads, 0, st>>>(s->dev, P, Q);
-        k_finalize<<<nb, kShadeThreads, 0, st>>>(P, Q, rs->kmax);
+        if (c.cache && b == c.cache_depth) {
+            // rendering paths that ended here: encode, infer, add throughput * prediction
+            float4* qo = rs->q_out.as<float4>();
+            if ((rc = nrc_encode(c.cache, rs->q_feat.as<float>(), Q.n_query, 0, 0, 0, st))) return rc;
+            if ((rc = nrc_infer(c.cache, Q.n_query, 0, qo, st))) return rc;
+            k_cache_resolve<<<nb, kShadeThreads, 0, st>>>(P, Q, qo);
+            if (ins) ins->launches += 3;
+        }
+        k_finalize<<<nb, kShadeThreads, 0, st>>>(P, Q, rs->kmax, c.maxdepth, c.cache ? c.train_stride : 0, c.train_phase);
         if (ins) ins->launches += 3;
         cur = 1 - cur;
         pass_queues(rs, cur, Q);
@@ -622,7 +742,8 @@ static int launch_pass_graph(bg_scene* s, RenderState* rs, const CamDev& cam, co
     CamDev camv = cam;
     int np = c.np, ns = c.ns, p0 = c.p0, s0 = c.s0, W = c.W, H = c.H;
     uint64_t seed = c.seed;
-    void* gargs[] = {&camv, &np, &ns, &p0, &s0, &W, &H, &seed, &P, &Q, &total};
+    int tstride = 0, tphase = 0;
+    void* gargs[] = {&camv, &np, &ns, &p0, &s0, &W, &H, &seed, &P, &Q, &total, &tstride, &tphase};
     cudaKernelNodeParams kp;
     BG_CUDA(cudaGraphKernelNodeGetParams(rs->gen_node, &kp));
     kp.kernelParams = gargs;
@@ -638,8 +759,8 @@ static int launch_pass_graph(bg_scene* s, RenderState* rs, const CamDev& cam, co
     return BG_OK;
 }
 
-static int render_impl(bg_scene* s, const bg_camera_desc* cam, const bg_tracer_desc* tr, const bg_sampler_desc* sm,
-                       int W, int H, float4* accum, bg_render_stats* stats, cudaStream_t st) {
+static int render_impl(bg_scene* s, bg_cache* cache, const bg_camera_desc* cam, const bg_tracer_desc* tr,
+                       const bg_sampler_desc* sm, int W, int H, float4* accum, bg_render_stats* stats, cudaStream_t st) {
     if (!s) return set_error(BG_ERR_INVALID_ARG, "scene is NULL");
     if (!s->committed) return set_error(BG_ERR_STATE, "scene not committed");
     if (!cam || !tr || !sm || !accum) return set_error(BG_ERR_INVALID_ARG, "NULL argument");
@@ -665,7 +786,38 @@ static int render_impl(bg_scene* s, const bg_camera_desc* cam, const bg_tracer_d
     // Graph replay unless statistics were asked for or the caller's stream is capturing.
     cudaStreamCaptureStatus cap_st = cudaStreamCaptureStatusNone;
     BG_CUDA(cudaStreamIsCapturing(st, &cap_st));
-    const bool use_graph = !stats && cap_st == cudaStreamCaptureStatusNone;
+    const bool use_graph = !stats && !cache && cap_st == cudaStreamCaptureStatusNone;
+    // radiance-cache mode: training-path selection and buffers
+    int cache_depth = -1, stride = 0, phase = 0, tsteps = 0, tbatch = 0;
+    if (cache) {
+        const bg_cache_desc* cd = nrc_desc(cache);
+        if (tr->kind != BG_TRACER_GI) return set_error(BG_ERR_UNSUPPORTED, "the radiance cache serves GiTracer only");
+        cache_depth = cd->cache_depth;
+        if (cache_depth < 0 || cache_depth >= std::max(1, maxdepth)) return set_error(BG_ERR_INVALID_ARG, "cache_depth %d outside [0, maxdepth)", cache_depth);
+        const int64_t total = npix * int64_t(std::max(1, sm->spp));
+        const int64_t tp = std::max<int64_t>(1, cd->train_paths);
+        stride = int(std::max<int64_t>(1, std::min<int64_t>(total / tp, int64_t(1) << 24)));
+        phase = int(nrc_next_frame(cache) % stride);
+        tsteps = std::max(0, cd->train_steps);
+        tbatch = std::max(1, cd->train_batch);
+        const int64_t npass = (npix + cap - 1) / cap * ((std::max(1, sm->spp) + std::max<int64_t>(1, cap / std::max<int64_t>(1, npix)) - 1)
+                                                        / std::max<int64_t>(1, cap / std::max<int64_t>(1, npix)));
+        const int64_t tpaths_pass = cap / stride + 2;
+        const int64_t tr_cap = (total / stride + 2 * npass + 2) * maxdepth;
+        if (rs->q_cap < cap) {
+            if ((rc = rs->q_feat.ensure(size_t(cap) * 64)) || (rc = rs->q_path.ensure(size_t(cap) * 4)) ||
+                (rc = rs->q_thr.ensure(size_t(cap) * 16)) || (rc = rs->q_out.ensure(size_t(cap) * 16)))
+                return rc;
+            rs->q_cap = cap;
+        }
+        if ((rc = rs->rec.ensure(size_t(tpaths_pass) * maxdepth * 6 * 16))) return rc;
+        if (rs->tr_cap < tr_cap) {
+            if ((rc = rs->tr_feat.ensure(size_t(tr_cap) * 64)) || (rc = rs->tr_target.ensure(size_t(tr_cap) * 16))) return rc;
+            rs->tr_cap = tr_cap;
+        }
+        if ((rc = nrc_prepare(cache, std::max<int64_t>(cap, tbatch)))) return rc;
+        BG_CUDA(cudaMemsetAsync(rs->counts.as<int>() + kCntTrain, 0, sizeof(int), st));
+    }
     Instr ins;
     ins.st = st;
     ins.time_phases = stats && (tr->flags & BG_RENDER_TIME_PHASES);
@@ -688,12 +840,24 @@ static int render_impl(bg_scene* s, const bg_camera_desc* cam, const bg_tracer_d
         const int np = int(std::min<int64_t>(cap, npix - p0));
         for (int s0 = 0; s0 < sm->spp;) {
             const int ns = int(std::max<int64_t>(1, std::min<int64_t>(sm->spp - s0, cap / np)));
-            PassCfg c{np, ns, int(p0), sm->sample_offset + s0, W, H, maxdepth, tr->kind, sm->seed, accum};
+            PassCfg c{np, ns, int(p0), sm->sample_offset + s0, W, H, maxdepth, tr->kind, sm->seed, accum,
+                      cache, cache_depth, stride, phase};
             rc = use_graph ? launch_pass_graph(s, rs, camd, c) : enqueue_pass(s, rs, st, camd, c, &ins);
             if (rc) return rc;
             done_samples += int64_t(np) * ns;
             s0 += ns;
         }
+    }
+    if (cache && tsteps > 0) {
+        // online training on this frame's samples (gradients + Adam per step)
+        int* ntr = rs->counts.as<int>() + kCntTrain;
+        k_clamp_count<<<1, 1, 0, st>>>(ntr, int(rs->tr_cap));
+        for (int i = 0; i < tsteps; ++i) {
+            if ((rc = nrc_train_step(cache, rs->tr_feat.as<float>(), rs->tr_target.as<float4>(), ntr, i * tbatch, tbatch,
+                                     true, st)))
+                return rc;
+        }
+        ins.launches += 1 + 11 * tsteps;
     }
     if (use_graph) {
         BG_CUDA(cudaEventRecord(rs->ev_out, rs->gstream));
@@ -748,7 +912,16 @@ extern "C" int bg_render(bg_scene* s, const bg_camera_desc* cam, const bg_tracer
                          int32_t W, int32_t H, float* accum, bg_render_stats* stats, void* stream) {
     if (!s) return set_error(BG_ERR_INVALID_ARG, "scene is NULL");
     std::lock_guard<std::mutex> lk(s->mu);
-    return render_impl(s, cam, tr, sm, W, H, reinterpret_cast<float4*>(accum), stats, static_cast<cudaStream_t>(stream));
+    return render_impl(s, nullptr, cam, tr, sm, W, H, reinterpret_cast<float4*>(accum), stats, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int bg_render_cached(bg_scene* s, bg_cache* cache, const bg_camera_desc* cam, const bg_tracer_desc* tr,
+                                const bg_sampler_desc* sm, int32_t W, int32_t H, float* accum, bg_render_stats* stats,
+                                void* stream) {
+    if (!s || !cache) return set_error(BG_ERR_INVALID_ARG, "scene or cache is NULL");
+    if (nrc_scene(cache) != s) return set_error(BG_ERR_INVALID_ARG, "the cache was created for another scene");
+    std::lock_guard<std::mutex> lk(s->mu);
+    return render_impl(s, cache, cam, tr, sm, W, H, reinterpret_cast<float4*>(accum), stats, static_cast<cudaStream_t>(stream));
 }
 
 extern "C" int bg_render_host(bg_scene* s, const bg_camera_desc* cam, const bg_tracer_desc* tr, const bg_sampler_desc* sm,
@@ -763,7 +936,7 @@ extern "C" int bg_render_host(bg_scene* s, const bg_camera_desc* cam, const bg_t
     if (rc) return rc;
     float4* d = s->host_out.as<float4>();
     BG_CUDA(cudaMemcpy(d, accum, bytes, cudaMemcpyHostToDevice));
-    rc = render_impl(s, cam, tr, sm, W, H, d, stats, 0);
+    rc = render_impl(s, nullptr, cam, tr, sm, W, H, d, stats, 0);
     if (rc) return rc;
     BG_CUDA(cudaMemcpy(accum, d, bytes, cudaMemcpyDeviceToHost));
     unsigned flags = 0;

@@ -280,6 +280,56 @@ int bg_render_host(bg_scene* scene, const bg_camera_desc* camera, const bg_trace
                    const bg_sampler_desc* sampler, int32_t width, int32_t height,
                    float* accum_rgbw, bg_render_stats* stats);
 
+/* ------------------------------------------------------ radiance cache */
+/* Neural radiance cache.  No counterpart in the reference: Banshee has no
+ * learned component.  A hash-grid + one-blob encoded, 64-wide, 5-hidden-layer
+ * BF16 MLP (fp32 accumulation) predicts the outgoing radiance at a path
+ * vertex; it is trained online (Adam, relative L2 loss) on radiance that
+ * training paths of the tracer itself produce, and rendering paths end into it
+ * after cache_depth bounces (bg_render_cached). */
+typedef struct bg_cache bg_cache;
+
+typedef struct bg_cache_desc {
+    int32_t levels;            /* hash-grid levels: 16 (0 = 16)                */
+    int32_t log2_table_size;   /* entries per level = 2^this (19 in C5)        */
+    int32_t base_resolution;   /* coarsest grid resolution (16)                */
+    int32_t max_resolution;    /* finest grid resolution (2048)                */
+    int32_t train_paths;       /* training paths per frame (65536)             */
+    int32_t cache_depth;       /* rendering paths end into the cache here (2)  */
+    int32_t train_batch;       /* rows per Adam step (16384)                   */
+    int32_t train_steps;       /* Adam steps per frame at most (4)             */
+    float learning_rate;       /* Adam learning rate (1e-2)                    */
+    float bbox_min[3];         /* position normalisation; all zero = scene     */
+    float bbox_max[3];         /* bounds                                       */
+    uint64_t seed;             /* parameter initialisation                     */
+} bg_cache_desc;
+
+/* Query record: 16 floats per row = position (3), outgoing direction (3),
+ * shading normal (3), roughness, albedo (3), 3 unused.  Outputs / targets are
+ * 4 floats per row (rgb, unused). */
+int bg_cache_create(bg_scene* scene, const bg_cache_desc* desc, bg_cache** out);
+int bg_cache_destroy(bg_cache* cache);
+/* resolutions: 16 ints; norm6: position normalisation u = (p - norm6[0:3]) * norm6[3:6]. */
+int bg_cache_info(bg_cache* cache, int32_t* nparams_mlp, int64_t* nparams_grid, int32_t* resolutions, float* norm6);
+int bg_cache_query(bg_cache* cache, const float* features_dev, float* out_rgba_dev, int64_t n, void* stream);
+/* One training step on n rows: loss, gradients and (apply != 0) an Adam
+ * update.  loss (may be NULL) receives the mean relative L2 loss; passing it
+ * synchronises. */
+int bg_cache_train(bg_cache* cache, const float* features_dev, const float* target_rgba_dev, int64_t n,
+                   int32_t apply, float* loss, void* stream);
+/* Host copies of the fp32 parameters / last gradients (any may be NULL):
+ * MLP packed as [64][128], 4 x [64][64], [16][64] row-major ([out][in]);
+ * grid as [levels][2^log2_table_size][2]. */
+int bg_cache_params(bg_cache* cache, float* mlp, float* grid, float* mlp_grad, float* grid_grad);
+int bg_cache_set_params(bg_cache* cache, const float* mlp, const float* grid);
+/* Renders like bg_render with GiTracer(tracer->maxdepth), except that
+ * rendering paths end into the cache at vertex desc.cache_depth, and
+ * desc.train_paths paths per call are traced in full and train the cache
+ * (desc.train_steps Adam steps) after the frame. */
+int bg_render_cached(bg_scene* scene, bg_cache* cache, const bg_camera_desc* camera, const bg_tracer_desc* tracer,
+                     const bg_sampler_desc* sampler, int32_t width, int32_t height, float* accum_rgbw_dev,
+                     bg_render_stats* stats, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
