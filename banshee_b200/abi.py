@@ -85,6 +85,7 @@ class RenderStats(C.Structure):
                 ("rays_any", C.c_int64), ("kernel_launches", C.c_int64),
                 ("ms_total", C.c_float), ("ms_extend", C.c_float), ("ms_mis", C.c_float), ("ms_shadow", C.c_float),
                 ("ms_shade", C.c_float), ("launches_extend", C.c_int32),
+                ("ms_cache_query", C.c_float), ("ms_cache_train", C.c_float),
                 ("sub_rays_extension", C.c_int64), ("sub_nodes_extension", C.c_int64),
                 ("sub_tris_extension", C.c_int64),
                 ("sub_rays_any", C.c_int64), ("sub_nodes_any", C.c_int64), ("sub_tris_any", C.c_int64),

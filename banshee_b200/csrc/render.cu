@@ -680,11 +680,12 @@ static int enqueue_pass(bg_scene* s, RenderState* rs, cudaStream_t st, const Cam
         k_resolve_mis<<<nb, kShadeThreads, 0, st>>>(s->dev, P, Q);
         if (c.cache && b == c.cache_depth) {
             // rendering paths that ended here: encode, infer, add throughput * prediction
+            if (ins) ins->mark(3);
             float4* qo = rs->q_out.as<float4>();
             if ((rc = nrc_encode(c.cache, rs->q_feat.as<float>(), Q.n_query, 0, 0, 0, st))) return rc;
             if ((rc = nrc_infer(c.cache, Q.n_query, 0, qo, st))) return rc;
             k_cache_resolve<<<nb, kShadeThreads, 0, st>>>(P, Q, qo);
-            if (ins) ins->launches += 3;
+            if (ins) { ins->launches += 3; ins->mark(3); }
         }
         k_finalize<<<nb, kShadeThreads, 0, st>>>(P, Q, rs->kmax, c.maxdepth, c.cache ? c.train_stride : 0, c.train_phase);
         if (ins) ins->launches += 3;
@@ -851,6 +852,7 @@ static int render_impl(bg_scene* s, bg_cache* cache, const bg_camera_desc* cam, 
     if (cache && tsteps > 0) {
         // online training on this frame's samples (gradients + Adam per step)
         int* ntr = rs->counts.as<int>() + kCntTrain;
+        ins.mark(4);
         k_clamp_count<<<1, 1, 0, st>>>(ntr, int(rs->tr_cap));
         for (int i = 0; i < tsteps; ++i) {
             if ((rc = nrc_train_step(cache, rs->tr_feat.as<float>(), rs->tr_target.as<float4>(), ntr, i * tbatch, tbatch,
@@ -858,6 +860,7 @@ static int render_impl(bg_scene* s, bg_cache* cache, const bg_camera_desc* cam, 
                 return rc;
         }
         ins.launches += 1 + 11 * tsteps;
+        ins.mark(4);
     }
     if (use_graph) {
         BG_CUDA(cudaEventRecord(rs->ev_out, rs->gstream));
@@ -878,7 +881,7 @@ static int render_impl(bg_scene* s, bg_cache* cache, const bg_camera_desc* cam, 
         stats->kernel_launches = ins.launches;
         stats->launches_extend = ins.launches_extend;
         stats->ms_total = ms;
-        float phase[3] = {0.f, 0.f, 0.f};
+        float phase[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
         for (size_t i = 0; i + 1 < ins.evs.size(); i += 2) {
             float m = 0.f;
             cudaEventElapsedTime(&m, ins.evs[i], ins.evs[i + 1]);
@@ -888,7 +891,9 @@ static int render_impl(bg_scene* s, bg_cache* cache, const bg_camera_desc* cam, 
         stats->ms_extend = phase[0];
         stats->ms_shadow = phase[1];
         stats->ms_mis = phase[2];
-        stats->ms_shade = ins.time_phases ? ms - phase[0] - phase[1] - phase[2] : 0.f;
+        stats->ms_cache_query = phase[3];
+        stats->ms_cache_train = phase[4];
+        stats->ms_shade = ins.time_phases ? ms - phase[0] - phase[1] - phase[2] - phase[3] - phase[4] : 0.f;
         stats->sub_rays_extension = int64_t(t[3]);
         stats->sub_nodes_extension = int64_t(t[4]);
         stats->sub_tris_extension = int64_t(t[5]);

@@ -164,6 +164,114 @@ def run_reference_arm(args, rank):
     return 0
 
 
+def raycast_c2(ctx, nrays=1 << 24, reps=5):
+    """C2: 1M-triangle soup, 16M rays per set (coherent 4096^2 pinhole / incoherent),
+    closest hit (tmax = FLT_MAX) and any hit (tmax U[0,1]); device-resident rays,
+    CUDA-event timing; bytes/ray from an instrumented replay of every 64th ray."""
+    import torch
+    from banshee_b200 import capi, scenes
+    gs = capi.GpuScene(ctx, scenes.soup(1 << 20, seed=1))
+    info = gs.info()
+    out = {"triangles": info["ntriangles"], "rays_per_set": nrays, "bvh_nodes": info["nnodes"],
+           "build_ms": info["build_ms"]}
+    for kind in ("coherent", "incoherent"):
+        for anyhit in (False, True):
+            rays = scenes.soup_rays(nrays, kind, seed=2, any_hit=anyhit)
+            dr = torch.from_numpy(rays.view(np.uint8)).cuda()
+            res = torch.zeros(nrays * (1 if anyhit else 16), dtype=torch.uint8, device="cuda")
+            fn = gs.intersect_any if anyhit else gs.intersect_closest
+            for _ in range(2):
+                fn(dr.data_ptr(), res.data_ptr(), nrays)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(reps):
+                fn(dr.data_ptr(), res.data_ptr(), nrays)
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / reps
+            sub = torch.from_numpy(np.ascontiguousarray(rays[::64]).view(np.uint8)).cuda()
+            nodes, tris = gs.traversal_counts(sub.data_ptr(), sub.numel() // 32, anyhit)
+            nsub = sub.numel() // 32
+            bpr = 32 + (1 if anyhit else 16) + info["node_stride"] * nodes / nsub + 48 * tris / nsub
+            out[kind + ("_any" if anyhit else "_closest")] = {
+                "mrays_per_s": nrays / ms / 1e3, "ms": ms, "nodes_per_ray": nodes / nsub, "tris_per_ray": tris / nsub,
+                "bytes_per_ray": bpr, "achieved_gbs": bpr * nrays / (ms * 1e-3) / 1e9}
+            del dr, res, sub
+    gs.close()
+    return out
+
+
+def cornell_c1(ctx, ref_seconds_cap=60.0):
+    """C1: Cornell box 256x256, 64 spp, GiTracer(5): GPU Msamples/s and relMSE of the
+    GPU image against Banshee's own CPU render of the same samples (oracle/_ref)."""
+    import torch
+    from banshee_b200 import capi, scenes
+    from banshee_b200.metrics import mean_image, relmse
+    sc = scenes.cornell(256, 256)
+    gs = capi.GpuScene(ctx, sc)
+    acc = torch.zeros((256, 256, 4), dtype=torch.float32, device="cuda")
+    gs.render(acc.data_ptr(), 256, 256, 64, seed=1, maxdepth=5, stats=False)
+    acc.zero_()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    gs.render(acc.data_ptr(), 256, 256, 64, seed=1, maxdepth=5, stats=False)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    out = {"resolution": [256, 256], "spp": 64, "maxdepth": 5, "gpu_ms": ms, "gpu_msamples_per_s": 256 * 256 * 64 / ms / 1e3}
+    try:
+        from oracle.oracle import Reference
+        t0 = time.perf_counter()
+        ref = Reference(sc).render(spp=64, seed=1, maxdepth=5)
+        dt = time.perf_counter() - t0
+        out.update({"reference_cpu_s": dt, "reference_cpu_msamples_per_s": 256 * 256 * 64 / dt / 1e6,
+                    "reference_cores": os.cpu_count(),
+                    "relmse_gpu_vs_reference": relmse(mean_image(acc.cpu().numpy()), mean_image(ref))})
+    except Exception as exc:
+        out["reference"] = "unavailable: %s" % exc
+    gs.close()
+    return out
+
+
+def time_to_relmse(gs, sc, args, target=1e-3):
+    """Second half of the metric: wall (GPU) time for the radiance-cache tracer and
+    the plain tracer to reach relMSE 1e-3 on a centred 240x136 window of the 1080p
+    frame, against a plain render of that window at args.gt_spp spp accumulated in
+    float64.  Both tracers render full 1080p frames, 1 spp per frame."""
+    from banshee_b200 import capi
+    from banshee_b200 import convergence as CV
+    Wc, Hc = 240, 136
+    wcam = CV.window_camera(sc.camera, WIDTH, HEIGHT, Wc, Hc)
+    t0 = time.perf_counter()
+    gt = CV.ground_truth(gs, Wc, Hc, args.gt_spp, MAXDEPTH, seed=7777, camera=wcam)
+    gt_s = time.perf_counter() - t0
+    plain = CV.converge(lambda p, f: gs.render(p, WIDTH, HEIGHT, 1, seed=SEED, sample_offset=f, maxdepth=MAXDEPTH,
+                                               stats=False),
+                        WIDTH, HEIGHT, Wc, Hc, gt, args.conv_seconds, 100000, target=target, every=4)
+    cache = capi.RadianceCache(gs, log2_table_size=19, base_resolution=16, max_resolution=2048, train_paths=65536,
+                               cache_depth=2, train_batch=16384, train_steps=1, learning_rate=1e-2)
+    cached = CV.converge(lambda p, f: cache.render(p, WIDTH, HEIGHT, 1, seed=SEED, sample_offset=f,
+                                                   maxdepth=MAXDEPTH),
+                         WIDTH, HEIGHT, Wc, Hc, gt, args.conv_seconds, 100000, target=target, every=4)
+    cache.close()
+
+    def summ(r):
+        return {"seconds_to_target": r["t_target"], "frames": r["frames"], "final_relmse": r["final_relmse"],
+                "ms_per_frame": 1e3 * r["seconds"] / max(1, r["frames"]),
+                "curve": [[round(t, 4), n, float("%.4g" % e)] for t, n, e in r["curve"][::max(1, len(r["curve"]) // 12)]]}
+
+    ratio = (cached["t_target"] / plain["t_target"]) if (cached["t_target"] and plain["t_target"]) else None
+    return {"target_relmse": target, "window": [Wc, Hc], "reference_spp": args.gt_spp, "reference_seconds": gt_s,
+            "reference": "plain GiTracer(8), float64 accumulation of 256-spp chunks",
+            "relmse": "mean over pixels and channels of (x - ref)^2 / (ref^2 + 0.01)",
+            "cache_config": "hash grid 16 levels x 2 features, 2^19 entries/level, res 16..2048; MLP 64x5 bf16; "
+                            "Adam lr 1e-2; 65536 training paths/frame, 1 step of 16384 rows/frame; paths end into "
+                            "the cache after 2 bounces",
+            "plain": summ(plain), "cache": summ(cached), "cache_over_plain_time": ratio}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -173,6 +281,10 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="bounded CPU-baseline sample (seconds)")
     ap.add_argument("--ref-rows", type=int, default=8, help="rows per step of the reference arm")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-cache", action="store_true", help="skip the time-to-relMSE measurement")
+    ap.add_argument("--no-extra", action="store_true", help="skip the C1 / C2 sections")
+    ap.add_argument("--gt-spp", type=int, default=65536, help="reference spp of the relMSE window")
+    ap.add_argument("--conv-seconds", type=float, default=20.0, help="time budget per tracer for time-to-relMSE")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -312,6 +424,14 @@ def main():
             cpu = {"value": None, "unit": "Msamples/s", "cores": 0, "kind": "reference",
                    "sample": "unavailable: %s" % exc}
 
+    cache_res = c2 = c1 = None
+    if rank == 0 and world == 1 and not args.no_cache:
+        cache_res = time_to_relmse(gs, sc, args)
+    if rank == 0 and world == 1 and not args.no_extra:
+        gs.close()
+        c2 = raycast_c2(ctx)
+        c1 = cornell_c1(ctx)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "Msamples/s", "n_gpus": world, "steps": args.steps,
@@ -333,6 +453,9 @@ def main():
             "error_flags": flags_err,
             "phase_ms": {"extend": st_plain["ms_extend"], "shadow": st_plain["ms_shadow"],
                          "mis": st_plain["ms_mis"], "shade_and_rest": st_plain["ms_shade"]},
+            "relmse_time": cache_res,
+            "raycast_c2": c2,
+            "cornell_c1": c1,
         }
         print(json.dumps(line), flush=True)
     if dist is not None:

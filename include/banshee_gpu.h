@@ -208,6 +208,8 @@ typedef struct bg_render_stats {
     float   ms_shadow;      /* any-hit traversal                          */
     float   ms_shade;       /* generate + shade + resolve + accumulate    */
     int32_t launches_extend;/* extension traversal launches               */
+    float   ms_cache_query; /* radiance cache: encode + inference + resolve */
+    float   ms_cache_train; /* radiance cache: training steps             */
     /* BG_RENDER_COUNT_TRAVERSAL: replay of every 64th ray of each queue:
      * rays replayed, nodes fetched, triangles tested                      */
     int64_t sub_rays_extension, sub_nodes_extension, sub_tris_extension;
