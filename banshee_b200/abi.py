@@ -99,6 +99,16 @@ class CacheDesc(C.Structure):
                 ("bbox_min", C.c_float * 3), ("bbox_max", C.c_float * 3), ("seed", C.c_uint64)]
 
 
+class BatchJob(C.Structure):
+    _fields_ = [("scene", C.c_int32), ("width", C.c_int32), ("height", C.c_int32), ("reserved", C.c_int32),
+                ("camera", CameraDesc), ("sampler", SamplerDesc), ("accum_rgbw_dev", C.c_void_p)]
+
+
+class TuneResult(C.Structure):
+    _fields_ = [("trace_threads", C.c_int32), ("paths_per_pass", C.c_int32), ("candidates", C.c_int32),
+                ("ms", C.c_float), ("msamples_per_s", C.c_float)]
+
+
 def fptr(a):
     return a.ctypes.data_as(_fp) if a is not None else None
 

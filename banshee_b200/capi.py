@@ -59,6 +59,15 @@ def lib():
                           _i32, _i32, _vp, C.POINTER(abi.RenderStats), _vp],
             "bg_render_host": [_vp, C.POINTER(abi.CameraDesc), C.POINTER(abi.TracerDesc),
                                C.POINTER(abi.SamplerDesc), _i32, _i32, _vp, C.POINTER(abi.RenderStats)],
+            "bg_batch_create": [_vp, C.POINTER(_vp)],
+            "bg_batch_add_scene": [_vp, _vp, C.POINTER(_i32)],
+            "bg_batch_commit": [_vp],
+            "bg_batch_info": [_vp, C.POINTER(abi.SceneInfo)],
+            "bg_batch_render": [_vp, C.POINTER(abi.BatchJob), _i32, C.POINTER(abi.TracerDesc),
+                                C.POINTER(abi.RenderStats), _vp],
+            "bg_batch_autotune": [_vp, C.POINTER(abi.BatchJob), _i32, C.POINTER(abi.TracerDesc), _i32,
+                                  C.POINTER(abi.TuneResult), _vp],
+            "bg_batch_destroy": [_vp],
             "bg_cache_create": [_vp, C.POINTER(abi.CacheDesc), C.POINTER(_vp)],
             "bg_cache_destroy": [_vp],
             "bg_cache_info": [_vp, C.POINTER(_i32), C.POINTER(_i64), C.POINTER(_i32), C.POINTER(C.c_float)],
@@ -287,6 +296,63 @@ class RadianceCache:
     def close(self):
         if self.h:
             lib().bg_cache_destroy(self.h)
+            self.h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """bg_batch: several committed scenes rendered together from one set of queues."""
+
+    def __init__(self, ctx, gscenes):
+        self.ctx = ctx
+        self.gscenes = list(gscenes)
+        self.h = _vp()
+        check(lib().bg_batch_create(ctx.h, C.byref(self.h)))
+        for g in self.gscenes:
+            check(lib().bg_batch_add_scene(self.h, g.h, None))
+        check(lib().bg_batch_commit(self.h))
+
+    def info(self):
+        i = abi.SceneInfo()
+        check(lib().bg_batch_info(self.h, C.byref(i)))
+        return {k: getattr(i, k) for k, _ in abi.SceneInfo._fields_}
+
+    def _jobs(self, jobs):
+        arr = (abi.BatchJob * max(1, len(jobs)))()
+        for i, j in enumerate(jobs):
+            g = self.gscenes[j["scene"]]
+            arr[i].scene = j["scene"]
+            arr[i].width = j["width"]
+            arr[i].height = j["height"]
+            arr[i].camera = j.get("camera") or g.scene.camera_desc()
+            arr[i].sampler = abi.SamplerDesc(0, j["spp"], j.get("seed", 1), j.get("sample_offset", 0), 0)
+            arr[i].accum_rgbw_dev = j["accum_dev"]
+        return arr
+
+    def render(self, jobs, maxdepth=8, tracer=abi.BG_TRACER_GI, stream=None, stats=False, flags=0):
+        arr = self._jobs(jobs)
+        tr = abi.TracerDesc(tracer, maxdepth, flags, 0)
+        st = abi.RenderStats()
+        check(lib().bg_batch_render(self.h, arr, len(jobs), C.byref(tr), C.byref(st) if stats else None,
+                                    _stream_handle(stream)))
+        return {k: getattr(st, k) for k, _ in abi.RenderStats._fields_} if stats else None
+
+    def autotune(self, jobs, probe_spp=2, maxdepth=8, stream=None):
+        arr = self._jobs(jobs)
+        tr = abi.TracerDesc(abi.BG_TRACER_GI, maxdepth, 0, 0)
+        res = abi.TuneResult()
+        check(lib().bg_batch_autotune(self.h, arr, len(jobs), C.byref(tr), int(probe_spp), C.byref(res),
+                                      _stream_handle(stream)))
+        return {k: getattr(res, k) for k, _ in abi.TuneResult._fields_}
+
+    def close(self):
+        if self.h:
+            lib().bg_batch_destroy(self.h)
             self.h = _vp()
 
     def __del__(self):

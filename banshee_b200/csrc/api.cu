@@ -57,11 +57,12 @@ void DevBuf::release() {
 // take new ray indices from one global counter with a single warp-aggregated
 // atomicAdd, every kRefillSteps traversal steps.  Termination: the counter is
 // monotone and every ray finishes after at most one visit per node.
-template <bool ANY, bool COUNT>
-__global__ void __launch_bounds__(kTraceThreads, 8)
+template <bool ANY, bool COUNT, int THREADS = kTraceThreads>
+__global__ void __launch_bounds__(THREADS, 1024 / THREADS)
 k_trace(DevScene S, const float4* __restrict__ rays, int64_t n_static, const int* __restrict__ n_dev,
         bg_hit* __restrict__ hits, uint8_t* __restrict__ occ, unsigned long long* __restrict__ work,
-        unsigned long long* __restrict__ counters, int stride) {
+        unsigned long long* __restrict__ counters, int stride, const int* __restrict__ roots) {
+    // roots (optional): per-ray root node, for rays of several scenes merged into one
     // COUNT: instrumented replay of rays 0, stride, 2*stride, ... (outputs compacted)
     const int64_t n_all = n_dev ? int64_t(*n_dev) : n_static;
     const int64_t n = COUNT ? (n_all + stride - 1) / stride : n_all;
@@ -88,6 +89,7 @@ k_trace(DevScene S, const float4* __restrict__ rays, int64_t n_static, const int
                         const int64_t src = COUNT ? my * stride : my;
                         float4 a = __ldg(rays + 2 * src), b = __ldg(rays + 2 * src + 1);
                         trav_init(s, a, b);
+                        if (roots) s.item = __ldg(roots + src);
                         if (COUNT) ++cnt.rays;
                         active = true;
                     }
@@ -125,12 +127,20 @@ k_trace(DevScene S, const float4* __restrict__ rays, int64_t n_static, const int
     }
 }
 
-template <bool ANY, bool COUNT>
+template <bool ANY, bool COUNT, int THREADS = kTraceThreads>
 static int trace_blocks(bg_scene* s) {
     int nb = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_trace<ANY, COUNT>, kTraceThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_trace<ANY, COUNT, THREADS>, THREADS, 0);
     if (nb < 1) nb = 1;
     return nb * s->ctx->num_sms;
+}
+
+void scene_launch_setup(bg_scene* s) {
+    s->trace_blocks_closest = trace_blocks<false, false>(s);
+    s->trace_blocks_any = trace_blocks<true, false>(s);
+    s->trace_blocks_count = trace_blocks<false, true>(s);
+    s->trace_blocks_closest256 = trace_blocks<false, false, 256>(s);
+    s->trace_blocks_any256 = trace_blocks<true, false, 256>(s);
 }
 
 unsigned long long* next_work_counter(bg_scene* s) {
@@ -140,18 +150,23 @@ unsigned long long* next_work_counter(bg_scene* s) {
 
 int launch_trace(bg_scene* s, bool any_hit, const float4* rays, int64_t n_static, const int* n_dev,
                  bg_hit* hits, uint8_t* occ, cudaStream_t st, unsigned long long* counters, int stride,
-                 unsigned long long* work) {
+                 unsigned long long* work, const int* roots) {
     unsigned long long* w = work ? work : next_work_counter(s);
     BG_CUDA(cudaMemsetAsync(w, 0, sizeof(unsigned long long), st));
     if (counters) {
         if (any_hit)
-            k_trace<true, true><<<s->trace_blocks_count, kTraceThreads, 0, st>>>(s->dev, rays, n_static, n_dev, hits, occ, w, counters, stride);
+            k_trace<true, true><<<s->trace_blocks_count, kTraceThreads, 0, st>>>(s->dev, rays, n_static, n_dev, hits, occ, w, counters, stride, roots);
         else
-            k_trace<false, true><<<s->trace_blocks_count, kTraceThreads, 0, st>>>(s->dev, rays, n_static, n_dev, hits, occ, w, counters, stride);
+            k_trace<false, true><<<s->trace_blocks_count, kTraceThreads, 0, st>>>(s->dev, rays, n_static, n_dev, hits, occ, w, counters, stride, roots);
+    } else if (s->tune_threads == 256) {
+        if (any_hit)
+            k_trace<true, false, 256><<<s->trace_blocks_any256, 256, 0, st>>>(s->dev, rays, n_static, n_dev, hits, occ, w, nullptr, 1, roots);
+        else
+            k_trace<false, false, 256><<<s->trace_blocks_closest256, 256, 0, st>>>(s->dev, rays, n_static, n_dev, hits, occ, w, nullptr, 1, roots);
     } else if (any_hit) {
-        k_trace<true, false><<<s->trace_blocks_any, kTraceThreads, 0, st>>>(s->dev, rays, n_static, n_dev, hits, occ, w, nullptr, 1);
+        k_trace<true, false><<<s->trace_blocks_any, kTraceThreads, 0, st>>>(s->dev, rays, n_static, n_dev, hits, occ, w, nullptr, 1, roots);
     } else {
-        k_trace<false, false><<<s->trace_blocks_closest, kTraceThreads, 0, st>>>(s->dev, rays, n_static, n_dev, hits, occ, w, nullptr, 1);
+        k_trace<false, false><<<s->trace_blocks_closest, kTraceThreads, 0, st>>>(s->dev, rays, n_static, n_dev, hits, occ, w, nullptr, 1, roots);
     }
     BG_CUDA(cudaGetLastError());
     return BG_OK;
@@ -347,9 +362,7 @@ static int commit_scene(bg_scene* s, const bg_build_opts* opts) {
     d.nmats = nmat;
     d.nlights = int(lights.size());
     d.bg[0] = s->bg[0]; d.bg[1] = s->bg[1]; d.bg[2] = s->bg[2];
-    s->trace_blocks_closest = trace_blocks<false, false>(s);
-    s->trace_blocks_any = trace_blocks<true, false>(s);
-    s->trace_blocks_count = trace_blocks<false, true>(s);
+    scene_launch_setup(s);
     auto t1 = std::chrono::steady_clock::now();
     bg_scene_info& info = s->info;
     info.ntriangles = ntris;
@@ -715,10 +728,10 @@ extern "C" int bg_traversal_counts_noalloc(bg_scene* s, const bg_ray* rays, int6
     if (e == cudaSuccess && n > 0) {
         if (any_hit)
             k_trace<true, true><<<s->trace_blocks_count, kTraceThreads, 0, st>>>(
-                s->dev, reinterpret_cast<const float4*>(rays), n, nullptr, nullptr, occ, work, cnt, 1);
+                s->dev, reinterpret_cast<const float4*>(rays), n, nullptr, nullptr, occ, work, cnt, 1, nullptr);
         else
             k_trace<false, true><<<s->trace_blocks_count, kTraceThreads, 0, st>>>(
-                s->dev, reinterpret_cast<const float4*>(rays), n, nullptr, hits, nullptr, work, cnt, 1);
+                s->dev, reinterpret_cast<const float4*>(rays), n, nullptr, hits, nullptr, work, cnt, 1, nullptr);
         e = cudaGetLastError();
     }
     unsigned long long h[3] = {0, 0, 0};

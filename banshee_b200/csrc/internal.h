@@ -72,6 +72,10 @@ struct bg_scene {
     bg_scene_info info{};
     bg::RenderState* render = nullptr;
     int trace_blocks_closest = 0, trace_blocks_any = 0, trace_blocks_count = 0;
+    int64_t tune_paths = 0;   // autotuned paths per pass (0 = default)
+    int tune_threads = 0;     // autotuned traversal block size (0 = default 128)
+    int trace_blocks_closest256 = 0, trace_blocks_any256 = 0;
+    bool owns_buffers = true;
 };
 
 namespace bg {
@@ -79,7 +83,8 @@ namespace bg {
 constexpr int kTraceThreads = 128;
 constexpr int kWorkSlots = 256;
 unsigned long long* next_work_counter(bg_scene* s);
+void scene_launch_setup(bg_scene* s);
 int launch_trace(bg_scene* s, bool any_hit, const float4* rays, int64_t n_static, const int* n_dev,
                  bg_hit* hits, uint8_t* occ, cudaStream_t st, unsigned long long* counters = nullptr,
-                 int stride = 1, unsigned long long* work = nullptr);
+                 int stride = 1, unsigned long long* work = nullptr, const int* roots = nullptr);
 }  // namespace bg

@@ -24,6 +24,7 @@
 
 #include "cache.h"
 #include "internal.h"
+#include "render.h"
 #include "shading.cuh"
 
 namespace bg {
@@ -45,10 +46,18 @@ __global__ void k_clamp_count(int* n, int cap) {
 constexpr int kShadeThreads = 128;
 constexpr int kMaxBounceCounters = 6 * 1024;   // 6 work counters per bounce, maxdepth <= 1024
 
-struct CamDev {        // PerscpectiveCamera frame, computed on the host (perspective_camera.cpp:5-23)
-    float fwd[3], right[3], up[3], p[3];
-    float znear, zfar, dimx, dimy;
+
+// A pass segment: `ns` samples of pixels [p0, p0 + np) of job `job`, as paths
+// [path0, path0 + np * ns) of the pass.
+struct SegRec {
+    CamDev cam;
+    float4* accum;
+    uint64_t seed;
+    int job, np, ns, p0, s0, W, H, path0, pix0;   // pix0: prefix sum of np over earlier segments
 };
+constexpr int kMaxSegs = 1024;
+
+
 
 struct RenderState {
     int64_t cap = 0;   // paths per pass
@@ -66,6 +75,14 @@ struct RenderState {
     // radiance-cache mode: cache queries, training-path vertex records, training samples
     DevBuf q_feat, q_path, q_thr, q_out, rec, tr_feat, tr_target;
     int64_t q_cap = 0, tr_cap = 0;
+    // segment table of the pass in flight: int header {nseg, total} + SegRec[kMaxSegs]
+    DevBuf segs, jobs;
+    int njobs_cap = 0;
+    void* host_tab[2] = {nullptr, nullptr};     // pinned staging of the segment + job tables
+    size_t host_tab_bytes[2] = {0, 0};
+    cudaEvent_t tab_ev[2] = {nullptr, nullptr};
+    int tab_i = 0;
+    DevBuf ext_root[2], sh_root, mis_root;   // per-ray root node (batched renders)
     int blocks = 0;
     // CUDA graph of one pass, replayed on an internal stream
     cudaStream_t gstream = nullptr;
@@ -77,6 +94,10 @@ struct RenderState {
 };
 
 void render_state_free(RenderState* rs) {
+    for (int i = 0; i < 2; ++i) {
+        if (rs->tab_ev[i]) { cudaEventSynchronize(rs->tab_ev[i]); cudaEventDestroy(rs->tab_ev[i]); }
+        if (rs->host_tab[i]) cudaFreeHost(rs->host_tab[i]);
+    }
     if (rs->exec) cudaGraphExecDestroy(rs->exec);
     if (rs->graph) cudaGraphDestroy(rs->graph);
     if (rs->ev_in) cudaEventDestroy(rs->ev_in);
@@ -87,7 +108,8 @@ void render_state_free(RenderState* rs) {
                       &rs->mis_c, &rs->mis_hits, &rs->end_path, &rs->counts, &rs->st_key, &rs->st_cnt, &rs->st_rng,
                       &rs->st_bs, &rs->st_thr, &rs->st_rad, &rs->st_dithr, &rs->st_flags, &rs->slots,
                       &rs->sample_rad, &rs->cnt_out, &rs->work, &rs->q_feat, &rs->q_path, &rs->q_thr,
-                      &rs->q_out, &rs->rec, &rs->tr_feat, &rs->tr_target})
+                      &rs->q_out, &rs->rec, &rs->tr_feat, &rs->tr_target, &rs->segs, &rs->jobs,
+                      &rs->ext_root[0], &rs->ext_root[1], &rs->sh_root, &rs->mis_root})
         b->release();
     delete rs;
 }
@@ -119,6 +141,8 @@ struct Queues {
     unsigned long long* totals;   // [0] closest rays, [1] any rays
     float4* q_feat; int* q_path; float4* q_thr; int* n_query;        // cache queries
     float4* tr_feat; float4* tr_target; int* n_train; int tr_cap;   // training samples
+    int* ext_root_in; int* ext_root_out; int* sh_root; int* mis_root; // per-ray roots, batched only
+    const JobRec* jobs;
 };
 
 // Warp-aggregated slot allocation: one atomicAdd per converged group of lanes.
@@ -138,15 +162,28 @@ __device__ __forceinline__ void put_ray(float4* rays, int i, v3 o, float tmin, v
 }
 
 // ------------------------------------------------------------- generate
+__device__ __forceinline__ int find_seg(const SegRec* segs, int nseg, int i) {
+    int lo = 0, hi = nseg - 1;
+    while (lo < hi) {                 // last segment with path0 <= i
+        int mid = (lo + hi + 1) >> 1;
+        if (segs[mid].path0 <= i) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
 __global__ void __launch_bounds__(kShadeThreads)
-k_generate(CamDev cam, int np, int ns, int p0, int s0, int W, int H, uint64_t seed, PathState P, Queues Q, int total,
-           int train_stride, int train_phase) {
+k_generate(const SegRec* __restrict__ segs, int nseg, int total, PathState P, Queues Q, int train_stride,
+           int train_phase) {
     const int nthreads = gridDim.x * blockDim.x;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += nthreads) {
-        const int sl = i / np;
-        const int pix = p0 + (i - sl * np);
-        const uint32_t s = uint32_t(s0 + sl);
-        const uint64_t key = keyed_key(seed, uint32_t(pix), s);
+        const SegRec& G = segs[find_seg(segs, nseg, i)];
+        const CamDev& cam = G.cam;
+        const int li = i - G.path0;
+        const int sl = li / G.np;
+        const int pix = G.p0 + (li - sl * G.np);
+        const uint32_t s = uint32_t(G.s0 + sl);
+        const int W = G.W, H = G.H;
+        const uint64_t key = keyed_key(G.seed, uint32_t(pix), s);
         McRng img{keyed_rand(key, 0), keyed_rand(key, 1)};
         McRng lr{keyed_rand(key, 2), keyed_rand(key, 3)};
         McRng br{keyed_rand(key, 4), keyed_rand(key, 5)};
@@ -162,12 +199,14 @@ k_generate(CamDev cam, int np, int ns, int p0, int s0, int W, int H, uint64_t se
                              muls(mk(cam.up[0], cam.up[1], cam.up[2]), cy)));
         put_ray(Q.ext_rays_in, i, mk(cam.p[0], cam.p[1], cam.p[2]), cam.znear, d, cam.zfar);
         Q.ext_path_in[i] = i;
+        if (Q.ext_root_in) Q.ext_root_in[i] = Q.jobs[G.job].root;
         P.key[i] = key;
         P.cnt[i] = 6u;
         P.rng[i] = make_uint4(lr.z, lr.w, br.z, br.w);
         P.thr[i] = make_float4(1.f, 1.f, 1.f, 0.f);
         P.rad[i] = make_float4(0.f, 0.f, 0.f, __int_as_float(0));
-        P.flags[i] = (train_stride > 0 && (i + train_phase) % train_stride == 0) ? kFlagTrain : 0u;
+        P.flags[i] = ((train_stride > 0 && (i + train_phase) % train_stride == 0) ? kFlagTrain : 0u) |
+                     (unsigned(G.job) << 16);
         P.sample_rad[i] = make_float4(0.f, 0.f, 0.f, 0.f);
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) *Q.n_ext_in = total;
@@ -189,7 +228,7 @@ __device__ __forceinline__ v3 gather_pending(const PathState& P, int kmax, int p
 }
 
 struct ShadeArgs {
-    int bounce, maxdepth, kind, kmax, nlights;
+    int bounce, maxdepth, kind, kmax, batched;
     int cache_depth;              // -1: plain tracer
     int train_stride, train_phase;
 };
@@ -213,7 +252,7 @@ __device__ __forceinline__ void cache_features(const SHit& h, v3 wo, const MatRe
 
 // One light's DirectIllumination terms (DiTracer::GetDi, ditracer.cpp:57-239, n = 1).
 __device__ __noinline__ void emit_di(const DevScene& S, const Queues& Q, int li, const SHit& h, const MatRec& M, v3 wo,
-                                        McRng& lr, McRng& br, int slot0, int path) {
+                                        McRng& lr, McRng& br, int slot0, int path, int root) {
     const LightRec L = load_light(S, li);
     float lx, ly, bx, by;
     sample2d(lr, lx, ly);
@@ -240,6 +279,7 @@ __device__ __noinline__ void emit_di(const DevScene& S, const Queues& Q, int li,
             put_ray(Q.sh_rays, e, h.p, 0.01f, wi, dist - 0.01f);
             Q.sh_contrib[e] = make_float4(ls.x, ls.y, ls.z, 0.f);
             Q.sh_slot[e] = slot0;
+            if (root >= 0) Q.sh_root[e] = root;
         }
     }
     if (!singular) {
@@ -266,6 +306,7 @@ __device__ __noinline__ void emit_di(const DevScene& S, const Queues& Q, int li,
                         put_ray(Q.sh_rays, e, h.p, 0.01f, wi, 10000000.f);
                         Q.sh_contrib[e] = make_float4(bs.x, bs.y, bs.z, 0.f);
                         Q.sh_slot[e] = slot0 + 1;
+                        if (root >= 0) Q.sh_root[e] = root;
                     }
                 } else {
                     int e = warp_push(Q.n_mis);
@@ -273,6 +314,7 @@ __device__ __noinline__ void emit_di(const DevScene& S, const Queues& Q, int li,
                     Q.mis_a[e] = make_float4(f.x, f.y, f.z, c);
                     Q.mis_b[e] = make_float4(h.p.x, h.p.y, h.p.z, w);
                     Q.mis_c[e] = make_int4(path, slot0 + 1, li, __float_as_int(1.f / bsdfpdf));
+                    if (root >= 0) Q.mis_root[e] = root;
                 }
             }
         }
@@ -291,13 +333,15 @@ k_shade(DevScene S, ShadeArgs A, PathState P, Queues Q) {
         float4 r4 = P.rad[path];
         v3 rad = mk(r4.x, r4.y, r4.z);
         rad = gather_pending(P, A.kmax, path, rad, __float_as_int(r4.w));
+        const JobRec J = Q.jobs[P.flags[path] >> 16];
+        const int root = A.batched ? J.root : -1;
         unsigned flags = 0u;
         int pending = 0;
         bool end = false;
         if (hit.primid < 0) {
             if (A.bounce == 0) {        // primary miss: bgcolor + sum of GetLe, unclamped (gitracer.cpp:22-33)
-                rad = add(rad, mk(S.bg[0], S.bg[1], S.bg[2]));
-                for (int i = 0; i < S.nlights; ++i) {
+                rad = add(rad, mk(J.bg[0], J.bg[1], J.bg[2]));
+                for (int i = J.light0; i < J.light0 + J.nlights; ++i) {
                     LightRec L = load_light(S, i);
                     if (L.type == BG_LIGHT_ENVIRONMENT) rad = add(rad, mk(L.env[0], L.env[1], L.env[2]));
                 }
@@ -354,16 +398,16 @@ k_shade(DevScene S, ShadeArgs A, PathState P, Queues Q) {
                 const int base = path * A.kmax;
                 // bounce 0: every light, weight 1; later: one light picked by rand(), weight L
                 // (gitracer.cpp:72-84)
-                int first = 0, nl = A.nlights;
+                int first = J.light0, nl = J.nlights;
                 float mult = 1.f;
                 if (A.bounce != 0) {
-                    first = int(keyed_rand(P.key[path], cnt++) % unsigned(A.nlights));
+                    first = J.light0 + int(keyed_rand(P.key[path], cnt++) % unsigned(J.nlights));
                     nl = 1;
-                    mult = (float)A.nlights;
+                    mult = (float)J.nlights;
                 }
                 pending = 2 * nl;
                 for (int j = 0; j < pending; ++j) P.slots[size_t(base) + j] = make_float4(0.f, 0.f, 0.f, 0.f);
-                for (int i = 0; i < nl; ++i) emit_di(S, Q, first + i, h, M, wo, lr, br, base + 2 * i, path);
+                for (int i = 0; i < nl; ++i) emit_di(S, Q, first + i, h, M, wo, lr, br, base + 2 * i, path, root);
                 P.dithr[path] = make_float4(thr.x, thr.y, thr.z, mult);
                 if (A.kind == BG_TRACER_DI) {
                     flags |= kFlagNoClamp;
@@ -391,6 +435,7 @@ k_shade(DevScene S, ShadeArgs A, PathState P, Queues Q) {
                             int k = warp_push(Q.n_ext_out);
                             put_ray(Q.ext_rays_out, k, h.p, 0.01f, nd, 1000000.f);
                             Q.ext_path_out[k] = path;
+                            if (root >= 0) Q.ext_root_out[k] = root;
                         }
                         P.thr[path] = make_float4(thr.x, thr.y, thr.z, 0.f);
                     }
@@ -504,22 +549,29 @@ k_cache_resolve(PathState P, Queues Q, const float4* __restrict__ pred) {
 
 // FileImagePlane::WriteSample per pixel, samples in order (rows flipped).
 __global__ void __launch_bounds__(kShadeThreads)
-k_accumulate(PathState P, int np, int ns, int p0, int W, int H, float4* accum) {
+k_accumulate(PathState P, const SegRec* __restrict__ segs, int nseg, int npix) {
     const int nthreads = gridDim.x * blockDim.x;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np; i += nthreads) {
-        const int pix = p0 + i;
-        const int x = pix % W, y = pix / W;
-        float4* px = accum + size_t(W) * size_t(H - 1 - y) + x;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < npix; t += nthreads) {
+        int lo = 0, hi = nseg - 1;
+        while (lo < hi) {
+            int mid = (lo + hi + 1) >> 1;
+            if (segs[mid].pix0 <= t) lo = mid; else hi = mid - 1;
+        }
+        const SegRec& G = segs[lo];
+        const int i = t - G.pix0;
+        const int pix = G.p0 + i;
+        const int x = pix % G.W, y = pix / G.W;
+        float4* px = G.accum + size_t(G.W) * size_t(G.H - 1 - y) + x;
         float4 acc = *px;
-        for (int s = 0; s < ns; ++s) {
-            float4 v = P.sample_rad[size_t(s) * np + i];
+        for (int s = 0; s < G.ns; ++s) {
+            float4 v = P.sample_rad[size_t(G.path0) + size_t(s) * G.np + i];
             acc.x += v.x; acc.y += v.y; acc.z += v.z; acc.w += 1.f;
         }
         *px = acc;
     }
 }
 
-static CamDev make_camera(const bg_camera_desc* c) {
+CamDev make_camera(const bg_camera_desc* c) {
     CamDev k;
     v3 eye = mk(c->eye[0], c->eye[1], c->eye[2]), at = mk(c->at[0], c->at[1], c->at[2]), up = mk(c->up[0], c->up[1], c->up[2]);
     v3 fwd = normalize(sub(at, eye));
@@ -536,9 +588,9 @@ static CamDev make_camera(const bg_camera_desc* c) {
     return k;
 }
 
-static int ensure_state(bg_scene* s, int64_t cap) {
+static int ensure_state(bg_scene* s, int64_t cap, int maxL) {
     RenderState* rs = s->render;
-    const int L = std::max(1, s->dev.nlights);
+    const int L = std::max(1, maxL);
     if (rs && rs->cap >= cap && rs->nlights == L) return BG_OK;
     if (rs) render_state_free(rs);
     rs = s->render = new RenderState();
@@ -548,14 +600,18 @@ static int ensure_state(bg_scene* s, int64_t cap) {
     const size_t C = size_t(cap);
     int rc;
     for (int k = 0; k < 2; ++k) {
-        if ((rc = rs->ext_rays[k].ensure(C * 32)) || (rc = rs->ext_path[k].ensure(C * 4))) return rc;
+        if ((rc = rs->ext_rays[k].ensure(C * 32)) || (rc = rs->ext_path[k].ensure(C * 4)) ||
+            (rc = rs->ext_root[k].ensure(C * 4)))
+            return rc;
     }
     if ((rc = rs->ext_hits.ensure(C * 16)) ||
         (rc = rs->sh_rays.ensure(C * 2 * L * 32)) || (rc = rs->sh_contrib.ensure(C * 2 * L * 16)) ||
         (rc = rs->sh_slot.ensure(C * 2 * L * 4)) || (rc = rs->sh_occ.ensure(C * 2 * L)) ||
+        (rc = rs->sh_root.ensure(C * 2 * L * 4)) ||
         (rc = rs->mis_rays.ensure(C * L * 32)) || (rc = rs->mis_a.ensure(C * L * 16)) ||
         (rc = rs->mis_b.ensure(C * L * 16)) || (rc = rs->mis_c.ensure(C * L * 16)) ||
-        (rc = rs->mis_hits.ensure(C * L * 16)) || (rc = rs->end_path.ensure(C * 4)) ||
+        (rc = rs->mis_hits.ensure(C * L * 16)) || (rc = rs->mis_root.ensure(C * L * 4)) ||
+        (rc = rs->end_path.ensure(C * 4)) ||
         (rc = rs->counts.ensure(256)) ||
         (rc = rs->st_key.ensure(C * 8)) || (rc = rs->st_cnt.ensure(C * 4)) || (rc = rs->st_rng.ensure(C * 16)) ||
         (rc = rs->st_bs.ensure(C * 8)) || (rc = rs->st_thr.ensure(C * 16)) || (rc = rs->st_rad.ensure(C * 16)) ||
@@ -590,15 +646,17 @@ struct Instr {
     }
 };
 
+// One pass: a slice of the device segment table plus the bounce-loop settings.
 struct PassCfg {
-    int np, ns, p0, s0, W, H, maxdepth, kind;
-    uint64_t seed;
-    float4* accum;
+    const SegRec* segs;        // device pointer to this pass's segments
+    int nseg, total, npix;
+    int maxdepth, kind;
+    bool batched;
     bg_cache* cache;           // radiance-cache mode when non-null
     int cache_depth, train_stride, train_phase;
 };
 
-static void pass_queues(RenderState* rs, int c, Queues& Q) {
+static void pass_queues(RenderState* rs, int c, bool batched, Queues& Q) {
     int* cnt = rs->counts.as<int>();
     Q.ext_hits = rs->ext_hits.as<bg_hit>();
     Q.sh_rays = rs->sh_rays.as<float4>(); Q.sh_contrib = rs->sh_contrib.as<float4>();
@@ -617,6 +675,11 @@ static void pass_queues(RenderState* rs, int c, Queues& Q) {
     Q.tr_feat = rs->tr_feat.as<float4>(); Q.tr_target = rs->tr_target.as<float4>();
     Q.n_train = cnt + kCntTrain;
     Q.tr_cap = int(rs->tr_cap);
+    Q.ext_root_in = batched ? rs->ext_root[c].as<int>() : nullptr;
+    Q.ext_root_out = batched ? rs->ext_root[1 - c].as<int>() : nullptr;
+    Q.sh_root = batched ? rs->sh_root.as<int>() : nullptr;
+    Q.mis_root = batched ? rs->mis_root.as<int>() : nullptr;
+    Q.jobs = rs->jobs.as<JobRec>();
 }
 
 static PathState path_state(RenderState* rs) {
@@ -635,19 +698,17 @@ static PathState path_state(RenderState* rs) {
     return P;
 }
 
-// Enqueues one pass (np pixels x ns samples) on `st`: generate, maxdepth bounces
-// of extend / shade / shadow / MIS / resolve / finalize, accumulate.
-static int enqueue_pass(bg_scene* s, RenderState* rs, cudaStream_t st, const CamDev& cam, const PassCfg& c, Instr* ins) {
+// Enqueues one pass on `st`: generate, maxdepth bounces of extend / shade /
+// shadow / MIS / resolve / finalize, accumulate.
+static int enqueue_pass(bg_scene* s, RenderState* rs, cudaStream_t st, const PassCfg& c, Instr* ins) {
     const int nb = rs->blocks;
-    const int total = c.np * c.ns;
     PathState P = path_state(rs);
     Queues Q;
     int cur = 0;
-    pass_queues(rs, cur, Q);
+    pass_queues(rs, cur, c.batched, Q);
     int* cnt = rs->counts.as<int>();
     int rc;
-    k_generate<<<nb, kShadeThreads, 0, st>>>(cam, c.np, c.ns, c.p0, c.s0, c.W, c.H, c.seed, P, Q, total,
-                                             c.cache ? c.train_stride : 0, c.train_phase);
+    k_generate<<<nb, kShadeThreads, 0, st>>>(c.segs, c.nseg, c.total, P, Q, c.cache ? c.train_stride : 0, c.train_phase);
     if (ins) ++ins->launches;
     bg_hit* cnt_hits = rs->cnt_out.as<bg_hit>();
     uint8_t* cnt_occ = rs->cnt_out.as<uint8_t>();
@@ -656,24 +717,24 @@ static int enqueue_pass(bg_scene* s, RenderState* rs, cudaStream_t st, const Cam
         BG_CUDA(cudaMemsetAsync(Q.n_ext_out, 0, sizeof(int), st));
         BG_CUDA(cudaMemsetAsync(cnt + kCntSh, 0, 3 * sizeof(int), st));
         if (ins) ins->mark(0);
-        if ((rc = launch_trace(s, false, Q.ext_rays_in, 0, Q.n_ext_in, Q.ext_hits, nullptr, st, nullptr, 1, wk))) return rc;
+        if ((rc = launch_trace(s, false, Q.ext_rays_in, 0, Q.n_ext_in, Q.ext_hits, nullptr, st, nullptr, 1, wk, Q.ext_root_in))) return rc;
         if (ins) { ins->mark(0); ++ins->launches; ++ins->launches_extend; }
         if (ins && ins->count_trav) {
-            if ((rc = launch_trace(s, false, Q.ext_rays_in, 0, Q.n_ext_in, cnt_hits, nullptr, st, Q.totals + 3, 64, wk + 1))) return rc;
+            if ((rc = launch_trace(s, false, Q.ext_rays_in, 0, Q.n_ext_in, cnt_hits, nullptr, st, Q.totals + 3, 64, wk + 1, Q.ext_root_in))) return rc;
             ++ins->launches;
         }
-        ShadeArgs A{b, c.maxdepth, c.kind, rs->kmax, s->dev.nlights, c.cache ? c.cache_depth : -1,
+        ShadeArgs A{b, c.maxdepth, c.kind, rs->kmax, c.batched ? 1 : 0, c.cache ? c.cache_depth : -1,
                     c.cache ? c.train_stride : 0, c.train_phase};
         if (c.cache && b == c.cache_depth) BG_CUDA(cudaMemsetAsync(Q.n_query, 0, sizeof(int), st));
         k_shade<<<nb, kShadeThreads, 0, st>>>(s->dev, A, P, Q);
         if (ins) { ++ins->launches; ins->mark(1); }
-        if ((rc = launch_trace(s, true, Q.sh_rays, 0, Q.n_sh, nullptr, Q.sh_occ, st, nullptr, 1, wk + 2))) return rc;
+        if ((rc = launch_trace(s, true, Q.sh_rays, 0, Q.n_sh, nullptr, Q.sh_occ, st, nullptr, 1, wk + 2, Q.sh_root))) return rc;
         if (ins) { ins->mark(1); ins->mark(2); }
-        if ((rc = launch_trace(s, false, Q.mis_rays, 0, Q.n_mis, Q.mis_hits, nullptr, st, nullptr, 1, wk + 3))) return rc;
+        if ((rc = launch_trace(s, false, Q.mis_rays, 0, Q.n_mis, Q.mis_hits, nullptr, st, nullptr, 1, wk + 3, Q.mis_root))) return rc;
         if (ins) { ins->mark(2); ins->launches += 2; }
         if (ins && ins->count_trav) {
-            if ((rc = launch_trace(s, true, Q.sh_rays, 0, Q.n_sh, nullptr, cnt_occ, st, Q.totals + 6, 64, wk + 4))) return rc;
-            if ((rc = launch_trace(s, false, Q.mis_rays, 0, Q.n_mis, cnt_hits, nullptr, st, Q.totals + 9, 64, wk + 5))) return rc;
+            if ((rc = launch_trace(s, true, Q.sh_rays, 0, Q.n_sh, nullptr, cnt_occ, st, Q.totals + 6, 64, wk + 4, Q.sh_root))) return rc;
+            if ((rc = launch_trace(s, false, Q.mis_rays, 0, Q.n_mis, cnt_hits, nullptr, st, Q.totals + 9, 64, wk + 5, Q.mis_root))) return rc;
             ins->launches += 2;
         }
         k_resolve_shadow<<<nb, kShadeThreads, 0, st>>>(P, Q);
@@ -690,24 +751,23 @@ static int enqueue_pass(bg_scene* s, RenderState* rs, cudaStream_t st, const Cam
         k_finalize<<<nb, kShadeThreads, 0, st>>>(P, Q, rs->kmax, c.maxdepth, c.cache ? c.train_stride : 0, c.train_phase);
         if (ins) ins->launches += 3;
         cur = 1 - cur;
-        pass_queues(rs, cur, Q);
+        pass_queues(rs, cur, c.batched, Q);
     }
-    k_accumulate<<<nb, kShadeThreads, 0, st>>>(P, c.np, c.ns, c.p0, c.W, c.H, c.accum);
+    k_accumulate<<<nb, kShadeThreads, 0, st>>>(P, c.segs, c.nseg, c.npix);
     if (ins) ++ins->launches;
     BG_CUDA(cudaGetLastError());
     return BG_OK;
 }
 
-// Captures one pass into a CUDA graph (once per pass shape) and finds the two
-// kernel nodes whose arguments change from pass to pass.
-static int pass_graph(bg_scene* s, RenderState* rs, const CamDev& cam, const PassCfg& c) {
-    const int64_t key[8] = {c.np, c.ns, c.W, c.H, c.maxdepth, c.kind, int64_t(reinterpret_cast<uintptr_t>(c.accum)),
-                            s->dev.nlights};
+// Captures one pass into a CUDA graph (once per bounce-loop shape) and finds
+// the two kernel nodes whose arguments (the segment slice) change per pass.
+static int pass_graph(bg_scene* s, RenderState* rs, const PassCfg& c) {
+    const int64_t key[8] = {c.maxdepth, c.kind, c.batched ? 1 : 0, rs->kmax, int64_t(rs->cap), s->tune_threads, 0, 0};
     if (rs->exec && memcmp(key, rs->graph_key, sizeof(key)) == 0) return BG_OK;
     if (rs->exec) { cudaGraphExecDestroy(rs->exec); rs->exec = nullptr; }
     if (rs->graph) { cudaGraphDestroy(rs->graph); rs->graph = nullptr; }
     BG_CUDA(cudaStreamBeginCapture(rs->gstream, cudaStreamCaptureModeThreadLocal));
-    int rc = enqueue_pass(s, rs, rs->gstream, cam, c, nullptr);
+    int rc = enqueue_pass(s, rs, rs->gstream, c, nullptr);
     cudaGraph_t g = nullptr;
     cudaError_t e = cudaStreamEndCapture(rs->gstream, &g);
     if (rc) { if (g) cudaGraphDestroy(g); return rc; }
@@ -733,25 +793,22 @@ static int pass_graph(bg_scene* s, RenderState* rs, const CamDev& cam, const Pas
     return BG_OK;
 }
 
-static int launch_pass_graph(bg_scene* s, RenderState* rs, const CamDev& cam, const PassCfg& c) {
-    int rc = pass_graph(s, rs, cam, c);
+static int launch_pass_graph(bg_scene* s, RenderState* rs, const PassCfg& c) {
+    int rc = pass_graph(s, rs, c);
     if (rc) return rc;
     PathState P = path_state(rs);
     Queues Q;
-    pass_queues(rs, 0, Q);
-    int total = c.np * c.ns;
-    CamDev camv = cam;
-    int np = c.np, ns = c.ns, p0 = c.p0, s0 = c.s0, W = c.W, H = c.H;
-    uint64_t seed = c.seed;
+    pass_queues(rs, 0, c.batched, Q);
+    const SegRec* segs = c.segs;
+    int nseg = c.nseg, total = c.total, npix = c.npix;
     int tstride = 0, tphase = 0;
-    void* gargs[] = {&camv, &np, &ns, &p0, &s0, &W, &H, &seed, &P, &Q, &total, &tstride, &tphase};
+    void* gargs[] = {&segs, &nseg, &total, &P, &Q, &tstride, &tphase};
     cudaKernelNodeParams kp;
     BG_CUDA(cudaGraphKernelNodeGetParams(rs->gen_node, &kp));
     kp.kernelParams = gargs;
     kp.extra = nullptr;
     BG_CUDA(cudaGraphExecKernelNodeSetParams(rs->exec, rs->gen_node, &kp));
-    float4* accum = c.accum;
-    void* aargs[] = {&P, &np, &ns, &p0, &W, &H, &accum};
+    void* aargs[] = {&P, &segs, &nseg, &npix};
     BG_CUDA(cudaGraphKernelNodeGetParams(rs->acc_node, &kp));
     kp.kernelParams = aargs;
     kp.extra = nullptr;
@@ -760,64 +817,128 @@ static int launch_pass_graph(bg_scene* s, RenderState* rs, const CamDev& cam, co
     return BG_OK;
 }
 
-static int render_impl(bg_scene* s, bg_cache* cache, const bg_camera_desc* cam, const bg_tracer_desc* tr,
-                       const bg_sampler_desc* sm, int W, int H, float4* accum, bg_render_stats* stats, cudaStream_t st) {
+// Splits jobs into sample chunks and packs them into passes of at most `cap`
+// paths; two chunks of one job whose pixels overlap never share a pass (their
+// per-pixel sums must stay ordered by sample).
+static void plan_passes(const std::vector<JobSpec>& jobs, int64_t cap, std::vector<SegRec>& segs,
+                        std::vector<int>& pass_begin) {
+    std::vector<SegRec> all;
+    for (size_t j = 0; j < jobs.size(); ++j) {
+        const JobSpec& J = jobs[j];
+        const int64_t npix = int64_t(J.W) * J.H;
+        if (npix <= cap) {
+            for (int s0 = 0; s0 < J.spp;) {
+                int ns = int(std::max<int64_t>(1, std::min<int64_t>(J.spp - s0, cap / npix)));
+                SegRec g{};
+                g.cam = J.cam; g.accum = J.accum; g.seed = J.seed; g.job = int(j);
+                g.np = int(npix); g.ns = ns; g.p0 = 0; g.s0 = J.soff + s0; g.W = J.W; g.H = J.H;
+                all.push_back(g);
+                s0 += ns;
+            }
+        } else {
+            for (int s = 0; s < J.spp; ++s)
+                for (int64_t p0 = 0; p0 < npix; p0 += cap) {
+                    SegRec g{};
+                    g.cam = J.cam; g.accum = J.accum; g.seed = J.seed; g.job = int(j);
+                    g.np = int(std::min<int64_t>(cap, npix - p0)); g.ns = 1; g.p0 = int(p0); g.s0 = J.soff + s;
+                    g.W = J.W; g.H = J.H;
+                    all.push_back(g);
+                }
+        }
+    }
+    int64_t used = 0;
+    int first = 0;
+    pass_begin.clear();
+    segs.clear();
+    for (size_t k = 0; k < all.size(); ++k) {
+        SegRec g = all[k];
+        const int64_t size = int64_t(g.np) * g.ns;
+        bool conflict = used + size > cap || int(segs.size()) - first >= kMaxSegs;
+        for (int q = first; q < int(segs.size()) && !conflict; ++q) {
+            const SegRec& o = segs[size_t(q)];
+            if (o.job == g.job && o.p0 < g.p0 + g.np && g.p0 < o.p0 + o.np) conflict = true;
+        }
+        if (segs.empty() || conflict) {
+            pass_begin.push_back(int(segs.size()));
+            first = int(segs.size());
+            used = 0;
+        }
+        int pix0 = 0;
+        for (int q = first; q < int(segs.size()); ++q) pix0 += segs[size_t(q)].np;
+        g.path0 = int(used);
+        g.pix0 = pix0;
+        segs.push_back(g);
+        used += size;
+    }
+    pass_begin.push_back(int(segs.size()));
+}
+
+int render_jobs(bg_scene* s, bg_cache* cache, const std::vector<JobSpec>& jobs, const bg_tracer_desc* tr,
+                bg_render_stats* stats, cudaStream_t st, bool batched) {
     if (!s) return set_error(BG_ERR_INVALID_ARG, "scene is NULL");
     if (!s->committed) return set_error(BG_ERR_STATE, "scene not committed");
-    if (!cam || !tr || !sm || !accum) return set_error(BG_ERR_INVALID_ARG, "NULL argument");
-    if (W <= 0 || H <= 0 || int64_t(W) * H > (int64_t(1) << 28)) return set_error(BG_ERR_INVALID_ARG, "bad resolution %dx%d", W, H);
-    if (sm->kind != 0) return set_error(BG_ERR_UNSUPPORTED, "sampler kind %d", sm->kind);
-    if (sm->spp < 0 || sm->sample_offset < 0) return set_error(BG_ERR_INVALID_ARG, "negative spp / sample offset");
+    if (!tr) return set_error(BG_ERR_INVALID_ARG, "NULL tracer");
     if (tr->kind != BG_TRACER_GI && tr->kind != BG_TRACER_DI) return set_error(BG_ERR_UNSUPPORTED, "tracer kind %d", tr->kind);
     if (tr->kind == BG_TRACER_GI && (tr->maxdepth < 0 || tr->maxdepth > 1024)) return set_error(BG_ERR_INVALID_ARG, "maxdepth %d", tr->maxdepth);
-    if (s->dev.nlights == 0) return set_error(BG_ERR_UNSUPPORTED, "a scene without lights (GiTracer divides by the light count)");
-    if (reinterpret_cast<uintptr_t>(accum) & 15u) return set_error(BG_ERR_INVALID_ARG, "accumulation buffer must be 16-byte aligned");
-    const int64_t npix = int64_t(W) * H;
-    const int64_t target = int64_t(1) << 21;   // paths per pass
-    int64_t cap = std::min<int64_t>(std::max<int64_t>(npix, 1), target);
-    if (npix < target) cap = std::min<int64_t>(target, npix * std::max(1, sm->spp));
-    cap = std::max<int64_t>(cap, 1);
-    int rc = ensure_state(s, cap);
+    if (jobs.empty()) return BG_OK;
+    if (jobs.size() > 65535) return set_error(BG_ERR_INVALID_ARG, "too many jobs (%zu > 65535)", jobs.size());
+    int maxL = 1;
+    int64_t total_samples = 0, max_job = 0;
+    for (const JobSpec& J : jobs) {
+        if (J.W <= 0 || J.H <= 0 || int64_t(J.W) * J.H > (int64_t(1) << 28)) return set_error(BG_ERR_INVALID_ARG, "bad resolution %dx%d", J.W, J.H);
+        if (J.spp < 0 || J.soff < 0) return set_error(BG_ERR_INVALID_ARG, "negative spp / sample offset");
+        if (!J.accum || (reinterpret_cast<uintptr_t>(J.accum) & 15u)) return set_error(BG_ERR_INVALID_ARG, "accumulation buffer must be non-NULL and 16-byte aligned");
+        if (J.rec.nlights <= 0) return set_error(BG_ERR_UNSUPPORTED, "a scene without lights (GiTracer divides by the light count)");
+        maxL = std::max(maxL, J.rec.nlights);
+        total_samples += int64_t(J.W) * J.H * J.spp;
+        max_job = std::max(max_job, int64_t(J.W) * J.H * std::max(1, J.spp));
+    }
+    const int64_t target = s->tune_paths > 0 ? s->tune_paths : (int64_t(1) << 21);   // paths per pass
+    int64_t cap = std::max<int64_t>(1, std::min<int64_t>(target, std::max<int64_t>(total_samples, 1)));
+    int rc = ensure_state(s, cap, maxL);
     if (rc) return rc;
-    RenderState* rs = s->render;
-    const CamDev camd = make_camera(cam);
+    RenderState* rs = s->render;   // buffers may be larger than this call's pass size
     const int maxdepth = tr->kind == BG_TRACER_DI ? 1 : tr->maxdepth;
     unsigned long long* totals = reinterpret_cast<unsigned long long*>(rs->counts.as<char>() + 64);
 
-    // Graph replay unless statistics were asked for or the caller's stream is capturing.
+    std::vector<SegRec> segs;
+    std::vector<int> pass_begin;
+    plan_passes(jobs, cap, segs, pass_begin);
+    const int npass = int(pass_begin.size()) - 1;
+    if ((rc = rs->segs.ensure(std::max<size_t>(1, segs.size()) * sizeof(SegRec)))) return rc;
+    if ((rc = rs->jobs.ensure(jobs.size() * sizeof(JobRec)))) return rc;
+    std::vector<JobRec> jrec(jobs.size());
+    for (size_t j = 0; j < jobs.size(); ++j) jrec[j] = jobs[j].rec;
+
+    // Graph replay unless statistics were asked for, the cache is in use, or
+    // the caller's stream is capturing.
     cudaStreamCaptureStatus cap_st = cudaStreamCaptureStatusNone;
     BG_CUDA(cudaStreamIsCapturing(st, &cap_st));
     const bool use_graph = !stats && !cache && cap_st == cudaStreamCaptureStatusNone;
-    // radiance-cache mode: training-path selection and buffers
-    int cache_depth = -1, stride = 0, phase = 0, tsteps = 0, tbatch = 0;
-    if (cache) {
-        const bg_cache_desc* cd = nrc_desc(cache);
-        if (tr->kind != BG_TRACER_GI) return set_error(BG_ERR_UNSUPPORTED, "the radiance cache serves GiTracer only");
-        cache_depth = cd->cache_depth;
-        if (cache_depth < 0 || cache_depth >= std::max(1, maxdepth)) return set_error(BG_ERR_INVALID_ARG, "cache_depth %d outside [0, maxdepth)", cache_depth);
-        const int64_t total = npix * int64_t(std::max(1, sm->spp));
-        const int64_t tp = std::max<int64_t>(1, cd->train_paths);
-        stride = int(std::max<int64_t>(1, std::min<int64_t>(total / tp, int64_t(1) << 24)));
-        phase = int(nrc_next_frame(cache) % stride);
-        tsteps = std::max(0, cd->train_steps);
-        tbatch = std::max(1, cd->train_batch);
-        const int64_t npass = (npix + cap - 1) / cap * ((std::max(1, sm->spp) + std::max<int64_t>(1, cap / std::max<int64_t>(1, npix)) - 1)
-                                                        / std::max<int64_t>(1, cap / std::max<int64_t>(1, npix)));
-        const int64_t tpaths_pass = cap / stride + 2;
-        const int64_t tr_cap = (total / stride + 2 * npass + 2) * maxdepth;
-        if (rs->q_cap < cap) {
-            if ((rc = rs->q_feat.ensure(size_t(cap) * 64)) || (rc = rs->q_path.ensure(size_t(cap) * 4)) ||
-                (rc = rs->q_thr.ensure(size_t(cap) * 16)) || (rc = rs->q_out.ensure(size_t(cap) * 16)))
-                return rc;
-            rs->q_cap = cap;
+    cudaStream_t ws = use_graph ? rs->gstream : st;
+    if (use_graph) {
+        BG_CUDA(cudaEventRecord(rs->ev_in, st));
+        BG_CUDA(cudaStreamWaitEvent(rs->gstream, rs->ev_in, 0));
+    }
+    {
+        // tables go through pinned, double-buffered staging so the upload stays asynchronous
+        const int i = rs->tab_i ^= 1;
+        const size_t sb = segs.size() * sizeof(SegRec), jb = jrec.size() * sizeof(JobRec);
+        if (rs->tab_ev[i]) BG_CUDA(cudaEventSynchronize(rs->tab_ev[i]));
+        else BG_CUDA(cudaEventCreateWithFlags(&rs->tab_ev[i], cudaEventDisableTiming));
+        if (rs->host_tab_bytes[i] < sb + jb) {
+            if (rs->host_tab[i]) cudaFreeHost(rs->host_tab[i]);
+            rs->host_tab[i] = nullptr;
+            rs->host_tab_bytes[i] = 0;
+            BG_CUDA(cudaMallocHost(&rs->host_tab[i], (sb + jb) * 2));
+            rs->host_tab_bytes[i] = (sb + jb) * 2;
         }
-        if ((rc = rs->rec.ensure(size_t(tpaths_pass) * maxdepth * 6 * 16))) return rc;
-        if (rs->tr_cap < tr_cap) {
-            if ((rc = rs->tr_feat.ensure(size_t(tr_cap) * 64)) || (rc = rs->tr_target.ensure(size_t(tr_cap) * 16))) return rc;
-            rs->tr_cap = tr_cap;
-        }
-        if ((rc = nrc_prepare(cache, std::max<int64_t>(cap, tbatch)))) return rc;
-        BG_CUDA(cudaMemsetAsync(rs->counts.as<int>() + kCntTrain, 0, sizeof(int), st));
+        char* h = static_cast<char*>(rs->host_tab[i]);
+        memcpy(h, segs.data(), sb);
+        memcpy(h + sb, jrec.data(), jb);
+        BG_CUDA(cudaMemcpyAsync(rs->segs.ptr, h, sb, cudaMemcpyHostToDevice, ws));
+        BG_CUDA(cudaMemcpyAsync(rs->jobs.ptr, h + sb, jb, cudaMemcpyHostToDevice, ws));
+        BG_CUDA(cudaEventRecord(rs->tab_ev[i], ws));
     }
     Instr ins;
     ins.st = st;
@@ -832,22 +953,55 @@ static int render_impl(bg_scene* s, bg_cache* cache, const bg_camera_desc* cam, 
         cudaEventCreate(&ev1);
         cudaEventRecord(ev0, st);
     }
-    if (use_graph) {
-        BG_CUDA(cudaEventRecord(rs->ev_in, st));
-        BG_CUDA(cudaStreamWaitEvent(rs->gstream, rs->ev_in, 0));
+    // radiance-cache mode: training-path selection and buffers
+    int cache_depth = -1, stride = 0, phase = 0, tsteps = 0, tbatch = 0;
+    if (cache) {
+        const bg_cache_desc* cd = nrc_desc(cache);
+        if (tr->kind != BG_TRACER_GI) return set_error(BG_ERR_UNSUPPORTED, "the radiance cache serves GiTracer only");
+        cache_depth = cd->cache_depth;
+        if (cache_depth < 0 || cache_depth >= std::max(1, maxdepth)) return set_error(BG_ERR_INVALID_ARG, "cache_depth %d outside [0, maxdepth)", cache_depth);
+        const int64_t tp = std::max<int64_t>(1, cd->train_paths);
+        stride = int(std::max<int64_t>(1, std::min<int64_t>(total_samples / tp, int64_t(1) << 24)));
+        phase = int(nrc_next_frame(cache) % stride);
+        tsteps = std::max(0, cd->train_steps);
+        tbatch = std::max(1, cd->train_batch);
+        const int64_t tpaths_pass = cap / stride + 2;
+        const int64_t tr_cap = (total_samples / stride + 2 * npass + 2) * maxdepth;
+        if (rs->q_cap < cap) {
+            if ((rc = rs->q_feat.ensure(size_t(cap) * 64)) || (rc = rs->q_path.ensure(size_t(cap) * 4)) ||
+                (rc = rs->q_thr.ensure(size_t(cap) * 16)) || (rc = rs->q_out.ensure(size_t(cap) * 16)))
+                return rc;
+            rs->q_cap = cap;
+        }
+        if ((rc = rs->rec.ensure(size_t(tpaths_pass) * maxdepth * 6 * 16))) return rc;
+        if (rs->tr_cap < tr_cap) {
+            if ((rc = rs->tr_feat.ensure(size_t(tr_cap) * 64)) || (rc = rs->tr_target.ensure(size_t(tr_cap) * 16))) return rc;
+            rs->tr_cap = tr_cap;
+        }
+        if ((rc = nrc_prepare(cache, std::max<int64_t>(cap, tbatch)))) return rc;
+        BG_CUDA(cudaMemsetAsync(rs->counts.as<int>() + kCntTrain, 0, sizeof(int), st));
     }
     int64_t done_samples = 0;
-    for (int64_t p0 = 0; p0 < npix; p0 += cap) {
-        const int np = int(std::min<int64_t>(cap, npix - p0));
-        for (int s0 = 0; s0 < sm->spp;) {
-            const int ns = int(std::max<int64_t>(1, std::min<int64_t>(sm->spp - s0, cap / np)));
-            PassCfg c{np, ns, int(p0), sm->sample_offset + s0, W, H, maxdepth, tr->kind, sm->seed, accum,
-                      cache, cache_depth, stride, phase};
-            rc = use_graph ? launch_pass_graph(s, rs, camd, c) : enqueue_pass(s, rs, st, camd, c, &ins);
-            if (rc) return rc;
-            done_samples += int64_t(np) * ns;
-            s0 += ns;
+    for (int p = 0; p < npass; ++p) {
+        PassCfg c;
+        c.segs = rs->segs.as<SegRec>() + pass_begin[size_t(p)];
+        c.nseg = pass_begin[size_t(p) + 1] - pass_begin[size_t(p)];
+        c.total = 0;
+        c.npix = 0;
+        for (int q = pass_begin[size_t(p)]; q < pass_begin[size_t(p) + 1]; ++q) {
+            c.total += segs[size_t(q)].np * segs[size_t(q)].ns;
+            c.npix += segs[size_t(q)].np;
         }
+        c.maxdepth = maxdepth;
+        c.kind = tr->kind;
+        c.batched = batched;
+        c.cache = cache;
+        c.cache_depth = cache_depth;
+        c.train_stride = stride;
+        c.train_phase = phase;
+        rc = use_graph ? launch_pass_graph(s, rs, c) : enqueue_pass(s, rs, st, c, &ins);
+        if (rc) return rc;
+        done_samples += c.total;
     }
     if (cache && tsteps > 0) {
         // online training on this frame's samples (gradients + Adam per step)
@@ -881,19 +1035,19 @@ static int render_impl(bg_scene* s, bg_cache* cache, const bg_camera_desc* cam, 
         stats->kernel_launches = ins.launches;
         stats->launches_extend = ins.launches_extend;
         stats->ms_total = ms;
-        float phase[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+        float phase_ms[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
         for (size_t i = 0; i + 1 < ins.evs.size(); i += 2) {
             float m = 0.f;
             cudaEventElapsedTime(&m, ins.evs[i], ins.evs[i + 1]);
-            phase[ins.tags[i]] += m;
+            phase_ms[ins.tags[i]] += m;
         }
         for (cudaEvent_t e : ins.evs) cudaEventDestroy(e);
-        stats->ms_extend = phase[0];
-        stats->ms_shadow = phase[1];
-        stats->ms_mis = phase[2];
-        stats->ms_cache_query = phase[3];
-        stats->ms_cache_train = phase[4];
-        stats->ms_shade = ins.time_phases ? ms - phase[0] - phase[1] - phase[2] - phase[3] - phase[4] : 0.f;
+        stats->ms_extend = phase_ms[0];
+        stats->ms_shadow = phase_ms[1];
+        stats->ms_mis = phase_ms[2];
+        stats->ms_cache_query = phase_ms[3];
+        stats->ms_cache_train = phase_ms[4];
+        stats->ms_shade = ins.time_phases ? ms - phase_ms[0] - phase_ms[1] - phase_ms[2] - phase_ms[3] - phase_ms[4] : 0.f;
         stats->sub_rays_extension = int64_t(t[3]);
         stats->sub_nodes_extension = int64_t(t[4]);
         stats->sub_tris_extension = int64_t(t[5]);
@@ -907,6 +1061,24 @@ static int render_impl(bg_scene* s, bg_cache* cache, const bg_camera_desc* cam, 
         cudaEventDestroy(ev1);
     }
     return BG_OK;
+}
+
+static int render_impl(bg_scene* s, bg_cache* cache, const bg_camera_desc* cam, const bg_tracer_desc* tr,
+                       const bg_sampler_desc* sm, int W, int H, float4* accum, bg_render_stats* stats, cudaStream_t st) {
+    if (!s) return set_error(BG_ERR_INVALID_ARG, "scene is NULL");
+    if (!s->committed) return set_error(BG_ERR_STATE, "scene not committed");
+    if (!cam || !tr || !sm || !accum) return set_error(BG_ERR_INVALID_ARG, "NULL argument");
+    if (sm->kind != 0) return set_error(BG_ERR_UNSUPPORTED, "sampler kind %d", sm->kind);
+    std::vector<JobSpec> jobs(1);
+    JobSpec& J = jobs[0];
+    J.rec.root = 0;
+    J.rec.light0 = 0;
+    J.rec.nlights = s->dev.nlights;
+    J.rec.pad = 0;
+    J.rec.bg[0] = s->dev.bg[0]; J.rec.bg[1] = s->dev.bg[1]; J.rec.bg[2] = s->dev.bg[2]; J.rec.bg[3] = 0.f;
+    J.cam = make_camera(cam);
+    J.W = W; J.H = H; J.spp = sm->spp; J.soff = sm->sample_offset; J.seed = sm->seed; J.accum = accum;
+    return render_jobs(s, cache, jobs, tr, stats, st, false);
 }
 
 }  // namespace bg

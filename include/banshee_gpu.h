@@ -282,6 +282,48 @@ int bg_render_host(bg_scene* scene, const bg_camera_desc* camera, const bg_trace
                    const bg_sampler_desc* sampler, int32_t width, int32_t height,
                    float* accum_rgbw, bg_render_stats* stats);
 
+/* ----------------------------------------------------- multi-scene batch */
+/* Many independent scenes, cameras, resolutions and sample counts traced
+ * together: the committed scenes are merged into one device scene, and every
+ * job's camera samples share the same wavefront queues, persistent kernels and
+ * per-pass CUDA graph.  No counterpart in the reference (one World per
+ * Renderer::Render call, renderer/renderer.h:49).  Each job's image is
+ * bit-identical to rendering its scene alone with the same sampler. */
+typedef struct bg_batch bg_batch;
+
+typedef struct bg_batch_job {
+    int32_t scene;             /* index from bg_batch_add_scene              */
+    int32_t width, height;
+    int32_t reserved;
+    bg_camera_desc camera;
+    bg_sampler_desc sampler;   /* spp, seed, sample_offset                   */
+    float* accum_rgbw_dev;     /* width*height float4, as bg_render          */
+} bg_batch_job;
+
+typedef struct bg_tune_result {
+    int32_t trace_threads;     /* traversal block size chosen                */
+    int32_t paths_per_pass;    /* wavefront size chosen                      */
+    int32_t candidates;        /* configurations timed                       */
+    float ms;                  /* time of the best probe render              */
+    float msamples_per_s;      /* its throughput                             */
+} bg_tune_result;
+
+int bg_batch_create(bg_ctx* ctx, bg_batch** out);
+/* The scene must be committed; its device data is copied at bg_batch_commit,
+ * after which the scene may be destroyed. */
+int bg_batch_add_scene(bg_batch* batch, bg_scene* scene, int32_t* index);
+int bg_batch_commit(bg_batch* batch);
+int bg_batch_info(bg_batch* batch, bg_scene_info* info);
+int bg_batch_render(bg_batch* batch, const bg_batch_job* jobs, int32_t njobs, const bg_tracer_desc* tracer,
+                    bg_render_stats* stats, void* stream);
+/* Times traversal block sizes {128, 256} x paths per pass {2^19 .. 2^22} on
+ * the jobs with spp capped at probe_spp and keeps the fastest for later
+ * bg_batch_render calls.  The jobs' accumulation buffers receive the probe
+ * samples: clear them before the real render.  Synchronises. */
+int bg_batch_autotune(bg_batch* batch, const bg_batch_job* jobs, int32_t njobs, const bg_tracer_desc* tracer,
+                      int32_t probe_spp, bg_tune_result* result, void* stream);
+int bg_batch_destroy(bg_batch* batch);
+
 /* ------------------------------------------------------ radiance cache */
 /* Neural radiance cache.  No counterpart in the reference: Banshee has no
  * learned component.  A hash-grid + one-blob encoded, 64-wide, 5-hidden-layer
