@@ -235,6 +235,48 @@ def cornell_c1(ctx, ref_seconds_cap=60.0):
     return out
 
 
+def batch_c4(ctx, nscenes=64, seed=7, timed_frames=1):
+    """C4: 64 procedural scenes (triangles log-uniform in [1e4, 5e5], resolutions from
+    {256^2, 512^2, 1024x768}, 16..128 spp each) traced together by one batch: one set of
+    queues, persistent kernels, one pass graph; autotuned block / wavefront sizes."""
+    import torch
+    from banshee_b200 import capi, scenes
+    t0 = time.perf_counter()
+    items = scenes.batch(nscenes, seed=seed)
+    gss = [capi.GpuScene(ctx, sc) for sc, _ in items]
+    batch = capi.Batch(ctx, gss)
+    build_s = time.perf_counter() - t0
+    for g in gss:
+        g.close()
+    bufs, jobs = [], []
+    for k, (sc, spp) in enumerate(items):
+        acc = torch.zeros((sc.height, sc.width, 4), dtype=torch.float32, device="cuda")
+        bufs.append(acc)
+        jobs.append(dict(scene=k, width=sc.width, height=sc.height, spp=spp, seed=1, camera=None,
+                         accum_dev=acc.data_ptr()))
+    for k, (sc, _) in enumerate(items):
+        jobs[k]["camera"] = sc.camera_desc()
+    tune = batch.autotune(jobs, probe_spp=2, maxdepth=MAXDEPTH)
+    for b in bufs:
+        b.zero_()
+    samples = sum(sc.width * sc.height * spp for sc, spp in items)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(timed_frames):
+        batch.render(jobs, maxdepth=MAXDEPTH)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / timed_frames
+    info = batch.info()
+    batch.close()
+    return {"scenes": nscenes, "triangles_total": info["ntriangles"], "camera_samples": samples,
+            "ms": ms, "msamples_per_s": samples / ms / 1e3, "autotune": tune, "build_s": build_s,
+            "resolutions": sorted({"%dx%d" % (sc.width, sc.height) for sc, _ in items}),
+            "spp_range": [min(s for _, s in items), max(s for _, s in items)],
+            "triangle_range": [min(sc.ntriangles for sc, _ in items), max(sc.ntriangles for sc, _ in items)]}
+
+
 def time_to_relmse(gs, sc, args, target=1e-3):
     """Second half of the metric: wall (GPU) time for the radiance-cache tracer and
     the plain tracer to reach relMSE 1e-3 on a centred 240x136 window of the 1080p
@@ -283,6 +325,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-cache", action="store_true", help="skip the time-to-relMSE measurement")
     ap.add_argument("--no-extra", action="store_true", help="skip the C1 / C2 sections")
+    ap.add_argument("--c4", action="store_true", help="also run the 64-scene batch (C4)")
     ap.add_argument("--gt-spp", type=int, default=65536, help="reference spp of the relMSE window")
     ap.add_argument("--conv-seconds", type=float, default=20.0, help="time budget per tracer for time-to-relMSE")
     args = ap.parse_args()
@@ -431,6 +474,7 @@ def main():
         gs.close()
         c2 = raycast_c2(ctx)
         c1 = cornell_c1(ctx)
+    c4 = batch_c4(ctx) if (rank == 0 and world == 1 and args.c4) else None
 
     if rank == 0:
         line = {
@@ -456,6 +500,7 @@ def main():
             "relmse_time": cache_res,
             "raycast_c2": c2,
             "cornell_c1": c1,
+            "batch_c4": c4,
         }
         print(json.dumps(line), flush=True)
     if dist is not None:
