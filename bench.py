@@ -339,14 +339,12 @@ def main():
         return run_reference_arm(args, rank)
 
     import torch
-    from banshee_b200 import abi, capi, scenes
+    from banshee_b200 import abi, capi, multigpu, scenes
 
     torch.cuda.set_device(local)
     dist = None
     if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+        dist = multigpu.init("nccl", timeout_s=120, device=torch.device("cuda", local))
 
     t_scene = time.perf_counter()
     sc = scenes.production(WIDTH, HEIGHT)
@@ -359,13 +357,12 @@ def main():
     npix = WIDTH * HEIGHT
 
     def step(i, stats=False, flags=0):
-        return gs.render(acc.data_ptr(), WIDTH, HEIGHT, 1, seed=SEED, sample_offset=i * world + rank,
-                         tracer=abi.BG_TRACER_GI, maxdepth=MAXDEPTH, stream=stream.cuda_stream, flags=flags,
+        return gs.render(acc.data_ptr(), WIDTH, HEIGHT, 1, seed=SEED,
+                         sample_offset=multigpu.sample_offset(i, rank, world), tracer=abi.BG_TRACER_GI, maxdepth=MAXDEPTH, stream=stream.cuda_stream, flags=flags,
                          stats=stats)
 
     def exchange():
-        if dist is not None:
-            dist.all_reduce(acc)
+        multigpu.combine(acc, dist)
 
     # warm-up (untimed)
     for i in range(args.warmup):
@@ -394,10 +391,7 @@ def main():
     time.sleep(0.25)
     clocks.stop()
     clocks.window(w0, w1 + 0.05)
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = multigpu.max_over_ranks(ms, dist, device="cuda")
     samples_total = world * npix * args.steps
     value = samples_total / (ms * 1e-3) / 1e6
     flags_err = gs.error_flags()
@@ -447,13 +441,10 @@ def main():
         dist.barrier()
     t0 = time.perf_counter()
     for i in range(ek):
-        gs.render_host(WIDTH, HEIGHT, 1, seed=SEED, sample_offset=(2 + i) * world + rank, maxdepth=MAXDEPTH,
-                       accum=host_np)
+        gs.render_host(WIDTH, HEIGHT, 1, seed=SEED, sample_offset=multigpu.sample_offset(2 + i, rank, world),
+                       maxdepth=MAXDEPTH, accum=host_np)
     e2e_s = time.perf_counter() - t0
-    if dist is not None:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = multigpu.max_over_ranks(e2e_s, dist, device="cuda")
     e2e_value = world * npix * ek / e2e_s / 1e6
 
     cpu = None
