@@ -358,8 +358,8 @@ def main():
 
     def step(i, stats=False, flags=0):
         return gs.render(acc.data_ptr(), WIDTH, HEIGHT, 1, seed=SEED,
-                         sample_offset=multigpu.sample_offset(i, rank, world), tracer=abi.BG_TRACER_GI, maxdepth=MAXDEPTH, stream=stream.cuda_stream, flags=flags,
-                         stats=stats)
+                         sample_offset=multigpu.sample_offset(i, rank, world), tracer=abi.BG_TRACER_GI,
+                         maxdepth=MAXDEPTH, stream=stream.cuda_stream, flags=flags, stats=stats)
 
     def exchange():
         multigpu.combine(acc, dist)
