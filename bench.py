@@ -298,6 +298,16 @@ def time_to_relmse(gs, sc, args, target=1e-3):
                                                    maxdepth=MAXDEPTH),
                          WIDTH, HEIGHT, Wc, Hc, gt, args.conv_seconds, 100000, target=target, every=4)
     cache.close()
+    # Bound for any cache that ends paths after 2 bounces: the plain tracer
+    # truncated there (max depth 2, nothing added at the 3rd vertex), judged
+    # against its own deep reference -- a perfect cache at zero cost would
+    # converge at this rate and frame time, no faster.
+    t0 = time.perf_counter()
+    gt2 = CV.ground_truth(gs, Wc, Hc, args.gt_spp, 2, seed=7777, camera=wcam)
+    gt2_s = time.perf_counter() - t0
+    trunc = CV.converge(lambda p, f: gs.render(p, WIDTH, HEIGHT, 1, seed=SEED, sample_offset=f, maxdepth=2,
+                                               stats=False),
+                        WIDTH, HEIGHT, Wc, Hc, gt2, args.conv_seconds, 100000, target=target, every=4)
 
     def summ(r):
         return {"seconds_to_target": r["t_target"], "frames": r["frames"], "final_relmse": r["final_relmse"],
@@ -305,13 +315,18 @@ def time_to_relmse(gs, sc, args, target=1e-3):
                 "curve": [[round(t, 4), n, float("%.4g" % e)] for t, n, e in r["curve"][::max(1, len(r["curve"]) // 12)]]}
 
     ratio = (cached["t_target"] / plain["t_target"]) if (cached["t_target"] and plain["t_target"]) else None
+    bound = (trunc["t_target"] / plain["t_target"]) if (trunc["t_target"] and plain["t_target"]) else None
     return {"target_relmse": target, "window": [Wc, Hc], "reference_spp": args.gt_spp, "reference_seconds": gt_s,
             "reference": "plain GiTracer(8), float64 accumulation of 256-spp chunks",
             "relmse": "mean over pixels and channels of (x - ref)^2 / (ref^2 + 0.01)",
             "cache_config": "hash grid 16 levels x 2 features, 2^19 entries/level, res 16..2048; MLP 64x5 bf16; "
                             "Adam lr 1e-2; 65536 training paths/frame, 1 step of 16384 rows/frame; paths end into "
                             "the cache after 2 bounces",
-            "plain": summ(plain), "cache": summ(cached), "cache_over_plain_time": ratio}
+            "plain": summ(plain), "cache": summ(cached), "cache_over_plain_time": ratio,
+            "perfect_cache_bound": {
+                "what": "plain tracer truncated after 2 bounces (max depth 2) against its own reference: the "
+                        "time-to-target of a free, exact cache ending paths there",
+                "reference_seconds": gt2_s, **summ(trunc), "over_plain_time": bound}}
 
 
 def main():
