@@ -64,7 +64,8 @@ class SceneInfo(C.Structure):
     _fields_ = [("ntriangles", C.c_int64), ("nnodes", C.c_int64), ("node_bytes", C.c_int64),
                 ("tri_bytes", C.c_int64), ("shade_bytes", C.c_int64), ("node_stride", C.c_int32),
                 ("max_depth", C.c_int32), ("max_stack", C.c_int32), ("nmeshes", C.c_int32),
-                ("nmaterials", C.c_int32), ("nlights", C.c_int32), ("build_ms", C.c_double)]
+                ("nmaterials", C.c_int32), ("nlights", C.c_int32), ("build_ms", C.c_double),
+                ("node_width", C.c_int32), ("node_widths", C.c_int32)]
 
 
 BG_RENDER_TIME_PHASES = 0x1
@@ -106,7 +107,7 @@ class BatchJob(C.Structure):
 
 class TuneResult(C.Structure):
     _fields_ = [("trace_threads", C.c_int32), ("paths_per_pass", C.c_int32), ("candidates", C.c_int32),
-                ("ms", C.c_float), ("msamples_per_s", C.c_float)]
+                ("ms", C.c_float), ("msamples_per_s", C.c_float), ("node_width", C.c_int32)]
 
 
 def fptr(a):

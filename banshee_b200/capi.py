@@ -48,6 +48,7 @@ def lib():
             "bg_scene_commit": [_vp, C.POINTER(abi.BuildOpts)],
             "bg_scene_info_get": [_vp, C.POINTER(abi.SceneInfo)],
             "bg_scene_error_flags": [_vp, C.POINTER(C.c_uint32), _i32],
+            "bg_scene_set_node_width": [_vp, _i32],
             "bg_intersect_closest": [_vp, _vp, _vp, _i64, _vp],
             "bg_intersect_any": [_vp, _vp, _vp, _i64, _vp],
             "bg_intersect_closest_host": [_vp, _vp, _vp, _i64],
@@ -125,7 +126,9 @@ class Context:
 class GpuScene:
     """A committed scene on the device: World::Commit + the Intersectable surface."""
 
-    def __init__(self, ctx, scene, node_width=4, max_leaf=4, bins=32):
+    def __init__(self, ctx, scene, node_width=0, max_leaf=4, bins=32):
+        """node_width: 4 (128-byte nodes), 8 (96-byte compressed nodes) or 0 (both
+        built; the active one is chosen with set_node_width)."""
         self.ctx = ctx
         self.scene = scene
         self.h = _vp()
@@ -156,6 +159,9 @@ class GpuScene:
         f = C.c_uint32()
         check(lib().bg_scene_error_flags(self.h, C.byref(f), int(clear)))
         return f.value
+
+    def set_node_width(self, width):
+        check(lib().bg_scene_set_node_width(self.h, int(width)))
 
     # -- host-buffer entry points (synchronous) --------------------------------
     def intersect_closest_host(self, rays):

@@ -57,7 +57,7 @@ void DevBuf::release() {
 // take new ray indices from one global counter with a single warp-aggregated
 // atomicAdd, every kRefillSteps traversal steps.  Termination: the counter is
 // monotone and every ray finishes after at most one visit per node.
-template <bool ANY, bool COUNT, int THREADS = kTraceThreads>
+template <bool ANY, bool COUNT, int THREADS = kTraceThreads, int WIDTH = 4>
 __global__ void __launch_bounds__(THREADS, 1024 / THREADS)
 k_trace(DevScene S, const float4* __restrict__ rays, int64_t n_static, const int* __restrict__ n_dev,
         bg_hit* __restrict__ hits, uint8_t* __restrict__ occ, unsigned long long* __restrict__ work,
@@ -67,7 +67,7 @@ k_trace(DevScene S, const float4* __restrict__ rays, int64_t n_static, const int
     const int64_t n_all = n_dev ? int64_t(*n_dev) : n_static;
     const int64_t n = COUNT ? (n_all + stride - 1) / stride : n_all;
     const unsigned lane = threadIdx.x & 31u;
-    int2 stack[kStackSize];
+    int2 stack[stack_entries<WIDTH>()];
     TravState s;
     Counters cnt{0ull, 0ull, 0ull};
     int64_t ridx = -1;
@@ -98,7 +98,7 @@ k_trace(DevScene S, const float4* __restrict__ rays, int64_t n_static, const int
         }
         if (!__any_sync(0xffffffffu, active)) break;
         if (active) {
-            if (trav_steps<ANY, COUNT>(S, s, stack, kRefillSteps, cnt)) {
+            if (trav_steps<ANY, COUNT, WIDTH>(S, s, stack, kRefillSteps, cnt)) {
                 if (ANY) {
                     occ[ridx] = s.prim >= 0 ? 1 : 0;
                 } else {
@@ -127,20 +127,28 @@ k_trace(DevScene S, const float4* __restrict__ rays, int64_t n_static, const int
     }
 }
 
-template <bool ANY, bool COUNT, int THREADS = kTraceThreads>
+template <bool ANY, bool COUNT, int THREADS, int WIDTH>
 static int trace_blocks(bg_scene* s) {
     int nb = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_trace<ANY, COUNT, THREADS>, THREADS, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_trace<ANY, COUNT, THREADS, WIDTH>, THREADS, 0);
     if (nb < 1) nb = 1;
     return nb * s->ctx->num_sms;
 }
 
+// Grid sizes of every traversal variant: [width 4/8][any][count][128/256 threads].
+template <int WIDTH>
+static void setup_width(bg_scene* s, int w) {
+    s->trace_blocks[w][0][0][0] = trace_blocks<false, false, 128, WIDTH>(s);
+    s->trace_blocks[w][1][0][0] = trace_blocks<true, false, 128, WIDTH>(s);
+    s->trace_blocks[w][0][1][0] = trace_blocks<false, true, 128, WIDTH>(s);
+    s->trace_blocks[w][1][1][0] = trace_blocks<true, true, 128, WIDTH>(s);
+    s->trace_blocks[w][0][0][1] = trace_blocks<false, false, 256, WIDTH>(s);
+    s->trace_blocks[w][1][0][1] = trace_blocks<true, false, 256, WIDTH>(s);
+}
+
 void scene_launch_setup(bg_scene* s) {
-    s->trace_blocks_closest = trace_blocks<false, false>(s);
-    s->trace_blocks_any = trace_blocks<true, false>(s);
-    s->trace_blocks_count = trace_blocks<false, true>(s);
-    s->trace_blocks_closest256 = trace_blocks<false, false, 256>(s);
-    s->trace_blocks_any256 = trace_blocks<true, false, 256>(s);
+    setup_width<4>(s, 0);
+    setup_width<8>(s, 1);
 }
 
 unsigned long long* next_work_counter(bg_scene* s) {
@@ -148,28 +156,53 @@ unsigned long long* next_work_counter(bg_scene* s) {
     return s->work.as<unsigned long long>() + slot;
 }
 
+template <int WIDTH>
+static void launch_width(bg_scene* s, bool any_hit, const float4* rays, int64_t n_static, const int* n_dev,
+                         bg_hit* hits, uint8_t* occ, cudaStream_t st, unsigned long long* counters, int stride,
+                         unsigned long long* w, const int* roots) {
+    const int wi = WIDTH == 8 ? 1 : 0;
+    const DevScene& d = s->dev;
+    if (counters) {
+        if (any_hit)
+            k_trace<true, true, 128, WIDTH><<<s->trace_blocks[wi][1][1][0], 128, 0, st>>>(d, rays, n_static, n_dev, hits, occ, w, counters, stride, roots);
+        else
+            k_trace<false, true, 128, WIDTH><<<s->trace_blocks[wi][0][1][0], 128, 0, st>>>(d, rays, n_static, n_dev, hits, occ, w, counters, stride, roots);
+    } else if (s->tune_threads == 256) {
+        if (any_hit)
+            k_trace<true, false, 256, WIDTH><<<s->trace_blocks[wi][1][0][1], 256, 0, st>>>(d, rays, n_static, n_dev, hits, occ, w, nullptr, 1, roots);
+        else
+            k_trace<false, false, 256, WIDTH><<<s->trace_blocks[wi][0][0][1], 256, 0, st>>>(d, rays, n_static, n_dev, hits, occ, w, nullptr, 1, roots);
+    } else if (any_hit) {
+        k_trace<true, false, 128, WIDTH><<<s->trace_blocks[wi][1][0][0], 128, 0, st>>>(d, rays, n_static, n_dev, hits, occ, w, nullptr, 1, roots);
+    } else {
+        k_trace<false, false, 128, WIDTH><<<s->trace_blocks[wi][0][0][0], 128, 0, st>>>(d, rays, n_static, n_dev, hits, occ, w, nullptr, 1, roots);
+    }
+}
+
 int launch_trace(bg_scene* s, bool any_hit, const float4* rays, int64_t n_static, const int* n_dev,
                  bg_hit* hits, uint8_t* occ, cudaStream_t st, unsigned long long* counters, int stride,
                  unsigned long long* work, const int* roots) {
     unsigned long long* w = work ? work : next_work_counter(s);
     BG_CUDA(cudaMemsetAsync(w, 0, sizeof(unsigned long long), st));
-    if (counters) {
-        if (any_hit)
-            k_trace<true, true><<<s->trace_blocks_count, kTraceThreads, 0, st>>>(s->dev, rays, n_static, n_dev, hits, occ, w, counters, stride, roots);
-        else
-            k_trace<false, true><<<s->trace_blocks_count, kTraceThreads, 0, st>>>(s->dev, rays, n_static, n_dev, hits, occ, w, counters, stride, roots);
-    } else if (s->tune_threads == 256) {
-        if (any_hit)
-            k_trace<true, false, 256><<<s->trace_blocks_any256, 256, 0, st>>>(s->dev, rays, n_static, n_dev, hits, occ, w, nullptr, 1, roots);
-        else
-            k_trace<false, false, 256><<<s->trace_blocks_closest256, 256, 0, st>>>(s->dev, rays, n_static, n_dev, hits, occ, w, nullptr, 1, roots);
-    } else if (any_hit) {
-        k_trace<true, false><<<s->trace_blocks_any, kTraceThreads, 0, st>>>(s->dev, rays, n_static, n_dev, hits, occ, w, nullptr, 1, roots);
-    } else {
-        k_trace<false, false><<<s->trace_blocks_closest, kTraceThreads, 0, st>>>(s->dev, rays, n_static, n_dev, hits, occ, w, nullptr, 1, roots);
-    }
+    if (s->dev.width == 8)
+        launch_width<8>(s, any_hit, rays, n_static, n_dev, hits, occ, st, counters, stride, w, roots);
+    else
+        launch_width<4>(s, any_hit, rays, n_static, n_dev, hits, occ, st, counters, stride, w, roots);
     BG_CUDA(cudaGetLastError());
     return BG_OK;
+}
+
+// Node-layout fields of bg_scene_info for the active width.
+void set_width_info(bg_scene* s) {
+    bg_scene_info& info = s->info;
+    const bool w8 = s->dev.width == 8;
+    info.node_width = s->dev.width;
+    info.nnodes = w8 ? s->nnodes8 : s->nnodes4;
+    info.node_stride = int32_t(w8 ? sizeof(QNode8) : sizeof(WideNode4));
+    info.node_bytes = info.nnodes * info.node_stride;
+    info.max_depth = w8 ? s->max_depth8 : s->max_depth4;
+    info.max_stack = w8 ? s->max_stack8 : s->max_stack4;
+    info.node_widths = (s->dev.nodes ? 4 : 0) | (s->dev.nodes8 ? 8 : 0);
 }
 
 // ------------------------------------------------------------ commit
@@ -282,17 +315,29 @@ static int commit_scene(bg_scene* s, const bg_build_opts* opts) {
             if (std::isfinite(hi[3 * size_t(t) + k])) s->bbox_hi[k] = std::max(s->bbox_hi[k], hi[3 * size_t(t) + k]);
         }
     BuildParams bp;
+    int want_width = 0;
     if (opts) {
-        if (opts->node_width != 0 && opts->node_width != 4)
-            return set_error(BG_ERR_UNSUPPORTED, "node_width %d: this build supports 4-wide nodes", opts->node_width);
+        want_width = opts->node_width;
+        if (want_width != 0 && want_width != 4 && want_width != 8)
+            return set_error(BG_ERR_UNSUPPORTED, "node_width %d: supported widths are 4 and 8 (0: both)", want_width);
         if (opts->max_leaf_size) bp.max_leaf = opts->max_leaf_size;
         if (opts->sah_bins) bp.bins = opts->sah_bins;
     }
     if (bp.max_leaf < 1 || bp.max_leaf > 16 || bp.bins < 2 || bp.bins > 256)
         return set_error(BG_ERR_INVALID_ARG, "build options out of range (leaf 1..16, bins 2..256)");
+    bp.wide4 = want_width != 8;
+    bp.wide8 = want_width != 4;
     BuildResult br = build_wide_bvh(lo.data(), hi.data(), ntris, bp);
-    if (br.max_stack > kStackSize)
+    if (want_width == 8 && br.nodes8.empty())
+        return set_error(BG_ERR_UNSUPPORTED, "scene coordinates too large for the 8-wide compressed nodes");
+    if (bp.wide4 && br.max_stack > kStackSize)
         return set_error(BG_ERR_UNSUPPORTED, "BVH needs a %d-entry traversal stack (> %d)", br.max_stack, kStackSize);
+    if (!br.nodes8.empty() && br.max_stack8 > kStackSize8) {
+        if (want_width == 8)
+            return set_error(BG_ERR_UNSUPPORTED, "8-wide BVH needs a %d-entry traversal stack (> %d)", br.max_stack8,
+                             kStackSize8);
+        br.nodes8.clear();
+    }
     // per-triangle records
     std::vector<int> tri_bundle(static_cast<size_t>(ntris));
     for (int i = 0; i < nm; ++i)
@@ -331,7 +376,8 @@ static int commit_scene(bg_scene* s, const bg_build_opts* opts) {
         }
     }
     int rc;
-    if ((rc = s->nodes.ensure(br.nodes.size() * sizeof(WideNode4))) ||
+    if ((rc = s->nodes.ensure(std::max<size_t>(1, br.nodes.size()) * sizeof(WideNode4))) ||
+        (rc = s->nodes8.ensure(std::max<size_t>(1, br.nodes8.size()) * sizeof(QNode8))) ||
         (rc = s->tris.ensure(tris.size() * sizeof(TriRec))) ||
         (rc = s->shade.ensure(shade.size() * sizeof(ShadeRec))) ||
         (rc = s->bundles.ensure(bundles.size() * sizeof(BundleRec))) ||
@@ -340,7 +386,10 @@ static int commit_scene(bg_scene* s, const bg_build_opts* opts) {
         (rc = s->err.ensure(sizeof(unsigned))) ||
         (rc = s->work.ensure(kWorkSlots * sizeof(unsigned long long))))
         return rc;
-    BG_CUDA(cudaMemcpy(s->nodes.ptr, br.nodes.data(), br.nodes.size() * sizeof(WideNode4), cudaMemcpyHostToDevice));
+    if (!br.nodes.empty())
+        BG_CUDA(cudaMemcpy(s->nodes.ptr, br.nodes.data(), br.nodes.size() * sizeof(WideNode4), cudaMemcpyHostToDevice));
+    if (!br.nodes8.empty())
+        BG_CUDA(cudaMemcpy(s->nodes8.ptr, br.nodes8.data(), br.nodes8.size() * sizeof(QNode8), cudaMemcpyHostToDevice));
     BG_CUDA(cudaMemcpy(s->tris.ptr, tris.data(), tris.size() * sizeof(TriRec), cudaMemcpyHostToDevice));
     BG_CUDA(cudaMemcpy(s->shade.ptr, shade.data(), shade.size() * sizeof(ShadeRec), cudaMemcpyHostToDevice));
     BG_CUDA(cudaMemcpy(s->bundles.ptr, bundles.data(), bundles.size() * sizeof(BundleRec), cudaMemcpyHostToDevice));
@@ -350,7 +399,13 @@ static int commit_scene(bg_scene* s, const bg_build_opts* opts) {
     BG_CUDA(cudaMemset(s->err.ptr, 0, sizeof(unsigned)));
     BG_CUDA(cudaMemset(s->work.ptr, 0, kWorkSlots * sizeof(unsigned long long)));
     DevScene& d = s->dev;
-    d.nodes = s->nodes.as<WideNode4>();
+    d.nodes = br.nodes.empty() ? nullptr : s->nodes.as<WideNode4>();
+    d.nodes8 = br.nodes8.empty() ? nullptr : s->nodes8.as<QNode8>();
+    s->nnodes4 = int64_t(br.nodes.size());
+    s->nnodes8 = int64_t(br.nodes8.size());
+    s->max_stack4 = br.max_stack; s->max_depth4 = br.max_depth;
+    s->max_stack8 = br.max_stack8; s->max_depth8 = br.max_depth8;
+    d.width = d.nodes ? (want_width == 0 && d.nodes8 ? kDefaultNodeWidth : 4) : 8;
     d.tris = s->tris.as<TriRec>();
     d.shade = s->shade.as<ShadeRec>();
     d.bundles = s->bundles.as<BundleRec>();
@@ -366,13 +421,9 @@ static int commit_scene(bg_scene* s, const bg_build_opts* opts) {
     auto t1 = std::chrono::steady_clock::now();
     bg_scene_info& info = s->info;
     info.ntriangles = ntris;
-    info.nnodes = int64_t(br.nodes.size());
-    info.node_bytes = int64_t(br.nodes.size() * sizeof(WideNode4));
     info.tri_bytes = int64_t(tris.size() * sizeof(TriRec));
     info.shade_bytes = int64_t(shade.size() * sizeof(ShadeRec));
-    info.node_stride = int32_t(sizeof(WideNode4));
-    info.max_depth = br.max_depth;
-    info.max_stack = br.max_stack;
+    set_width_info(s);
     info.nmeshes = nm;
     info.nmaterials = nmat;
     info.nlights = int(lights.size());
@@ -457,7 +508,7 @@ int bg_scene_destroy(bg_scene* s) {
     if (!s) return BG_OK;
     cudaSetDevice(s->ctx->device);
     cudaDeviceSynchronize();
-    for (DevBuf* b : {&s->nodes, &s->tris, &s->shade, &s->bundles, &s->mats_d, &s->lights_d, &s->err, &s->work,
+    for (DevBuf* b : {&s->nodes, &s->nodes8, &s->tris, &s->shade, &s->bundles, &s->mats_d, &s->lights_d, &s->err, &s->work,
                       &s->host_rays, &s->host_out})
         b->release();
     if (s->render) render_state_free(s->render);
@@ -581,6 +632,18 @@ int bg_scene_error_flags(bg_scene* s, uint32_t* flags, int32_t clear) {
     BG_CUDA(cudaMemcpy(&v, s->err.ptr, sizeof(unsigned), cudaMemcpyDeviceToHost));
     if (clear) BG_CUDA(cudaMemset(s->err.ptr, 0, sizeof(unsigned)));
     *flags = v;
+    return BG_OK;
+}
+
+int bg_scene_set_node_width(bg_scene* s, int32_t width) {
+    int rc = check_scene(s);
+    if (rc) return rc;
+    if (width != 4 && width != 8) return set_error(BG_ERR_INVALID_ARG, "node width %d: 4 or 8", width);
+    if ((width == 4 && !s->dev.nodes) || (width == 8 && !s->dev.nodes8))
+        return set_error(BG_ERR_UNSUPPORTED, "the %d-wide layout of this scene was not built", width);
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->dev.width = width;
+    set_width_info(s);
     return BG_OK;
 }
 
@@ -726,12 +789,13 @@ extern "C" int bg_traversal_counts_noalloc(bg_scene* s, const bg_ray* rays, int6
     uint8_t* occ = base + kNoAllocHeader;
     cudaError_t e = cudaMemsetAsync(base, 0, kNoAllocHeader, st);   // counters and work counter start at zero
     if (e == cudaSuccess && n > 0) {
-        if (any_hit)
-            k_trace<true, true><<<s->trace_blocks_count, kTraceThreads, 0, st>>>(
-                s->dev, reinterpret_cast<const float4*>(rays), n, nullptr, nullptr, occ, work, cnt, 1, nullptr);
+        const float4* r4 = reinterpret_cast<const float4*>(rays);
+        if (s->dev.width == 8)
+            launch_width<8>(s, any_hit != 0, r4, n, nullptr, any_hit ? nullptr : hits, any_hit ? occ : nullptr, st,
+                            cnt, 1, work, nullptr);
         else
-            k_trace<false, true><<<s->trace_blocks_count, kTraceThreads, 0, st>>>(
-                s->dev, reinterpret_cast<const float4*>(rays), n, nullptr, hits, nullptr, work, cnt, 1, nullptr);
+            launch_width<4>(s, any_hit != 0, r4, n, nullptr, any_hit ? nullptr : hits, any_hit ? occ : nullptr, st,
+                            cnt, 1, work, nullptr);
         e = cudaGetLastError();
     }
     unsigned long long h[3] = {0, 0, 0};

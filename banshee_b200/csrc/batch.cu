@@ -35,6 +35,24 @@ __global__ void k_fix_nodes(WideNode4* nodes, int64_t n, int node_off, int tri_o
     }
 }
 
+__global__ void k_fix_nodes8(QNode8* nodes, int64_t n, int node_off, int tri_off) {
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+        QNode8& w = nodes[i];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            int32_t c = w.child[k];
+            if (c == kEmptyChild) continue;
+            if (c >= 0) {
+                w.child[k] = c + node_off;
+            } else {
+                uint32_t code = uint32_t(c);
+                uint32_t start = (code & uint32_t(kMaxLeafStart)) + uint32_t(tri_off);
+                w.child[k] = int32_t((code & ~uint32_t(kMaxLeafStart)) | start);
+            }
+        }
+    }
+}
+
 __global__ void k_fix_tris(TriRec* tris, int64_t n, int bundle_off, int prim_off) {
     for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
         TriRec& t = tris[i];
@@ -58,7 +76,8 @@ struct bg_batch {
     bg_ctx* ctx = nullptr;
     std::vector<bg_scene*> scenes;
     bg_scene merged;
-    std::vector<bg::JobRec> rec;    // per scene: root, light range, background
+    std::vector<bg::JobRec> rec;    // per scene: root (4-wide), light range, background
+    std::vector<int> root8;         // per scene: root of its 8-wide tree in the merged array
     bool committed = false;
 };
 
@@ -91,31 +110,47 @@ int bg_batch_commit(bg_batch* b) {
     if (b->scenes.empty()) return set_error(BG_ERR_STATE, "batch has no scenes");
     auto t0 = std::chrono::steady_clock::now();
     BG_CUDA(cudaSetDevice(b->ctx->device));
-    int64_t nn = 0, nt = 0, nb = 0, nm = 0, nl = 0;
+    int64_t nn = 0, nn8 = 0, nt = 0, nb = 0, nm = 0, nl = 0;
+    bool all4 = true, all8 = true;
     for (bg_scene* s : b->scenes) {
-        nn += s->info.nnodes; nt += s->info.ntriangles; nb += s->info.nmeshes;
+        nn += s->nnodes4; nn8 += s->nnodes8; nt += s->info.ntriangles; nb += s->info.nmeshes;
         nm += std::max(1, s->info.nmaterials); nl += s->info.nlights;
+        all4 = all4 && s->dev.nodes; all8 = all8 && s->dev.nodes8;
     }
+    if (!all4 && !all8) return set_error(BG_ERR_UNSUPPORTED, "the batch's scenes share no node layout");
+    if (!all4) nn = 0;
+    if (!all8) nn8 = 0;
     if (nt > int64_t(kMaxLeafStart)) return set_error(BG_ERR_UNSUPPORTED, "batch of %lld triangles exceeds %d", (long long)nt, kMaxLeafStart);
-    if (nn > (int64_t(1) << 31) - 2) return set_error(BG_ERR_UNSUPPORTED, "batch has too many nodes");
+    if (std::max(nn, nn8) > (int64_t(1) << 31) - 2) return set_error(BG_ERR_UNSUPPORTED, "batch has too many nodes");
     bg_scene& M = b->merged;
     int rc;
-    if ((rc = M.nodes.ensure(size_t(nn) * sizeof(WideNode4))) || (rc = M.tris.ensure(size_t(nt) * sizeof(TriRec))) ||
+    if ((rc = M.nodes.ensure(size_t(std::max<int64_t>(nn, 1)) * sizeof(WideNode4))) ||
+        (rc = M.nodes8.ensure(size_t(std::max<int64_t>(nn8, 1)) * sizeof(QNode8))) ||
+        (rc = M.tris.ensure(size_t(nt) * sizeof(TriRec))) ||
         (rc = M.shade.ensure(size_t(nt) * sizeof(ShadeRec))) || (rc = M.bundles.ensure(size_t(nb) * sizeof(BundleRec))) ||
         (rc = M.mats_d.ensure(size_t(nm) * sizeof(MatRec))) ||
         (rc = M.lights_d.ensure(size_t(std::max<int64_t>(nl, 1)) * sizeof(LightRec))) ||
         (rc = M.err.ensure(sizeof(unsigned))) || (rc = M.work.ensure(kWorkSlots * sizeof(unsigned long long))))
         return rc;
-    int64_t no = 0, to = 0, bo = 0, mo = 0, lo = 0;
+    int64_t no = 0, no8 = 0, to = 0, bo = 0, mo = 0, lo = 0;
     b->rec.clear();
+    b->root8.clear();
     for (bg_scene* s : b->scenes) {
         const bg_scene_info& I = s->info;
         const int64_t nmat = std::max(1, I.nmaterials);
-        BG_CUDA(cudaMemcpy(M.nodes.as<WideNode4>() + no, s->nodes.ptr, size_t(I.nnodes) * sizeof(WideNode4), cudaMemcpyDeviceToDevice));
+        if (all4) {
+            BG_CUDA(cudaMemcpy(M.nodes.as<WideNode4>() + no, s->nodes.ptr, size_t(s->nnodes4) * sizeof(WideNode4),
+                               cudaMemcpyDeviceToDevice));
+            k_fix_nodes<<<1024, 256>>>(M.nodes.as<WideNode4>() + no, s->nnodes4, int(no), int(to));
+        }
+        if (all8) {
+            BG_CUDA(cudaMemcpy(M.nodes8.as<QNode8>() + no8, s->nodes8.ptr, size_t(s->nnodes8) * sizeof(QNode8),
+                               cudaMemcpyDeviceToDevice));
+            k_fix_nodes8<<<1024, 256>>>(M.nodes8.as<QNode8>() + no8, s->nnodes8, int(no8), int(to));
+        }
         BG_CUDA(cudaMemcpy(M.tris.as<TriRec>() + to, s->tris.ptr, size_t(I.ntriangles) * sizeof(TriRec), cudaMemcpyDeviceToDevice));
         BG_CUDA(cudaMemcpy(M.shade.as<ShadeRec>() + to, s->shade.ptr, size_t(I.ntriangles) * sizeof(ShadeRec), cudaMemcpyDeviceToDevice));
         BG_CUDA(cudaMemcpy(M.mats_d.as<MatRec>() + mo, s->mats_d.ptr, size_t(nmat) * sizeof(MatRec), cudaMemcpyDeviceToDevice));
-        k_fix_nodes<<<1024, 256>>>(M.nodes.as<WideNode4>() + no, I.nnodes, int(no), int(to));
         k_fix_tris<<<1024, 256>>>(M.tris.as<TriRec>() + to, I.ntriangles, int(bo), int(to));
         k_fix_shade<<<1024, 256>>>(M.shade.as<ShadeRec>() + to, I.ntriangles, int(bo), int(mo));
         BG_CUDA(cudaGetLastError());
@@ -142,13 +177,18 @@ int bg_batch_commit(bg_batch* b) {
         jr.pad = 0;
         jr.bg[0] = s->bg[0]; jr.bg[1] = s->bg[1]; jr.bg[2] = s->bg[2]; jr.bg[3] = 0.f;
         b->rec.push_back(jr);
-        no += I.nnodes; to += I.ntriangles; bo += I.nmeshes; mo += nmat; lo += I.nlights;
+        b->root8.push_back(int(no8));
+        no += all4 ? s->nnodes4 : 0; no8 += all8 ? s->nnodes8 : 0;
+        to += I.ntriangles; bo += I.nmeshes; mo += nmat; lo += I.nlights;
     }
     BG_CUDA(cudaMemset(M.err.ptr, 0, sizeof(unsigned)));
     BG_CUDA(cudaMemset(M.work.ptr, 0, kWorkSlots * sizeof(unsigned long long)));
     BG_CUDA(cudaDeviceSynchronize());
     DevScene& d = M.dev;
-    d.nodes = M.nodes.as<WideNode4>();
+    d.nodes = all4 ? M.nodes.as<WideNode4>() : nullptr;
+    d.nodes8 = all8 ? M.nodes8.as<QNode8>() : nullptr;
+    d.width = all4 ? (all8 ? kDefaultNodeWidth : 4) : 8;
+    M.nnodes4 = nn; M.nnodes8 = nn8;
     d.tris = M.tris.as<TriRec>();
     d.shade = M.shade.as<ShadeRec>();
     d.bundles = M.bundles.as<BundleRec>();
@@ -162,18 +202,18 @@ int bg_batch_commit(bg_batch* b) {
     scene_launch_setup(&M);
     bg_scene_info& info = M.info;
     info.ntriangles = nt;
-    info.nnodes = nn;
-    info.node_bytes = nn * int64_t(sizeof(WideNode4));
     info.tri_bytes = nt * int64_t(sizeof(TriRec));
     info.shade_bytes = nt * int64_t(sizeof(ShadeRec));
-    info.node_stride = int32_t(sizeof(WideNode4));
     info.nmeshes = int(nb);
     info.nmaterials = int(nm);
     info.nlights = int(nl);
     for (bg_scene* s : b->scenes) {
-        info.max_depth = std::max(info.max_depth, s->info.max_depth);
-        info.max_stack = std::max(info.max_stack, s->info.max_stack);
+        M.max_depth4 = std::max(M.max_depth4, s->max_depth4);
+        M.max_stack4 = std::max(M.max_stack4, s->max_stack4);
+        M.max_depth8 = std::max(M.max_depth8, s->max_depth8);
+        M.max_stack8 = std::max(M.max_stack8, s->max_stack8);
     }
+    set_width_info(&M);
     info.build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     M.committed = true;
     b->committed = true;
@@ -198,6 +238,7 @@ static int batch_jobs(bg_batch* b, const bg_batch_job* jobs, int32_t njobs, std:
         if (j.sampler.kind != 0) return set_error(BG_ERR_UNSUPPORTED, "job %d: sampler kind %d", i, j.sampler.kind);
         JobSpec& J = out[size_t(i)];
         J.rec = b->rec[size_t(j.scene)];
+        if (b->merged.dev.width == 8) J.rec.root = b->root8[size_t(j.scene)];
         J.cam = make_camera(&j.camera);
         J.W = j.width;
         J.H = j.height;
@@ -218,45 +259,56 @@ int bg_batch_render(bg_batch* b, const bg_batch_job* jobs, int32_t njobs, const 
     return render_jobs(&b->merged, nullptr, js, tracer, stats, static_cast<cudaStream_t>(stream), true);
 }
 
-// Autotuner: times every (traversal block size, paths per pass) candidate on
-// the given jobs with spp capped to `probe_spp` (their accumulation buffers
-// receive those samples), keeps the fastest per camera sample.
+// Autotuner: times every (node layout, traversal block size, paths per pass)
+// candidate on the given jobs with spp capped to `probe_spp` (their
+// accumulation buffers receive those samples), keeps the fastest.
 int bg_batch_autotune(bg_batch* b, const bg_batch_job* jobs, int32_t njobs, const bg_tracer_desc* tracer,
                       int32_t probe_spp, bg_tune_result* result, void* stream) {
+    if (!b) return set_error(BG_ERR_INVALID_ARG, "batch is NULL");
+    if (!b->committed) return set_error(BG_ERR_STATE, "batch not committed");
     std::vector<JobSpec> js;
-    int rc = batch_jobs(b, jobs, njobs, js, std::max(1, probe_spp));
-    if (rc) return rc;
     std::lock_guard<std::mutex> lk(b->merged.mu);
     bg_scene& M = b->merged;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    std::vector<int> widths;
+    if (M.dev.nodes) widths.push_back(4);
+    if (M.dev.nodes8) widths.push_back(8);
     const int threads[2] = {128, 256};
     const int64_t paths[4] = {int64_t(1) << 19, int64_t(1) << 20, int64_t(1) << 21, int64_t(1) << 22};
     float best = 1e30f;
-    int best_t = 128;
+    int best_t = 128, best_w = M.dev.width;
     int64_t best_p = int64_t(1) << 21;
     int tried = 0;
+    int rc = BG_OK;
     cudaEvent_t e0, e1;
     BG_CUDA(cudaEventCreate(&e0));
     BG_CUDA(cudaEventCreate(&e1));
-    for (int t : threads) {
-        for (int64_t p : paths) {
-            M.tune_threads = t;
-            M.tune_paths = p;
-            // first call warms the graph and buffers for this candidate, the second is timed
-            if ((rc = render_jobs(&M, nullptr, js, tracer, nullptr, st, true))) break;
-            BG_CUDA(cudaEventRecord(e0, st));
-            if ((rc = render_jobs(&M, nullptr, js, tracer, nullptr, st, true))) break;
-            BG_CUDA(cudaEventRecord(e1, st));
-            BG_CUDA(cudaEventSynchronize(e1));
-            float ms = 0.f;
-            BG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-            ++tried;
-            if (ms < best) { best = ms; best_t = t; best_p = p; }
+    for (int w : widths) {
+        M.dev.width = w;
+        if ((rc = batch_jobs(b, jobs, njobs, js, std::max(1, probe_spp)))) break;   // roots of this layout
+        for (int t : threads) {
+            for (int64_t p : paths) {
+                M.tune_threads = t;
+                M.tune_paths = p;
+                // first call warms the graph and buffers for this candidate, the second is timed
+                if ((rc = render_jobs(&M, nullptr, js, tracer, nullptr, st, true))) break;
+                BG_CUDA(cudaEventRecord(e0, st));
+                if ((rc = render_jobs(&M, nullptr, js, tracer, nullptr, st, true))) break;
+                BG_CUDA(cudaEventRecord(e1, st));
+                BG_CUDA(cudaEventSynchronize(e1));
+                float ms = 0.f;
+                BG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+                ++tried;
+                if (ms < best) { best = ms; best_t = t; best_p = p; best_w = w; }
+            }
+            if (rc) break;
         }
         if (rc) break;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    M.dev.width = best_w;
+    set_width_info(&M);
     if (rc) return rc;
     M.tune_threads = best_t;
     M.tune_paths = best_p;
@@ -268,6 +320,7 @@ int bg_batch_autotune(bg_batch* b, const bg_batch_job* jobs, int32_t njobs, cons
         result->candidates = tried;
         result->ms = best;
         result->msamples_per_s = best > 0.f ? float(double(samples) / (double(best) * 1e3)) : 0.f;
+        result->node_width = best_w;
     }
     return BG_OK;
 }

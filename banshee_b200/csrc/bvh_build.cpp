@@ -70,16 +70,30 @@ public:
     BuildResult collapse() {
         BuildResult r;
         r.order = idx_;
-        r.nodes.reserve(size_t(n_ / 2 + 16));
-        if (nodes_[0].count > 0) {           // whole scene is one leaf
-            WideNode4 w = empty_node();
-            set_child(w, 0, nodes_[0]);
-            w.child[0] = encode_leaf(nodes_[0].start, nodes_[0].count);
-            r.nodes.push_back(w);
-            r.max_depth = 1; r.max_stack = 1; r.nleaves = 1;
-            return r;
+        if (p_.wide4) {
+            r.nodes.reserve(size_t(n_ / 2 + 16));
+            if (nodes_[0].count > 0) {           // whole scene is one leaf
+                WideNode4 w = empty_node();
+                set_child(w, 0, nodes_[0]);
+                w.child[0] = encode_leaf(nodes_[0].start, nodes_[0].count);
+                r.nodes.push_back(w);
+                r.max_depth = 1; r.max_stack = 1; r.nleaves = 1;
+            } else {
+                emit(r, 0, 1, 0);
+            }
         }
-        emit(r, 0, 1, 0);
+        if (p_.wide8) {
+            r.nodes8.reserve(size_t(n_ / 6 + 16));
+            if (nodes_[0].count > 0) {
+                int32_t kids[1] = {0};
+                r.nodes8.push_back(QNode8{});
+                int32_t code = encode_leaf(nodes_[0].start, nodes_[0].count);
+                fill_qnode(r.nodes8[0], kids, &code, 1);
+                r.max_depth8 = 1; r.max_stack8 = 1;
+            } else {
+                emit8(r, 0, 1, 0);
+            }
+        }
         return r;
     }
 
@@ -134,6 +148,111 @@ private:
             w.child[i] = code;
         }
         return me;
+    }
+
+    // 8-wide collapse: open the largest-area internal child until 8 children.
+    int emit8(BuildResult& r, int32_t b, int depth, int stack_acc) {
+        int32_t kids[8] = {nodes_[b].left, nodes_[b].right, -1, -1, -1, -1, -1, -1};
+        int nk = 2;
+        while (nk < 8) {
+            int best = -1;
+            float ba = -1.f;
+            for (int i = 0; i < nk; ++i) {
+                const BNode& c = nodes_[kids[i]];
+                if (c.count == 0 && c.box.area() > ba) { ba = c.box.area(); best = i; }
+            }
+            if (best < 0) break;
+            int32_t l = nodes_[kids[best]].left, rr = nodes_[kids[best]].right;
+            kids[best] = l;
+            kids[nk++] = rr;
+        }
+        int me = int(r.nodes8.size());
+        r.nodes8.push_back(QNode8{});
+        r.max_depth8 = std::max(r.max_depth8, depth);
+        int stack_here = stack_acc + (nk - 1);
+        r.max_stack8 = std::max(r.max_stack8, stack_here);
+        int32_t codes[8];
+        for (int i = 0; i < nk; ++i) {
+            const BNode& c = nodes_[kids[i]];
+            codes[i] = c.count > 0 ? encode_leaf(c.start, c.count) : emit8(r, kids[i], depth + 1, stack_here);
+        }
+        fill_qnode(r.nodes8[me], kids, codes, nk);
+        return me;
+    }
+
+    // Slot assignment (greedy over child x slot by projected centroid: slot s
+    // takes the child furthest upstream for directions with sign bits s) and
+    // conservative quantisation of the children's boxes.
+    void fill_qnode(QNode8& q, const int32_t* kids, const int32_t* codes, int nk) const {
+        Box u; u.clear();
+        for (int i = 0; i < nk; ++i) u.grow(nodes_[kids[i]].box);
+        double cen[8][3];
+        for (int i = 0; i < nk; ++i)
+            for (int k = 0; k < 3; ++k)
+                cen[i][k] = 0.5 * (double(nodes_[kids[i]].box.lo[k]) + double(nodes_[kids[i]].box.hi[k])) -
+                            0.5 * (double(u.lo[k]) + double(u.hi[k]));
+        int slot_of[8];
+        bool cused[8] = {false}, sused[8] = {false};
+        for (int n = 0; n < nk; ++n) {
+            double best = 1e300;
+            int bc = -1, bs = -1;
+            for (int c = 0; c < nk; ++c) {
+                if (cused[c]) continue;
+                for (int sl = 0; sl < 8; ++sl) {
+                    if (sused[sl]) continue;
+                    double cost = 0.0;
+                    for (int k = 0; k < 3; ++k) cost += ((sl >> k) & 1 ? -cen[c][k] : cen[c][k]);
+                    if (cost < best) { best = cost; bc = c; bs = sl; }
+                }
+            }
+            cused[bc] = true; sused[bs] = true; slot_of[bc] = bs;
+        }
+        int e[3];
+        double k[3];
+        for (int a = 0; a < 3; ++a) {
+            e[a] = qnode_axis(u.lo[a], u.hi[a], &k[a]);
+            if (e[a] > kQMaxExp) { q8_failed_ = true; e[a] = kQMaxExp; }
+        }
+        float* o2[3] = {&q.o2x, &q.o2y, &q.o2z};
+        for (int a = 0; a < 3; ++a) *o2[a] = float(std::ldexp(k[a] - 8388608.0, e[a]));
+        uint32_t valid = 0;
+        uint8_t qb[3][2][8];
+        for (int a = 0; a < 3; ++a)
+            for (int h = 0; h < 2; ++h)
+                for (int sl = 0; sl < 8; ++sl) qb[a][h][sl] = h ? 0 : 255;   // unused slot: inverted box
+        for (int sl = 0; sl < 8; ++sl) q.child[sl] = kEmptyChild;
+        for (int c = 0; c < nk; ++c) {
+            const int sl = slot_of[c];
+            valid |= 1u << sl;
+            q.child[sl] = codes[c];
+            const Box& b = nodes_[kids[c]].box;
+            for (int a = 0; a < 3; ++a) {
+                double lo = std::floor(std::ldexp(double(b.lo[a]), -e[a])) - k[a];
+                double hi = std::ceil(std::ldexp(double(b.hi[a]), -e[a])) - k[a];
+                qb[a][0][sl] = uint8_t(std::min(255.0, std::max(0.0, lo)));
+                qb[a][1][sl] = uint8_t(std::min(255.0, std::max(0.0, hi)));
+            }
+        }
+        q.meta = uint32_t(e[0] + 127) | (uint32_t(e[1] + 127) << 8) | (uint32_t(e[2] + 127) << 16) | (valid << 24);
+        // self-check with the device's dequantisation: fmaf(2^23 + q, 2^e, o2)
+        for (int c = 0; c < nk; ++c) {
+            const int sl = slot_of[c];
+            const Box& b = nodes_[kids[c]].box;
+            for (int a = 0; a < 3; ++a) {
+                const float st = std::ldexp(1.0f, e[a]);
+                const float plo = std::fma(8388608.0f + float(qb[a][0][sl]), st, *o2[a]);
+                const float phi = std::fma(8388608.0f + float(qb[a][1][sl]), st, *o2[a]);
+                if (!(plo <= b.lo[a] && phi >= b.hi[a])) q8_failed_ = true;
+            }
+        }
+        uint32_t* w[3] = {q.qx, q.qy, q.qz};
+        for (int a = 0; a < 3; ++a)
+            for (int h = 0; h < 2; ++h)
+                for (int half = 0; half < 2; ++half) {
+                    uint32_t v = 0;
+                    for (int j = 0; j < 4; ++j) v |= uint32_t(qb[a][h][4 * half + j]) << (8 * j);
+                    w[a][2 * h + half] = v;
+                }
     }
 
     void make_leaf(int64_t nodeidx, int64_t begin, int64_t end, const Box& box) {
@@ -245,14 +364,44 @@ private:
     std::vector<int32_t> idx_;
     std::vector<BNode> nodes_;
     std::atomic<int> spare_threads_{0};
+
+public:
+    mutable bool q8_failed_ = false;
 };
 
 }  // namespace
 
+// Smallest grid step 2^e (e in [-120, kQMaxExp]) with an origin k * 2^e <= L,
+// |k| <= 2^23 - 257 and (k + 255) * 2^e >= H.  All arithmetic is exact in
+// double: L, H are floats, k is an integer below 2^24, the steps are powers of
+// two.  e <= kQMaxExp keeps o2 = (k - 2^23) * 2^e finite; returns kQMaxExp + 1
+// when no such step exists (node coordinates beyond ~1e33).
+int qnode_axis(float L, float H, double* k) {
+    int e = -120;
+    const double ext = double(H) - double(L);
+    if (ext > 0.0) e = std::max(e, int(std::ceil(std::log2(ext / 255.0))) - 1);
+    const double aL = std::fabs(double(L));
+    if (aL > 0.0) e = std::max(e, int(std::floor(std::log2(aL))) - 23);
+    for (; e <= kQMaxExp; ++e) {
+        const double kk = std::floor(std::ldexp(double(L), -e));
+        if (std::fabs(kk) > 8388608.0 - 257.0) continue;
+        if (std::ldexp(kk + 255.0, e) < double(H)) continue;
+        *k = kk;
+        return e;
+    }
+    *k = 0.0;
+    return kQMaxExp + 1;
+}
+
 BuildResult build_wide_bvh(const float* lo, const float* hi, int64_t n, const BuildParams& p) {
     Builder b(lo, hi, n, p);
     b.run();
-    return b.collapse();
+    BuildResult r = b.collapse();
+    if (b.q8_failed_) {              // coordinates too large to quantise: 4-wide only
+        r.nodes8.clear();
+        r.max_depth8 = r.max_stack8 = 0;
+    }
+    return r;
 }
 
 }  // namespace bg

@@ -71,16 +71,20 @@ struct bg_scene {
     bg::DevScene dev{};
     bg_scene_info info{};
     bg::RenderState* render = nullptr;
-    int trace_blocks_closest = 0, trace_blocks_any = 0, trace_blocks_count = 0;
+    int trace_blocks[2][2][2][2] = {};   // [width 4/8][any][count][128/256 threads]: persistent grid sizes
     int64_t tune_paths = 0;   // autotuned paths per pass (0 = default)
     int tune_threads = 0;     // autotuned traversal block size (0 = default 128)
-    int trace_blocks_closest256 = 0, trace_blocks_any256 = 0;
+    bg::DevBuf nodes8;        // 8-wide compressed tree (empty if not built)
+    int64_t nnodes4 = 0, nnodes8 = 0;
+    int max_stack4 = 0, max_stack8 = 0, max_depth4 = 0, max_depth8 = 0;
     bool owns_buffers = true;
 };
 
 namespace bg {
 // Launch helpers (api.cu)
 constexpr int kTraceThreads = 128;
+constexpr int kDefaultNodeWidth = 4;   // active layout when both are built
+void set_width_info(bg_scene* s);
 constexpr int kWorkSlots = 256;
 unsigned long long* next_work_counter(bg_scene* s);
 void scene_launch_setup(bg_scene* s);

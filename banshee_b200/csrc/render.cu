@@ -762,7 +762,7 @@ static int enqueue_pass(bg_scene* s, RenderState* rs, cudaStream_t st, const Pas
 // Captures one pass into a CUDA graph (once per bounce-loop shape) and finds
 // the two kernel nodes whose arguments (the segment slice) change per pass.
 static int pass_graph(bg_scene* s, RenderState* rs, const PassCfg& c) {
-    const int64_t key[8] = {c.maxdepth, c.kind, c.batched ? 1 : 0, rs->kmax, int64_t(rs->cap), s->tune_threads, 0, 0};
+    const int64_t key[8] = {c.maxdepth, c.kind, c.batched ? 1 : 0, rs->kmax, int64_t(rs->cap), s->tune_threads, s->dev.width, 0};
     if (rs->exec && memcmp(key, rs->graph_key, sizeof(key)) == 0) return BG_OK;
     if (rs->exec) { cudaGraphExecDestroy(rs->exec); rs->exec = nullptr; }
     if (rs->graph) { cudaGraphDestroy(rs->graph); rs->graph = nullptr; }

@@ -1,6 +1,7 @@
 // Device-resident scene layout (HBM), shared by host upload code and kernels.
 //
 //   nodes    WideNode4[nnodes]   128 B, one L2 line per 4-wide node
+//   nodes8   QNode8[nnodes8]      96 B, three 32-byte sectors per 8-wide compressed node
 //   tris     TriRec[ntris]        48 B, leaf order; what traversal streams
 //   shade    ShadeRec[ntris]     112 B, global primitive order; read once per hit
 //   bundles  BundleRec[nmeshes]   per-mesh transform, identity flag, area-light owner
@@ -64,6 +65,7 @@ struct LightRec {
 
 struct DevScene {
     const WideNode4* nodes;
+    const QNode8* nodes8;
     const TriRec* tris;
     const ShadeRec* shade;
     const BundleRec* bundles;
@@ -71,7 +73,8 @@ struct DevScene {
     const LightRec* lights;
     unsigned int* errflags;
     int64_t ntris;
-    int32_t nbundles, nmats, nlights, pad;
+    int32_t nbundles, nmats, nlights;
+    int32_t width;          // node layout traversed: 4 (nodes) or 8 (nodes8)
     float bg[3];
     float pad2;
 };

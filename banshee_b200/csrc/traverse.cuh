@@ -1,4 +1,5 @@
-// Closest-hit / any-hit traversal of the 4-wide BVH.
+// Closest-hit / any-hit traversal of the 4-wide BVH and of the 8-wide
+// compressed BVH.
 //
 // Replaces Bvh::Intersect(ray, Hit&) and Bvh::Intersect(ray)
 // (accelerator/bvh.cpp:499-647) together with Mesh::IntersectShape /
@@ -20,7 +21,10 @@
 
 namespace bg {
 
-constexpr int kStackSize = 64;     // entries per ray; the builder checks max_stack against it
+constexpr int kStackSize = 64;     // entries per ray, 4-wide; the builder checks max_stack against it
+constexpr int kStackSize8 = 96;    // entries per ray, 8-wide (up to 7 pushes per level)
+template <int WIDTH>
+__host__ __device__ constexpr int stack_entries() { return WIDTH == 8 ? kStackSize8 : kStackSize; }
 constexpr int kRefillSteps = 24;   // traversal steps between warp refill points
 constexpr float kBoxSlack = 4e-7f;
 
@@ -105,6 +109,64 @@ __device__ __forceinline__ uint32_t box4(const WideNode4* __restrict__ nodes, in
     return mask;
 }
 
+// Test the 8 children of compressed node `ni`.  Each plane is dequantised
+// exactly (P = fmaf(2^23 + q, s, o2), see QNode8) and then tested exactly as in
+// box4, so the same slack argument holds.  Returns the hit mask over slots.
+__device__ __forceinline__ uint32_t box8(const QNode8* __restrict__ nodes, int ni, const Ray& r, float best,
+                                         float tn[8], int32_t ch[8]) {
+    const float4* p = reinterpret_cast<const float4*>(nodes + ni);
+    const float4 hd = __ldg(p);
+    const int4 c0 = __ldg(reinterpret_cast<const int4*>(p + 1));
+    const int4 c1 = __ldg(reinterpret_cast<const int4*>(p + 2));
+    const uint4 qx = __ldg(reinterpret_cast<const uint4*>(p + 3));
+    const uint4 qy = __ldg(reinterpret_cast<const uint4*>(p + 4));
+    const uint4 qz = __ldg(reinterpret_cast<const uint4*>(p + 5));
+    const uint32_t meta = __float_as_uint(hd.w);
+    const float sx = __uint_as_float((meta & 0xffu) << 23);
+    const float sy = __uint_as_float(((meta >> 8) & 0xffu) << 23);
+    const float sz = __uint_as_float(((meta >> 16) & 0xffu) << 23);
+    const uint32_t valid = meta >> 24;
+    const bool nx = r.oct & 1u, ny = r.oct & 2u, nz = r.oct & 4u;
+    // near / far plane bytes of slots 0-3 (A) and 4-7 (B) for this ray's octant
+    const uint32_t nxA = nx ? qx.z : qx.x, nxB = nx ? qx.w : qx.y, fxA = nx ? qx.x : qx.z, fxB = nx ? qx.y : qx.w;
+    const uint32_t nyA = ny ? qy.z : qy.x, nyB = ny ? qy.w : qy.y, fyA = ny ? qy.x : qy.z, fyB = ny ? qy.y : qy.w;
+    const uint32_t nzA = nz ? qz.z : qz.x, nzB = nz ? qz.w : qz.y, fzA = nz ? qz.x : qz.z, fzB = nz ? qz.y : qz.w;
+    ch[0] = c0.x; ch[1] = c0.y; ch[2] = c0.z; ch[3] = c0.w;
+    ch[4] = c1.x; ch[5] = c1.y; ch[6] = c1.z; ch[7] = c1.w;
+    uint32_t mask = 0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        // byte (i & 3) of the word as the float 2^23 + q
+        const uint32_t sel = 0x7540u | uint32_t(i & 3);
+        const float qnx = __uint_as_float(__byte_perm(i < 4 ? nxA : nxB, 0x4B000000u, sel));
+        const float qfx = __uint_as_float(__byte_perm(i < 4 ? fxA : fxB, 0x4B000000u, sel));
+        const float qny = __uint_as_float(__byte_perm(i < 4 ? nyA : nyB, 0x4B000000u, sel));
+        const float qfy = __uint_as_float(__byte_perm(i < 4 ? fyA : fyB, 0x4B000000u, sel));
+        const float qnz = __uint_as_float(__byte_perm(i < 4 ? nzA : nzB, 0x4B000000u, sel));
+        const float qfz = __uint_as_float(__byte_perm(i < 4 ? fzA : fzB, 0x4B000000u, sel));
+        const float ax = (fmaf(qnx, sx, hd.x) - r.o.x) * r.inv.x;
+        const float bx = (fmaf(qfx, sx, hd.x) - r.o.x) * r.inv.x;
+        const float ay = (fmaf(qny, sy, hd.y) - r.o.y) * r.inv.y;
+        const float by = (fmaf(qfy, sy, hd.y) - r.o.y) * r.inv.y;
+        const float az = (fmaf(qnz, sz, hd.z) - r.o.z) * r.inv.z;
+        const float bz = (fmaf(qfz, sz, hd.z) - r.o.z) * r.inv.z;
+        float t0 = fmaxf(fmaxf(ax, ay), fmaxf(az, r.tmin));
+        float t1 = fminf(fminf(bx, by), fminf(bz, best));
+        t1 = t1 + fabsf(t1) * kBoxSlack;
+        tn[i] = t0;
+        if (t0 <= t1) mask |= 1u << i;
+    }
+    return mask & valid;
+}
+
+// Slot permutation s -> s ^ oct applied to an 8-bit mask.
+__device__ __forceinline__ uint32_t octant_order(uint32_t m, uint32_t oct) {
+    if (oct & 1u) m = ((m & 0x55u) << 1) | ((m >> 1) & 0x55u);
+    if (oct & 2u) m = ((m & 0x33u) << 2) | ((m >> 2) & 0x33u);
+    if (oct & 4u) m = ((m & 0x0Fu) << 4) | ((m >> 4) & 0x0Fu);
+    return m;
+}
+
 struct Counters {
     unsigned long long rays, nodes, tris;
 };
@@ -131,7 +193,7 @@ __device__ __forceinline__ void trav_init(TravState& s, float4 a, float4 b) {
 }
 
 // Runs at most `steps` node / leaf visits.  Returns true when the ray is done.
-template <bool ANY, bool COUNT>
+template <bool ANY, bool COUNT, int WIDTH>
 __device__ __forceinline__ bool trav_steps(const DevScene& S, TravState& s, int2* stack, int steps, Counters& cnt) {
     for (int it = 0; it < steps; ++it) {
         int item = s.item;
@@ -147,7 +209,32 @@ __device__ __forceinline__ bool trav_steps(const DevScene& S, TravState& s, int2
             }
             if (!found) return true;
         }
-        if (item >= 0) {
+        if (WIDTH == 8 && item >= 0) {
+            float tn[8];
+            int32_t ch[8];
+            if (COUNT) ++cnt.nodes;
+            const uint32_t mask = box8(S.nodes8, item, s.r, s.best, tn, ch);
+            if (mask == 0) { s.item = kNone; continue; }
+            // visit order i = slot ^ octant: continue with the first hit, push the
+            // others so that they pop in visit order
+            const uint32_t om = octant_order(mask, s.r.oct);
+            const uint32_t rest = om & (om - 1u);
+            const int first = __ffs(om) - 1;
+            const int nrest = __popc(rest);
+            if (s.sp + nrest > kStackSize8) {
+                atomicOr(S.errflags, BG_FLAG_STACK_OVERFLOW);
+                return true;
+            }
+            int next = kNone;
+#pragma unroll
+            for (int sl = 0; sl < 8; ++sl) {
+                const int i = sl ^ int(s.r.oct);
+                if ((rest >> i) & 1u) stack[s.sp + __popc(rest >> (i + 1))] = make_int2(ch[sl], __float_as_int(tn[sl]));
+                if (i == first) next = ch[sl];
+            }
+            s.sp += nrest;
+            s.item = next;
+        } else if (WIDTH == 4 && item >= 0) {
             float tn[4];
             int32_t ch[4];
             if (COUNT) ++cnt.nodes;

@@ -172,32 +172,34 @@ def raycast_c2(ctx, nrays=1 << 24, reps=5):
     from banshee_b200 import capi, scenes
     gs = capi.GpuScene(ctx, scenes.soup(1 << 20, seed=1))
     info = gs.info()
-    out = {"triangles": info["ntriangles"], "rays_per_set": nrays, "bvh_nodes": info["nnodes"],
-           "build_ms": info["build_ms"]}
-    for kind in ("coherent", "incoherent"):
-        for anyhit in (False, True):
-            rays = scenes.soup_rays(nrays, kind, seed=2, any_hit=anyhit)
-            dr = torch.from_numpy(rays.view(np.uint8)).cuda()
-            res = torch.zeros(nrays * (1 if anyhit else 16), dtype=torch.uint8, device="cuda")
-            fn = gs.intersect_any if anyhit else gs.intersect_closest
-            for _ in range(2):
-                fn(dr.data_ptr(), res.data_ptr(), nrays)
-            torch.cuda.synchronize()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record()
-            for _ in range(reps):
-                fn(dr.data_ptr(), res.data_ptr(), nrays)
-            e1.record()
-            torch.cuda.synchronize()
-            ms = e0.elapsed_time(e1) / reps
-            sub = torch.from_numpy(np.ascontiguousarray(rays[::64]).view(np.uint8)).cuda()
-            nodes, tris = gs.traversal_counts(sub.data_ptr(), sub.numel() // 32, anyhit)
-            nsub = sub.numel() // 32
-            bpr = 32 + (1 if anyhit else 16) + info["node_stride"] * nodes / nsub + 48 * tris / nsub
-            out[kind + ("_any" if anyhit else "_closest")] = {
-                "mrays_per_s": nrays / ms / 1e3, "ms": ms, "nodes_per_ray": nodes / nsub, "tris_per_ray": tris / nsub,
-                "bytes_per_ray": bpr, "achieved_gbs": bpr * nrays / (ms * 1e-3) / 1e9}
-            del dr, res, sub
+    out = {"triangles": info["ntriangles"], "rays_per_set": nrays, "build_ms": info["build_ms"]}
+    for width, kind, anyhit in [(w, k, a) for w in (4, 8) for k in ("coherent", "incoherent") for a in (False, True)]:
+        gs.set_node_width(width)
+        info = gs.info()
+        lay = out.setdefault("layout%d" % width, {"node_width": width, "bvh_nodes": info["nnodes"],
+                                                   "node_bytes": info["node_stride"]})
+        rays = scenes.soup_rays(nrays, kind, seed=2, any_hit=anyhit)
+        dr = torch.from_numpy(rays.view(np.uint8)).cuda()
+        res = torch.zeros(nrays * (1 if anyhit else 16), dtype=torch.uint8, device="cuda")
+        fn = gs.intersect_any if anyhit else gs.intersect_closest
+        for _ in range(2):
+            fn(dr.data_ptr(), res.data_ptr(), nrays)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn(dr.data_ptr(), res.data_ptr(), nrays)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        sub = torch.from_numpy(np.ascontiguousarray(rays[::64]).view(np.uint8)).cuda()
+        nodes, tris = gs.traversal_counts(sub.data_ptr(), sub.numel() // 32, anyhit)
+        nsub = sub.numel() // 32
+        bpr = 32 + (1 if anyhit else 16) + info["node_stride"] * nodes / nsub + 48 * tris / nsub
+        lay[kind + ("_any" if anyhit else "_closest")] = {
+            "mrays_per_s": nrays / ms / 1e3, "ms": ms, "nodes_per_ray": nodes / nsub, "tris_per_ray": tris / nsub,
+            "bytes_per_ray": bpr, "achieved_gbs": bpr * nrays / (ms * 1e-3) / 1e9}
+        del dr, res, sub
     gs.close()
     return out
 

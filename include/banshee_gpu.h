@@ -142,7 +142,9 @@ typedef struct bg_camera_desc {
 } bg_camera_desc;
 
 typedef struct bg_build_opts {
-    int32_t node_width;     /* BVH fan-out: 4 (0 = default 4)           */
+    int32_t node_width;     /* BVH layout: 4 (128-byte nodes), 8 (96-byte
+                               compressed nodes) or 0 = build both, the
+                               active one switchable (bg_scene_set_node_width) */
     int32_t max_leaf_size;  /* triangles per leaf, 1..16 (0 = default 4)*/
     int32_t sah_bins;       /* binned-SAH bins (0 = default 32)         */
     int32_t reserved;
@@ -161,6 +163,8 @@ typedef struct bg_scene_info {
     int32_t nmaterials;
     int32_t nlights;
     double  build_ms;       /* host build + upload time                   */
+    int32_t node_width;     /* active node layout: 4 or 8                  */
+    int32_t node_widths;    /* layouts built: 4 | 8                        */
 } bg_scene_info;
 
 /* ---------------------------------------------------------------- tracing */
@@ -236,6 +240,9 @@ int bg_scene_set_background(bg_scene* scene, const float rgb[3]);
 int bg_scene_commit(bg_scene* scene, const bg_build_opts* opts);
 int bg_scene_info_get(bg_scene* scene, bg_scene_info* info);
 int bg_scene_error_flags(bg_scene* scene, uint32_t* flags, int32_t clear);
+/* Selects the node layout traversal uses (4 or 8; it must have been built).
+ * No counterpart in the reference, whose Bvh has one binary layout. */
+int bg_scene_set_node_width(bg_scene* scene, int32_t width);
 
 /* Closest hit: replaces World::Intersect(ray, Hit&) -> Bvh::Intersect
  * (world/world.cpp:19-23, accelerator/bvh.cpp:499-573).  A triangle is
@@ -306,6 +313,7 @@ typedef struct bg_tune_result {
     int32_t candidates;        /* configurations timed                       */
     float ms;                  /* time of the best probe render              */
     float msamples_per_s;      /* its throughput                             */
+    int32_t node_width;        /* node layout chosen (4 or 8)                */
 } bg_tune_result;
 
 int bg_batch_create(bg_ctx* ctx, bg_batch** out);
@@ -316,7 +324,8 @@ int bg_batch_commit(bg_batch* batch);
 int bg_batch_info(bg_batch* batch, bg_scene_info* info);
 int bg_batch_render(bg_batch* batch, const bg_batch_job* jobs, int32_t njobs, const bg_tracer_desc* tracer,
                     bg_render_stats* stats, void* stream);
-/* Times traversal block sizes {128, 256} x paths per pass {2^19 .. 2^22} on
+/* Times node layouts {4-wide, 8-wide compressed} (those every scene built) x
+ * traversal block sizes {128, 256} x paths per pass {2^19 .. 2^22} on
  * the jobs with spp capped at probe_spp and keeps the fastest for later
  * bg_batch_render calls.  The jobs' accumulation buffers receive the probe
  * samples: clear them before the real render.  Synchronises. */

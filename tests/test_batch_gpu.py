@@ -44,7 +44,8 @@ def test_batch_jobs_match_single_scene_renders(ctx, tune):
             jobs.append(dict(scene=k, width=sc.width, height=sc.height, spp=spp, seed=seed, accum_dev=acc.data_ptr()))
     if tune:
         res = batch.autotune(jobs, probe_spp=1, maxdepth=maxdepth)
-        assert res["candidates"] == 8 and res["trace_threads"] in (128, 256)
+        assert res["candidates"] == 16 and res["trace_threads"] in (128, 256) and res["node_width"] in (4, 8)
+        assert batch.info()["node_width"] == res["node_width"]
         for b in bufs:
             b.zero_()
     batch.render(jobs, maxdepth=maxdepth)

@@ -1,6 +1,8 @@
 """Ray-cast parity on the GPU: closest-hit primitive ids bit-exact with the
 oracle (exact-t ties classified), hit t / barycentrics bit-exact, any-hit
-occlusion bits exact; through the C ABI (host and device entry points)."""
+occlusion bits exact; through the C ABI (host and device entry points).
+Every test runs on both node layouts: 4-wide 128-byte nodes and 8-wide
+96-byte compressed nodes."""
 import os
 
 import numpy as np
@@ -8,7 +10,7 @@ import pytest
 
 from banshee_b200 import abi, scenes
 
-pytestmark = pytest.mark.gpu
+pytestmark = [pytest.mark.gpu, pytest.mark.parametrize("width", [4, 8])]
 GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 
@@ -37,11 +39,12 @@ def classify(oracle, rays, got, want):
     return ties, unexplained
 
 
-def test_golden_soup_closest_and_any(ctx):
+def test_golden_soup_closest_and_any(width, ctx):
     from banshee_b200 import capi
     from tests.golden.make_golden import SOUP
     g = np.load(os.path.join(GOLD, "raycast_soup.npz"))
     gs = capi.GpuScene(ctx, scenes.soup(**SOUP))
+    gs.set_node_width(width)
     for kind in ("incoherent", "coherent"):
         rays, want = g[kind + "_rays"], g[kind + "_hits"]
         got = gs.intersect_closest_host(rays)
@@ -55,21 +58,23 @@ def test_golden_soup_closest_and_any(ctx):
     assert gs.error_flags() == 0
 
 
-def test_golden_cornell_transformed_bundles(ctx):
+def test_golden_cornell_transformed_bundles(width, ctx):
     from banshee_b200 import capi
     from tests.golden.make_golden import CORNELL
     g = np.load(os.path.join(GOLD, "raycast_cornell.npz"))
     gs = capi.GpuScene(ctx, scenes.cornell(**CORNELL))
+    gs.set_node_width(width)
     got = gs.intersect_closest_host(g["rays"])
     assert (got["primid"] == g["hits"]["primid"]).all()
     assert (_bits(got["t"]) == _bits(g["hits"]["t"])).all()
 
 
 @pytest.mark.parametrize("kind", ["incoherent", "coherent"])
-def test_soup_100k_vs_oracle(ctx, oracle_built, kind):
+def test_soup_100k_vs_oracle(width, ctx, oracle_built, kind):
     from banshee_b200 import capi
     sc = scenes.soup(100_000, seed=11)
     gs = capi.GpuScene(ctx, sc)
+    gs.set_node_width(width)
     o = oracle_built.Oracle(sc)
     rays = scenes.soup_rays(1 << 16, kind, seed=12)
     want = o.intersect_closest(rays)
@@ -84,11 +89,12 @@ def test_soup_100k_vs_oracle(ctx, oracle_built, kind):
     assert gs.error_flags() == 0
 
 
-def test_device_entry_points_and_edge_cases(ctx, oracle_built):
+def test_device_entry_points_and_edge_cases(width, ctx, oracle_built):
     import torch
     from banshee_b200 import capi
     sc = scenes.soup(20_000, seed=4)
     gs = capi.GpuScene(ctx, sc)
+    gs.set_node_width(width)
     o = oracle_built.Oracle(sc)
     rays = scenes.soup_rays(10_007, "incoherent", seed=5)          # ragged size
     # edge cases: zero-length interval, tmin > tmax, axis-parallel directions, -0 components
@@ -116,12 +122,13 @@ def test_device_entry_points_and_edge_cases(ctx, oracle_built):
         gs.intersect_closest(dr.data_ptr() + 4, dh.data_ptr(), 10)
 
 
-def test_one_triangle_scene_and_uncommitted_errors(ctx):
+def test_one_triangle_scene_and_uncommitted_errors(width, ctx):
     from banshee_b200 import capi
     from banshee_b200.scene import Mesh, Scene, lambert
     m = Mesh([[0, 0, 0], [1, 0, 0], [0, 1, 0]], [[0, 0, 1]], [[0, 1, 2]], [[0, 0, 0]], [0])
     sc = Scene(meshes=[m], materials=[lambert((0.5, 0.5, 0.5))])
     gs = capi.GpuScene(ctx, sc)
+    gs.set_node_width(width)
     rays = np.zeros(3, dtype=abi.RAY_DTYPE)
     rays["o"] = [(0.2, 0.2, 1.0), (2.0, 2.0, 1.0), (0.0, 0.0, 1.0)]
     rays["d"] = (0.0, 0.0, -1.0)
@@ -131,14 +138,15 @@ def test_one_triangle_scene_and_uncommitted_errors(ctx):
     assert hits["t"][0] == np.float32(1.0)
 
 
-def test_full_size_soup_properties(ctx):
+def test_full_size_soup_properties(width, ctx):
     """1M triangles, 1M incoherent rays: size-independent properties (every
     reported hit is accepted by the per-triangle test, results are idempotent)."""
     from banshee_b200 import capi
     sc = scenes.soup(1 << 20, seed=1)
     gs = capi.GpuScene(ctx, sc)
+    gs.set_node_width(width)
     info = gs.info()
-    assert info["ntriangles"] == 1 << 20 and info["max_stack"] <= 64
+    assert info["ntriangles"] == 1 << 20 and info["max_stack"] <= (96 if width == 8 else 64)
     rays = scenes.soup_rays(1 << 20, "incoherent", seed=2)
     h1 = gs.intersect_closest_host(rays)
     h2 = gs.intersect_closest_host(rays)
@@ -147,3 +155,24 @@ def test_full_size_soup_properties(ctx):
     assert 0.3 < hit.mean() < 1.0
     assert (h1["t"][hit] > rays["tmin"][hit]).all()
     assert gs.error_flags() == 0
+
+
+def test_layout_info_and_work(width, ctx):
+    """The active layout is reported, and the 8-wide tree visits fewer nodes."""
+    from banshee_b200 import capi
+    gs = capi.GpuScene(ctx, scenes.soup(200_000, seed=3))
+    gs.set_node_width(width)
+    info = gs.info()
+    assert info["node_width"] == width and info["node_widths"] == 12
+    assert info["node_stride"] == (96 if width == 8 else 128)
+    assert info["node_bytes"] == info["nnodes"] * info["node_stride"]
+    import torch
+    rays = scenes.soup_rays(1 << 15, "incoherent", seed=4)
+    dr = torch.from_numpy(rays.view(np.uint8)).cuda()
+    n_this, t_this = gs.traversal_counts(dr.data_ptr(), rays.shape[0])
+    gs.set_node_width(12 - width)
+    n_other, t_other = gs.traversal_counts(dr.data_ptr(), rays.shape[0])
+    if width == 8:
+        assert n_this < 0.8 * n_other, (n_this, n_other)
+    with pytest.raises(capi.BansheeError):
+        gs.set_node_width(2)

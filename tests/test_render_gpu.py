@@ -24,30 +24,35 @@ def ctx():
     return capi.Context(0)
 
 
-def _render(ctx, sc, spp, seed, tracer, maxdepth, **kw):
+def _render(ctx, sc, spp, seed, tracer, maxdepth, width=4, **kw):
     from banshee_b200 import capi
     gs = capi.GpuScene(ctx, sc)
+    gs.set_node_width(width)
     img = gs.render_host(sc.width, sc.height, spp, seed=seed, tracer=tracer, maxdepth=maxdepth, **kw)
     assert gs.error_flags() == 0
     return img
 
 
+@pytest.mark.parametrize("width", [4, 8])
 @pytest.mark.parametrize("tracer", ["gi", "di"])
-def test_cornell_matches_reference_golden(ctx, tracer):
+def test_cornell_matches_reference_golden(ctx, tracer, width):
     from tests.golden.make_golden import CORNELL
     g = np.load(os.path.join(GOLD, "render_cornell.npz"))
     kind = abi.BG_TRACER_GI if tracer == "gi" else abi.BG_TRACER_DI
-    img = _render(ctx, scenes.cornell(**CORNELL), int(g["spp"]), int(g["seed"]), kind, int(g["maxdepth"]))
+    img = _render(ctx, scenes.cornell(**CORNELL), int(g["spp"]), int(g["seed"]), kind, int(g["maxdepth"]),
+                  width=width)
     ref = g[tracer]
     assert (img[..., 3] == ref[..., 3]).all()          # sample counts
     e = relmse(mean_image(img), mean_image(ref))
     assert e < TOL, e
 
 
-def test_production_ggx_matches_reference_golden(ctx):
+@pytest.mark.parametrize("width", [4, 8])
+def test_production_ggx_matches_reference_golden(ctx, width):
     from tests.golden.make_golden import PROD
     g = np.load(os.path.join(GOLD, "render_production.npz"))
-    img = _render(ctx, scenes.production(**PROD), int(g["spp"]), int(g["seed"]), abi.BG_TRACER_GI, int(g["maxdepth"]))
+    img = _render(ctx, scenes.production(**PROD), int(g["spp"]), int(g["seed"]), abi.BG_TRACER_GI, int(g["maxdepth"]),
+                  width=width)
     e = relmse(mean_image(img), mean_image(g["gi"]))
     assert e < TOL, e
 
@@ -61,9 +66,10 @@ def test_cornell_vs_oracle_larger(ctx, oracle_built, maxdepth):
     assert e < TOL, e
 
 
-def test_production_vs_oracle_larger(ctx, oracle_built):
+@pytest.mark.parametrize("width", [4, 8])
+def test_production_vs_oracle_larger(ctx, oracle_built, width):
     sc = scenes.production(160, 90, nterrain=96, nspheres=24, sphere_seg=16, seed=5)
-    img = _render(ctx, sc, 4, 4, abi.BG_TRACER_GI, 8)
+    img = _render(ctx, sc, 4, 4, abi.BG_TRACER_GI, 8, width=width)
     ref = oracle_built.Oracle(sc).render(spp=4, seed=4, maxdepth=8)
     e = relmse(mean_image(img), mean_image(ref))
     assert e < TOL, e
