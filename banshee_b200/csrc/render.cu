@@ -321,7 +321,7 @@ __device__ __noinline__ void emit_di(const DevScene& S, const Queues& Q, int li,
     }
 }
 
-__global__ void __launch_bounds__(kShadeThreads, 3)
+__global__ void __launch_bounds__(kShadeThreads, 8)
 k_shade(DevScene S, ShadeArgs A, PathState P, Queues Q) {
     const int n = *Q.n_ext_in;
     const int nthreads = gridDim.x * blockDim.x;

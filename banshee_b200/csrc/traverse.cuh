@@ -82,24 +82,27 @@ __device__ __forceinline__ void obj_ray(const DevScene& S, const Ray& r, int b, 
 // Test the 4 children of node `ni`; returns a hit mask and entry distances.
 __device__ __forceinline__ uint32_t box4(const WideNode4* __restrict__ nodes, int ni, const Ray& r, float best,
                                          float tn[4], int32_t ch[4]) {
+    // the near / far planes of each axis are picked by load address (the node
+    // stores lo and hi of an axis in adjacent float4s), not by per-plane selects
     const float4* p = reinterpret_cast<const float4*>(nodes + ni);
-    float4 lx = __ldg(p + 0), hx = __ldg(p + 1), ly = __ldg(p + 2), hy = __ldg(p + 3);
-    float4 lz = __ldg(p + 4), hz = __ldg(p + 5);
+    const int fx = int(r.oct & 1u), fy = int((r.oct >> 1) & 1u), fz = int((r.oct >> 2) & 1u);
+    const float4 nx4 = __ldg(p + fx), fx4 = __ldg(p + (1 - fx));
+    const float4 ny4 = __ldg(p + 2 + fy), fy4 = __ldg(p + 3 - fy);
+    const float4 nz4 = __ldg(p + 4 + fz), fz4 = __ldg(p + 5 - fz);
     int4 c = __ldg(reinterpret_cast<const int4*>(p + 6));
-    const bool nx = r.oct & 1u, ny = r.oct & 2u, nz = r.oct & 4u;
-    float lxa[4] = {lx.x, lx.y, lx.z, lx.w}, hxa[4] = {hx.x, hx.y, hx.z, hx.w};
-    float lya[4] = {ly.x, ly.y, ly.z, ly.w}, hya[4] = {hy.x, hy.y, hy.z, hy.w};
-    float lza[4] = {lz.x, lz.y, lz.z, lz.w}, hza[4] = {hz.x, hz.y, hz.z, hz.w};
+    const float nxa[4] = {nx4.x, nx4.y, nx4.z, nx4.w}, fxa[4] = {fx4.x, fx4.y, fx4.z, fx4.w};
+    const float nya[4] = {ny4.x, ny4.y, ny4.z, ny4.w}, fya[4] = {fy4.x, fy4.y, fy4.z, fy4.w};
+    const float nza[4] = {nz4.x, nz4.y, nz4.z, nz4.w}, fza[4] = {fz4.x, fz4.y, fz4.z, fz4.w};
     ch[0] = c.x; ch[1] = c.y; ch[2] = c.z; ch[3] = c.w;
     uint32_t mask = 0;
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-        float ax = ((nx ? hxa[i] : lxa[i]) - r.o.x) * r.inv.x;
-        float bx = ((nx ? lxa[i] : hxa[i]) - r.o.x) * r.inv.x;
-        float ay = ((ny ? hya[i] : lya[i]) - r.o.y) * r.inv.y;
-        float by = ((ny ? lya[i] : hya[i]) - r.o.y) * r.inv.y;
-        float az = ((nz ? hza[i] : lza[i]) - r.o.z) * r.inv.z;
-        float bz = ((nz ? lza[i] : hza[i]) - r.o.z) * r.inv.z;
+        float ax = (nxa[i] - r.o.x) * r.inv.x;
+        float bx = (fxa[i] - r.o.x) * r.inv.x;
+        float ay = (nya[i] - r.o.y) * r.inv.y;
+        float by = (fya[i] - r.o.y) * r.inv.y;
+        float az = (nza[i] - r.o.z) * r.inv.z;
+        float bz = (fza[i] - r.o.z) * r.inv.z;
         float t0 = fmaxf(fmaxf(ax, ay), fmaxf(az, r.tmin));
         float t1 = fminf(fminf(bx, by), fminf(bz, best));
         t1 = t1 + fabsf(t1) * kBoxSlack;
@@ -126,11 +129,14 @@ __device__ __forceinline__ uint32_t box8(const QNode8* __restrict__ nodes, int n
     const float sy = __uint_as_float(((meta >> 8) & 0xffu) << 23);
     const float sz = __uint_as_float(((meta >> 16) & 0xffu) << 23);
     const uint32_t valid = meta >> 24;
+    // near / far plane bytes of slots 0-3 (.x) and 4-7 (.y) for this ray's octant
     const bool nx = r.oct & 1u, ny = r.oct & 2u, nz = r.oct & 4u;
-    // near / far plane bytes of slots 0-3 (A) and 4-7 (B) for this ray's octant
-    const uint32_t nxA = nx ? qx.z : qx.x, nxB = nx ? qx.w : qx.y, fxA = nx ? qx.x : qx.z, fxB = nx ? qx.y : qx.w;
-    const uint32_t nyA = ny ? qy.z : qy.x, nyB = ny ? qy.w : qy.y, fyA = ny ? qy.x : qy.z, fyB = ny ? qy.y : qy.w;
-    const uint32_t nzA = nz ? qz.z : qz.x, nzB = nz ? qz.w : qz.y, fzA = nz ? qz.x : qz.z, fzB = nz ? qz.y : qz.w;
+    const uint2 qnx = nx ? make_uint2(qx.z, qx.w) : make_uint2(qx.x, qx.y);
+    const uint2 qfx = nx ? make_uint2(qx.x, qx.y) : make_uint2(qx.z, qx.w);
+    const uint2 qny = ny ? make_uint2(qy.z, qy.w) : make_uint2(qy.x, qy.y);
+    const uint2 qfy = ny ? make_uint2(qy.x, qy.y) : make_uint2(qy.z, qy.w);
+    const uint2 qnz = nz ? make_uint2(qz.z, qz.w) : make_uint2(qz.x, qz.y);
+    const uint2 qfz = nz ? make_uint2(qz.x, qz.y) : make_uint2(qz.z, qz.w);
     ch[0] = c0.x; ch[1] = c0.y; ch[2] = c0.z; ch[3] = c0.w;
     ch[4] = c1.x; ch[5] = c1.y; ch[6] = c1.z; ch[7] = c1.w;
     uint32_t mask = 0;
@@ -138,18 +144,18 @@ __device__ __forceinline__ uint32_t box8(const QNode8* __restrict__ nodes, int n
     for (int i = 0; i < 8; ++i) {
         // byte (i & 3) of the word as the float 2^23 + q
         const uint32_t sel = 0x7540u | uint32_t(i & 3);
-        const float qnx = __uint_as_float(__byte_perm(i < 4 ? nxA : nxB, 0x4B000000u, sel));
-        const float qfx = __uint_as_float(__byte_perm(i < 4 ? fxA : fxB, 0x4B000000u, sel));
-        const float qny = __uint_as_float(__byte_perm(i < 4 ? nyA : nyB, 0x4B000000u, sel));
-        const float qfy = __uint_as_float(__byte_perm(i < 4 ? fyA : fyB, 0x4B000000u, sel));
-        const float qnz = __uint_as_float(__byte_perm(i < 4 ? nzA : nzB, 0x4B000000u, sel));
-        const float qfz = __uint_as_float(__byte_perm(i < 4 ? fzA : fzB, 0x4B000000u, sel));
-        const float ax = (fmaf(qnx, sx, hd.x) - r.o.x) * r.inv.x;
-        const float bx = (fmaf(qfx, sx, hd.x) - r.o.x) * r.inv.x;
-        const float ay = (fmaf(qny, sy, hd.y) - r.o.y) * r.inv.y;
-        const float by = (fmaf(qfy, sy, hd.y) - r.o.y) * r.inv.y;
-        const float az = (fmaf(qnz, sz, hd.z) - r.o.z) * r.inv.z;
-        const float bz = (fmaf(qfz, sz, hd.z) - r.o.z) * r.inv.z;
+        const float nqx = __uint_as_float(__byte_perm(i < 4 ? qnx.x : qnx.y, 0x4B000000u, sel));
+        const float fqx = __uint_as_float(__byte_perm(i < 4 ? qfx.x : qfx.y, 0x4B000000u, sel));
+        const float nqy = __uint_as_float(__byte_perm(i < 4 ? qny.x : qny.y, 0x4B000000u, sel));
+        const float fqy = __uint_as_float(__byte_perm(i < 4 ? qfy.x : qfy.y, 0x4B000000u, sel));
+        const float nqz = __uint_as_float(__byte_perm(i < 4 ? qnz.x : qnz.y, 0x4B000000u, sel));
+        const float fqz = __uint_as_float(__byte_perm(i < 4 ? qfz.x : qfz.y, 0x4B000000u, sel));
+        const float ax = (fmaf(nqx, sx, hd.x) - r.o.x) * r.inv.x;
+        const float bx = (fmaf(fqx, sx, hd.x) - r.o.x) * r.inv.x;
+        const float ay = (fmaf(nqy, sy, hd.y) - r.o.y) * r.inv.y;
+        const float by = (fmaf(fqy, sy, hd.y) - r.o.y) * r.inv.y;
+        const float az = (fmaf(nqz, sz, hd.z) - r.o.z) * r.inv.z;
+        const float bz = (fmaf(fqz, sz, hd.z) - r.o.z) * r.inv.z;
         float t0 = fmaxf(fmaxf(ax, ay), fmaxf(az, r.tmin));
         float t1 = fminf(fminf(bx, by), fminf(bz, best));
         t1 = t1 + fabsf(t1) * kBoxSlack;
