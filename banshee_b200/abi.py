@@ -16,7 +16,7 @@ BG_ERR = {
 
 BG_MAT_LAMBERT, BG_MAT_MICROFACET_GGX, BG_MAT_EMISSIVE = 0, 1, 2
 BG_LIGHT_AREA, BG_LIGHT_DIRECTIONAL, BG_LIGHT_ENVIRONMENT = 0, 1, 2
-BG_TRACER_GI, BG_TRACER_DI = 0, 1
+BG_TRACER_GI, BG_TRACER_DI, BG_TRACER_AO = 0, 1, 2
 
 RAY_DTYPE = np.dtype([("o", "<f4", 3), ("tmin", "<f4"), ("d", "<f4", 3), ("tmax", "<f4")])
 HIT_DTYPE = np.dtype([("t", "<f4"), ("primid", "<i4"), ("u", "<f4"), ("v", "<f4")])
@@ -68,17 +68,19 @@ class SceneInfo(C.Structure):
                 ("node_width", C.c_int32), ("node_widths", C.c_int32)]
 
 
+BG_SAMPLER_RANDOM, BG_SAMPLER_SOBOL, BG_SAMPLER_CMJ = 0, 1, 2
+
 BG_RENDER_TIME_PHASES = 0x1
 BG_RENDER_COUNT_TRAVERSAL = 0x2
 
 
 class TracerDesc(C.Structure):
-    _fields_ = [("kind", C.c_int32), ("maxdepth", C.c_int32), ("flags", C.c_int32), ("reserved", C.c_int32)]
+    _fields_ = [("kind", C.c_int32), ("maxdepth", C.c_int32), ("flags", C.c_int32), ("ao_radius", C.c_float)]
 
 
 class SamplerDesc(C.Structure):
     _fields_ = [("kind", C.c_int32), ("spp", C.c_int32), ("seed", C.c_uint64),
-                ("sample_offset", C.c_int32), ("reserved", C.c_int32)]
+                ("sample_offset", C.c_int32), ("grid", C.c_int32)]
 
 
 class RenderStats(C.Structure):

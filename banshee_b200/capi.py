@@ -197,23 +197,25 @@ class GpuScene:
         return a.value, b.value
 
     def render(self, accum_dev, width, height, spp, seed=1, sample_offset=0, tracer=abi.BG_TRACER_GI,
-               maxdepth=5, camera=None, stream=None, flags=0, stats=True):
+               maxdepth=5, camera=None, stream=None, flags=0, stats=True, sampler=abi.BG_SAMPLER_RANDOM, grid=0,
+               ao_radius=0.0):
         """Asynchronous on `stream` unless stats=True (statistics synchronize)."""
         cam = self.scene.camera_desc() if camera is None else camera
-        tr = abi.TracerDesc(tracer, maxdepth, flags, 0)
-        sm = abi.SamplerDesc(0, spp, seed, sample_offset, 0)
+        tr = abi.TracerDesc(tracer, maxdepth, flags, ao_radius)
+        sm = abi.SamplerDesc(sampler, spp, seed, sample_offset, grid)
         st = abi.RenderStats()
         check(lib().bg_render(self.h, C.byref(cam), C.byref(tr), C.byref(sm), int(width), int(height),
                               accum_dev, C.byref(st) if stats else None, _stream_handle(stream)))
         return {k: getattr(st, k) for k, _ in abi.RenderStats._fields_} if stats else None
 
     def render_host(self, width, height, spp, seed=1, sample_offset=0, tracer=abi.BG_TRACER_GI, maxdepth=5,
-                    camera=None, accum=None, stats=None, flags=0):
+                    camera=None, accum=None, stats=None, flags=0, sampler=abi.BG_SAMPLER_RANDOM, grid=0,
+                    ao_radius=0.0):
         cam = self.scene.camera_desc() if camera is None else camera
         if accum is None:
             accum = np.zeros((height, width, 4), dtype=np.float32)
-        tr = abi.TracerDesc(tracer, maxdepth, flags, 0)
-        sm = abi.SamplerDesc(0, spp, seed, sample_offset, 0)
+        tr = abi.TracerDesc(tracer, maxdepth, flags, ao_radius)
+        sm = abi.SamplerDesc(sampler, spp, seed, sample_offset, grid)
         st = abi.RenderStats()
         check(lib().bg_render_host(self.h, C.byref(cam), C.byref(tr), C.byref(sm), int(width), int(height),
                                    accum.ctypes.data, C.byref(st) if stats is not None else None))
@@ -336,13 +338,14 @@ class Batch:
             arr[i].width = j["width"]
             arr[i].height = j["height"]
             arr[i].camera = j.get("camera") or g.scene.camera_desc()
-            arr[i].sampler = abi.SamplerDesc(0, j["spp"], j.get("seed", 1), j.get("sample_offset", 0), 0)
+            arr[i].sampler = abi.SamplerDesc(j.get("sampler", 0), j["spp"], j.get("seed", 1),
+                                             j.get("sample_offset", 0), j.get("grid", 0))
             arr[i].accum_rgbw_dev = j["accum_dev"]
         return arr
 
-    def render(self, jobs, maxdepth=8, tracer=abi.BG_TRACER_GI, stream=None, stats=False, flags=0):
+    def render(self, jobs, maxdepth=8, tracer=abi.BG_TRACER_GI, stream=None, stats=False, flags=0, ao_radius=0.0):
         arr = self._jobs(jobs)
-        tr = abi.TracerDesc(tracer, maxdepth, flags, 0)
+        tr = abi.TracerDesc(tracer, maxdepth, flags, ao_radius)
         st = abi.RenderStats()
         check(lib().bg_batch_render(self.h, arr, len(jobs), C.byref(tr), C.byref(st) if stats else None,
                                     _stream_handle(stream)))

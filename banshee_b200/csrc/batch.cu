@@ -235,7 +235,7 @@ static int batch_jobs(bg_batch* b, const bg_batch_job* jobs, int32_t njobs, std:
     for (int32_t i = 0; i < njobs; ++i) {
         const bg_batch_job& j = jobs[i];
         if (j.scene < 0 || j.scene >= int32_t(b->scenes.size())) return set_error(BG_ERR_INVALID_ARG, "job %d: scene %d out of range", i, j.scene);
-        if (j.sampler.kind != 0) return set_error(BG_ERR_UNSUPPORTED, "job %d: sampler kind %d", i, j.sampler.kind);
+
         JobSpec& J = out[size_t(i)];
         J.rec = b->rec[size_t(j.scene)];
         if (b->merged.dev.width == 8) J.rec.root = b->root8[size_t(j.scene)];
@@ -246,6 +246,8 @@ static int batch_jobs(bg_batch* b, const bg_batch_job* jobs, int32_t njobs, std:
         J.soff = j.sampler.sample_offset;
         J.seed = j.sampler.seed;
         J.accum = reinterpret_cast<float4*>(j.accum_rgbw_dev);
+        J.skind = j.sampler.kind;
+        J.grid = j.sampler.grid;
     }
     return BG_OK;
 }

@@ -25,6 +25,7 @@
 #include "cache.h"
 #include "internal.h"
 #include "render.h"
+#include "samplers.cuh"
 #include "shading.cuh"
 
 namespace bg {
@@ -54,6 +55,7 @@ struct SegRec {
     float4* accum;
     uint64_t seed;
     int job, np, ns, p0, s0, W, H, path0, pix0;   // pix0: prefix sum of np over earlier segments
+    int skind, grid;                               // image sampler of the job
 };
 constexpr int kMaxSegs = 1024;
 
@@ -188,7 +190,7 @@ k_generate(const SegRec* __restrict__ segs, int nseg, int total, PathState P, Qu
         McRng lr{keyed_rand(key, 2), keyed_rand(key, 3)};
         McRng br{keyed_rand(key, 4), keyed_rand(key, 5)};
         float sx, sy;
-        sample2d(img, sx, sy);
+        image_sample(G.skind, G.grid, G.seed, uint32_t(pix), s, img, sx, sy);
         const int x = pix % W, y = pix / W;
         float ix = (float)x / W + (1.f / W) * sx;
         float iy = (float)y / H + (1.f / H) * sy;
@@ -231,6 +233,7 @@ struct ShadeArgs {
     int bounce, maxdepth, kind, kmax, batched;
     int cache_depth;              // -1: plain tracer
     int train_stride, train_phase;
+    float ao_radius;              // BG_TRACER_AO
 };
 
 // Radiance-cache query record of a surface point: position, outgoing
@@ -339,7 +342,9 @@ k_shade(DevScene S, ShadeArgs A, PathState P, Queues Q) {
         int pending = 0;
         bool end = false;
         if (hit.primid < 0) {
-            if (A.bounce == 0) {        // primary miss: bgcolor + sum of GetLe, unclamped (gitracer.cpp:22-33)
+            if (A.kind == BG_TRACER_AO) {
+                flags |= kFlagNoClamp;  // AoTracer: a miss is black (aotracer.cpp:47)
+            } else if (A.bounce == 0) { // primary miss: bgcolor + sum of GetLe, unclamped (gitracer.cpp:22-33)
                 rad = add(rad, mk(J.bg[0], J.bg[1], J.bg[2]));
                 for (int i = J.light0; i < J.light0 + J.nlights; ++i) {
                     LightRec L = load_light(S, i);
@@ -367,7 +372,27 @@ k_shade(DevScene S, ShadeArgs A, PathState P, Queues Q) {
             const unsigned pflags = P.flags[path];
             const bool train = (pflags & kFlagTrain) != 0;
             flags = pflags;
-            if (A.bounce == 0 && M.type == BG_MAT_EMISSIVE) {
+            if (A.kind == BG_TRACER_AO) {
+                // AoTracer::GetLi (aotracer.cpp:9-49), one light-sampler sample:
+                // a cosine ray about the shading normal, t in (0.00002, radius);
+                // the visibility 1 lands in the first slot unless the ray is occluded
+                float ax, ay;
+                sample2d(lr, ax, ay);
+                const v3 dir = map_to_hemisphere(h.n, ax, ay, 1.f);
+                const int base = path * A.kmax;
+                P.slots[size_t(base)] = make_float4(0.f, 0.f, 0.f, 0.f);
+                P.slots[size_t(base) + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
+                const int k = warp_push(Q.n_sh);
+                put_ray(Q.sh_rays, k, h.p, 0.00002f, dir, A.ao_radius);
+                Q.sh_contrib[k] = make_float4(1.f, 1.f, 1.f, 0.f);
+                Q.sh_slot[k] = base;
+                if (root >= 0) Q.sh_root[k] = root;
+                P.dithr[path] = make_float4(1.f, 1.f, 1.f, 1.f);
+                pending = 2;
+                flags |= kFlagNoClamp;
+                P.rng[path] = make_uint4(lr.z, lr.w, br.z, br.w);
+                end = true;
+            } else if (A.bounce == 0 && M.type == BG_MAT_EMISSIVE) {
                 if (A.kind == BG_TRACER_GI) rad = add(rad, emissive_le(M, h.n, wo));   // gitracer.cpp:61-68
                 if (A.kind == BG_TRACER_DI) flags |= kFlagNoClamp;                    // ditracer.cpp:29-32
                 end = true;
@@ -654,6 +679,7 @@ struct PassCfg {
     bool batched;
     bg_cache* cache;           // radiance-cache mode when non-null
     int cache_depth, train_stride, train_phase;
+    float ao_radius;
 };
 
 static void pass_queues(RenderState* rs, int c, bool batched, Queues& Q) {
@@ -724,7 +750,7 @@ static int enqueue_pass(bg_scene* s, RenderState* rs, cudaStream_t st, const Pas
             ++ins->launches;
         }
         ShadeArgs A{b, c.maxdepth, c.kind, rs->kmax, c.batched ? 1 : 0, c.cache ? c.cache_depth : -1,
-                    c.cache ? c.train_stride : 0, c.train_phase};
+                    c.cache ? c.train_stride : 0, c.train_phase, c.ao_radius};
         if (c.cache && b == c.cache_depth) BG_CUDA(cudaMemsetAsync(Q.n_query, 0, sizeof(int), st));
         k_shade<<<nb, kShadeThreads, 0, st>>>(s->dev, A, P, Q);
         if (ins) { ++ins->launches; ins->mark(1); }
@@ -762,7 +788,10 @@ static int enqueue_pass(bg_scene* s, RenderState* rs, cudaStream_t st, const Pas
 // Captures one pass into a CUDA graph (once per bounce-loop shape) and finds
 // the two kernel nodes whose arguments (the segment slice) change per pass.
 static int pass_graph(bg_scene* s, RenderState* rs, const PassCfg& c) {
-    const int64_t key[8] = {c.maxdepth, c.kind, c.batched ? 1 : 0, rs->kmax, int64_t(rs->cap), s->tune_threads, s->dev.width, 0};
+    uint32_t aob;
+    memcpy(&aob, &c.ao_radius, sizeof(aob));
+    const int64_t key[8] = {c.maxdepth, c.kind, c.batched ? 1 : 0, rs->kmax, int64_t(rs->cap), s->tune_threads,
+                            s->dev.width, int64_t(aob)};
     if (rs->exec && memcmp(key, rs->graph_key, sizeof(key)) == 0) return BG_OK;
     if (rs->exec) { cudaGraphExecDestroy(rs->exec); rs->exec = nullptr; }
     if (rs->graph) { cudaGraphDestroy(rs->graph); rs->graph = nullptr; }
@@ -831,6 +860,7 @@ static void plan_passes(const std::vector<JobSpec>& jobs, int64_t cap, std::vect
                 int ns = int(std::max<int64_t>(1, std::min<int64_t>(J.spp - s0, cap / npix)));
                 SegRec g{};
                 g.cam = J.cam; g.accum = J.accum; g.seed = J.seed; g.job = int(j);
+                g.skind = J.skind; g.grid = J.grid;
                 g.np = int(npix); g.ns = ns; g.p0 = 0; g.s0 = J.soff + s0; g.W = J.W; g.H = J.H;
                 all.push_back(g);
                 s0 += ns;
@@ -840,6 +870,8 @@ static void plan_passes(const std::vector<JobSpec>& jobs, int64_t cap, std::vect
                 for (int64_t p0 = 0; p0 < npix; p0 += cap) {
                     SegRec g{};
                     g.cam = J.cam; g.accum = J.accum; g.seed = J.seed; g.job = int(j);
+                    g.skind = J.skind; g.grid = J.grid;
+                g.skind = J.skind; g.grid = J.grid;
                     g.np = int(std::min<int64_t>(cap, npix - p0)); g.ns = 1; g.p0 = int(p0); g.s0 = J.soff + s;
                     g.W = J.W; g.H = J.H;
                     all.push_back(g);
@@ -878,7 +910,10 @@ int render_jobs(bg_scene* s, bg_cache* cache, const std::vector<JobSpec>& jobs, 
     if (!s) return set_error(BG_ERR_INVALID_ARG, "scene is NULL");
     if (!s->committed) return set_error(BG_ERR_STATE, "scene not committed");
     if (!tr) return set_error(BG_ERR_INVALID_ARG, "NULL tracer");
-    if (tr->kind != BG_TRACER_GI && tr->kind != BG_TRACER_DI) return set_error(BG_ERR_UNSUPPORTED, "tracer kind %d", tr->kind);
+    if (tr->kind != BG_TRACER_GI && tr->kind != BG_TRACER_DI && tr->kind != BG_TRACER_AO)
+        return set_error(BG_ERR_UNSUPPORTED, "tracer kind %d", tr->kind);
+    if (tr->kind == BG_TRACER_AO && !std::isfinite(tr->ao_radius))
+        return set_error(BG_ERR_INVALID_ARG, "AO radius must be finite");
     if (tr->kind == BG_TRACER_GI && (tr->maxdepth < 0 || tr->maxdepth > 1024)) return set_error(BG_ERR_INVALID_ARG, "maxdepth %d", tr->maxdepth);
     if (jobs.empty()) return BG_OK;
     if (jobs.size() > 65535) return set_error(BG_ERR_INVALID_ARG, "too many jobs (%zu > 65535)", jobs.size());
@@ -887,6 +922,11 @@ int render_jobs(bg_scene* s, bg_cache* cache, const std::vector<JobSpec>& jobs, 
     for (const JobSpec& J : jobs) {
         if (J.W <= 0 || J.H <= 0 || int64_t(J.W) * J.H > (int64_t(1) << 28)) return set_error(BG_ERR_INVALID_ARG, "bad resolution %dx%d", J.W, J.H);
         if (J.spp < 0 || J.soff < 0) return set_error(BG_ERR_INVALID_ARG, "negative spp / sample offset");
+        if (int64_t(J.soff) + J.spp > (int64_t(1) << 31)) return set_error(BG_ERR_INVALID_ARG, "sample indices must stay below 2^31");
+        if (J.skind != BG_SAMPLER_RANDOM && J.skind != BG_SAMPLER_SOBOL && J.skind != BG_SAMPLER_CMJ)
+            return set_error(BG_ERR_UNSUPPORTED, "sampler kind %d", J.skind);
+        if (J.skind == BG_SAMPLER_CMJ && (J.grid < 1 || J.grid > 16))
+            return set_error(BG_ERR_INVALID_ARG, "CMJ grid %d outside 1..16", J.grid);
         if (!J.accum || (reinterpret_cast<uintptr_t>(J.accum) & 15u)) return set_error(BG_ERR_INVALID_ARG, "accumulation buffer must be non-NULL and 16-byte aligned");
         if (J.rec.nlights <= 0) return set_error(BG_ERR_UNSUPPORTED, "a scene without lights (GiTracer divides by the light count)");
         maxL = std::max(maxL, J.rec.nlights);
@@ -898,7 +938,7 @@ int render_jobs(bg_scene* s, bg_cache* cache, const std::vector<JobSpec>& jobs, 
     int rc = ensure_state(s, cap, maxL);
     if (rc) return rc;
     RenderState* rs = s->render;   // buffers may be larger than this call's pass size
-    const int maxdepth = tr->kind == BG_TRACER_DI ? 1 : tr->maxdepth;
+    const int maxdepth = tr->kind == BG_TRACER_GI ? tr->maxdepth : 1;
     unsigned long long* totals = reinterpret_cast<unsigned long long*>(rs->counts.as<char>() + 64);
 
     std::vector<SegRec> segs;
@@ -994,6 +1034,7 @@ int render_jobs(bg_scene* s, bg_cache* cache, const std::vector<JobSpec>& jobs, 
         }
         c.maxdepth = maxdepth;
         c.kind = tr->kind;
+        c.ao_radius = tr->kind == BG_TRACER_AO ? tr->ao_radius : 0.f;
         c.batched = batched;
         c.cache = cache;
         c.cache_depth = cache_depth;
@@ -1068,7 +1109,6 @@ static int render_impl(bg_scene* s, bg_cache* cache, const bg_camera_desc* cam, 
     if (!s) return set_error(BG_ERR_INVALID_ARG, "scene is NULL");
     if (!s->committed) return set_error(BG_ERR_STATE, "scene not committed");
     if (!cam || !tr || !sm || !accum) return set_error(BG_ERR_INVALID_ARG, "NULL argument");
-    if (sm->kind != 0) return set_error(BG_ERR_UNSUPPORTED, "sampler kind %d", sm->kind);
     std::vector<JobSpec> jobs(1);
     JobSpec& J = jobs[0];
     J.rec.root = 0;
@@ -1078,6 +1118,7 @@ static int render_impl(bg_scene* s, bg_cache* cache, const bg_camera_desc* cam, 
     J.rec.bg[0] = s->dev.bg[0]; J.rec.bg[1] = s->dev.bg[1]; J.rec.bg[2] = s->dev.bg[2]; J.rec.bg[3] = 0.f;
     J.cam = make_camera(cam);
     J.W = W; J.H = H; J.spp = sm->spp; J.soff = sm->sample_offset; J.seed = sm->seed; J.accum = accum;
+    J.skind = sm->kind; J.grid = sm->grid;
     return render_jobs(s, cache, jobs, tr, stats, st, false);
 }
 

@@ -28,6 +28,7 @@ struct JobSpec {       // host-side job description
     int W, H, spp, soff;
     uint64_t seed;
     float4* accum;
+    int skind = 0, grid = 0;   // image sampler (BG_SAMPLER_*), CMJ grid size
 };
 
 CamDev make_camera(const bg_camera_desc* c);

@@ -170,7 +170,8 @@ typedef struct bg_scene_info {
 /* ---------------------------------------------------------------- tracing */
 enum {
     BG_TRACER_GI = 0,       /* GiTracer(maxdepth), tracer/gitracer.cpp    */
-    BG_TRACER_DI = 1        /* DiTracer, tracer/ditracer.cpp:19-55        */
+    BG_TRACER_DI = 1,       /* DiTracer, tracer/ditracer.cpp:19-55        */
+    BG_TRACER_AO = 2        /* AoTracer(radius), tracer/aotracer.cpp:9-49 */
 };
 
 #define BG_RENDER_TIME_PHASES   0x1  /* per-phase CUDA-event timing into bg_render_stats */
@@ -180,7 +181,7 @@ typedef struct bg_tracer_desc {
     int32_t kind;
     int32_t maxdepth;
     int32_t flags;          /* BG_RENDER_* instrumentation bits (0 = none)   */
-    int32_t reserved;
+    float ao_radius;        /* BG_TRACER_AO: occlusion radius (AoTracer ctor) */
 } bg_tracer_desc;
 
 /* Sampler plugin: every camera sample (pixel p, sample index s) gets fresh
@@ -192,12 +193,31 @@ typedef struct bg_tracer_desc {
  *   k = splitmix64(seed ^ splitmix64(p << 32 | s)),
  * counter = 0, 1, 2, ... within that camera sample.  This is the determinism
  * contract shared with the CPU oracle. */
+/* Image-sampler kinds.  The light and BSDF samplers are always the keyed
+ * RandomSampler(McRng) above; the image (camera) sample of (pixel p, sample s)
+ * comes from:
+ *   BG_SAMPLER_RANDOM  the keyed RandomSampler(McRng) above;
+ *   BG_SAMPLER_SOBOL   SobolSampler (sampler/sobol_sampler.cpp:3-49): point s
+ *                      of the pixel's scrambled (0,2) sequence, scrambles =
+ *                      the first two NextUint of a McRng seeded by the keyed
+ *                      rand() of (p, 0xFFFFFFFF);
+ *   BG_SAMPLER_CMJ     CmjSampler(grid) (sampler/cmj_sampler.cpp:3-73): sample
+ *                      s mod grid^2 of pattern j = s / grid^2, the pattern
+ *                      index being the first NextUint of a McRng seeded by
+ *                      the keyed rand() of (p, 0x80000000 + j).
+ * Sample indices s must stay below 2^31. */
+enum {
+    BG_SAMPLER_RANDOM = 0,
+    BG_SAMPLER_SOBOL = 1,
+    BG_SAMPLER_CMJ = 2
+};
+
 typedef struct bg_sampler_desc {
-    int32_t kind;           /* 0 = keyed RandomSampler(McRng)             */
+    int32_t kind;           /* BG_SAMPLER_* image sampler                 */
     int32_t spp;            /* camera samples per pixel in this call      */
     uint64_t seed;
     int32_t sample_offset;  /* index of the first sample of this call     */
-    int32_t reserved;
+    int32_t grid;           /* BG_SAMPLER_CMJ: grid size (1..16)          */
 } bg_sampler_desc;
 
 typedef struct bg_render_stats {

@@ -1037,6 +1037,82 @@ static int light_singular(const light_t* L) { return L->d.type == BG_LIGHT_DIREC
 /* ------------------------------------------------------------- tracers */
 typedef struct { mcrng_t light, brdf; keyed_t* key; } samplers_t;
 
+/* ------------------------------------------------------ image samplers */
+/* SobolSampler::Sample2D, sampler/sobol_sampler.cpp:3-37: x from the
+ * scrambled radical inverse in base 2, y from the scrambled Sobol (0,2)
+ * generator matrix; both keep the top 24 bits. */
+static float sobol_vdc(uint32_t n, uint32_t scramble) {
+    uint32_t r = 0;
+    for (int b = 0; b < 32; ++b) r |= ((n >> b) & 1u) << (31 - b);      /* bit reversal */
+    r ^= scramble;
+    return (float)((r >> 8) & 0xffffffu) / (float)(1 << 24);
+}
+static float sobol_02(uint32_t n, uint32_t scramble) {
+    uint32_t col = 0x80000000u;
+    while (n) {
+        if (n & 1u) scramble ^= col;
+        n >>= 1;
+        col ^= col >> 1;
+    }
+    return (float)((scramble >> 8) & 0xffffffu) / (float)(1 << 24);
+}
+
+/* CmjSampler, sampler/cmj_sampler.cpp:3-73 (Kensler, "Correlated
+ * Multi-Jittered Sampling", 2013): hashed permutation within [0, l) by
+ * cycle walking, hashed jitter in [0, 1). */
+static uint32_t cmj_permute(uint32_t i, uint32_t l, uint32_t p) {
+    uint32_t w = l - 1;
+    w |= w >> 1; w |= w >> 2; w |= w >> 4; w |= w >> 8; w |= w >> 16;
+    do {
+        i ^= p;             i *= 0xe170893du;
+        i ^= p >> 16;       i ^= (i & w) >> 4;
+        i ^= p >> 8;        i *= 0x0929eb3fu;
+        i ^= p >> 23;       i ^= (i & w) >> 1;
+        i *= 1u | p >> 27;  i *= 0x6935fa69u;
+        i ^= (i & w) >> 11; i *= 0x74dcb303u;
+        i ^= (i & w) >> 2;  i *= 0x9e501cc3u;
+        i ^= (i & w) >> 2;  i *= 0xc860a3dfu;
+        i &= w;
+        i ^= i >> 5;
+    } while (i >= l);
+    return (i + p) % l;
+}
+static float cmj_jitter(uint32_t i, uint32_t p) {
+    i ^= p;
+    i ^= i >> 17; i ^= i >> 10; i *= 0xb36534e5u;
+    i ^= i >> 12; i ^= i >> 21; i *= 0x93fc4795u;
+    i ^= 0xdf6e307fu; i ^= i >> 17; i *= 1u | p >> 18;
+    return (float)i * (1.0f / 4294967808.0f);
+}
+static v2 cmj_sample(int s, int m, int n, int p) {
+    const uint32_t up = (uint32_t)p;
+    int sx = (int)cmj_permute((uint32_t)(s % m), (uint32_t)m, up * 0xa511e9b3u);
+    int sy = (int)cmj_permute((uint32_t)(s / m), (uint32_t)n, up * 0x63d83595u);
+    float jx = cmj_jitter((uint32_t)s, up * 0xa399d265u);
+    float jy = cmj_jitter((uint32_t)s, up * 0x711ad6a5u);
+    return V2(((float)(s % m) + ((float)sy + jx) / (float)n) / (float)m,
+              ((float)(s / m) + ((float)sx + jy) / (float)m) / (float)n);
+}
+
+/* Image sample of camera sample (pixel, s); img is the sample's keyed McRng. */
+static v2 image_sample(int kind, int grid, uint64_t seed, uint32_t pixel, uint32_t s, mcrng_t* img) {
+    if (kind == BG_SAMPLER_SOBOL) {
+        keyed_t k; keyed_init(&k, seed, pixel, 0xFFFFFFFFu);
+        mcrng_t m; mcrng_init(&m, &k);
+        uint32_t sc0 = mc_next_uint(&m);
+        uint32_t sc1 = mc_next_uint(&m);
+        return V2(sobol_vdc(s, sc0), sobol_02(s, sc1));
+    }
+    if (kind == BG_SAMPLER_CMJ) {
+        uint32_t g2 = (uint32_t)(grid * grid);
+        keyed_t k; keyed_init(&k, seed, pixel, 0x80000000u + s / g2);
+        mcrng_t m; mcrng_init(&m, &k);
+        int pattern = (int)mc_next_uint(&m);
+        return cmj_sample((int)(s % g2), grid, grid, pattern);
+    }
+    return sample2d(img);
+}
+
 /* DiTracer::GetDi, tracer/ditracer.cpp:57-239 (num_samples = 1) */
 static v3 get_di(const or_world* w, int li, samplers_t* S, v3 wo, const hit_t* hit) {
     const light_t* L = &w->lights[li];
@@ -1202,11 +1278,24 @@ void or_camera_rays(const bg_camera_desc* cam, const float* samples, bg_ray* ray
     }
 }
 
+/* AoTracer::GetLi, tracer/aotracer.cpp:9-49 (lightsampler.num_samples() = 1):
+ * one cosine-distributed ray about the shading normal, t in (0.00002, radius). */
+static v3 ao_getli(const or_world* w, float radius, v3 ro, v3 rd, float rtmin, float rtmax, samplers_t* S) {
+    hit_t hit;
+    if (!world_intersect(w, ro, rd, rtmin, rtmax, &hit, NULL, NULL)) return V3(0.f, 0.f, 0.f);
+    v2 sample = sample2d(&S->light);
+    v3 d = map_to_hemisphere(hit.n, sample, 1.f);
+    float occlusion = world_occluded(w, hit.p, d, 0.00002f, radius, NULL, NULL) ? 1.f : 0.f;
+    occlusion *= 1.f / 1.f;
+    return V3(1.f - occlusion, 1.f - occlusion, 1.f - occlusion);
+}
+
 /* ------------------------------------------------------------- renderer */
 typedef struct {
     const or_world* w;
     camera_t cam;
-    int kind, maxdepth, W, H, spp, soff;
+    int kind, maxdepth, W, H, spp, soff, skind, sgrid;
+    float ao_radius;
     uint64_t seed;
     float* accum;
     int x0, x1, y0;
@@ -1227,12 +1316,14 @@ static void render_rows(void* a, int64_t b, int64_t e) {
                 mcrng_init(&S.light, &key);
                 mcrng_init(&S.brdf, &key);
                 S.key = &key;
-                v2 smp = sample2d(&img);
+                v2 smp = image_sample(r->skind, r->sgrid, r->seed, (uint32_t)(y * r->W + x),
+                                      (uint32_t)(r->soff + s), &img);
                 v2 is = V2((float)x / r->W + (1.f / r->W) * smp.x, (float)y / r->H + (1.f / r->H) * smp.y);
                 v3 o, d; float t0, t1;
                 camera_ray(&r->cam, is, &o, &d, &t0, &t1);
-                v3 L = r->kind == BG_TRACER_DI ? di_getli(r->w, o, d, t0, t1, &S)
-                                               : gi_getli(r->w, r->maxdepth, o, d, t0, t1, &S);
+                v3 L = r->kind == BG_TRACER_DI   ? di_getli(r->w, o, d, t0, t1, &S)
+                       : r->kind == BG_TRACER_AO ? ao_getli(r->w, r->ao_radius, o, d, t0, t1, &S)
+                                                 : gi_getli(r->w, r->maxdepth, o, d, t0, t1, &S);
                 /* FileImagePlane::WriteSample, imageplane/fileimageplane.cpp:29-34 */
                 float* px = &r->accum[4 * ((size_t)r->W * (size_t)(r->H - 1 - y) + (size_t)x)];
                 px[0] += L.x; px[1] += L.y; px[2] += L.z; px[3] += 1.f;
@@ -1243,9 +1334,11 @@ static void render_rows(void* a, int64_t b, int64_t e) {
 
 void or_render(const or_world* w, const bg_camera_desc* cam, int32_t tracer_kind, int32_t maxdepth,
                int32_t width, int32_t height, int32_t spp, int32_t sample_offset, uint64_t seed,
-               float* accum, int32_t x0, int32_t y0, int32_t x1, int32_t y1, int32_t nthreads) {
+               float* accum, int32_t x0, int32_t y0, int32_t x1, int32_t y1, int32_t nthreads,
+               int32_t sampler_kind, int32_t sampler_grid, float ao_radius) {
     render_arg_t r;
     r.w = w; r.cam = camera_make(cam); r.kind = tracer_kind; r.maxdepth = maxdepth;
+    r.skind = sampler_kind; r.sgrid = sampler_grid; r.ao_radius = ao_radius;
     r.W = width; r.H = height; r.spp = spp; r.soff = sample_offset; r.seed = seed; r.accum = accum;
     r.x0 = x0; r.x1 = x1; r.y0 = y0;
     parallel_for(y1 - y0, 1, nthreads, render_rows, &r);

@@ -52,7 +52,8 @@ int32_t or_triangle_test(const or_world* w, int64_t primid, const bg_ray* ray,
 void or_render(const or_world* w, const bg_camera_desc* cam, int32_t tracer_kind,
                int32_t maxdepth, int32_t width, int32_t height, int32_t spp,
                int32_t sample_offset, uint64_t seed, float* accum_rgbw,
-               int32_t x0, int32_t y0, int32_t x1, int32_t y1, int32_t nthreads);
+               int32_t x0, int32_t y0, int32_t x1, int32_t y1, int32_t nthreads,
+               int32_t sampler_kind, int32_t sampler_grid, float ao_radius);
 
 /* Primary rays of PerscpectiveCamera::GenerateRay for an image-plane sample
  * (camera/perspective_camera.cpp:25-38). */

@@ -36,7 +36,8 @@ def _load_oracle():
     lib.or_triangle_test.restype = C.c_int32
     lib.or_triangle_test.argtypes = [_vp, C.c_int64, _vp, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float)]
     lib.or_render.argtypes = [_vp, _vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
-                              C.c_uint64, _vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32]
+                              C.c_uint64, _vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                              C.c_int32, C.c_int32, C.c_float]
     lib.or_camera_rays.argtypes = [_vp, _vp, _vp, C.c_int64]
     lib.or_keyed_rand.restype = C.c_uint32
     lib.or_keyed_rand.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32]
@@ -51,7 +52,8 @@ def _load_ref():
     lib.ref_intersect_closest.argtypes = [_vp, _vp, _vp, C.c_int64, C.c_int32]
     lib.ref_intersect_any.argtypes = [_vp, _vp, _vp, C.c_int64, C.c_int32]
     lib.ref_render.argtypes = [_vp, _vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
-                               C.c_uint64, _vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32]
+                               C.c_uint64, _vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                               C.c_int32, C.c_int32, C.c_float]
     lib.ref_mcrng_draws.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_int32, _vp]
     lib.ref_world_ntriangles.restype = C.c_int64
     lib.ref_world_ntriangles.argtypes = [_vp]
@@ -112,7 +114,8 @@ class _Checker:
         return occ
 
     def render(self, camera=None, width=None, height=None, spp=1, seed=1, tracer=abi.BG_TRACER_GI,
-               maxdepth=5, sample_offset=0, region=None, nthreads=0, accum=None):
+               maxdepth=5, sample_offset=0, region=None, nthreads=0, accum=None, sampler=abi.BG_SAMPLER_RANDOM,
+               grid=0, ao_radius=0.0):
         sc = self.scene
         width = width or sc.width
         height = height or sc.height
@@ -121,7 +124,7 @@ class _Checker:
             accum = np.zeros((height, width, 4), dtype=np.float32)
         x0, y0, x1, y1 = region if region is not None else (0, 0, width, height)
         self._render(self.w, C.addressof(cam), tracer, maxdepth, width, height, spp, sample_offset, seed,
-                     _addr(accum), x0, y0, x1, y1, nthreads)
+                     _addr(accum), x0, y0, x1, y1, nthreads, sampler, grid, ao_radius)
         return accum
 
 

@@ -47,6 +47,9 @@
 #include "camera/perspective_camera.h"
 #include "tracer/gitracer.h"
 #include "tracer/ditracer.h"
+#include "tracer/aotracer.h"
+#include "sampler/sobol_sampler.h"
+#include "sampler/cmj_sampler.h"
 #include "sampler/random_sampler.h"
 #include "rng/mcrng.h"
 #include "renderer/renderer.h"
@@ -105,12 +108,29 @@ private:
     float* buf_;
 };
 
+// Rng whose NextUint is the first NextUint of a McRng seeded under a fixed
+// key: the CMJ pattern index of pattern j of a pixel (the sampler contract).
+class PatternRng : public Rng {
+public:
+    PatternRng(uint64_t seed, uint32_t pixel, uint32_t j) : seed_(seed), pixel_(pixel), j_(j) {}
+    float NextFloat() const override { return NextUint() * 2.328306e-10f; }
+    unsigned NextUint() const override {
+        set_key(seed_, pixel_, 0x80000000u + j_);
+        McRng m;
+        return m.NextUint();
+    }
+    Rng* Clone() const override { return new PatternRng(seed_, pixel_, j_); }
+private:
+    uint64_t seed_;
+    uint32_t pixel_, j_;
+};
+
 class KeyedRenderer : public Renderer {
 public:
     KeyedRenderer(ImagePlane& plane, Tracer const& tracer, uint64_t seed, int spp, int soff,
-                  int x0, int y0, int x1, int y1, int nthreads)
+                  int x0, int y0, int x1, int y1, int nthreads, int skind = BG_SAMPLER_RANDOM, int grid = 0)
         : plane_(plane), tracer_(tracer), seed_(seed), spp_(spp), soff_(soff),
-          x0_(x0), y0_(y0), x1_(x1), y1_(y1), nthreads_(nthreads) {}
+          x0_(x0), y0_(y0), x1_(x1), y1_(y1), nthreads_(nthreads), skind_(skind), grid_(grid) {}
 
     void Render(World const& world) const override {
         int nt = nthreads_ > 0 ? nthreads_ : static_cast<int>(std::thread::hardware_concurrency());
@@ -134,12 +154,30 @@ private:
         int2 imgres = plane_.resolution();
         Camera const& cam(*world.camera_.get());
         for (int x = x0_; x < x1_; ++x) {
+            const uint32_t pixel = static_cast<uint32_t>(y * imgres.x + x);
+            // Sobol: one sampler per pixel, scrambled from the key (pixel, 0xFFFFFFFF),
+            // advanced to the first sample index of this call
+            std::unique_ptr<SobolSampler> sobol;
+            if (skind_ == BG_SAMPLER_SOBOL) {
+                set_key(seed_, pixel, 0xFFFFFFFFu);
+                sobol.reset(new SobolSampler(1, new McRng()));
+                for (int k = 0; k < soff_; ++k) sobol->Sample2D();
+            }
             for (int s = 0; s < spp_; ++s) {
-                set_key(seed_, static_cast<uint32_t>(y * imgres.x + x), static_cast<uint32_t>(soff_ + s));
+                const uint32_t si = static_cast<uint32_t>(soff_ + s);
+                float2 cmj;
+                if (skind_ == BG_SAMPLER_CMJ) {
+                    const uint32_t g2 = static_cast<uint32_t>(grid_ * grid_);
+                    CmjSampler c(grid_, new PatternRng(seed_, pixel, si / g2));
+                    for (uint32_t k = 0; k <= si % g2; ++k) cmj = c.Sample2D();
+                }
+                set_key(seed_, pixel, si);
                 RandomSampler imgsampler(1, new McRng());
                 RandomSampler lightsampler(1, new McRng());
                 RandomSampler brdfsampler(1, new McRng());
                 float2 sample = imgsampler.Sample2D();
+                if (skind_ == BG_SAMPLER_SOBOL) sample = sobol->Sample2D();
+                if (skind_ == BG_SAMPLER_CMJ) sample = cmj;
                 float2 imgsample((float)x / imgres.x + (1.f / imgres.x) * sample.x,
                                  (float)y / imgres.y + (1.f / imgres.y) * sample.y);
                 ray r;
@@ -152,7 +190,7 @@ private:
     ImagePlane& plane_;
     Tracer const& tracer_;
     uint64_t seed_;
-    int spp_, soff_, x0_, y0_, x1_, y1_, nthreads_;
+    int spp_, soff_, x0_, y0_, x1_, y1_, nthreads_, skind_, grid_;
 };
 
 matrix mat_from(const float* a) {
@@ -288,7 +326,8 @@ void ref_intersect_any(void* w, const bg_ray* rays, uint8_t* occ, int64_t n, int
 
 void ref_render(void* w, const bg_camera_desc* c, int32_t tracer_kind, int32_t maxdepth,
                 int32_t width, int32_t height, int32_t spp, int32_t sample_offset, uint64_t seed,
-                float* accum_rgbw, int32_t x0, int32_t y0, int32_t x1, int32_t y1, int32_t nthreads) {
+                float* accum_rgbw, int32_t x0, int32_t y0, int32_t x1, int32_t y1, int32_t nthreads,
+                int32_t sampler_kind, int32_t sampler_grid, float ao_radius) {
     RefWorld* rw = static_cast<RefWorld*>(w);
     rw->world.camera_.reset(new PerscpectiveCamera(float3(c->eye[0], c->eye[1], c->eye[2]),
                                                    float3(c->at[0], c->at[1], c->at[2]),
@@ -297,8 +336,10 @@ void ref_render(void* w, const bg_camera_desc* c, int32_t tracer_kind, int32_t m
     BufferImagePlane plane(width, height, accum_rgbw);
     std::unique_ptr<Tracer> tracer;
     if (tracer_kind == BG_TRACER_DI) tracer.reset(new DiTracer());
+    else if (tracer_kind == BG_TRACER_AO) tracer.reset(new AoTracer(ao_radius));
     else tracer.reset(new GiTracer(maxdepth));
-    KeyedRenderer renderer(plane, *tracer, seed, spp, sample_offset, x0, y0, x1, y1, nthreads);
+    KeyedRenderer renderer(plane, *tracer, seed, spp, sample_offset, x0, y0, x1, y1, nthreads, sampler_kind,
+                           sampler_grid);
     renderer.Render(rw->world);
 }
 

@@ -10,8 +10,11 @@ seeded scenes and stores inputs + outputs as .npz:
   render_cornell.npz    -- Cornell 32x32, 8 spp, GiTracer(5) and DiTracer images
   render_production.npz -- small production scene (GGX, sun, environment),
                            48x27, 4 spp, GiTracer(8)
+  render_samplers.npz   -- Cornell 32x32: GiTracer(5) with the Sobol and the
+                           CMJ (grid 4, from sample 3) image samplers, and
+                           AoTracer(0.25) with the random and Sobol samplers
 
-Usage:  python tests/golden/make_golden.py
+Usage:  python tests/golden/make_golden.py [--only samplers]
 """
 import hashlib
 import os
@@ -42,7 +45,27 @@ CORNELL = dict(width=32, height=32)
 PROD = dict(width=48, height=27, nterrain=48, nspheres=12, sphere_seg=12, seed=3)
 
 
+def samplers():
+    cb = scenes.cornell(**CORNELL)
+    refr = Reference(cb)
+    out = {"scene_sha256": np.array(scene_hash(cb))}
+    out["gi_sobol"] = refr.render(spp=8, seed=4, tracer=abi.BG_TRACER_GI, maxdepth=5, nthreads=1,
+                                  sampler=abi.BG_SAMPLER_SOBOL)
+    out["gi_cmj4"] = refr.render(spp=8, seed=4, tracer=abi.BG_TRACER_GI, maxdepth=5, nthreads=1,
+                                 sampler=abi.BG_SAMPLER_CMJ, grid=4, sample_offset=3)
+    out["ao"] = refr.render(spp=8, seed=4, tracer=abi.BG_TRACER_AO, maxdepth=1, nthreads=1, ao_radius=0.25)
+    out["ao_sobol"] = refr.render(spp=8, seed=4, tracer=abi.BG_TRACER_AO, maxdepth=1, nthreads=1, ao_radius=0.25,
+                                  sampler=abi.BG_SAMPLER_SOBOL)
+    np.savez_compressed(os.path.join(HERE, "render_samplers.npz"), spp=8, seed=4, maxdepth=5, ao_radius=0.25,
+                        cmj_grid=4, cmj_offset=3, **out)
+
+
 def main():
+    if "--only" in sys.argv and sys.argv[sys.argv.index("--only") + 1] == "samplers":
+        samplers()
+        print("golden fixtures written to", HERE)
+        return
+    samplers()
     sc = scenes.soup(**SOUP)
     ref = Reference(sc, raycast=True)
     out = {"scene_sha256": np.array(scene_hash(sc))}

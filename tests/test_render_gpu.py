@@ -126,3 +126,37 @@ def test_render_argument_errors(ctx):
         gs.render_host(0, 8, 1)
     with pytest.raises(capi.BansheeError):
         gs.render_host(8, 8, 1, tracer=7)
+
+
+SAMPLER_CASES = [
+    ("gi_sobol", dict(tracer=abi.BG_TRACER_GI, maxdepth=5, sampler=abi.BG_SAMPLER_SOBOL)),
+    ("gi_cmj4", dict(tracer=abi.BG_TRACER_GI, maxdepth=5, sampler=abi.BG_SAMPLER_CMJ, grid=4, sample_offset=3)),
+    ("ao", dict(tracer=abi.BG_TRACER_AO, maxdepth=1, ao_radius=0.25)),
+    ("ao_sobol", dict(tracer=abi.BG_TRACER_AO, maxdepth=1, ao_radius=0.25, sampler=abi.BG_SAMPLER_SOBOL)),
+]
+
+
+@pytest.mark.parametrize("name,kw", SAMPLER_CASES, ids=[c[0] for c in SAMPLER_CASES])
+def test_samplers_and_ao_match_reference_golden(ctx, name, kw):
+    """Sobol / CMJ image samplers and AoTracer against the reference's own
+    SobolSampler, CmjSampler and AoTracer."""
+    from tests.golden.make_golden import CORNELL
+    g = np.load(os.path.join(GOLD, "render_samplers.npz"))
+    kw = dict(kw)
+    img = _render(ctx, scenes.cornell(**CORNELL), int(g["spp"]), int(g["seed"]), kw.pop("tracer"), kw.pop("maxdepth"),
+                  **kw)
+    ref = g[name]
+    assert (img[..., 3] == ref[..., 3]).all()
+    e = relmse(mean_image(img), mean_image(ref))
+    assert e < TOL, e
+
+
+def test_ao_and_samplers_vs_oracle_production(ctx, oracle_built):
+    sc = scenes.production(120, 68, nterrain=64, nspheres=16, sphere_seg=12, seed=6)
+    o = oracle_built.Oracle(sc)
+    for kw in (dict(tracer=abi.BG_TRACER_AO, maxdepth=1, ao_radius=2.0, sampler=abi.BG_SAMPLER_CMJ, grid=2),
+               dict(tracer=abi.BG_TRACER_GI, maxdepth=8, sampler=abi.BG_SAMPLER_SOBOL, sample_offset=11)):
+        img = _render(ctx, sc, 4, 5, **kw)
+        ref = o.render(spp=4, seed=5, **kw)
+        e = relmse(mean_image(img), mean_image(ref))
+        assert e < TOL, (kw, e)
