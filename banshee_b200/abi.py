@@ -99,7 +99,8 @@ class CacheDesc(C.Structure):
     _fields_ = [("levels", C.c_int32), ("log2_table_size", C.c_int32), ("base_resolution", C.c_int32),
                 ("max_resolution", C.c_int32), ("train_paths", C.c_int32), ("cache_depth", C.c_int32),
                 ("train_batch", C.c_int32), ("train_steps", C.c_int32), ("learning_rate", C.c_float),
-                ("bbox_min", C.c_float * 3), ("bbox_max", C.c_float * 3), ("seed", C.c_uint64)]
+                ("bbox_min", C.c_float * 3), ("bbox_max", C.c_float * 3), ("seed", C.c_uint64),
+                ("mlp_kernel", C.c_int32), ("reserved", C.c_int32)]
 
 
 class BatchJob(C.Structure):

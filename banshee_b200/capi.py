@@ -239,7 +239,9 @@ class RadianceCache:
     """bg_cache: the online-trained neural radiance cache of a committed scene."""
 
     def __init__(self, gscene, log2_table_size=19, base_resolution=16, max_resolution=2048, train_paths=65536,
-                 cache_depth=2, train_batch=16384, train_steps=4, learning_rate=1e-2, bbox=None, seed=1):
+                 cache_depth=2, train_batch=16384, train_steps=4, learning_rate=1e-2, bbox=None, seed=1,
+                 mlp_kernel=0):
+        """mlp_kernel: inference on tcgen05 with TMEM accumulators (0) or on mma.sync (1)."""
         d = abi.CacheDesc()
         d.levels = 16
         d.log2_table_size = log2_table_size
@@ -254,6 +256,7 @@ class RadianceCache:
             d.bbox_min[:] = list(bbox[0])
             d.bbox_max[:] = list(bbox[1])
         d.seed = seed
+        d.mlp_kernel = mlp_kernel
         self.gs = gscene
         self.h = _vp()
         check(lib().bg_cache_create(gscene.h, C.byref(d), C.byref(self.h)))

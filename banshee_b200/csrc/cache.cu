@@ -13,6 +13,7 @@
 
 #include "cache.h"
 #include "internal.h"
+#include "nrc_tcgen05.cuh"
 
 namespace bg {
 
@@ -534,7 +535,11 @@ int nrc_encode(bg_cache* c, const float* feat, const int* n_dev, int64_t n_stati
 }
 
 int nrc_infer(bg_cache* c, const int* n_dev, int64_t n_static, float4* out, cudaStream_t st) {
-    k_nrc_infer<<<c->sms * 4, 128, kInferSmem, st>>>(c->dev, c->X.as<__nv_bfloat16>(), n_dev, n_static, out);
+    if (c->desc.mlp_kernel == 0)
+        k_nrc_infer_tc<<<c->sms * 2, 128, kTcSmem, st>>>(c->dev, c->X.as<__nv_bfloat16>(), n_dev, n_static, out,
+                                                          c->scene->dev.errflags);
+    else
+        k_nrc_infer<<<c->sms * 4, 128, kInferSmem, st>>>(c->dev, c->X.as<__nv_bfloat16>(), n_dev, n_static, out);
     BG_CUDA(cudaGetLastError());
     return BG_OK;
 }
@@ -636,7 +641,12 @@ int bg_cache_create(bg_scene* s, const bg_cache_desc* d, bg_cache** out) {
     D.w = c->w.as<float>(); D.w_grad = c->w_grad.as<float>(); D.w_m = c->w_m.as<float>(); D.w_v = c->w_v.as<float>();
     D.wb = c->wb.as<__nv_bfloat16>();
     D.step = c->step.as<int>();
+    if (c->desc.mlp_kernel != 0 && c->desc.mlp_kernel != 1) {
+        bg_cache_destroy(c);
+        return set_error(BG_ERR_INVALID_ARG, "mlp_kernel %d: 0 (tcgen05) or 1 (mma.sync)", d->mlp_kernel);
+    }
     cudaFuncSetAttribute(k_nrc_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, kInferSmem);
+    cudaFuncSetAttribute(k_nrc_infer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
     cudaFuncSetAttribute(k_nrc_train, cudaFuncAttributeMaxDynamicSharedMemorySize, kTrainSmem);
     if ((rc = cache_init_params(c))) { bg_cache_destroy(c); return rc; }
     *out = c;

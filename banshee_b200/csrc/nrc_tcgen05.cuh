@@ -1,0 +1,212 @@
+// Radiance-cache MLP inference on the 5th-generation tensor cores (tcgen05).
+//
+// One persistent CTA of 128 threads per tile of 128 query rows:
+//   * the six weight matrices live in shared memory for the whole kernel, in
+//     the K-major no-swizzle canonical layout of the UMMA shared-memory
+//     descriptors: 8x8 bf16 core matrices of 128 contiguous bytes, core
+//     matrices adjacent in K 128 bytes apart (LBO), 8-row groups K/8 * 128
+//     bytes apart (SBO);
+//   * the activation tile (A operand, 128 x K bf16) is in the same layout;
+//   * the fp32 accumulator (128 lanes x 64 columns) is in tensor memory;
+//   * thread 0 issues tcgen05.mma (M = 128, N = 64 or 16, K = 16 per
+//     instruction) and commits to an mbarrier; every thread then reads its own
+//     accumulator row (TMEM lane = tile row) with tcgen05.ld, applies ReLU,
+//     rounds to bf16 and writes the next layer's A row.
+// Waits on the mbarrier are bounded: on timeout the kernel raises
+// BG_FLAG_TIMEOUT, stops, releases its tensor memory and returns.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cstdint>
+
+#include "cache.h"
+
+namespace bg {
+
+constexpr int kTcRows = 128;                               // rows per tile (UMMA M)
+constexpr int kTcW0 = 0;                                   // [64 x 128]
+constexpr int kTcW1 = kTcW0 + 64 * 128 * 2;                // 4 x [64 x 64]
+constexpr int kTcW5 = kTcW1 + 4 * 64 * 64 * 2;             // [16 x 64]
+constexpr int kTcA0 = kTcW5 + 16 * 64 * 2;                 // [128 x 128]
+constexpr int kTcA1 = kTcA0 + kTcRows * 128 * 2;           // [128 x 64]
+constexpr int kTcBar = kTcA1 + kTcRows * 64 * 2;           // mbarrier (8 B) + TMEM base (4 B)
+constexpr int kTcSmem = kTcBar + 16;
+constexpr uint32_t kTcCols = 64;                           // TMEM columns allocated
+constexpr uint32_t kTcWaitLimit = 1u << 24;                // mbarrier polls before giving up
+
+// byte offset of core-matrix row `r`, 16-byte chunk `kc` in a K-major tile with KC chunks per row
+__host__ __device__ constexpr uint32_t tc_off(int r, int kc, int KC) {
+    return uint32_t((r >> 3) * (KC * 128) + kc * 128 + (r & 7) * 16);
+}
+
+__device__ __forceinline__ uint64_t tc_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    return uint64_t((saddr >> 4) & 0x3FFFu) | (uint64_t((lbo >> 4) & 0x3FFFu) << 16) |
+           (uint64_t((sbo >> 4) & 0x3FFFu) << 32) | (uint64_t(1) << 46);   // version 1, no swizzle
+}
+
+// kind::f16 instruction descriptor: bf16 x bf16 -> f32, both K-major, M = 128
+__host__ __device__ constexpr uint32_t tc_idesc(int N) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(N >> 3) << 17) | (uint32_t(kTcRows >> 4) << 24);
+}
+
+__device__ __forceinline__ void tc_mma(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+        :: "r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+__device__ __forceinline__ void tc_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" :: "r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// true once the phase of parity `phase` of the mbarrier has completed; false after kTcWaitLimit polls
+__device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t phase) {
+    for (uint32_t it = 0; it < kTcWaitLimit; ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done) : "r"(bar), "r"(phase) : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+// 16 consecutive fp32 columns of this thread's TMEM lane
+__device__ __forceinline__ void tc_ld16(uint32_t taddr, float (&v)[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ uint32_t tc_pack(float lo, float hi) {
+    __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<uint32_t*>(&v);
+}
+
+// weight matrix [N][K] (row-major bf16 in global memory) -> canonical K-major smem tile
+__device__ __forceinline__ void tc_load_weights(const __nv_bfloat16* __restrict__ w, int N, int K, unsigned char* dst) {
+    const int KC = K / 8;
+    for (int i = threadIdx.x; i < N * KC; i += blockDim.x) {
+        const int n = i / KC, kc = i % KC;
+        *reinterpret_cast<uint4*>(dst + tc_off(n, kc, KC)) = *reinterpret_cast<const uint4*>(w + size_t(n) * K + kc * 8);
+    }
+}
+
+__global__ void __launch_bounds__(128, 2) k_nrc_infer_tc(NrcDev C, const __nv_bfloat16* __restrict__ X,
+                                                         const int* n_dev, int64_t n_static, float4* __restrict__ out,
+                                                         unsigned* __restrict__ errflags) {
+    extern __shared__ __align__(1024) unsigned char tc_smem[];
+    unsigned char* smem = tc_smem;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t sbase = uint32_t(__cvta_generic_to_shared(smem));
+    const uint32_t bar = sbase + kTcBar;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + kTcBar + 8);
+    __shared__ int abort_flag;
+
+    tc_load_weights(C.wb + kNrcW0, 64, 128, smem + kTcW0);
+    for (int l = 0; l < 4; ++l) tc_load_weights(C.wb + kNrcW1 + l * 4096, 64, 64, smem + kTcW1 + l * 8192);
+    tc_load_weights(C.wb + kNrcW5, 16, 64, smem + kTcW5);
+    if (tid == 0) {
+        abort_flag = 0;
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(bar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     :: "r"(sbase + kTcBar + 8), "r"(kTcCols) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+    const uint32_t trow = tmem + (uint32_t(warp * 32) << 16);   // this warp's 32 lanes
+
+    const int64_t n = n_dev ? int64_t(*n_dev) : n_static;
+    const int64_t ntiles = (n + kTcRows - 1) / kTcRows;
+    uint32_t phase = 0;
+    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int64_t row0 = tile * kTcRows;
+        // input rows -> A0; 8 lanes write 8 rows of one chunk (conflict-free), 4 chunks per warp
+        for (int j = 0; j < 16; ++j) {
+            const int u = j * 4 + warp, rg = u >> 2, kq4 = u & 3;
+            const int r = rg * 8 + (lane & 7), kc = kq4 * 4 + (lane >> 3);
+            const int64_t g = row0 + r;
+            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+            if (g < n) v = *reinterpret_cast<const uint4*>(X + size_t(g) * kNrcIn + kc * 8);
+            *reinterpret_cast<uint4*>(smem + kTcA0 + tc_off(r, kc, 16)) = v;
+        }
+        tc_fence_async_smem();
+        tc_fence_before();
+        __syncthreads();
+        for (int layer = 0; layer < 6; ++layer) {
+            if (tid == 0) {
+                tc_fence_after();
+                const int KC = layer == 0 ? 16 : 8;
+                const uint32_t a = sbase + (layer == 0 ? kTcA0 : kTcA1);
+                const uint32_t b = sbase + (layer == 0 ? kTcW0 : layer < 5 ? kTcW1 + (layer - 1) * 8192 : kTcW5);
+                const uint32_t idesc = tc_idesc(layer < 5 ? 64 : 16);
+                for (int s = 0; s < KC / 2; ++s)
+                    tc_mma(tmem, tc_desc(a + s * 256, 128, KC * 128), tc_desc(b + s * 256, 128, KC * 128), idesc,
+                           s > 0 ? 1u : 0u);
+                tc_commit(bar);
+            }
+            if (!tc_wait(bar, phase)) {
+                atomicOr(errflags, BG_FLAG_TIMEOUT);
+                abort_flag = 1;
+            }
+            phase ^= 1u;
+            tc_fence_after();
+            __syncthreads();
+            if (abort_flag) break;
+            const int r = tid;                       // TMEM lane = tile row
+            if (layer < 5) {
+#pragma unroll
+                for (int c4 = 0; c4 < 4; ++c4) {
+                    float v[16];
+                    tc_ld16(trow + uint32_t(c4 * 16), v);
+                    uint4 p0, p1;
+                    p0.x = tc_pack(fmaxf(v[0], 0.f), fmaxf(v[1], 0.f));
+                    p0.y = tc_pack(fmaxf(v[2], 0.f), fmaxf(v[3], 0.f));
+                    p0.z = tc_pack(fmaxf(v[4], 0.f), fmaxf(v[5], 0.f));
+                    p0.w = tc_pack(fmaxf(v[6], 0.f), fmaxf(v[7], 0.f));
+                    p1.x = tc_pack(fmaxf(v[8], 0.f), fmaxf(v[9], 0.f));
+                    p1.y = tc_pack(fmaxf(v[10], 0.f), fmaxf(v[11], 0.f));
+                    p1.z = tc_pack(fmaxf(v[12], 0.f), fmaxf(v[13], 0.f));
+                    p1.w = tc_pack(fmaxf(v[14], 0.f), fmaxf(v[15], 0.f));
+                    *reinterpret_cast<uint4*>(smem + kTcA1 + tc_off(r, 2 * c4, 8)) = p0;
+                    *reinterpret_cast<uint4*>(smem + kTcA1 + tc_off(r, 2 * c4 + 1, 8)) = p1;
+                }
+                tc_fence_async_smem();
+            } else {
+                float v[16];
+                tc_ld16(trow, v);
+                if (row0 + r < n) out[row0 + r] = make_float4(v[0], v[1], v[2], 0.f);
+            }
+            tc_fence_before();
+            __syncthreads();
+        }
+        if (abort_flag) break;
+    }
+    // after a timeout, give the outstanding MMA group one more bounded wait before freeing its TMEM
+    if (abort_flag && tid == 0) tc_wait(bar, phase ^ 1u);
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(kTcCols) : "memory");
+    }
+}
+
+}  // namespace bg

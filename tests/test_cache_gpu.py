@@ -82,10 +82,11 @@ def test_gradients_match_fp64_oracle(ctx):
     assert cos > 0.999 and np.linalg.norm(a - b) / np.linalg.norm(b) < 2e-2, cos
 
 
-def test_forward_matches_oracle(ctx):
+@pytest.mark.parametrize("mlp_kernel", [0, 1], ids=["tcgen05", "mma_sync"])
+def test_forward_matches_oracle(ctx, mlp_kernel):
     import torch
     from oracle import nrc_oracle as O
-    gs, cache = _cache(ctx, log2t=10)
+    gs, cache = _cache(ctx, log2t=10, mlp_kernel=mlp_kernel)
     rng = np.random.default_rng(5)
     n = 1000
     feat = _features(n, rng)
@@ -176,3 +177,29 @@ def test_trained_cache_recovers_truncated_radiance(ctx):
     print("relMSE truncated %.3g cache %.3g plain %.3g" % (e_trunc, e_cache, e_plain))
     assert e_cache < 0.2 * e_trunc, (e_cache, e_trunc)
     assert e_cache < 3.0 * e_plain, (e_cache, e_plain)
+
+
+def test_tcgen05_and_mma_sync_inference_agree(ctx):
+    """The tcgen05 kernel (TMEM accumulators) and the mma.sync kernel compute the
+    same bf16 network; only the fp32 summation order differs.  Ragged row counts
+    exercise partial 128-row tiles."""
+    import torch
+    from banshee_b200 import capi
+    gs, c0 = _cache(ctx, log2t=12, mlp_kernel=0)
+    c1 = capi.RadianceCache(gs, log2_table_size=12, base_resolution=4, max_resolution=64,
+                            bbox=((0, 0, 0), (1, 1, 1)), mlp_kernel=1)
+    m, g, _, _ = c0.params()
+    c1.set_params(m, g)
+    rng = np.random.default_rng(8)
+    for n in (1, 127, 129, 5000, 65536 + 77):
+        fd = torch.from_numpy(_features(n, rng)).cuda()
+        o0 = torch.zeros((n, 4), dtype=torch.float32, device="cuda")
+        o1 = torch.zeros((n, 4), dtype=torch.float32, device="cuda")
+        c0.query(fd.data_ptr(), o0.data_ptr(), n)
+        c1.query(fd.data_ptr(), o1.data_ptr(), n)
+        torch.cuda.synchronize()
+        a, b = o0.cpu().numpy(), o1.cpu().numpy()
+        assert np.isfinite(a).all() and (a[:, 3] == 0).all()
+        scale = np.abs(b[:, :3]).max() + 1e-6
+        assert np.abs(a[:, :3] - b[:, :3]).max() < 2e-2 * scale, (n, np.abs(a - b).max(), scale)
+    assert gs.error_flags() == 0
