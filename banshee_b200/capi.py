@@ -49,6 +49,8 @@ def lib():
             "bg_scene_info_get": [_vp, C.POINTER(abi.SceneInfo)],
             "bg_scene_error_flags": [_vp, C.POINTER(C.c_uint32), _i32],
             "bg_scene_set_node_width": [_vp, _i32],
+            "bg_image_finalize": [_vp, _i32, _i32, _vp],
+            "bg_image_write": [C.c_char_p, _vp, _i32, _i32],
             "bg_intersect_closest": [_vp, _vp, _vp, _i64, _vp],
             "bg_intersect_any": [_vp, _vp, _vp, _i64, _vp],
             "bg_intersect_closest_host": [_vp, _vp, _vp, _i64],
@@ -372,3 +374,18 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def image_finalize(rgbw):
+    """FileImagePlane::Finalize of a (H, W, 4) accumulation buffer -> (H, W, 3) floats."""
+    a = np.ascontiguousarray(rgbw, dtype=np.float32)
+    h, w = a.shape[0], a.shape[1]
+    out = np.zeros((h, w, 3), np.float32)
+    check(lib().bg_image_finalize(a.ctypes.data, w, h, out.ctypes.data))
+    return out
+
+
+def image_write(path, rgbw):
+    """Write a (H, W, 4) accumulation buffer as .ppm (8-bit) or .pfm (float)."""
+    a = np.ascontiguousarray(rgbw, dtype=np.float32)
+    check(lib().bg_image_write(str(path).encode(), a.ctypes.data, a.shape[1], a.shape[0]))

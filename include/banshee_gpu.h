@@ -353,6 +353,16 @@ int bg_batch_autotune(bg_batch* batch, const bg_batch_job* jobs, int32_t njobs, 
                       int32_t probe_spp, bg_tune_result* result, void* stream);
 int bg_batch_destroy(bg_batch* batch);
 
+/* ------------------------------------------------------------ images */
+/* FileImagePlane::Finalize (imageplane/fileimageplane.cpp:13-27): rgb[i] =
+ * (sum / samples)^(1/2.2) per channel of the W*H RGBW accumulation buffer
+ * (rows bottom-up, as WriteSample stores them).  Host buffers. */
+int bg_image_finalize(const float* rgbw, int32_t width, int32_t height, float* rgb);
+/* Finalize + write, replacing OiioImageIo::Write (imageio/oiioimageio.cpp:
+ * 40-56) for headless use: ".ppm" = 8-bit (clamped to [0,1], rounded), ".pfm"
+ * = 32-bit float.  Host buffer. */
+int bg_image_write(const char* path, const float* rgbw, int32_t width, int32_t height);
+
 /* ------------------------------------------------------ radiance cache */
 /* Neural radiance cache.  No counterpart in the reference: Banshee has no
  * learned component.  A hash-grid + one-blob encoded, 64-wide, 5-hidden-layer
