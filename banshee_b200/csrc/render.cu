@@ -324,6 +324,9 @@ __device__ __noinline__ void emit_di(const DevScene& S, const Queues& Q, int li,
     }
 }
 
+// One instantiation per tracer kind and cache mode keeps each kernel's code
+// (and its instruction-cache footprint) to what that configuration runs.
+template <int KIND, bool CACHE>
 __global__ void __launch_bounds__(kShadeThreads, 8)
 k_shade(DevScene S, ShadeArgs A, PathState P, Queues Q) {
     const int n = *Q.n_ext_in;
@@ -342,7 +345,7 @@ k_shade(DevScene S, ShadeArgs A, PathState P, Queues Q) {
         int pending = 0;
         bool end = false;
         if (hit.primid < 0) {
-            if (A.kind == BG_TRACER_AO) {
+            if (KIND == BG_TRACER_AO) {
                 flags |= kFlagNoClamp;  // AoTracer: a miss is black (aotracer.cpp:47)
             } else if (A.bounce == 0) { // primary miss: bgcolor + sum of GetLe, unclamped (gitracer.cpp:22-33)
                 rad = add(rad, mk(J.bg[0], J.bg[1], J.bg[2]));
@@ -359,7 +362,7 @@ k_shade(DevScene S, ShadeArgs A, PathState P, Queues Q) {
             uint4 rg = P.rng[path];
             McRng lr{rg.x, rg.y}, br{rg.z, rg.w};
             float2 bs;
-            if (A.bounce == 0 && A.kind == BG_TRACER_GI) {
+            if (A.bounce == 0 && KIND == BG_TRACER_GI) {
                 sample2d(br, bs.x, bs.y);
                 P.bs[path] = bs;
             } else {
@@ -372,7 +375,7 @@ k_shade(DevScene S, ShadeArgs A, PathState P, Queues Q) {
             const unsigned pflags = P.flags[path];
             const bool train = (pflags & kFlagTrain) != 0;
             flags = pflags;
-            if (A.kind == BG_TRACER_AO) {
+            if (KIND == BG_TRACER_AO) {
                 // AoTracer::GetLi (aotracer.cpp:9-49), one light-sampler sample:
                 // a cosine ray about the shading normal, t in (0.00002, radius);
                 // the visibility 1 lands in the first slot unless the ray is occluded
@@ -393,10 +396,10 @@ k_shade(DevScene S, ShadeArgs A, PathState P, Queues Q) {
                 P.rng[path] = make_uint4(lr.z, lr.w, br.z, br.w);
                 end = true;
             } else if (A.bounce == 0 && M.type == BG_MAT_EMISSIVE) {
-                if (A.kind == BG_TRACER_GI) rad = add(rad, emissive_le(M, h.n, wo));   // gitracer.cpp:61-68
-                if (A.kind == BG_TRACER_DI) flags |= kFlagNoClamp;                    // ditracer.cpp:29-32
+                if (KIND == BG_TRACER_GI) rad = add(rad, emissive_le(M, h.n, wo));   // gitracer.cpp:61-68
+                if (KIND == BG_TRACER_DI) flags |= kFlagNoClamp;                    // ditracer.cpp:29-32
                 end = true;
-            } else if (A.cache_depth >= 0 && !train && A.bounce == A.cache_depth) {
+            } else if ((CACHE && A.cache_depth >= 0) && !train && A.bounce == A.cache_depth) {
                 // the rendering path ends into the radiance cache at this vertex
                 float4 f[4];
                 cache_features(h, wo, M, f);
@@ -407,7 +410,7 @@ k_shade(DevScene S, ShadeArgs A, PathState P, Queues Q) {
                 Q.q_thr[q] = make_float4(thr.x, thr.y, thr.z, 0.f);
                 end = true;
             } else {
-                if (A.cache_depth >= 0 && train) {
+                if ((CACHE && A.cache_depth >= 0) && train) {
                     // training path: remember the vertex, its throughput and the radiance so far
                     const int t = (path + A.train_phase) / A.train_stride;
                     float4* rr = P.rec + (size_t(t) * A.maxdepth + A.bounce) * 6;
@@ -434,7 +437,7 @@ k_shade(DevScene S, ShadeArgs A, PathState P, Queues Q) {
                 for (int j = 0; j < pending; ++j) P.slots[size_t(base) + j] = make_float4(0.f, 0.f, 0.f, 0.f);
                 for (int i = 0; i < nl; ++i) emit_di(S, Q, first + i, h, M, wo, lr, br, base + 2 * i, path, root);
                 P.dithr[path] = make_float4(thr.x, thr.y, thr.z, mult);
-                if (A.kind == BG_TRACER_DI) {
+                if (KIND == BG_TRACER_DI) {
                     flags |= kFlagNoClamp;
                     end = true;
                 } else {
@@ -646,7 +649,7 @@ static int ensure_state(bg_scene* s, int64_t cap, int maxL) {
         (rc = rs->work.ensure(size_t(kMaxBounceCounters) * 8)))
         return rc;
     int nb = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_shade, kShadeThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_shade<BG_TRACER_GI, false>, kShadeThreads, 0);
     rs->blocks = std::max(1, nb) * s->ctx->num_sms;
     BG_CUDA(cudaStreamCreateWithFlags(&rs->gstream, cudaStreamNonBlocking));
     BG_CUDA(cudaEventCreateWithFlags(&rs->ev_in, cudaEventDisableTiming));
@@ -752,7 +755,10 @@ static int enqueue_pass(bg_scene* s, RenderState* rs, cudaStream_t st, const Pas
         ShadeArgs A{b, c.maxdepth, c.kind, rs->kmax, c.batched ? 1 : 0, c.cache ? c.cache_depth : -1,
                     c.cache ? c.train_stride : 0, c.train_phase, c.ao_radius};
         if (c.cache && b == c.cache_depth) BG_CUDA(cudaMemsetAsync(Q.n_query, 0, sizeof(int), st));
-        k_shade<<<nb, kShadeThreads, 0, st>>>(s->dev, A, P, Q);
+        if (c.kind == BG_TRACER_DI) k_shade<BG_TRACER_DI, false><<<nb, kShadeThreads, 0, st>>>(s->dev, A, P, Q);
+        else if (c.kind == BG_TRACER_AO) k_shade<BG_TRACER_AO, false><<<nb, kShadeThreads, 0, st>>>(s->dev, A, P, Q);
+        else if (c.cache) k_shade<BG_TRACER_GI, true><<<nb, kShadeThreads, 0, st>>>(s->dev, A, P, Q);
+        else k_shade<BG_TRACER_GI, false><<<nb, kShadeThreads, 0, st>>>(s->dev, A, P, Q);
         if (ins) { ++ins->launches; ins->mark(1); }
         if ((rc = launch_trace(s, true, Q.sh_rays, 0, Q.n_sh, nullptr, Q.sh_occ, st, nullptr, 1, wk + 2, Q.sh_root))) return rc;
         if (ins) { ins->mark(1); ins->mark(2); }
