@@ -6,6 +6,8 @@ inside the path tracer: rank r of N renders the samples
 of every pixel into its own RGBW accumulation buffer, and one all-reduce (sum)
 per step combines the ranks' buffers (NCCL over NVLink on GPUs; gloo on CPU in
 the tests).  The scene is replicated per GPU.  Timing is the maximum over ranks.
+Multi-scene batches shard by scene instead (rank r takes scenes r, r + N, ...),
+with no exchange at all.
 """
 import datetime
 import os
@@ -18,6 +20,11 @@ def rank_world():
 def sample_offset(step, rank, world, spp_per_step=1):
     """First sample index of this rank's share of step `step`."""
     return (step * world + rank) * spp_per_step
+
+
+def shard(items, rank, world):
+    """This rank's share of independent items (scenes of a batch): every N-th."""
+    return list(items)[rank::world]
 
 
 def init(backend, timeout_s=120.0, device=None):

@@ -237,14 +237,16 @@ def cornell_c1(ctx, ref_seconds_cap=60.0):
     return out
 
 
-def batch_c4(ctx, nscenes=64, seed=7, timed_frames=1):
+def batch_c4(ctx, nscenes=64, seed=7, timed_frames=1, rank=0, world=1, dist=None):
     """C4: 64 procedural scenes (triangles log-uniform in [1e4, 5e5], resolutions from
     {256^2, 512^2, 1024x768}, 16..128 spp each) traced together by one batch: one set of
-    queues, persistent kernels, one pass graph; autotuned block / wavefront sizes."""
+    queues, persistent kernels, one pass graph; autotuned node width / block / wavefront
+    sizes.  On N GPUs each rank takes every N-th scene (no exchange); time = max over ranks."""
     import torch
-    from banshee_b200 import capi, scenes
+    from banshee_b200 import capi, multigpu, scenes
     t0 = time.perf_counter()
-    items = scenes.batch(nscenes, seed=seed)
+    all_items = scenes.batch(nscenes, seed=seed)
+    items = multigpu.shard(all_items, rank, world)
     gss = [capi.GpuScene(ctx, sc) for sc, _ in items]
     batch = capi.Batch(ctx, gss)
     build_s = time.perf_counter() - t0
@@ -269,14 +271,17 @@ def batch_c4(ctx, nscenes=64, seed=7, timed_frames=1):
         batch.render(jobs, maxdepth=MAXDEPTH)
     e1.record()
     torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / timed_frames
+    ms = multigpu.max_over_ranks(e0.elapsed_time(e1) / timed_frames, dist, device="cuda")
     info = batch.info()
     batch.close()
-    return {"scenes": nscenes, "triangles_total": info["ntriangles"], "camera_samples": samples,
+    samples = sum(sc.width * sc.height * spp for sc, spp in all_items)
+    return {"scenes": nscenes, "triangles_total": sum(sc.ntriangles for sc, _ in all_items),
+            "camera_samples": samples, "scenes_per_rank": len(items), "node_width": info["node_width"],
             "ms": ms, "msamples_per_s": samples / ms / 1e3, "autotune": tune, "build_s": build_s,
-            "resolutions": sorted({"%dx%d" % (sc.width, sc.height) for sc, _ in items}),
-            "spp_range": [min(s for _, s in items), max(s for _, s in items)],
-            "triangle_range": [min(sc.ntriangles for sc, _ in items), max(sc.ntriangles for sc, _ in items)]}
+            "resolutions": sorted({"%dx%d" % (sc.width, sc.height) for sc, _ in all_items}),
+            "spp_range": [min(s for _, s in all_items), max(s for _, s in all_items)],
+            "triangle_range": [min(sc.ntriangles for sc, _ in all_items),
+                               max(sc.ntriangles for sc, _ in all_items)]}
 
 
 def time_to_relmse(gs, sc, args, target=1e-3):
@@ -295,7 +300,7 @@ def time_to_relmse(gs, sc, args, target=1e-3):
                                                stats=False),
                         WIDTH, HEIGHT, Wc, Hc, gt, args.conv_seconds, 100000, target=target, every=4)
     cache = capi.RadianceCache(gs, log2_table_size=19, base_resolution=16, max_resolution=2048, train_paths=65536,
-                               cache_depth=2, train_batch=16384, train_steps=1, learning_rate=1e-2)
+                               cache_depth=2, train_batch=16384, train_steps=4, learning_rate=1e-2)
     cached = CV.converge(lambda p, f: cache.render(p, WIDTH, HEIGHT, 1, seed=SEED, sample_offset=f,
                                                    maxdepth=MAXDEPTH),
                          WIDTH, HEIGHT, Wc, Hc, gt, args.conv_seconds, 100000, target=target, every=4)
@@ -322,7 +327,7 @@ def time_to_relmse(gs, sc, args, target=1e-3):
             "reference": "plain GiTracer(8), float64 accumulation of 256-spp chunks",
             "relmse": "mean over pixels and channels of (x - ref)^2 / (ref^2 + 0.01)",
             "cache_config": "hash grid 16 levels x 2 features, 2^19 entries/level, res 16..2048; MLP 64x5 bf16; "
-                            "Adam lr 1e-2; 65536 training paths/frame, 1 step of 16384 rows/frame; paths end into "
+                            "Adam lr 1e-2; 65536 training paths/frame, up to 4 steps of 16384 rows/frame; paths end into "
                             "the cache after 2 bounces",
             "plain": summ(plain), "cache": summ(cached), "cache_over_plain_time": ratio,
             "perfect_cache_bound": {
@@ -482,7 +487,7 @@ def main():
         gs.close()
         c2 = raycast_c2(ctx)
         c1 = cornell_c1(ctx)
-    c4 = batch_c4(ctx) if (rank == 0 and world == 1 and args.c4) else None
+    c4 = batch_c4(ctx, rank=rank, world=world, dist=dist) if args.c4 else None
 
     if rank == 0:
         line = {

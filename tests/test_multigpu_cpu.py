@@ -89,3 +89,12 @@ def test_rank_leaving_is_reported_not_hung(tmp_path):
         p.join(timeout=120)
     assert all(not p.is_alive() for p in procs)
     assert open(out).read().startswith("error"), open(out).read()
+
+
+def test_scene_sharding_covers_every_scene_once():
+    from banshee_b200 import multigpu
+    items = list(range(64))
+    for world in (1, 2, 3, 8):
+        parts = [multigpu.shard(items, r, world) for r in range(world)]
+        assert sorted(x for p in parts for x in p) == items
+        assert max(map(len, parts)) - min(map(len, parts)) <= 1
