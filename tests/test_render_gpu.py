@@ -160,3 +160,16 @@ def test_ao_and_samplers_vs_oracle_production(ctx, oracle_built):
         ref = o.render(spp=4, seed=5, **kw)
         e = relmse(mean_image(img), mean_image(ref))
         assert e < TOL, (kw, e)
+
+
+def test_node_layouts_give_identical_images(ctx):
+    """Both node layouts return the same closest hits, so whole images agree bit for bit."""
+    from banshee_b200 import capi
+    sc = scenes.production(96, 54, nterrain=64, nspheres=16, sphere_seg=12, seed=8)
+    gs = capi.GpuScene(ctx, sc)
+    imgs = []
+    for w in (4, 8):
+        gs.set_node_width(w)
+        imgs.append(gs.render_host(96, 54, 8, seed=2, maxdepth=8))
+    assert (imgs[0].view(np.uint32) == imgs[1].view(np.uint32)).all()
+    assert gs.error_flags() == 0
