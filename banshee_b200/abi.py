@@ -57,7 +57,7 @@ class CameraDesc(C.Structure):
 
 class BuildOpts(C.Structure):
     _fields_ = [("node_width", C.c_int32), ("max_leaf_size", C.c_int32),
-                ("sah_bins", C.c_int32), ("reserved", C.c_int32)]
+                ("sah_bins", C.c_int32), ("builder", C.c_int32)]
 
 
 class SceneInfo(C.Structure):
@@ -65,7 +65,8 @@ class SceneInfo(C.Structure):
                 ("tri_bytes", C.c_int64), ("shade_bytes", C.c_int64), ("node_stride", C.c_int32),
                 ("max_depth", C.c_int32), ("max_stack", C.c_int32), ("nmeshes", C.c_int32),
                 ("nmaterials", C.c_int32), ("nlights", C.c_int32), ("build_ms", C.c_double),
-                ("node_width", C.c_int32), ("node_widths", C.c_int32)]
+                ("node_width", C.c_int32), ("node_widths", C.c_int32), ("bvh_ms", C.c_double),
+                ("records_ms", C.c_double), ("upload_ms", C.c_double)]
 
 
 BG_SAMPLER_RANDOM, BG_SAMPLER_SOBOL, BG_SAMPLER_CMJ = 0, 1, 2

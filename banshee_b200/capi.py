@@ -128,9 +128,10 @@ class Context:
 class GpuScene:
     """A committed scene on the device: World::Commit + the Intersectable surface."""
 
-    def __init__(self, ctx, scene, node_width=0, max_leaf=4, bins=32):
+    def __init__(self, ctx, scene, node_width=0, max_leaf=4, bins=32, builder=0):
         """node_width: 4 (128-byte nodes), 8 (96-byte compressed nodes) or 0 (both
-        built; the active one is chosen with set_node_width)."""
+        built; the active one is chosen with set_node_width).  builder: 0 = host
+        binned SAH, 1 = device LBVH."""
         self.ctx = ctx
         self.scene = scene
         self.h = _vp()
@@ -149,7 +150,7 @@ class GpuScene:
             check(L.bg_scene_add_light(self.h, C.byref(d), None))
         bg = (C.c_float * 3)(*scene.bgcolor)
         check(L.bg_scene_set_background(self.h, bg))
-        opts = abi.BuildOpts(node_width, max_leaf, bins, 0)
+        opts = abi.BuildOpts(node_width, max_leaf, bins, builder)
         check(L.bg_scene_commit(self.h, C.byref(opts)))
 
     def info(self):

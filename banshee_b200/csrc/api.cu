@@ -6,6 +6,7 @@
 #include <cstdio>
 #include <cstring>
 #include <new>
+#include <thread>
 
 #include "bvh_build.h"
 #include "internal.h"
@@ -213,6 +214,23 @@ static bool is_identity(const float* m) {
     return true;
 }
 
+// Runs f(begin, end) over [0, n) in contiguous chunks on the host's cores;
+// each index is written by exactly one thread, so results do not depend on the
+// thread count.
+template <class F>
+static void host_parallel_for(int64_t n, F f) {
+    const int hw = std::max(1, std::min(64, int(std::thread::hardware_concurrency())));
+    const int nt = int(std::min<int64_t>(hw, std::max<int64_t>(1, n / 65536)));
+    if (nt <= 1) { f(int64_t(0), n); return; }
+    std::vector<std::thread> th;
+    const int64_t chunk = (n + nt - 1) / nt;
+    for (int k = 0; k < nt; ++k) {
+        const int64_t b = k * chunk, e = std::min(n, b + chunk);
+        if (b < e) th.emplace_back([=]() { f(b, e); });
+    }
+    for (auto& t : th) t.join();
+}
+
 static int commit_scene(bg_scene* s, const bg_build_opts* opts) {
     auto t0 = std::chrono::steady_clock::now();
     const int nm = int(s->meshes.size());
@@ -292,14 +310,18 @@ static int commit_scene(bg_scene* s, const bg_build_opts* opts) {
     }
     // world-space triangle bounds (Mesh::GetShapeWorldBounds, primitive/mesh.cpp:263-283)
     std::vector<float> lo(3 * size_t(ntris)), hi(3 * size_t(ntris));
-    for (int i = 0; i < nm; ++i) {
-        const MeshHost& mh = s->meshes[i];
-        const float* M = mh.xf;
-        float m12[12] = {M[0], M[1], M[2], M[3], M[4], M[5], M[6], M[7], M[8], M[9], M[10], M[11]};
-        for (int f = 0; f < mh.nfaces; ++f) {
+    std::vector<int> tri_bundle(static_cast<size_t>(ntris));
+    for (int i = 0; i < nm; ++i)
+        std::fill(tri_bundle.begin() + start[i], tri_bundle.begin() + start[i] + s->meshes[i].nfaces, i);
+    host_parallel_for(ntris, [&](int64_t tb, int64_t te) {
+        for (int64_t t = tb; t < te; ++t) {
+            const int i = tri_bundle[size_t(t)];
+            const MeshHost& mh = s->meshes[i];
+            const int f = int(t - start[i]);
+            const float* M = mh.xf;
+            float m12[12] = {M[0], M[1], M[2], M[3], M[4], M[5], M[6], M[7], M[8], M[9], M[10], M[11]};
             v3 p[3];
             for (int k = 0; k < 3; ++k) p[k] = xf_point(m12, mh.verts[mh.vi[3 * f + k]]);
-            size_t t = size_t(start[i] + f);
             lo[3 * t] = std::min(p[0].x, std::min(p[1].x, p[2].x));
             lo[3 * t + 1] = std::min(p[0].y, std::min(p[1].y, p[2].y));
             lo[3 * t + 2] = std::min(p[0].z, std::min(p[1].z, p[2].z));
@@ -307,7 +329,7 @@ static int commit_scene(bg_scene* s, const bg_build_opts* opts) {
             hi[3 * t + 1] = std::max(p[0].y, std::max(p[1].y, p[2].y));
             hi[3 * t + 2] = std::max(p[0].z, std::max(p[1].z, p[2].z));
         }
-    }
+    });
     for (int k = 0; k < 3; ++k) { s->bbox_lo[k] = FLT_MAX; s->bbox_hi[k] = -FLT_MAX; }
     for (int64_t t = 0; t < ntris; ++t)
         for (int k = 0; k < 3; ++k) {
@@ -322,12 +344,24 @@ static int commit_scene(bg_scene* s, const bg_build_opts* opts) {
             return set_error(BG_ERR_UNSUPPORTED, "node_width %d: supported widths are 4 and 8 (0: both)", want_width);
         if (opts->max_leaf_size) bp.max_leaf = opts->max_leaf_size;
         if (opts->sah_bins) bp.bins = opts->sah_bins;
+        if (opts->builder != 0 && opts->builder != 1)
+            return set_error(BG_ERR_INVALID_ARG, "builder %d: 0 (host SAH) or 1 (device LBVH)", opts->builder);
     }
+    const bool device_build = opts && opts->builder == 1 && ntris >= 2;
     if (bp.max_leaf < 1 || bp.max_leaf > 16 || bp.bins < 2 || bp.bins > 256)
         return set_error(BG_ERR_INVALID_ARG, "build options out of range (leaf 1..16, bins 2..256)");
     bp.wide4 = want_width != 8;
     bp.wide8 = want_width != 4;
-    BuildResult br = build_wide_bvh(lo.data(), hi.data(), ntris, bp);
+    const auto tb0 = std::chrono::steady_clock::now();
+    BuildResult br;
+    if (device_build) {
+        BinaryTree bt;
+        int brc = gpu_build_tree(lo.data(), hi.data(), ntris, bp.max_leaf, bt);
+        if (brc) return brc;
+        br = collapse_binary(bt, bp);
+    } else {
+        br = build_wide_bvh(lo.data(), hi.data(), ntris, bp);
+    }
     if (want_width == 8 && br.nodes8.empty())
         return set_error(BG_ERR_UNSUPPORTED, "scene coordinates too large for the 8-wide compressed nodes");
     if (bp.wide4 && br.max_stack > kStackSize)
@@ -338,29 +372,31 @@ static int commit_scene(bg_scene* s, const bg_build_opts* opts) {
                              kStackSize8);
         br.nodes8.clear();
     }
+    const auto tb1 = std::chrono::steady_clock::now();
     // per-triangle records
-    std::vector<int> tri_bundle(static_cast<size_t>(ntris));
-    for (int i = 0; i < nm; ++i)
-        for (int f = 0; f < s->meshes[i].nfaces; ++f) tri_bundle[size_t(start[i] + f)] = i;
     std::vector<TriRec> tris(static_cast<size_t>(ntris));
-    for (int64_t k = 0; k < ntris; ++k) {
-        int32_t t = br.order[size_t(k)];
-        int b = tri_bundle[size_t(t)];
-        const MeshHost& mh = s->meshes[b];
-        int f = int(t - start[b]);
-        v3 p1 = mh.verts[mh.vi[3 * f]], p2 = mh.verts[mh.vi[3 * f + 1]], p3 = mh.verts[mh.vi[3 * f + 2]];
-        v3 e1 = sub(p2, p1), e2 = sub(p3, p1);
-        TriRec& r = tris[size_t(k)];
-        int bcode = bundles[b].identity ? -1 : b;
-        r.v0 = make_float4(p1.x, p1.y, p1.z, i2f(bcode));
-        r.e1 = make_float4(e1.x, e1.y, e1.z, i2f(t));
-        r.e2 = make_float4(e2.x, e2.y, e2.z, 0.f);
-    }
+    host_parallel_for(ntris, [&](int64_t kb, int64_t ke) {
+        for (int64_t k = kb; k < ke; ++k) {
+            int32_t t = br.order[size_t(k)];
+            int b = tri_bundle[size_t(t)];
+            const MeshHost& mh = s->meshes[b];
+            int f = int(t - start[b]);
+            v3 p1 = mh.verts[mh.vi[3 * f]], p2 = mh.verts[mh.vi[3 * f + 1]], p3 = mh.verts[mh.vi[3 * f + 2]];
+            v3 e1 = sub(p2, p1), e2 = sub(p3, p1);
+            TriRec& r = tris[size_t(k)];
+            int bcode = bundles[b].identity ? -1 : b;
+            r.v0 = make_float4(p1.x, p1.y, p1.z, i2f(bcode));
+            r.e1 = make_float4(e1.x, e1.y, e1.z, i2f(t));
+            r.e2 = make_float4(e2.x, e2.y, e2.z, 0.f);
+        }
+    });
     std::vector<ShadeRec> shade(static_cast<size_t>(ntris));
-    for (int b = 0; b < nm; ++b) {
-        const MeshHost& mh = s->meshes[b];
-        for (int f = 0; f < mh.nfaces; ++f) {
-            ShadeRec& r = shade[size_t(start[b] + f)];
+    host_parallel_for(ntris, [&](int64_t tb, int64_t te) {
+        for (int64_t t = tb; t < te; ++t) {
+            const int b = tri_bundle[size_t(t)];
+            const MeshHost& mh = s->meshes[b];
+            const int f = int(t - start[b]);
+            ShadeRec& r = shade[size_t(t)];
             v3 p1 = mh.verts[mh.vi[3 * f]], p2 = mh.verts[mh.vi[3 * f + 1]], p3 = mh.verts[mh.vi[3 * f + 2]];
             v3 n1 = mh.normals[mh.ni[3 * f]], n2 = mh.normals[mh.ni[3 * f + 1]], n3 = mh.normals[mh.ni[3 * f + 2]];
             const float* t1 = &mh.uvs[2 * size_t(mh.ti[3 * f])];
@@ -374,7 +410,8 @@ static int commit_scene(bg_scene* s, const bg_build_opts* opts) {
             r.f = make_float4(n3.x, n3.y, n3.z, t2[1]);
             r.g = make_float4(t3[0], t3[1], 0.f, 0.f);
         }
-    }
+    });
+    const auto tb2 = std::chrono::steady_clock::now();
     int rc;
     if ((rc = s->nodes.ensure(std::max<size_t>(1, br.nodes.size()) * sizeof(WideNode4))) ||
         (rc = s->nodes8.ensure(std::max<size_t>(1, br.nodes8.size()) * sizeof(QNode8))) ||
@@ -428,6 +465,9 @@ static int commit_scene(bg_scene* s, const bg_build_opts* opts) {
     info.nmaterials = nmat;
     info.nlights = int(lights.size());
     info.build_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    info.bvh_ms = std::chrono::duration<double, std::milli>(tb1 - tb0).count();
+    info.records_ms = std::chrono::duration<double, std::milli>(tb2 - tb1).count();
+    info.upload_ms = std::chrono::duration<double, std::milli>(t1 - tb2).count();
     s->committed = true;
     return BG_OK;
 }

@@ -44,6 +44,10 @@ struct Bin {
 
 class Builder {
 public:
+    // adopt an existing binary tree (root = node 0) for the wide collapses only
+    Builder(std::vector<BNode>&& nodes, std::vector<int32_t>&& order, const BuildParams& p)
+        : n_(int64_t(order.size())), p_(p), idx_(std::move(order)), nodes_(std::move(nodes)) {}
+
     Builder(const float* lo, const float* hi, int64_t n, const BuildParams& p)
         : n_(n), p_(p), tlo_(3 * n), thi_(3 * n), cen_(3 * n), idx_(n), nodes_(2 * n) {
         for (int64_t i = 0; i < n; ++i) {
@@ -88,10 +92,11 @@ public:
                 int32_t kids[1] = {0};
                 r.nodes8.push_back(QNode8{});
                 int32_t code = encode_leaf(nodes_[0].start, nodes_[0].count);
-                fill_qnode(r.nodes8[0], kids, &code, 1);
+                if (!fill_qnode(r.nodes8[0], kids, &code, 1)) q8_failed_ = true;
                 r.max_depth8 = 1; r.max_stack8 = 1;
             } else {
                 emit8(r, 0, 1, 0);
+                run_q8_jobs(r);
             }
         }
         return r;
@@ -176,14 +181,56 @@ private:
             const BNode& c = nodes_[kids[i]];
             codes[i] = c.count > 0 ? encode_leaf(c.start, c.count) : emit8(r, kids[i], depth + 1, stack_here);
         }
-        fill_qnode(r.nodes8[me], kids, codes, nk);
+        Q8Job job;
+        job.node = me;
+        job.nk = nk;
+        for (int i = 0; i < nk; ++i) { job.kids[i] = kids[i]; job.codes[i] = codes[i]; }
+        q8_jobs_.push_back(job);
         return me;
+    }
+
+    struct Q8Job {
+        int32_t node, nk;
+        int32_t kids[8], codes[8];
+    };
+    std::vector<Q8Job> q8_jobs_;
+
+    // quantise every recorded 8-wide node (independent per node) on the host's cores
+    void run_q8_jobs(BuildResult& r) {
+        const int64_t n = int64_t(q8_jobs_.size());
+        const int hw = std::max(1, std::min(64, int(std::thread::hardware_concurrency())));
+        const int nt = int(std::min<int64_t>(hw, std::max<int64_t>(1, n / 4096)));
+        std::atomic<bool> failed{false};
+        auto work = [&](int64_t b, int64_t e) {
+            bool f = false;
+            for (int64_t i = b; i < e; ++i) {
+                const Q8Job& j = q8_jobs_[size_t(i)];
+                f = !fill_qnode(r.nodes8[size_t(j.node)], j.kids, j.codes, j.nk) || f;
+            }
+            if (f) failed = true;
+        };
+        if (nt <= 1) {
+            work(0, n);
+        } else {
+            std::vector<std::thread> th;
+            const int64_t chunk = (n + nt - 1) / nt;
+            for (int k = 0; k < nt; ++k) {
+                const int64_t b = k * chunk, e = std::min(n, b + chunk);
+                if (b < e) th.emplace_back(work, b, e);
+            }
+            for (auto& t : th) t.join();
+        }
+        if (failed) q8_failed_ = true;
+        q8_jobs_.clear();
+        q8_jobs_.shrink_to_fit();
     }
 
     // Slot assignment (greedy over child x slot by projected centroid: slot s
     // takes the child furthest upstream for directions with sign bits s) and
     // conservative quantisation of the children's boxes.
-    void fill_qnode(QNode8& q, const int32_t* kids, const int32_t* codes, int nk) const {
+    // returns false when a plane cannot be made conservative (coordinates too large)
+    bool fill_qnode(QNode8& q, const int32_t* kids, const int32_t* codes, int nk) const {
+        bool ok = true;
         Box u; u.clear();
         for (int i = 0; i < nk; ++i) u.grow(nodes_[kids[i]].box);
         double cen[8][3];
@@ -211,7 +258,7 @@ private:
         double k[3];
         for (int a = 0; a < 3; ++a) {
             e[a] = qnode_axis(u.lo[a], u.hi[a], &k[a]);
-            if (e[a] > kQMaxExp) { q8_failed_ = true; e[a] = kQMaxExp; }
+            if (e[a] > kQMaxExp) { ok = false; e[a] = kQMaxExp; }
         }
         float* o2[3] = {&q.o2x, &q.o2y, &q.o2z};
         for (int a = 0; a < 3; ++a) *o2[a] = float(std::ldexp(k[a] - 8388608.0, e[a]));
@@ -242,7 +289,7 @@ private:
                 const float st = std::ldexp(1.0f, e[a]);
                 const float plo = std::fma(8388608.0f + float(qb[a][0][sl]), st, *o2[a]);
                 const float phi = std::fma(8388608.0f + float(qb[a][1][sl]), st, *o2[a]);
-                if (!(plo <= b.lo[a] && phi >= b.hi[a])) q8_failed_ = true;
+                if (!(plo <= b.lo[a] && phi >= b.hi[a])) ok = false;
             }
         }
         uint32_t* w[3] = {q.qx, q.qy, q.qz};
@@ -253,6 +300,7 @@ private:
                     for (int j = 0; j < 4; ++j) v |= uint32_t(qb[a][h][4 * half + j]) << (8 * j);
                     w[a][2 * h + half] = v;
                 }
+        return ok;
     }
 
     void make_leaf(int64_t nodeidx, int64_t begin, int64_t end, const Box& box) {
@@ -272,23 +320,59 @@ private:
         Box bl, br, cbl, cbr;
         int64_t nl_best = 0;
         const int B = p_.bins;
-        std::vector<Bin> bins(size_t(3 * B));
+        // per-thread scratch, reused by every node this thread splits (bins are
+        // consumed before the recursion)
+        thread_local std::vector<Bin> bins;
+        thread_local std::vector<float> rarea;
+        thread_local std::vector<int64_t> rcount;
+        bins.resize(size_t(3 * B));
+        rarea.resize(size_t(B));
+        rcount.resize(size_t(B));
         float inv_area = box.area() > 0.f ? 1.f / box.area() : 0.f;
+        // large nodes (the top of the tree, where few subtrees run in parallel yet)
+        // bin their triangles in chunks on the host's cores and merge the bins;
+        // bin contents are unions and counts, so the result is order-independent
+        const int64_t kParBin = 262144;
+        int nbt = 1;
+        if (m >= kParBin) {
+            const int hw = std::max(1, std::min(32, int(std::thread::hardware_concurrency())));
+            nbt = int(std::min<int64_t>(hw, m / 65536));
+        }
         for (int axis = 0; axis < 3; ++axis) {
             float ext = cbox.hi[axis] - cbox.lo[axis];
             if (!(ext > 0.f)) continue;
             float scale = float(B) / ext;
             Bin* bb = &bins[size_t(axis * B)];
             for (int i = 0; i < B; ++i) { bb[i].box.clear(); bb[i].cbox.clear(); bb[i].count = 0; }
-            for (int64_t k = begin; k < end; ++k) {
-                int32_t t = idx_[k];
-                int bi = std::min(B - 1, std::max(0, int((cen_[3 * t + axis] - cbox.lo[axis]) * scale)));
-                bb[bi].box.grow(&tlo_[3 * t], &thi_[3 * t]);
-                bb[bi].cbox.grow_pt(&cen_[3 * t]);
-                ++bb[bi].count;
+            auto bin_range = [&](int64_t kb, int64_t ke, Bin* out) {
+                for (int64_t k = kb; k < ke; ++k) {
+                    int32_t t = idx_[k];
+                    int bi = std::min(B - 1, std::max(0, int((cen_[3 * t + axis] - cbox.lo[axis]) * scale)));
+                    out[bi].box.grow(&tlo_[3 * t], &thi_[3 * t]);
+                    out[bi].cbox.grow_pt(&cen_[3 * t]);
+                    ++out[bi].count;
+                }
+            };
+            if (nbt <= 1) {
+                bin_range(begin, end, bb);
+            } else {
+                std::vector<Bin> part(size_t(nbt) * B);
+                for (Bin& x : part) { x.box.clear(); x.cbox.clear(); x.count = 0; }
+                std::vector<std::thread> th;
+                const int64_t chunk = (m + nbt - 1) / nbt;
+                for (int k = 0; k < nbt; ++k) {
+                    const int64_t b = begin + k * chunk, e = std::min(end, b + chunk);
+                    if (b < e) th.emplace_back(bin_range, b, e, &part[size_t(k) * B]);
+                }
+                for (auto& t : th) t.join();
+                for (int k = 0; k < nbt; ++k)
+                    for (int i = 0; i < B; ++i) {
+                        const Bin& x = part[size_t(k) * B + i];
+                        bb[i].box.grow(x.box);
+                        bb[i].cbox.grow(x.cbox);
+                        bb[i].count += x.count;
+                    }
             }
-            std::vector<float> rarea(B);
-            std::vector<int64_t> rcount(B);
             Box acc; acc.clear();
             int64_t cnt = 0;
             for (int i = B - 1; i > 0; --i) {
@@ -391,6 +475,24 @@ int qnode_axis(float L, float H, double* k) {
     }
     *k = 0.0;
     return kQMaxExp + 1;
+}
+
+BuildResult collapse_binary(const BinaryTree& t, const BuildParams& p) {
+    std::vector<BNode> nodes(t.left.size());
+    for (size_t i = 0; i < nodes.size(); ++i) {
+        BNode& b = nodes[i];
+        for (int k = 0; k < 3; ++k) { b.box.lo[k] = t.box[6 * i + k]; b.box.hi[k] = t.box[6 * i + 3 + k]; }
+        b.left = t.left[i]; b.right = t.right[i];
+        b.start = t.start[i]; b.count = t.count[i];
+    }
+    std::vector<int32_t> order = t.order;
+    Builder b(std::move(nodes), std::move(order), p);
+    BuildResult r = b.collapse();
+    if (b.q8_failed_) {
+        r.nodes8.clear();
+        r.max_depth8 = r.max_stack8 = 0;
+    }
+    return r;
 }
 
 BuildResult build_wide_bvh(const float* lo, const float* hi, int64_t n, const BuildParams& p) {

@@ -85,6 +85,8 @@ namespace bg {
 constexpr int kTraceThreads = 128;
 constexpr int kDefaultNodeWidth = 4;   // active layout when both are built
 void set_width_info(bg_scene* s);
+struct BinaryTree;
+int gpu_build_tree(const float* lo, const float* hi, int64_t n, int max_leaf, BinaryTree& t);   // gpu_build.cu
 constexpr int kWorkSlots = 256;
 unsigned long long* next_work_counter(bg_scene* s);
 void scene_launch_setup(bg_scene* s);

@@ -201,6 +201,29 @@ def raycast_c2(ctx, nrays=1 << 24, reps=5):
             "bytes_per_ray": bpr, "achieved_gbs": bpr * nrays / (ms * 1e-3) / 1e9}
         del dr, res, sub
     gs.close()
+    # device LBVH build (Morton order) of the same soup: build time and traversal with the looser tree
+    t0 = time.perf_counter()
+    gl = capi.GpuScene(ctx, scenes.soup(1 << 20, seed=1), builder=1)
+    lb = {"build_ms": gl.info()["build_ms"], "build_wall_s": time.perf_counter() - t0}
+    for width in (4, 8):
+        gl.set_node_width(width)
+        for kind in ("coherent", "incoherent"):
+            rays = scenes.soup_rays(nrays, kind, seed=2)
+            dr = torch.from_numpy(rays.view(np.uint8)).cuda()
+            res = torch.zeros(nrays * 16, dtype=torch.uint8, device="cuda")
+            for _ in range(2):
+                gl.intersect_closest(dr.data_ptr(), res.data_ptr(), nrays)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(reps):
+                gl.intersect_closest(dr.data_ptr(), res.data_ptr(), nrays)
+            e1.record()
+            torch.cuda.synchronize()
+            lb["layout%d_%s_closest_mrays_per_s" % (width, kind)] = nrays / (e0.elapsed_time(e1) / reps) / 1e3
+            del dr, res
+    gl.close()
+    out["device_lbvh"] = lb
     return out
 
 
@@ -252,6 +275,11 @@ def batch_c4(ctx, nscenes=64, seed=7, timed_frames=1, rank=0, world=1, dist=None
     build_s = time.perf_counter() - t0
     for g in gss:
         g.close()
+    # the same scenes built by the device LBVH builder (build time only; the batch renders the SAH trees)
+    t1 = time.perf_counter()
+    for sc, _ in items:
+        capi.GpuScene(ctx, sc, builder=1).close()
+    lbvh_build_s = time.perf_counter() - t1
     bufs, jobs = [], []
     for k, (sc, spp) in enumerate(items):
         acc = torch.zeros((sc.height, sc.width, 4), dtype=torch.float32, device="cuda")
@@ -278,6 +306,7 @@ def batch_c4(ctx, nscenes=64, seed=7, timed_frames=1, rank=0, world=1, dist=None
     return {"scenes": nscenes, "triangles_total": sum(sc.ntriangles for sc, _ in all_items),
             "camera_samples": samples, "scenes_per_rank": len(items), "node_width": info["node_width"],
             "ms": ms, "msamples_per_s": samples / ms / 1e3, "autotune": tune, "build_s": build_s,
+            "build_s_device_lbvh": lbvh_build_s,
             "resolutions": sorted({"%dx%d" % (sc.width, sc.height) for sc, _ in all_items}),
             "spp_range": [min(s for _, s in all_items), max(s for _, s in all_items)],
             "triangle_range": [min(sc.ntriangles for sc, _ in all_items),

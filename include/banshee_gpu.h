@@ -147,7 +147,8 @@ typedef struct bg_build_opts {
                                active one switchable (bg_scene_set_node_width) */
     int32_t max_leaf_size;  /* triangles per leaf, 1..16 (0 = default 4)*/
     int32_t sah_bins;       /* binned-SAH bins (0 = default 32)         */
-    int32_t reserved;
+    int32_t builder;        /* 0 = host binned SAH; 1 = device LBVH
+                               (Morton order, faster build, looser tree)  */
 } bg_build_opts;
 
 typedef struct bg_scene_info {
@@ -165,6 +166,9 @@ typedef struct bg_scene_info {
     double  build_ms;       /* host build + upload time                   */
     int32_t node_width;     /* active node layout: 4 or 8                  */
     int32_t node_widths;    /* layouts built: 4 | 8                        */
+    double  bvh_ms;         /* of build_ms: tree build + wide collapses    */
+    double  records_ms;     /*              triangle / shading records     */
+    double  upload_ms;      /*              device allocation and upload   */
 } bg_scene_info;
 
 /* ---------------------------------------------------------------- tracing */
