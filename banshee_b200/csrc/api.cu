@@ -68,7 +68,10 @@ k_trace(DevScene S, const float4* __restrict__ rays, int64_t n_static, const int
     const int64_t n_all = n_dev ? int64_t(*n_dev) : n_static;
     const int64_t n = COUNT ? (n_all + stride - 1) / stride : n_all;
     const unsigned lane = threadIdx.x & 31u;
-    int2 stack[stack_entries<WIDTH>()];
+    constexpr int kSm = smem_stack_entries<WIDTH>();
+    int2 lstack[stack_entries<WIDTH>() - kSm];
+    __shared__ int2 sstack[kSm > 0 ? kSm : 1][THREADS];
+    const RayStack<kSm> stack{&sstack[0][threadIdx.x], lstack, THREADS};
     TravState s;
     Counters cnt{0ull, 0ull, 0ull};
     int64_t ridx = -1;

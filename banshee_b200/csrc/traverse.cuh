@@ -23,6 +23,10 @@ namespace bg {
 
 constexpr int kStackSize = 64;     // entries per ray, 4-wide; the builder checks max_stack against it
 constexpr int kStackSize8 = 96;    // entries per ray, 8-wide (up to 7 pushes per level)
+// stack entries per ray kept in shared memory: 8 for the 4-wide traversal
+// (measured: +6 % incoherent / +3 % coherent ray casts), none for the 8-wide one
+template <int WIDTH>
+__host__ __device__ constexpr int smem_stack_entries() { return WIDTH == 4 ? 8 : 0; }
 template <int WIDTH>
 __host__ __device__ constexpr int stack_entries() { return WIDTH == 8 ? kStackSize8 : kStackSize; }
 constexpr int kRefillSteps = 24;   // traversal steps between warp refill points
@@ -173,6 +177,23 @@ __device__ __forceinline__ uint32_t octant_order(uint32_t m, uint32_t oct) {
     return m;
 }
 
+// Traversal stack: the first SM entries of each ray live in shared memory
+// (entry-major, one column per thread), deeper entries in local memory.
+template <int SM>
+struct RayStack {
+    int2* sm;        // &shared[0][threadIdx.x]; entry i at sm[i * stride]
+    int2* lm;        // local array; entry i >= SM at lm[i - SM]
+    int stride;
+    __device__ __forceinline__ void put(int i, int2 v) const {
+        if (SM > 0 && i < SM) sm[i * stride] = v;
+        else lm[i - SM] = v;
+    }
+    __device__ __forceinline__ int2 get(int i) const {
+        if (SM > 0 && i < SM) return sm[i * stride];
+        return lm[i - SM];
+    }
+};
+
 struct Counters {
     unsigned long long rays, nodes, tris;
 };
@@ -199,15 +220,16 @@ __device__ __forceinline__ void trav_init(TravState& s, float4 a, float4 b) {
 }
 
 // Runs at most `steps` node / leaf visits.  Returns true when the ray is done.
-template <bool ANY, bool COUNT, int WIDTH>
-__device__ __forceinline__ bool trav_steps(const DevScene& S, TravState& s, int2* stack, int steps, Counters& cnt) {
+template <bool ANY, bool COUNT, int WIDTH, class STACK>
+__device__ __forceinline__ bool trav_steps(const DevScene& S, TravState& s, const STACK& stack, int steps,
+                                           Counters& cnt) {
     for (int it = 0; it < steps; ++it) {
         int item = s.item;
         if (item == kNone) {
             // pop, culling entries that start beyond the closest hit
             bool found = false;
             while (s.sp > 0) {
-                int2 e = stack[--s.sp];
+                int2 e = stack.get(--s.sp);
                 if (!ANY && __int_as_float(e.y) > s.best) continue;
                 item = e.x;
                 found = true;
@@ -235,7 +257,7 @@ __device__ __forceinline__ bool trav_steps(const DevScene& S, TravState& s, int2
 #pragma unroll
             for (int sl = 0; sl < 8; ++sl) {
                 const int i = sl ^ int(s.r.oct);
-                if ((rest >> i) & 1u) stack[s.sp + __popc(rest >> (i + 1))] = make_int2(ch[sl], __float_as_int(tn[sl]));
+                if ((rest >> i) & 1u) stack.put(s.sp + __popc(rest >> (i + 1)), make_int2(ch[sl], __float_as_int(tn[sl])));
                 if (i == first) next = ch[sl];
             }
             s.sp += nrest;
@@ -269,7 +291,7 @@ __device__ __forceinline__ bool trav_steps(const DevScene& S, TravState& s, int2
                 atomicOr(S.errflags, BG_FLAG_STACK_OVERFLOW);
                 return true;
             }
-            for (int i = nh - 1; i >= 1; --i) stack[s.sp++] = make_int2(hc[i], __float_as_int(ht[i]));
+            for (int i = nh - 1; i >= 1; --i) stack.put(s.sp++, make_int2(hc[i], __float_as_int(ht[i])));
             s.item = hc[0];
         } else {
             // leaf: bit 31 set, count-1 in bits 27..30, first triangle in bits 0..26

@@ -209,3 +209,24 @@ def test_device_builder_golden_cornell(width, ctx):
     got = gs.intersect_closest_host(g["rays"])
     assert (got["primid"] == g["hits"]["primid"]).all()
     assert (_bits(got["t"]) == _bits(g["hits"]["t"])).all()
+
+
+def test_traversal_work_guard_vs_reference_bvh(width, ctx, oracle_built):
+    """The roofline's algorithmic bytes count the triangles our traversal tests;
+    guard against inflating them: per ray we test no more triangles than the
+    reference Bvh (binary, one triangle per leaf, left-first) on the same rays,
+    and visit far fewer nodes."""
+    import torch
+    from banshee_b200 import capi
+    sc = scenes.soup(200_000, seed=31)
+    gs = capi.GpuScene(ctx, sc)
+    gs.set_node_width(width)
+    o = oracle_built.Oracle(sc)
+    for kind in ("incoherent", "coherent"):
+        rays = scenes.soup_rays(1 << 12, kind, seed=32)
+        dr = torch.from_numpy(rays.view(np.uint8)).cuda()
+        n_ours, t_ours = gs.traversal_counts(dr.data_ptr(), rays.shape[0])
+        n_ref, t_ref = o.traversal_counts(rays)
+        print("%s width %d: ours %.2f nodes %.2f tris / ray, reference Bvh %.2f nodes %.2f tris / ray" % (
+            kind, width, n_ours / len(rays), t_ours / len(rays), n_ref / len(rays), t_ref / len(rays)))
+        assert t_ours <= t_ref and n_ours < n_ref
