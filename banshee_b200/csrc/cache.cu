@@ -558,7 +558,12 @@ int nrc_train_step(bg_cache* c, const float* feat, const float4* target, const i
     T.dX = c->dX.as<float>();
     T.loss = c->loss.as<float>();
     T.B = B;
-    k_nrc_train<<<c->sms * 2, 128, kTrainSmem, st>>>(c->dev, T, n_dev, offset, B);
+    if (c->desc.mlp_kernel == 0) {
+        TcTrainArgs A{T.X, T.target, T.H, T.DZ, T.DZ5, T.dX, T.loss, T.B};
+        k_nrc_train_tc<<<c->sms * 2, 128, kTtSmem, st>>>(c->dev, A, n_dev, offset, B, c->scene->dev.errflags);
+    } else {
+        k_nrc_train<<<c->sms * 2, 128, kTrainSmem, st>>>(c->dev, T, n_dev, offset, B);
+    }
     const int wg = c->sms;
     const __nv_bfloat16* H = c->H.as<__nv_bfloat16>();
     const __nv_bfloat16* DZ = c->DZ.as<__nv_bfloat16>();
@@ -647,6 +652,7 @@ int bg_cache_create(bg_scene* s, const bg_cache_desc* d, bg_cache** out) {
     }
     cudaFuncSetAttribute(k_nrc_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, kInferSmem);
     cudaFuncSetAttribute(k_nrc_infer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
+    cudaFuncSetAttribute(k_nrc_train_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kTtSmem);
     cudaFuncSetAttribute(k_nrc_train, cudaFuncAttributeMaxDynamicSharedMemorySize, kTrainSmem);
     if ((rc = cache_init_params(c))) { bg_cache_destroy(c); return rc; }
     *out = c;

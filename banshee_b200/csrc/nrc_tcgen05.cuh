@@ -44,9 +44,11 @@ __device__ __forceinline__ uint64_t tc_desc(uint32_t saddr, uint32_t lbo, uint32
            (uint64_t((sbo >> 4) & 0x3FFFu) << 32) | (uint64_t(1) << 46);   // version 1, no swizzle
 }
 
-// kind::f16 instruction descriptor: bf16 x bf16 -> f32, both K-major, M = 128
-__host__ __device__ constexpr uint32_t tc_idesc(int N) {
-    return (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(N >> 3) << 17) | (uint32_t(kTcRows >> 4) << 24);
+// kind::f16 instruction descriptor: bf16 x bf16 -> f32, A K-major, B K-major
+// (b_mn = false) or MN-major (b_mn = true), M = 128
+__host__ __device__ constexpr uint32_t tc_idesc(int N, bool b_mn = false) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | (b_mn ? (1u << 16) : 0u) | (uint32_t(N >> 3) << 17) |
+           (uint32_t(kTcRows >> 4) << 24);
 }
 
 __device__ __forceinline__ void tc_mma(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t acc) {
@@ -201,6 +203,227 @@ __global__ void __launch_bounds__(128, 2) k_nrc_infer_tc(NrcDev C, const __nv_bf
         if (abort_flag) break;
     }
     // after a timeout, give the outstanding MMA group one more bounded wait before freeing its TMEM
+    if (abort_flag && tid == 0) tc_wait(bar, phase ^ 1u);
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(kTcCols) : "memory");
+    }
+}
+
+
+// ------------------------------------------------------------- training
+// Fused forward + backward of one Adam step's rows on tcgen05, same outputs as
+// the mma.sync k_nrc_train: hidden activations H[l] and layer-output gradients
+// DZ[l] (bf16, for the weight-gradient kernels), DZ5, the hash-grid feature
+// gradient dX (fp32, 32 columns) and the summed relative-L2 loss.
+//
+// The backward products dH = dZ * W need B = W with the layer's input features
+// as N: the forward weight tiles already hold W[out][in] in 8x8 core matrices
+// of 8 rows (out) x 16 contiguous bytes (in), which is exactly an MN-major B
+// core matrix (8 K-rows x 8 contiguous N elements), so the backward reads the
+// same shared memory through MN-major descriptors (SBO = 128 bytes between
+// groups of 8 inputs, LBO = KC * 128 bytes between groups of 8 outputs).
+// Each thread keeps its row's ReLU masks (64 bits per hidden layer) in registers.
+constexpr int kTtA0 = kTcA0;                 // input tile; reused for the dZ5 tile after layer 0
+constexpr int kTtSmem = kTcSmem;
+
+struct TcTrainArgs {
+    const __nv_bfloat16* X;      // encoded inputs of this step's rows [B][128]
+    const float4* target;        // this step's targets [B] (already offset)
+    __nv_bfloat16* H;            // [5][B][64]
+    __nv_bfloat16* DZ;           // [5][B][64]
+    __nv_bfloat16* DZ5;          // [B][16]
+    float* dX;                   // [B][32]
+    float* loss;
+    int B;
+};
+
+__global__ void __launch_bounds__(128, 2) k_nrc_train_tc(NrcDev C, TcTrainArgs T, const int* n_dev, int offset,
+                                                         int limit, unsigned* __restrict__ errflags) {
+    extern __shared__ __align__(1024) unsigned char tt_smem[];
+    unsigned char* smem = tt_smem;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t sbase = uint32_t(__cvta_generic_to_shared(smem));
+    const uint32_t bar = sbase + kTcBar;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + kTcBar + 8);
+    __shared__ int abort_flag;
+
+    tc_load_weights(C.wb + kNrcW0, 64, 128, smem + kTcW0);
+    for (int l = 0; l < 4; ++l) tc_load_weights(C.wb + kNrcW1 + l * 4096, 64, 64, smem + kTcW1 + l * 8192);
+    tc_load_weights(C.wb + kNrcW5, 16, 64, smem + kTcW5);
+    if (tid == 0) {
+        abort_flag = 0;
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(bar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     :: "r"(sbase + kTcBar + 8), "r"(kTcCols) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+    const uint32_t trow = tmem + (uint32_t(warp * 32) << 16);
+
+    int n = n_dev ? *n_dev - offset : T.B;
+    if (limit > 0 && n > limit) n = limit;
+    if (n < 0) n = 0;
+    const float invn = n > 0 ? 1.f / (3.f * float(n)) : 0.f;
+    const int ntiles = (n + kTcRows - 1) / kTcRows;
+    uint32_t phase = 0;
+    float lsum = 0.f;
+
+    // one MMA group on the tile in `a` (K-major, KC chunks) with weights at `b`
+    auto run = [&](uint32_t a, int KC, uint32_t b, uint32_t b_lbo, uint32_t b_sbo, uint32_t b_kstep, uint32_t idesc) {
+        if (tid == 0) {
+            tc_fence_after();
+            for (int s = 0; s < KC / 2; ++s)
+                tc_mma(tmem, tc_desc(a + s * 256, 128, KC * 128), tc_desc(b + s * b_kstep, b_lbo, b_sbo), idesc,
+                       s > 0 ? 1u : 0u);
+            tc_commit(bar);
+        }
+        if (!tc_wait(bar, phase)) {
+            atomicOr(errflags, BG_FLAG_TIMEOUT);
+            abort_flag = 1;
+        }
+        phase ^= 1u;
+        tc_fence_after();
+        __syncthreads();
+        return abort_flag == 0;
+    };
+    // this thread's accumulator row (64 columns) -> 8 bf16 chunks, optionally masked / rectified
+    auto row64 = [&](uint32_t (&packed)[32], uint32_t (&mask)[2], bool relu, bool apply_mask) {
+#pragma unroll
+        for (int c4 = 0; c4 < 4; ++c4) {
+            float v[16];
+            tc_ld16(trow + uint32_t(c4 * 16), v);
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                const int col = c4 * 16 + j;
+                if (relu) {
+                    if (v[j] > 0.f) mask[col >> 5] |= 1u << (col & 31);
+                    v[j] = fmaxf(v[j], 0.f);
+                }
+                if (apply_mask && !((mask[col >> 5] >> (col & 31)) & 1u)) v[j] = 0.f;
+            }
+#pragma unroll
+            for (int j = 0; j < 8; ++j) packed[c4 * 8 + j] = tc_pack(v[2 * j], v[2 * j + 1]);
+        }
+    };
+    auto store_row = [&](const uint32_t (&packed)[32], __nv_bfloat16* g, int64_t grow, bool to_global) {
+        const int r = tid;
+#pragma unroll
+        for (int kc = 0; kc < 8; ++kc) {
+            const uint4 v = make_uint4(packed[4 * kc], packed[4 * kc + 1], packed[4 * kc + 2], packed[4 * kc + 3]);
+            *reinterpret_cast<uint4*>(smem + kTcA1 + tc_off(r, kc, 8)) = v;
+            if (to_global) reinterpret_cast<uint4*>(g + size_t(grow) * 64)[kc] = v;
+        }
+    };
+
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int64_t row0 = int64_t(tile) * kTcRows;
+        const int64_t grow = row0 + tid;
+        const bool live = grow < n;
+        for (int j = 0; j < 16; ++j) {
+            const int u = j * 4 + warp, rg = u >> 2, kq4 = u & 3;
+            const int r = rg * 8 + (lane & 7), kc = kq4 * 4 + (lane >> 3);
+            const int64_t g = row0 + r;
+            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+            if (g < n) v = *reinterpret_cast<const uint4*>(T.X + size_t(g) * kNrcIn + kc * 8);
+            *reinterpret_cast<uint4*>(smem + kTtA0 + tc_off(r, kc, 16)) = v;
+        }
+        tc_fence_async_smem();
+        tc_fence_before();
+        __syncthreads();
+        uint32_t masks[5][2];
+#pragma unroll
+        for (int l = 0; l < 5; ++l) masks[l][0] = masks[l][1] = 0u;
+        bool ok = true;
+        // ---- forward: hidden layers
+#pragma unroll
+        for (int l = 0; l < 5 && ok; ++l) {
+            ok = l == 0 ? run(sbase + kTtA0, 16, sbase + kTcW0, 128, 16 * 128, 256, tc_idesc(64))
+                        : run(sbase + kTcA1, 8, sbase + kTcW1 + (l - 1) * 8192, 128, 8 * 128, 256, tc_idesc(64));
+            if (!ok) break;
+            uint32_t packed[32];
+            row64(packed, masks[l], true, false);
+            store_row(packed, T.H + size_t(l) * T.B * 64, grow, live);
+            tc_fence_async_smem();
+            tc_fence_before();
+            __syncthreads();
+        }
+        if (!ok) break;
+        // ---- output layer and the loss gradient (columns 0..2 of 16)
+        if (!run(sbase + kTcA1, 8, sbase + kTcW5, 128, 8 * 128, 256, tc_idesc(16))) break;
+        {
+            float v[16];
+            tc_ld16(trow, v);
+            float g[16];
+#pragma unroll
+            for (int j = 0; j < 16; ++j) g[j] = 0.f;
+            if (live) {
+                const float* y = reinterpret_cast<const float*>(T.target + grow);
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    const float p = v[j], den = p * p + 0.01f, d = p - y[j];
+                    lsum += d * d / den;
+                    g[j] = 2.f * d / den * invn;
+                }
+            }
+            uint4 z0, z1;
+            z0.x = tc_pack(g[0], g[1]); z0.y = tc_pack(g[2], g[3]); z0.z = tc_pack(g[4], g[5]); z0.w = tc_pack(g[6], g[7]);
+            z1.x = tc_pack(g[8], g[9]); z1.y = tc_pack(g[10], g[11]); z1.z = tc_pack(g[12], g[13]); z1.w = tc_pack(g[14], g[15]);
+            // dZ5 tile [128 x 16] (K-major, 2 chunks) in the free input-tile space
+            *reinterpret_cast<uint4*>(smem + kTtA0 + tc_off(tid, 0, 2)) = z0;
+            *reinterpret_cast<uint4*>(smem + kTtA0 + tc_off(tid, 1, 2)) = z1;
+            if (live) {
+                reinterpret_cast<uint4*>(T.DZ5 + size_t(grow) * 16)[0] = z0;
+                reinterpret_cast<uint4*>(T.DZ5 + size_t(grow) * 16)[1] = z1;
+            }
+        }
+        tc_fence_async_smem();
+        tc_fence_before();
+        __syncthreads();
+        // ---- backward: dH4 = dZ5 W5 (K = 16 outputs, N = 64 inputs), then dH_{l-1} = dZ_l W_l
+        if (!run(sbase + kTtA0, 2, sbase + kTcW5, 8 * 128, 128, 2 * 8 * 128, tc_idesc(64, true))) break;
+#pragma unroll
+        for (int l = 4; l >= 0 && ok; --l) {
+            uint32_t packed[32];
+            row64(packed, masks[l], false, true);              // dZ_l = dH_l masked by ReLU'(z_l)
+            store_row(packed, T.DZ + size_t(l) * T.B * 64, grow, live);
+            tc_fence_async_smem();
+            tc_fence_before();
+            __syncthreads();
+            if (l > 0) {
+                ok = run(sbase + kTcA1, 8, sbase + kTcW1 + (l - 1) * 8192, 8 * 128, 128, 2 * 8 * 128,
+                         tc_idesc(64, true));
+            } else {
+                // dX = dZ0 W0, hash-grid columns 0..31 only
+                ok = run(sbase + kTcA1, 8, sbase + kTcW0, 16 * 128, 128, 2 * 16 * 128, tc_idesc(32, true));
+                if (ok) {
+                    float v0[16], v1[16];
+                    tc_ld16(trow, v0);
+                    tc_ld16(trow + 16u, v1);
+                    if (live) {
+                        float4* dst = reinterpret_cast<float4*>(T.dX + size_t(grow) * 32);
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) dst[q] = make_float4(v0[4 * q], v0[4 * q + 1], v0[4 * q + 2], v0[4 * q + 3]);
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) dst[4 + q] = make_float4(v1[4 * q], v1[4 * q + 1], v1[4 * q + 2], v1[4 * q + 3]);
+                    }
+                    tc_fence_before();
+                    __syncthreads();
+                }
+            }
+        }
+        if (!ok || abort_flag) break;
+    }
+    for (int off = 16; off > 0; off >>= 1) lsum += __shfl_down_sync(0xffffffffu, lsum, off);
+    if (lane == 0 && lsum != 0.f) atomicAdd(T.loss, lsum);
     if (abort_flag && tid == 0) tc_wait(bar, phase ^ 1u);
     __syncthreads();
     if (warp == 0) {

@@ -389,8 +389,8 @@ typedef struct bg_cache_desc {
     float bbox_min[3];         /* position normalisation; all zero = scene     */
     float bbox_max[3];         /* bounds                                       */
     uint64_t seed;             /* parameter initialisation                     */
-    int32_t mlp_kernel;        /* inference: 0 = tcgen05 (TMEM accumulators),
-                                  1 = mma.sync (register accumulators)         */
+    int32_t mlp_kernel;        /* inference and training: 0 = tcgen05 (TMEM
+                                  accumulators), 1 = mma.sync (registers)      */
     int32_t reserved;
 } bg_cache_desc;
 

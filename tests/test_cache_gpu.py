@@ -50,10 +50,11 @@ def _oracle_args(cache):
     return inf["resolutions"], cache.log2_table_size, inf["bmin"], inf["bscale"]
 
 
-def test_gradients_match_fp64_oracle(ctx):
+@pytest.mark.parametrize("mlp_kernel", [0, 1], ids=["tcgen05", "mma_sync"])
+def test_gradients_match_fp64_oracle(ctx, mlp_kernel):
     import torch
     from oracle import nrc_oracle as O
-    gs, cache = _cache(ctx, log2t=8)
+    gs, cache = _cache(ctx, log2t=8, mlp_kernel=mlp_kernel)
     rng = np.random.default_rng(3)
     mlp0, grid0, _, _ = cache.params()
     # non-trivial grid values so that the grid features matter
@@ -103,9 +104,10 @@ def test_forward_matches_oracle(ctx, mlp_kernel):
     assert err < 2e-2, err
 
 
-def test_adam_training_reduces_loss(ctx):
+@pytest.mark.parametrize("mlp_kernel", [0, 1], ids=["tcgen05", "mma_sync"])
+def test_adam_training_reduces_loss(ctx, mlp_kernel):
     import torch
-    gs, cache = _cache(ctx, log2t=12, learning_rate=1e-2)
+    gs, cache = _cache(ctx, log2t=12, learning_rate=1e-2, mlp_kernel=mlp_kernel)
     rng = np.random.default_rng(7)
     n = 16384
     feat = _features(n, rng)
@@ -202,4 +204,35 @@ def test_tcgen05_and_mma_sync_inference_agree(ctx):
         assert np.isfinite(a).all() and (a[:, 3] == 0).all()
         scale = np.abs(b[:, :3]).max() + 1e-6
         assert np.abs(a[:, :3] - b[:, :3]).max() < 2e-2 * scale, (n, np.abs(a - b).max(), scale)
+    assert gs.error_flags() == 0
+
+
+def test_tcgen05_training_matches_mma_sync(ctx):
+    """One training step's loss and gradients from the tcgen05 kernel against the
+    mma.sync kernel on the same rows (ragged count: partial 128-row tiles)."""
+    import torch
+    from banshee_b200 import capi
+    gs, c0 = _cache(ctx, log2t=10, mlp_kernel=0)
+    c1 = capi.RadianceCache(gs, log2_table_size=10, base_resolution=4, max_resolution=64,
+                            bbox=((0, 0, 0), (1, 1, 1)), mlp_kernel=1)
+    rng = np.random.default_rng(12)
+    m, g, _, _ = c0.params()
+    g = (rng.random(g.shape).astype(np.float32) - 0.5) * 0.5
+    c0.set_params(m, g)
+    c1.set_params(m, g)
+    n = 3000 + 77
+    feat = _features(n, rng)
+    target = np.zeros((n, 4), np.float32)
+    target[:, :3] = rng.random((n, 3))
+    fd = torch.from_numpy(feat).cuda()
+    td = torch.from_numpy(target).cuda()
+    l0 = c0.train(fd.data_ptr(), td.data_ptr(), n, apply=False)
+    l1 = c1.train(fd.data_ptr(), td.data_ptr(), n, apply=False)
+    _, _, d0, dg0 = c0.params()
+    _, _, d1, dg1 = c1.params()
+    assert abs(l0 - l1) <= 1e-3 * abs(l1) + 1e-7, (l0, l1)
+    for a, b in ((d0, d1), (dg0, dg1)):
+        a, b = a.astype(np.float64), b.astype(np.float64)
+        cos = a @ b / (np.linalg.norm(a) * np.linalg.norm(b) + 1e-30)
+        assert cos > 0.999 and np.linalg.norm(a - b) / (np.linalg.norm(b) + 1e-30) < 2e-2, cos
     assert gs.error_flags() == 0
