@@ -254,7 +254,7 @@ __device__ __forceinline__ void cache_features(const SHit& h, v3 wo, const MatRe
 }
 
 // One light's DirectIllumination terms (DiTracer::GetDi, ditracer.cpp:57-239, n = 1).
-__device__ __noinline__ void emit_di(const DevScene& S, const Queues& Q, int li, const SHit& h, const MatRec& M, v3 wo,
+__device__ __forceinline__ void emit_di(const DevScene& S, const Queues& Q, int li, const SHit& h, const MatRec& M, v3 wo,
                                         McRng& lr, McRng& br, int slot0, int path, int root) {
     const LightRec L = load_light(S, li);
     float lx, ly, bx, by;
