@@ -220,99 +220,119 @@ __device__ __forceinline__ void trav_init(TravState& s, float4 a, float4 b) {
 }
 
 // Runs at most `steps` node / leaf visits.  Returns true when the ray is done.
+// Pops the next stack entry, skipping entries that start beyond the closest
+// hit; false when the stack is empty.
+template <bool ANY, class STACK>
+__device__ __forceinline__ bool trav_pop(TravState& s, const STACK& stack, int& item) {
+    while (s.sp > 0) {
+        const int2 e = stack.get(--s.sp);
+        if (!ANY && __int_as_float(e.y) > s.best) continue;
+        item = e.x;
+        return true;
+    }
+    return false;
+}
+
+// Visits internal node `item`: continues with the nearest hit child (s.item),
+// pushes the others.  False on stack overflow (error flag raised).
+template <bool COUNT, int WIDTH, class STACK>
+__device__ __forceinline__ bool trav_node(const DevScene& S, TravState& s, const STACK& stack, int item,
+                                          Counters& cnt) {
+    if (COUNT) ++cnt.nodes;
+    if (WIDTH == 8) {
+        float tn[8];
+        int32_t ch[8];
+        const uint32_t mask = box8(S.nodes8, item, s.r, s.best, tn, ch);
+        if (mask == 0) { s.item = kNone; return true; }
+        // visit order i = slot ^ octant: continue with the first hit, push the
+        // others so that they pop in visit order
+        const uint32_t om = octant_order(mask, s.r.oct);
+        const uint32_t rest = om & (om - 1u);
+        const int first = __ffs(om) - 1;
+        const int nrest = __popc(rest);
+        if (s.sp + nrest > kStackSize8) {
+            atomicOr(S.errflags, BG_FLAG_STACK_OVERFLOW);
+            return false;
+        }
+        int next = kNone;
+#pragma unroll
+        for (int sl = 0; sl < 8; ++sl) {
+            const int i = sl ^ int(s.r.oct);
+            if ((rest >> i) & 1u) stack.put(s.sp + __popc(rest >> (i + 1)), make_int2(ch[sl], __float_as_int(tn[sl])));
+            if (i == first) next = ch[sl];
+        }
+        s.sp += nrest;
+        s.item = next;
+        return true;
+    }
+    float tn[4];
+    int32_t ch[4];
+    const uint32_t mask = box4(S.nodes, item, s.r, s.best, tn, ch);
+    // order the children by entry distance with a 4-input sorting network on
+    // registers (missed children get +inf and sort last)
+    const int nh = __popc(mask);
+    if (nh == 0) { s.item = kNone; return true; }
+    float ht[4];
+    int hc[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        ht[i] = (mask & (1u << i)) ? tn[i] : __int_as_float(0x7f800000);
+        hc[i] = ch[i];
+    }
+    auto cex = [&](int a, int b) {
+        const bool sw = ht[a] > ht[b];
+        const float ta = ht[a], tb = ht[b];
+        const int ca = hc[a], cb = hc[b];
+        ht[a] = sw ? tb : ta; ht[b] = sw ? ta : tb;
+        hc[a] = sw ? cb : ca; hc[b] = sw ? ca : cb;
+    };
+    cex(0, 1); cex(2, 3); cex(0, 2); cex(1, 3); cex(1, 2);
+    // push the farther ones (farthest first), continue with the nearest
+    if (s.sp + nh - 1 > kStackSize) {
+        atomicOr(S.errflags, BG_FLAG_STACK_OVERFLOW);
+        return false;
+    }
+#pragma unroll
+    for (int i = 3; i >= 1; --i)
+        if (i < nh) stack.put(s.sp++, make_int2(hc[i], __float_as_int(ht[i])));
+    s.item = hc[0];
+    return true;
+}
+
+// Tests the triangles of leaf code `item` (bit 31 set, count-1 in bits 27..30,
+// first triangle in bits 0..26).  True when an any-hit query found its hit.
+template <bool ANY, bool COUNT>
+__device__ __forceinline__ bool trav_leaf(const DevScene& S, TravState& s, int item, Counters& cnt) {
+    const uint32_t code = uint32_t(item);
+    const int count = int((code >> kLeafStartBits) & 15u) + 1;
+    const int start = int(code & uint32_t(kMaxLeafStart));
+    for (int k = 0; k < count; ++k) {
+        const float4* tp = reinterpret_cast<const float4*>(S.tris + start + k);
+        float4 v0 = __ldg(tp), e1 = __ldg(tp + 1), e2 = __ldg(tp + 2);
+        if (COUNT) ++cnt.tris;
+        obj_ray(S, s.r, __float_as_int(v0.w), s.cache);
+        float t, a, b;
+        if (mt_test(s.cache.o, s.cache.d, mk(v0.x, v0.y, v0.z), mk(e1.x, e1.y, e1.z), mk(e2.x, e2.y, e2.z),
+                    s.r.tmin, ANY ? s.r.tmax : s.best, t, a, b)) {
+            s.prim = __float_as_int(e1.w);
+            if (ANY) return true;
+            s.best = t; s.u = a; s.v = b;
+        }
+    }
+    return false;
+}
+
+// Runs at most `steps` node / leaf visits.  Returns true when the ray is done.
 template <bool ANY, bool COUNT, int WIDTH, class STACK>
 __device__ __forceinline__ bool trav_steps(const DevScene& S, TravState& s, const STACK& stack, int steps,
                                            Counters& cnt) {
     for (int it = 0; it < steps; ++it) {
         int item = s.item;
-        if (item == kNone) {
-            // pop, culling entries that start beyond the closest hit
-            bool found = false;
-            while (s.sp > 0) {
-                int2 e = stack.get(--s.sp);
-                if (!ANY && __int_as_float(e.y) > s.best) continue;
-                item = e.x;
-                found = true;
-                break;
-            }
-            if (!found) return true;
-        }
-        if (WIDTH == 8 && item >= 0) {
-            float tn[8];
-            int32_t ch[8];
-            if (COUNT) ++cnt.nodes;
-            const uint32_t mask = box8(S.nodes8, item, s.r, s.best, tn, ch);
-            if (mask == 0) { s.item = kNone; continue; }
-            // visit order i = slot ^ octant: continue with the first hit, push the
-            // others so that they pop in visit order
-            const uint32_t om = octant_order(mask, s.r.oct);
-            const uint32_t rest = om & (om - 1u);
-            const int first = __ffs(om) - 1;
-            const int nrest = __popc(rest);
-            if (s.sp + nrest > kStackSize8) {
-                atomicOr(S.errflags, BG_FLAG_STACK_OVERFLOW);
-                return true;
-            }
-            int next = kNone;
-#pragma unroll
-            for (int sl = 0; sl < 8; ++sl) {
-                const int i = sl ^ int(s.r.oct);
-                if ((rest >> i) & 1u) stack.put(s.sp + __popc(rest >> (i + 1)), make_int2(ch[sl], __float_as_int(tn[sl])));
-                if (i == first) next = ch[sl];
-            }
-            s.sp += nrest;
-            s.item = next;
-        } else if (WIDTH == 4 && item >= 0) {
-            float tn[4];
-            int32_t ch[4];
-            if (COUNT) ++cnt.nodes;
-            uint32_t mask = box4(S.nodes, item, s.r, s.best, tn, ch);
-            // order the children by entry distance with a 4-input sorting network on
-            // registers (missed children get +inf and sort last)
-            const int nh = __popc(mask);
-            if (nh == 0) { s.item = kNone; continue; }
-            float ht[4];
-            int hc[4];
-#pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                ht[i] = (mask & (1u << i)) ? tn[i] : __int_as_float(0x7f800000);
-                hc[i] = ch[i];
-            }
-            auto cex = [&](int a, int b) {
-                const bool sw = ht[a] > ht[b];
-                const float ta = ht[a], tb = ht[b];
-                const int ca = hc[a], cb = hc[b];
-                ht[a] = sw ? tb : ta; ht[b] = sw ? ta : tb;
-                hc[a] = sw ? cb : ca; hc[b] = sw ? ca : cb;
-            };
-            cex(0, 1); cex(2, 3); cex(0, 2); cex(1, 3); cex(1, 2);
-            // push the farther ones (farthest first), continue with the nearest
-            if (s.sp + nh - 1 > kStackSize) {
-                atomicOr(S.errflags, BG_FLAG_STACK_OVERFLOW);
-                return true;
-            }
-#pragma unroll
-            for (int i = 3; i >= 1; --i)
-                if (i < nh) stack.put(s.sp++, make_int2(hc[i], __float_as_int(ht[i])));
-            s.item = hc[0];
+        if (item == kNone && !trav_pop<ANY>(s, stack, item)) return true;
+        if (item >= 0) {
+            if (!trav_node<COUNT, WIDTH>(S, s, stack, item, cnt)) return true;
         } else {
-            // leaf: bit 31 set, count-1 in bits 27..30, first triangle in bits 0..26
-            uint32_t code = uint32_t(item);
-            int count = int((code >> kLeafStartBits) & 15u) + 1;
-            int start = int(code & uint32_t(kMaxLeafStart));
-            for (int k = 0; k < count; ++k) {
-                const float4* tp = reinterpret_cast<const float4*>(S.tris + start + k);
-                float4 v0 = __ldg(tp), e1 = __ldg(tp + 1), e2 = __ldg(tp + 2);
-                if (COUNT) ++cnt.tris;
-                obj_ray(S, s.r, __float_as_int(v0.w), s.cache);
-                float t, a, b;
-                if (mt_test(s.cache.o, s.cache.d, mk(v0.x, v0.y, v0.z), mk(e1.x, e1.y, e1.z), mk(e2.x, e2.y, e2.z),
-                            s.r.tmin, ANY ? s.r.tmax : s.best, t, a, b)) {
-                    s.prim = __float_as_int(e1.w);
-                    if (ANY) return true;
-                    s.best = t; s.u = a; s.v = b;
-                }
-            }
+            if (trav_leaf<ANY, COUNT>(S, s, item, cnt)) return true;
             s.item = kNone;
         }
     }
