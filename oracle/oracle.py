@@ -17,6 +17,7 @@ from banshee_b200 import abi
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libbanshee_ref.so")
+REF_GPU_SO = os.path.join(HERE, "_ref", "libbanshee_ref_gpu.so")
 
 _vp = C.c_void_p
 
@@ -44,8 +45,8 @@ def _load_oracle():
     return lib
 
 
-def _load_ref():
-    lib = C.CDLL(REF_SO)
+def _load_ref(path=REF_SO):
+    lib = C.CDLL(path)
     lib.ref_world_create.restype = _vp
     lib.ref_world_create.argtypes = [_vp, C.c_int32, _vp, C.c_int32, _vp, C.c_int32, _vp, C.c_int32]
     lib.ref_world_destroy.argtypes = [_vp]
@@ -65,12 +66,20 @@ _LIBS = {}
 
 def _lib(kind):
     if kind not in _LIBS:
-        _LIBS[kind] = _load_oracle() if kind == "oracle" else _load_ref()
+        if kind == "oracle":
+            _LIBS[kind] = _load_oracle()
+        elif kind == "ref_gpu":
+            lib = _load_ref(REF_GPU_SO)
+            lib.ref_world_use_gpu.restype = C.c_int32
+            lib.ref_world_use_gpu.argtypes = [_vp, _vp]
+            _LIBS[kind] = lib
+        else:
+            _LIBS[kind] = _load_ref()
     return _LIBS[kind]
 
 
 def available(kind="oracle"):
-    return os.path.exists(ORACLE_SO if kind == "oracle" else REF_SO)
+    return os.path.exists({"oracle": ORACLE_SO, "ref_gpu": REF_GPU_SO}.get(kind, REF_SO))
 
 
 def _addr(a):
@@ -205,3 +214,13 @@ def ref_mcrng_draws(seed, pixel, sample, n):
     out = np.zeros((n, 2), dtype=np.float32)
     _lib("ref").ref_mcrng_draws(seed, pixel, sample, n, _addr(out))
     return out
+
+
+class ReferenceOnGpu(Reference):
+    """Banshee's own sources whose World answers Intersect through the
+    GpuAccelerator adapter once use_gpu() is called (before: its own Bvh)."""
+    kind = "ref_gpu"
+
+    def use_gpu(self, gpu_scene_handle):
+        if self.lib.ref_world_use_gpu(self.w, gpu_scene_handle) != 0:
+            raise ValueError("GpuAccelerator rejected the world")

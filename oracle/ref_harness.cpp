@@ -47,6 +47,9 @@
 #include "camera/perspective_camera.h"
 #include "tracer/gitracer.h"
 #include "tracer/ditracer.h"
+#ifdef BANSHEE_GPU_ADAPTER
+#include "adapters/gpu_accelerator.h"
+#endif
 #include "tracer/aotracer.h"
 #include "sampler/sobol_sampler.h"
 #include "sampler/cmj_sampler.h"
@@ -281,6 +284,20 @@ void* ref_world_create(const bg_mesh_desc* meshes, int32_t nmeshes,
 }
 
 void ref_world_destroy(void* w) { delete static_cast<RefWorld*>(w); }
+
+#ifdef BANSHEE_GPU_ADAPTER
+/* Replaces the committed World's Bvh by the B200 library's scene through the
+ * GpuAccelerator adapter (the drop-in the integration guide describes). */
+int ref_world_use_gpu(void* w, void* gpu_scene) {
+    RefWorld* rw = static_cast<RefWorld*>(w);
+    try {
+        rw->world.accel_.reset(new GpuAccelerator(rw->world, static_cast<bg_scene*>(gpu_scene)));
+    } catch (...) {
+        return -1;
+    }
+    return 0;
+}
+#endif
 
 static void parallel_rays(int64_t n, int nthreads, const std::function<void(int64_t)>& fn) {
     int nt = nthreads > 0 ? nthreads : static_cast<int>(std::thread::hardware_concurrency());

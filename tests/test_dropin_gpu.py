@@ -1,0 +1,56 @@
+"""The drop-in itself: Banshee's own World, tracers, samplers and renderer
+(the reference sources compiled unmodified) with World::accel_ replaced by the
+GpuAccelerator adapter over the C ABI.  Every closest hit and every shadow
+query of the reference's GiTracer / DiTracer then comes from the GPU, and the
+images must be bit-identical to the same code running on its own Bvh."""
+import os
+
+import numpy as np
+import pytest
+
+from banshee_b200 import abi, scenes
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    from banshee_b200 import capi
+    return capi.Context(0)
+
+
+@pytest.fixture(scope="module")
+def ref_gpu():
+    from oracle import oracle
+    if not oracle.available("ref_gpu"):
+        pytest.skip("oracle/_ref/libbanshee_ref_gpu.so not built (needs the reference tree at build time)")
+    return oracle
+
+
+@pytest.mark.parametrize("width", [4, 8])
+@pytest.mark.parametrize("tracer", [abi.BG_TRACER_GI, abi.BG_TRACER_DI])
+def test_reference_tracer_over_gpu_accelerator(ctx, ref_gpu, tracer, width):
+    from banshee_b200 import capi
+    sc = scenes.cornell(24, 24)
+    gs = capi.GpuScene(ctx, sc)
+    gs.set_node_width(width)
+    ref = ref_gpu.ReferenceOnGpu(sc)
+    kw = dict(spp=4, seed=9, tracer=tracer, maxdepth=5, nthreads=4)
+    own = ref.render(**kw)                 # the reference's Bvh
+    ref.use_gpu(gs.h.value)
+    gpu = ref.render(**kw)                 # the same reference code, hits from the GPU
+    assert (own.view(np.uint32) == gpu.view(np.uint32)).all()
+    assert gs.error_flags() == 0
+
+
+def test_reference_production_scene_over_gpu_accelerator(ctx, ref_gpu):
+    """Transformed bundles (spheres), GGX, sun and environment."""
+    from banshee_b200 import capi
+    sc = scenes.production(24, 14, nterrain=32, nspheres=6, sphere_seg=10, seed=4)
+    gs = capi.GpuScene(ctx, sc)
+    ref = ref_gpu.ReferenceOnGpu(sc)
+    kw = dict(spp=2, seed=3, maxdepth=8, nthreads=4)
+    own = ref.render(**kw)
+    ref.use_gpu(gs.h.value)
+    gpu = ref.render(**kw)
+    assert (own.view(np.uint32) == gpu.view(np.uint32)).all()
