@@ -72,6 +72,9 @@ def _lib(kind):
             lib = _load_ref(REF_GPU_SO)
             lib.ref_world_use_gpu.restype = C.c_int32
             lib.ref_world_use_gpu.argtypes = [_vp, _vp]
+            lib.ref_gpu_renderer.restype = C.c_int32
+            lib.ref_gpu_renderer.argtypes = [_vp, _vp, _vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                                             C.c_int32, C.c_uint64, _vp]
             _LIBS[kind] = lib
         else:
             _LIBS[kind] = _load_ref()
@@ -220,6 +223,16 @@ class ReferenceOnGpu(Reference):
     """Banshee's own sources whose World answers Intersect through the
     GpuAccelerator adapter once use_gpu() is called (before: its own Bvh)."""
     kind = "ref_gpu"
+
+    def gpu_renderer(self, gpu_scene_handle, spp, frames, seed=1, tracer=abi.BG_TRACER_GI, maxdepth=5):
+        """GpuRenderer::Render called `frames` times (spp samples each) on this world."""
+        sc = self.scene
+        cam = sc.camera_desc()
+        accum = np.zeros((sc.height, sc.width, 4), dtype=np.float32)
+        if self.lib.ref_gpu_renderer(self.w, gpu_scene_handle, C.addressof(cam), tracer, maxdepth, sc.width,
+                                     sc.height, spp, frames, seed, _addr(accum)) != 0:
+            raise ValueError("GpuRenderer failed")
+        return accum
 
     def use_gpu(self, gpu_scene_handle):
         if self.lib.ref_world_use_gpu(self.w, gpu_scene_handle) != 0:

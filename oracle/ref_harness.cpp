@@ -49,6 +49,7 @@
 #include "tracer/ditracer.h"
 #ifdef BANSHEE_GPU_ADAPTER
 #include "adapters/gpu_accelerator.h"
+#include "adapters/gpu_renderer.h"
 #endif
 #include "tracer/aotracer.h"
 #include "sampler/sobol_sampler.h"
@@ -292,6 +293,22 @@ int ref_world_use_gpu(void* w, void* gpu_scene) {
     RefWorld* rw = static_cast<RefWorld*>(w);
     try {
         rw->world.accel_.reset(new GpuAccelerator(rw->world, static_cast<bg_scene*>(gpu_scene)));
+    } catch (...) {
+        return -1;
+    }
+    return 0;
+}
+
+/* Renders `frames` progressive frames of spp samples each through the
+ * GpuRenderer adapter (Renderer::Render) into accum_rgbw. */
+int ref_gpu_renderer(void* w, void* gpu_scene, const bg_camera_desc* c, int32_t tracer_kind, int32_t maxdepth,
+                     int32_t width, int32_t height, int32_t spp, int32_t frames, uint64_t seed, float* accum_rgbw) {
+    RefWorld* rw = static_cast<RefWorld*>(w);
+    bg_tracer_desc t = {tracer_kind, maxdepth, 0, 0.f};
+    bg_sampler_desc smp = {BG_SAMPLER_RANDOM, spp, seed, 0, 0};
+    try {
+        GpuRenderer r(static_cast<bg_scene*>(gpu_scene), *c, t, smp, width, height, accum_rgbw);
+        for (int f = 0; f < frames; ++f) r.Render(rw->world);
     } catch (...) {
         return -1;
     }

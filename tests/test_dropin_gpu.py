@@ -54,3 +54,17 @@ def test_reference_production_scene_over_gpu_accelerator(ctx, ref_gpu):
     ref.use_gpu(gs.h.value)
     gpu = ref.render(**kw)
     assert (own.view(np.uint32) == gpu.view(np.uint32)).all()
+
+
+def test_gpu_renderer_adapter_matches_reference_renderer(ctx, ref_gpu):
+    """Renderer::Render through the GpuRenderer adapter, 3 progressive frames of
+    4 samples, against the reference's own renderer with the same 12 samples."""
+    from banshee_b200 import capi
+    from banshee_b200.metrics import mean_image, relmse
+    sc = scenes.cornell(32, 32)
+    gs = capi.GpuScene(ctx, sc)
+    ref = ref_gpu.ReferenceOnGpu(sc)
+    got = ref.gpu_renderer(gs.h.value, spp=4, frames=3, seed=5, maxdepth=5)
+    want = ref.render(spp=12, seed=5, maxdepth=5, nthreads=4)
+    assert (got[..., 3] == want[..., 3]).all()
+    assert relmse(mean_image(got), mean_image(want)) < 1e-4
