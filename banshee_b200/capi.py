@@ -71,6 +71,8 @@ def lib():
             "bg_batch_autotune": [_vp, C.POINTER(abi.BatchJob), _i32, C.POINTER(abi.TracerDesc), _i32,
                                   C.POINTER(abi.TuneResult), _vp],
             "bg_batch_destroy": [_vp],
+            "bg_scene_autotune": [_vp, C.POINTER(abi.CameraDesc), C.POINTER(abi.TracerDesc), _i32, _i32, _i32, _vp,
+                                  C.POINTER(abi.TuneResult), _vp],
             "bg_cache_create": [_vp, C.POINTER(abi.CacheDesc), C.POINTER(_vp)],
             "bg_cache_destroy": [_vp],
             "bg_cache_info": [_vp, C.POINTER(_i32), C.POINTER(_i64), C.POINTER(_i32), C.POINTER(C.c_float)],
@@ -165,6 +167,17 @@ class GpuScene:
 
     def set_node_width(self, width):
         check(lib().bg_scene_set_node_width(self.h, int(width)))
+
+    def autotune(self, accum_dev, width, height, probe_spp=1, tracer=abi.BG_TRACER_GI, maxdepth=8, camera=None,
+                 stream=None):
+        """bg_scene_autotune: picks node width, traversal block size and paths per pass
+        for this scene and camera; accum_dev receives the probe samples."""
+        cam = self.scene.camera_desc() if camera is None else camera
+        tr = abi.TracerDesc(tracer, maxdepth, 0, 0.0)
+        res = abi.TuneResult()
+        check(lib().bg_scene_autotune(self.h, C.byref(cam), C.byref(tr), int(probe_spp), int(width), int(height),
+                                      accum_dev, C.byref(res), _stream_handle(stream)))
+        return {k: getattr(res, k) for k, _ in abi.TuneResult._fields_}
 
     # -- host-buffer entry points (synchronous) --------------------------------
     def intersect_closest_host(self, rays):

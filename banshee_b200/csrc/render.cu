@@ -1128,9 +1128,76 @@ static int render_impl(bg_scene* s, bg_cache* cache, const bg_camera_desc* cam, 
     return render_jobs(s, cache, jobs, tr, stats, st, false);
 }
 
+// Times every (node layout, traversal block size, paths per pass) candidate
+// on this scene with `probe_spp` samples per pixel into accum (which receives
+// them), keeps the fastest for later renders of the scene.
+static int scene_autotune(bg_scene* s, const bg_camera_desc* cam, const bg_tracer_desc* tr, int32_t probe_spp,
+                          int W, int H, float4* accum, bg_tune_result* result, cudaStream_t st) {
+    if (!s) return set_error(BG_ERR_INVALID_ARG, "scene is NULL");
+    if (!s->committed) return set_error(BG_ERR_STATE, "scene not committed");
+    if (!cam || !tr || !accum) return set_error(BG_ERR_INVALID_ARG, "NULL argument");
+    std::vector<int> widths;
+    if (s->dev.nodes) widths.push_back(4);
+    if (s->dev.nodes8) widths.push_back(8);
+    const int threads[2] = {128, 256};
+    const int64_t paths[4] = {int64_t(1) << 19, int64_t(1) << 20, int64_t(1) << 21, int64_t(1) << 22};
+    bg_sampler_desc sm = {BG_SAMPLER_RANDOM, std::max(1, probe_spp), 1, 0, 0};
+    float best = 1e30f;
+    int best_t = 128, best_w = s->dev.width, tried = 0, rc = BG_OK;
+    int64_t best_p = int64_t(1) << 21;
+    cudaEvent_t e0, e1;
+    BG_CUDA(cudaEventCreate(&e0));
+    BG_CUDA(cudaEventCreate(&e1));
+    for (int w : widths) {
+        s->dev.width = w;
+        for (int t : threads) {
+            for (int64_t p : paths) {
+                s->tune_threads = t;
+                s->tune_paths = p;
+                // the first render warms the graph and buffers of this candidate, the second is timed
+                if ((rc = render_impl(s, nullptr, cam, tr, &sm, W, H, accum, nullptr, st))) break;
+                BG_CUDA(cudaEventRecord(e0, st));
+                if ((rc = render_impl(s, nullptr, cam, tr, &sm, W, H, accum, nullptr, st))) break;
+                BG_CUDA(cudaEventRecord(e1, st));
+                BG_CUDA(cudaEventSynchronize(e1));
+                float ms = 0.f;
+                BG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+                ++tried;
+                if (ms < best) { best = ms; best_t = t; best_p = p; best_w = w; }
+            }
+            if (rc) break;
+        }
+        if (rc) break;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    s->dev.width = best_w;
+    set_width_info(s);
+    if (rc) return rc;
+    s->tune_threads = best_t;
+    s->tune_paths = best_p;
+    if (result) {
+        result->trace_threads = best_t;
+        result->paths_per_pass = int32_t(best_p);
+        result->candidates = tried;
+        result->ms = best;
+        result->msamples_per_s = best > 0.f ? float(double(W) * H * sm.spp / (double(best) * 1e3)) : 0.f;
+        result->node_width = best_w;
+    }
+    return BG_OK;
+}
+
 }  // namespace bg
 
 using namespace bg;
+
+extern "C" int bg_scene_autotune(bg_scene* s, const bg_camera_desc* cam, const bg_tracer_desc* tr, int32_t probe_spp,
+                                 int32_t W, int32_t H, float* accum, bg_tune_result* result, void* stream) {
+    if (!s) return set_error(BG_ERR_INVALID_ARG, "scene is NULL");
+    std::lock_guard<std::mutex> lk(s->mu);
+    return scene_autotune(s, cam, tr, probe_spp, W, H, reinterpret_cast<float4*>(accum), result,
+                          static_cast<cudaStream_t>(stream));
+}
 
 extern "C" int bg_render(bg_scene* s, const bg_camera_desc* cam, const bg_tracer_desc* tr, const bg_sampler_desc* sm,
                          int32_t W, int32_t H, float* accum, bg_render_stats* stats, void* stream) {

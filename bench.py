@@ -406,6 +406,10 @@ def main():
     stream = torch.cuda.current_stream()
     acc = torch.zeros((HEIGHT, WIDTH, 4), dtype=torch.float32, device="cuda")
     npix = WIDTH * HEIGHT
+    # the framework's autotuner picks node layout, traversal block size and paths per pass
+    tune = gs.autotune(acc.data_ptr(), WIDTH, HEIGHT, probe_spp=1, maxdepth=MAXDEPTH, stream=stream.cuda_stream)
+    acc.zero_()
+    info = gs.info()
 
     def step(i, stats=False, flags=0):
         return gs.render(acc.data_ptr(), WIDTH, HEIGHT, 1, seed=SEED,
@@ -527,7 +531,7 @@ def main():
                        "spp_per_step": 1, "maxdepth": MAXDEPTH, "parallelism": "dp%d (samples)" % world,
                        "l2": "inputs larger than L2: scene %.2f GB resident in HBM (126 MB L2)"
                              % ((info["node_bytes"] + info["tri_bytes"] + info["shade_bytes"]) / 1e9),
-                       "scene_build_s": t_scene},
+                       "scene_build_s": t_scene, "autotune": tune},
             "mrays_per_s": world * rays_per_step * args.steps / (ms * 1e-3) / 1e6,
             "rays_per_sample": rays_per_step / npix,
             "roofline": roofline,

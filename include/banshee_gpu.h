@@ -356,6 +356,14 @@ int bg_batch_render(bg_batch* batch, const bg_batch_job* jobs, int32_t njobs, co
 int bg_batch_autotune(bg_batch* batch, const bg_batch_job* jobs, int32_t njobs, const bg_tracer_desc* tracer,
                       int32_t probe_spp, bg_tune_result* result, void* stream);
 int bg_batch_destroy(bg_batch* batch);
+/* Autotuner for one scene and camera: the same candidates as
+ * bg_batch_autotune, each probed with probe_spp samples per pixel rendered
+ * into accum_rgbw_dev (clear it before the real render); the fastest is kept
+ * for later bg_render / bg_render_host calls of this scene.  No counterpart
+ * in the reference.  Synchronises. */
+int bg_scene_autotune(bg_scene* scene, const bg_camera_desc* camera, const bg_tracer_desc* tracer,
+                      int32_t probe_spp, int32_t width, int32_t height, float* accum_rgbw_dev,
+                      bg_tune_result* result, void* stream);
 
 /* ------------------------------------------------------------ images */
 /* FileImagePlane::Finalize (imageplane/fileimageplane.cpp:13-27): rgb[i] =

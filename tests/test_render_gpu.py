@@ -173,3 +173,21 @@ def test_node_layouts_give_identical_images(ctx):
         imgs.append(gs.render_host(96, 54, 8, seed=2, maxdepth=8))
     assert (imgs[0].view(np.uint32) == imgs[1].view(np.uint32)).all()
     assert gs.error_flags() == 0
+
+
+def test_scene_autotune_keeps_images_bit_identical(ctx):
+    """bg_scene_autotune only changes node layout, block size and pass size:
+    renders before and after it agree bit for bit."""
+    import torch
+    from banshee_b200 import capi
+    sc = scenes.production(80, 45, nterrain=48, nspheres=8, sphere_seg=10, seed=2)
+    gs = capi.GpuScene(ctx, sc)
+    before = gs.render_host(80, 45, 6, seed=4, maxdepth=8)
+    probe = torch.zeros((45, 80, 4), dtype=torch.float32, device="cuda")
+    res = gs.autotune(probe.data_ptr(), 80, 45, probe_spp=1, maxdepth=8)
+    torch.cuda.synchronize()
+    assert res["candidates"] == 16 and res["node_width"] in (4, 8) and res["trace_threads"] in (128, 256)
+    assert gs.info()["node_width"] == res["node_width"]
+    assert (probe.cpu().numpy()[..., 3] == 32).all()       # 16 candidates x 2 probe renders x 1 spp
+    after = gs.render_host(80, 45, 6, seed=4, maxdepth=8)
+    assert (before.view(np.uint32) == after.view(np.uint32)).all()
