@@ -16,12 +16,6 @@ namespace bg {
 
 static thread_local std::string g_error;
 
-static inline float i2f(int32_t v) {
-    float f;
-    memcpy(&f, &v, sizeof(f));
-    return f;
-}
-
 int set_error(int code, const char* fmt, ...) {
     char buf[1024];
     va_list ap;
@@ -217,23 +211,6 @@ static bool is_identity(const float* m) {
     return true;
 }
 
-// Runs f(begin, end) over [0, n) in contiguous chunks on the host's cores;
-// each index is written by exactly one thread, so results do not depend on the
-// thread count.
-template <class F>
-static void host_parallel_for(int64_t n, F f) {
-    const int hw = std::max(1, std::min(64, int(std::thread::hardware_concurrency())));
-    const int nt = int(std::min<int64_t>(hw, std::max<int64_t>(1, n / 65536)));
-    if (nt <= 1) { f(int64_t(0), n); return; }
-    std::vector<std::thread> th;
-    const int64_t chunk = (n + nt - 1) / nt;
-    for (int k = 0; k < nt; ++k) {
-        const int64_t b = k * chunk, e = std::min(n, b + chunk);
-        if (b < e) th.emplace_back([=]() { f(b, e); });
-    }
-    for (auto& t : th) t.join();
-}
-
 static int commit_scene(bg_scene* s, const bg_build_opts* opts) {
     auto t0 = std::chrono::steady_clock::now();
     const int nm = int(s->meshes.size());
@@ -311,34 +288,6 @@ static int commit_scene(bg_scene* s, const bg_build_opts* opts) {
         m.eta = d.eta;
         m.a = d.roughness;
     }
-    // world-space triangle bounds (Mesh::GetShapeWorldBounds, primitive/mesh.cpp:263-283)
-    std::vector<float> lo(3 * size_t(ntris)), hi(3 * size_t(ntris));
-    std::vector<int> tri_bundle(static_cast<size_t>(ntris));
-    for (int i = 0; i < nm; ++i)
-        std::fill(tri_bundle.begin() + start[i], tri_bundle.begin() + start[i] + s->meshes[i].nfaces, i);
-    host_parallel_for(ntris, [&](int64_t tb, int64_t te) {
-        for (int64_t t = tb; t < te; ++t) {
-            const int i = tri_bundle[size_t(t)];
-            const MeshHost& mh = s->meshes[i];
-            const int f = int(t - start[i]);
-            const float* M = mh.xf;
-            float m12[12] = {M[0], M[1], M[2], M[3], M[4], M[5], M[6], M[7], M[8], M[9], M[10], M[11]};
-            v3 p[3];
-            for (int k = 0; k < 3; ++k) p[k] = xf_point(m12, mh.verts[mh.vi[3 * f + k]]);
-            lo[3 * t] = std::min(p[0].x, std::min(p[1].x, p[2].x));
-            lo[3 * t + 1] = std::min(p[0].y, std::min(p[1].y, p[2].y));
-            lo[3 * t + 2] = std::min(p[0].z, std::min(p[1].z, p[2].z));
-            hi[3 * t] = std::max(p[0].x, std::max(p[1].x, p[2].x));
-            hi[3 * t + 1] = std::max(p[0].y, std::max(p[1].y, p[2].y));
-            hi[3 * t + 2] = std::max(p[0].z, std::max(p[1].z, p[2].z));
-        }
-    });
-    for (int k = 0; k < 3; ++k) { s->bbox_lo[k] = FLT_MAX; s->bbox_hi[k] = -FLT_MAX; }
-    for (int64_t t = 0; t < ntris; ++t)
-        for (int k = 0; k < 3; ++k) {
-            if (std::isfinite(lo[3 * size_t(t) + k])) s->bbox_lo[k] = std::min(s->bbox_lo[k], lo[3 * size_t(t) + k]);
-            if (std::isfinite(hi[3 * size_t(t) + k])) s->bbox_hi[k] = std::max(s->bbox_hi[k], hi[3 * size_t(t) + k]);
-        }
     BuildParams bp;
     int want_width = 0;
     if (opts) {
@@ -347,104 +296,89 @@ static int commit_scene(bg_scene* s, const bg_build_opts* opts) {
             return set_error(BG_ERR_UNSUPPORTED, "node_width %d: supported widths are 4 and 8 (0: both)", want_width);
         if (opts->max_leaf_size) bp.max_leaf = opts->max_leaf_size;
         if (opts->sah_bins) bp.bins = opts->sah_bins;
-        if (opts->builder != 0 && opts->builder != 1)
-            return set_error(BG_ERR_INVALID_ARG, "builder %d: 0 (host SAH) or 1 (device LBVH)", opts->builder);
+        if (opts->builder < 0 || opts->builder > 2)
+            return set_error(BG_ERR_INVALID_ARG, "builder %d: 0 (host SAH), 1 (device LBVH) or 2 (device PLOC)",
+                             opts->builder);
     }
-    const bool device_build = opts && opts->builder == 1 && ntris >= 2;
+    const int device_build = (opts && ntris >= 2) ? opts->builder : 0;
     if (bp.max_leaf < 1 || bp.max_leaf > 16 || bp.bins < 2 || bp.bins > 256)
         return set_error(BG_ERR_INVALID_ARG, "build options out of range (leaf 1..16, bins 2..256)");
     bp.wide4 = want_width != 8;
     bp.wide8 = want_width != 4;
+    int rc;
+    // mesh arrays to the device; boxes, tree and records are built there
+    MeshArrays A;
+    if ((rc = upload_mesh_arrays(s->meshes, ntris, A))) return rc;
+    if ((rc = s->bundles.ensure(bundles.size() * sizeof(BundleRec)))) return rc;
+    BG_CUDA(cudaMemcpy(s->bundles.ptr, bundles.data(), bundles.size() * sizeof(BundleRec), cudaMemcpyHostToDevice));
     const auto tb0 = std::chrono::steady_clock::now();
-    BuildResult br;
+    // world-space triangle bounds (Mesh::GetShapeWorldBounds, primitive/mesh.cpp:263-283)
+    if ((rc = device_world_boxes(A, s->bundles.as<BundleRec>(), ntris, s->bbox_lo, s->bbox_hi))) return rc;
+    DevBuf order_d;
+    struct OrderRelease {
+        DevBuf& b;
+        ~OrderRelease() { b.release(); }
+    } order_release{order_d};
+    if ((rc = order_d.ensure(size_t(ntris) * 4))) return rc;
+    int64_t nn4 = 0, nn8 = 0;
+    int ms4 = 0, md4 = 0, ms8 = 0, md8 = 0;
     if (device_build) {
-        BinaryTree bt;
-        int brc = gpu_build_tree(lo.data(), hi.data(), ntris, bp.max_leaf, bt);
-        if (brc) return brc;
-        br = collapse_binary(bt, bp);
+        DeviceBvh db;
+        if ((rc = gpu_build_bvh(A.lo.as<float>(), A.hi.as<float>(), ntris, device_build, bp, order_d.as<int32_t>(),
+                                s->nodes, s->nodes8, db)))
+            return rc;
+        nn4 = db.nnodes4; ms4 = db.max_stack4; md4 = db.max_depth4;
+        nn8 = db.nnodes8; ms8 = db.max_stack8; md8 = db.max_depth8;
     } else {
-        br = build_wide_bvh(lo.data(), hi.data(), ntris, bp);
+        std::vector<float> lo(3 * size_t(ntris)), hi(3 * size_t(ntris));
+        BG_CUDA(cudaMemcpy(lo.data(), A.lo.ptr, lo.size() * 4, cudaMemcpyDeviceToHost));
+        BG_CUDA(cudaMemcpy(hi.data(), A.hi.ptr, hi.size() * 4, cudaMemcpyDeviceToHost));
+        BuildResult br = build_wide_bvh(lo.data(), hi.data(), ntris, bp);
+        nn4 = int64_t(br.nodes.size()); ms4 = br.max_stack; md4 = br.max_depth;
+        nn8 = int64_t(br.nodes8.size()); ms8 = br.max_stack8; md8 = br.max_depth8;
+        if ((rc = s->nodes.ensure(std::max<size_t>(1, br.nodes.size()) * sizeof(WideNode4))) ||
+            (rc = s->nodes8.ensure(std::max<size_t>(1, br.nodes8.size()) * sizeof(QNode8))))
+            return rc;
+        if (nn4)
+            BG_CUDA(cudaMemcpy(s->nodes.ptr, br.nodes.data(), size_t(nn4) * sizeof(WideNode4), cudaMemcpyHostToDevice));
+        if (nn8)
+            BG_CUDA(cudaMemcpy(s->nodes8.ptr, br.nodes8.data(), size_t(nn8) * sizeof(QNode8), cudaMemcpyHostToDevice));
+        BG_CUDA(cudaMemcpy(order_d.ptr, br.order.data(), size_t(ntris) * 4, cudaMemcpyHostToDevice));
     }
-    if (want_width == 8 && br.nodes8.empty())
+    if (want_width == 8 && nn8 == 0)
         return set_error(BG_ERR_UNSUPPORTED, "scene coordinates too large for the 8-wide compressed nodes");
-    if (bp.wide4 && br.max_stack > kStackSize)
-        return set_error(BG_ERR_UNSUPPORTED, "BVH needs a %d-entry traversal stack (> %d)", br.max_stack, kStackSize);
-    if (!br.nodes8.empty() && br.max_stack8 > kStackSize8) {
+    if (bp.wide4 && ms4 > kStackSize)
+        return set_error(BG_ERR_UNSUPPORTED, "BVH needs a %d-entry traversal stack (> %d)", ms4, kStackSize);
+    if (nn8 && ms8 > kStackSize8) {
         if (want_width == 8)
-            return set_error(BG_ERR_UNSUPPORTED, "8-wide BVH needs a %d-entry traversal stack (> %d)", br.max_stack8,
-                             kStackSize8);
-        br.nodes8.clear();
+            return set_error(BG_ERR_UNSUPPORTED, "8-wide BVH needs a %d-entry traversal stack (> %d)", ms8, kStackSize8);
+        nn8 = 0;
     }
     const auto tb1 = std::chrono::steady_clock::now();
-    // per-triangle records
-    std::vector<TriRec> tris(static_cast<size_t>(ntris));
-    host_parallel_for(ntris, [&](int64_t kb, int64_t ke) {
-        for (int64_t k = kb; k < ke; ++k) {
-            int32_t t = br.order[size_t(k)];
-            int b = tri_bundle[size_t(t)];
-            const MeshHost& mh = s->meshes[b];
-            int f = int(t - start[b]);
-            v3 p1 = mh.verts[mh.vi[3 * f]], p2 = mh.verts[mh.vi[3 * f + 1]], p3 = mh.verts[mh.vi[3 * f + 2]];
-            v3 e1 = sub(p2, p1), e2 = sub(p3, p1);
-            TriRec& r = tris[size_t(k)];
-            int bcode = bundles[b].identity ? -1 : b;
-            r.v0 = make_float4(p1.x, p1.y, p1.z, i2f(bcode));
-            r.e1 = make_float4(e1.x, e1.y, e1.z, i2f(t));
-            r.e2 = make_float4(e2.x, e2.y, e2.z, 0.f);
-        }
-    });
-    std::vector<ShadeRec> shade(static_cast<size_t>(ntris));
-    host_parallel_for(ntris, [&](int64_t tb, int64_t te) {
-        for (int64_t t = tb; t < te; ++t) {
-            const int b = tri_bundle[size_t(t)];
-            const MeshHost& mh = s->meshes[b];
-            const int f = int(t - start[b]);
-            ShadeRec& r = shade[size_t(t)];
-            v3 p1 = mh.verts[mh.vi[3 * f]], p2 = mh.verts[mh.vi[3 * f + 1]], p3 = mh.verts[mh.vi[3 * f + 2]];
-            v3 n1 = mh.normals[mh.ni[3 * f]], n2 = mh.normals[mh.ni[3 * f + 1]], n3 = mh.normals[mh.ni[3 * f + 2]];
-            const float* t1 = &mh.uvs[2 * size_t(mh.ti[3 * f])];
-            const float* t2 = &mh.uvs[2 * size_t(mh.ti[3 * f + 1])];
-            const float* t3 = &mh.uvs[2 * size_t(mh.ti[3 * f + 2])];
-            r.a = make_float4(p1.x, p1.y, p1.z, i2f(b));
-            r.b = make_float4(p2.x, p2.y, p2.z, i2f(mh.m[f]));
-            r.c = make_float4(p3.x, p3.y, p3.z, t1[0]);
-            r.d = make_float4(n1.x, n1.y, n1.z, t1[1]);
-            r.e = make_float4(n2.x, n2.y, n2.z, t2[0]);
-            r.f = make_float4(n3.x, n3.y, n3.z, t2[1]);
-            r.g = make_float4(t3[0], t3[1], 0.f, 0.f);
-        }
-    });
+    // traversal records in leaf order, shading records in primitive order
+    if ((rc = s->tris.ensure(size_t(ntris) * sizeof(TriRec))) || (rc = s->shade.ensure(size_t(ntris) * sizeof(ShadeRec))))
+        return rc;
+    if ((rc = device_records(A, s->bundles.as<BundleRec>(), order_d.as<int32_t>(), ntris, s->tris.as<TriRec>(),
+                             s->shade.as<ShadeRec>())))
+        return rc;
     const auto tb2 = std::chrono::steady_clock::now();
-    int rc;
-    if ((rc = s->nodes.ensure(std::max<size_t>(1, br.nodes.size()) * sizeof(WideNode4))) ||
-        (rc = s->nodes8.ensure(std::max<size_t>(1, br.nodes8.size()) * sizeof(QNode8))) ||
-        (rc = s->tris.ensure(tris.size() * sizeof(TriRec))) ||
-        (rc = s->shade.ensure(shade.size() * sizeof(ShadeRec))) ||
-        (rc = s->bundles.ensure(bundles.size() * sizeof(BundleRec))) ||
-        (rc = s->mats_d.ensure(mats.size() * sizeof(MatRec))) ||
+    if ((rc = s->mats_d.ensure(mats.size() * sizeof(MatRec))) ||
         (rc = s->lights_d.ensure(std::max<size_t>(1, lights.size()) * sizeof(LightRec))) ||
         (rc = s->err.ensure(sizeof(unsigned))) ||
         (rc = s->work.ensure(kWorkSlots * sizeof(unsigned long long))))
         return rc;
-    if (!br.nodes.empty())
-        BG_CUDA(cudaMemcpy(s->nodes.ptr, br.nodes.data(), br.nodes.size() * sizeof(WideNode4), cudaMemcpyHostToDevice));
-    if (!br.nodes8.empty())
-        BG_CUDA(cudaMemcpy(s->nodes8.ptr, br.nodes8.data(), br.nodes8.size() * sizeof(QNode8), cudaMemcpyHostToDevice));
-    BG_CUDA(cudaMemcpy(s->tris.ptr, tris.data(), tris.size() * sizeof(TriRec), cudaMemcpyHostToDevice));
-    BG_CUDA(cudaMemcpy(s->shade.ptr, shade.data(), shade.size() * sizeof(ShadeRec), cudaMemcpyHostToDevice));
-    BG_CUDA(cudaMemcpy(s->bundles.ptr, bundles.data(), bundles.size() * sizeof(BundleRec), cudaMemcpyHostToDevice));
     BG_CUDA(cudaMemcpy(s->mats_d.ptr, mats.data(), mats.size() * sizeof(MatRec), cudaMemcpyHostToDevice));
     if (!lights.empty())
         BG_CUDA(cudaMemcpy(s->lights_d.ptr, lights.data(), lights.size() * sizeof(LightRec), cudaMemcpyHostToDevice));
     BG_CUDA(cudaMemset(s->err.ptr, 0, sizeof(unsigned)));
     BG_CUDA(cudaMemset(s->work.ptr, 0, kWorkSlots * sizeof(unsigned long long)));
     DevScene& d = s->dev;
-    d.nodes = br.nodes.empty() ? nullptr : s->nodes.as<WideNode4>();
-    d.nodes8 = br.nodes8.empty() ? nullptr : s->nodes8.as<QNode8>();
-    s->nnodes4 = int64_t(br.nodes.size());
-    s->nnodes8 = int64_t(br.nodes8.size());
-    s->max_stack4 = br.max_stack; s->max_depth4 = br.max_depth;
-    s->max_stack8 = br.max_stack8; s->max_depth8 = br.max_depth8;
+    d.nodes = nn4 ? s->nodes.as<WideNode4>() : nullptr;
+    d.nodes8 = nn8 ? s->nodes8.as<QNode8>() : nullptr;
+    s->nnodes4 = nn4;
+    s->nnodes8 = nn8;
+    s->max_stack4 = ms4; s->max_depth4 = md4;
+    s->max_stack8 = ms8; s->max_depth8 = md8;
     d.width = d.nodes ? (want_width == 0 && d.nodes8 ? kDefaultNodeWidth : 4) : 8;
     d.tris = s->tris.as<TriRec>();
     d.shade = s->shade.as<ShadeRec>();
@@ -461,8 +395,8 @@ static int commit_scene(bg_scene* s, const bg_build_opts* opts) {
     auto t1 = std::chrono::steady_clock::now();
     bg_scene_info& info = s->info;
     info.ntriangles = ntris;
-    info.tri_bytes = int64_t(tris.size() * sizeof(TriRec));
-    info.shade_bytes = int64_t(shade.size() * sizeof(ShadeRec));
+    info.tri_bytes = ntris * int64_t(sizeof(TriRec));
+    info.shade_bytes = ntris * int64_t(sizeof(ShadeRec));
     set_width_info(s);
     info.nmeshes = nm;
     info.nmaterials = nmat;
@@ -470,7 +404,7 @@ static int commit_scene(bg_scene* s, const bg_build_opts* opts) {
     info.build_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
     info.bvh_ms = std::chrono::duration<double, std::milli>(tb1 - tb0).count();
     info.records_ms = std::chrono::duration<double, std::milli>(tb2 - tb1).count();
-    info.upload_ms = std::chrono::duration<double, std::milli>(t1 - tb2).count();
+    info.upload_ms = std::chrono::duration<double, std::milli>(tb0 - t0).count();
     s->committed = true;
     return BG_OK;
 }

@@ -4,6 +4,7 @@
 // [base, base + 2m - 1), so parallel recursion produces the same tree as the
 // serial one, and the wide tree is emitted in a fixed depth-first order.
 #include "bvh_build.h"
+#include "qnode.h"
 
 #include <algorithm>
 #include <atomic>
@@ -44,10 +45,6 @@ struct Bin {
 
 class Builder {
 public:
-    // adopt an existing binary tree (root = node 0) for the wide collapses only
-    Builder(std::vector<BNode>&& nodes, std::vector<int32_t>&& order, const BuildParams& p)
-        : n_(int64_t(order.size())), p_(p), idx_(std::move(order)), nodes_(std::move(nodes)) {}
-
     Builder(const float* lo, const float* hi, int64_t n, const BuildParams& p)
         : n_(n), p_(p), tlo_(3 * n), thi_(3 * n), cen_(3 * n), idx_(n), nodes_(2 * n) {
         for (int64_t i = 0; i < n; ++i) {
@@ -225,82 +222,16 @@ private:
         q8_jobs_.shrink_to_fit();
     }
 
-    // Slot assignment (greedy over child x slot by projected centroid: slot s
-    // takes the child furthest upstream for directions with sign bits s) and
-    // conservative quantisation of the children's boxes.
-    // returns false when a plane cannot be made conservative (coordinates too large)
+    // Quantises one recorded 8-wide node (qnode.h); false when a plane cannot
+    // be made conservative (coordinates too large)
     bool fill_qnode(QNode8& q, const int32_t* kids, const int32_t* codes, int nk) const {
-        bool ok = true;
-        Box u; u.clear();
-        for (int i = 0; i < nk; ++i) u.grow(nodes_[kids[i]].box);
-        double cen[8][3];
+        float kb[8][6];
         for (int i = 0; i < nk; ++i)
-            for (int k = 0; k < 3; ++k)
-                cen[i][k] = 0.5 * (double(nodes_[kids[i]].box.lo[k]) + double(nodes_[kids[i]].box.hi[k])) -
-                            0.5 * (double(u.lo[k]) + double(u.hi[k]));
-        int slot_of[8];
-        bool cused[8] = {false}, sused[8] = {false};
-        for (int n = 0; n < nk; ++n) {
-            double best = 1e300;
-            int bc = -1, bs = -1;
-            for (int c = 0; c < nk; ++c) {
-                if (cused[c]) continue;
-                for (int sl = 0; sl < 8; ++sl) {
-                    if (sused[sl]) continue;
-                    double cost = 0.0;
-                    for (int k = 0; k < 3; ++k) cost += ((sl >> k) & 1 ? -cen[c][k] : cen[c][k]);
-                    if (cost < best) { best = cost; bc = c; bs = sl; }
-                }
-            }
-            cused[bc] = true; sused[bs] = true; slot_of[bc] = bs;
-        }
-        int e[3];
-        double k[3];
-        for (int a = 0; a < 3; ++a) {
-            e[a] = qnode_axis(u.lo[a], u.hi[a], &k[a]);
-            if (e[a] > kQMaxExp) { ok = false; e[a] = kQMaxExp; }
-        }
-        float* o2[3] = {&q.o2x, &q.o2y, &q.o2z};
-        for (int a = 0; a < 3; ++a) *o2[a] = float(std::ldexp(k[a] - 8388608.0, e[a]));
-        uint32_t valid = 0;
-        uint8_t qb[3][2][8];
-        for (int a = 0; a < 3; ++a)
-            for (int h = 0; h < 2; ++h)
-                for (int sl = 0; sl < 8; ++sl) qb[a][h][sl] = h ? 0 : 255;   // unused slot: inverted box
-        for (int sl = 0; sl < 8; ++sl) q.child[sl] = kEmptyChild;
-        for (int c = 0; c < nk; ++c) {
-            const int sl = slot_of[c];
-            valid |= 1u << sl;
-            q.child[sl] = codes[c];
-            const Box& b = nodes_[kids[c]].box;
             for (int a = 0; a < 3; ++a) {
-                double lo = std::floor(std::ldexp(double(b.lo[a]), -e[a])) - k[a];
-                double hi = std::ceil(std::ldexp(double(b.hi[a]), -e[a])) - k[a];
-                qb[a][0][sl] = uint8_t(std::min(255.0, std::max(0.0, lo)));
-                qb[a][1][sl] = uint8_t(std::min(255.0, std::max(0.0, hi)));
+                kb[i][a] = nodes_[kids[i]].box.lo[a];
+                kb[i][3 + a] = nodes_[kids[i]].box.hi[a];
             }
-        }
-        q.meta = uint32_t(e[0] + 127) | (uint32_t(e[1] + 127) << 8) | (uint32_t(e[2] + 127) << 16) | (valid << 24);
-        // self-check with the device's dequantisation: fmaf(2^23 + q, 2^e, o2)
-        for (int c = 0; c < nk; ++c) {
-            const int sl = slot_of[c];
-            const Box& b = nodes_[kids[c]].box;
-            for (int a = 0; a < 3; ++a) {
-                const float st = std::ldexp(1.0f, e[a]);
-                const float plo = std::fma(8388608.0f + float(qb[a][0][sl]), st, *o2[a]);
-                const float phi = std::fma(8388608.0f + float(qb[a][1][sl]), st, *o2[a]);
-                if (!(plo <= b.lo[a] && phi >= b.hi[a])) ok = false;
-            }
-        }
-        uint32_t* w[3] = {q.qx, q.qy, q.qz};
-        for (int a = 0; a < 3; ++a)
-            for (int h = 0; h < 2; ++h)
-                for (int half = 0; half < 2; ++half) {
-                    uint32_t v = 0;
-                    for (int j = 0; j < 4; ++j) v |= uint32_t(qb[a][h][4 * half + j]) << (8 * j);
-                    w[a][2 * h + half] = v;
-                }
-        return ok;
+        return fill_qnode8(q, kb, codes, nk);
     }
 
     void make_leaf(int64_t nodeidx, int64_t begin, int64_t end, const Box& box) {
@@ -460,40 +391,7 @@ public:
 // double: L, H are floats, k is an integer below 2^24, the steps are powers of
 // two.  e <= kQMaxExp keeps o2 = (k - 2^23) * 2^e finite; returns kQMaxExp + 1
 // when no such step exists (node coordinates beyond ~1e33).
-int qnode_axis(float L, float H, double* k) {
-    int e = -120;
-    const double ext = double(H) - double(L);
-    if (ext > 0.0) e = std::max(e, int(std::ceil(std::log2(ext / 255.0))) - 1);
-    const double aL = std::fabs(double(L));
-    if (aL > 0.0) e = std::max(e, int(std::floor(std::log2(aL))) - 23);
-    for (; e <= kQMaxExp; ++e) {
-        const double kk = std::floor(std::ldexp(double(L), -e));
-        if (std::fabs(kk) > 8388608.0 - 257.0) continue;
-        if (std::ldexp(kk + 255.0, e) < double(H)) continue;
-        *k = kk;
-        return e;
-    }
-    *k = 0.0;
-    return kQMaxExp + 1;
-}
-
-BuildResult collapse_binary(const BinaryTree& t, const BuildParams& p) {
-    std::vector<BNode> nodes(t.left.size());
-    for (size_t i = 0; i < nodes.size(); ++i) {
-        BNode& b = nodes[i];
-        for (int k = 0; k < 3; ++k) { b.box.lo[k] = t.box[6 * i + k]; b.box.hi[k] = t.box[6 * i + 3 + k]; }
-        b.left = t.left[i]; b.right = t.right[i];
-        b.start = t.start[i]; b.count = t.count[i];
-    }
-    std::vector<int32_t> order = t.order;
-    Builder b(std::move(nodes), std::move(order), p);
-    BuildResult r = b.collapse();
-    if (b.q8_failed_) {
-        r.nodes8.clear();
-        r.max_depth8 = r.max_stack8 = 0;
-    }
-    return r;
-}
+int qnode_axis(float L, float H, double* k) { return qnode_axis_exact(L, H, k); }
 
 BuildResult build_wide_bvh(const float* lo, const float* hi, int64_t n, const BuildParams& p) {
     Builder b(lo, hi, n, p);

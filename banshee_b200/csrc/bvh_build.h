@@ -77,16 +77,6 @@ struct BuildResult {
 constexpr int kQMaxExp = 104;
 int qnode_axis(float L, float H, double* k);
 
-// A binary tree built elsewhere (the device builder): node 0 is the root;
-// per node a box (lo xyz, hi xyz), children (internal nodes: left/right >= 0,
-// count = 0) or a leaf range [start, start + count) of `order`.
-struct BinaryTree {
-    std::vector<float> box;
-    std::vector<int32_t> left, right, start, count;
-    std::vector<int32_t> order;
-};
-BuildResult collapse_binary(const BinaryTree& t, const BuildParams& p);
-
 // lo/hi/centroid: world-space triangle boxes, 3 floats each, n entries.
 // Non-finite boxes are treated as a point at the origin.
 BuildResult build_wide_bvh(const float* lo, const float* hi, int64_t n, const BuildParams& p);

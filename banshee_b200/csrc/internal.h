@@ -85,8 +85,30 @@ namespace bg {
 constexpr int kTraceThreads = 128;
 constexpr int kDefaultNodeWidth = 4;   // active layout when both are built
 void set_width_info(bg_scene* s);
-struct BinaryTree;
-int gpu_build_tree(const float* lo, const float* hi, int64_t n, int max_leaf, BinaryTree& t);   // gpu_build.cu
+// Device BVH build (gpu_build.cu) from device world boxes lo/hi (3 floats per
+// triangle): builder 1 = LBVH, 2 = PLOC.  Writes the leaf order (n entries,
+// device) and the node arrays the params ask for, grown to their exact sizes.
+struct DeviceBvh {
+    int64_t nnodes4 = 0, nnodes8 = 0;
+    int max_depth4 = 0, max_stack4 = 0, max_depth8 = 0, max_stack8 = 0;
+    bool quant_ok = true;     // false: 8-wide planes could not be made conservative
+};
+int gpu_build_bvh(const float* lo, const float* hi, int64_t n, int builder, const BuildParams& bp, int32_t* order,
+                  DevBuf& nodes4, DevBuf& nodes8, DeviceBvh& out);
+
+// One commit's mesh arrays on the device (scene_records.cu): the meshes'
+// vertex, normal and uv arrays and per-face index arrays concatenated, with
+// each face's bundle, and the world-space triangle boxes.
+struct MeshArrays {
+    DevBuf verts, normals, uvs, vi, ni, ti, mat, offs, bundle, lo, hi, bbox;
+    ~MeshArrays();
+};
+int upload_mesh_arrays(const std::vector<MeshHost>& meshes, int64_t ntris, MeshArrays& A);
+// world boxes into A.lo / A.hi (Mesh::GetShapeWorldBounds) and the scene bounds of their finite values
+int device_world_boxes(MeshArrays& A, const BundleRec* bundles, int64_t ntris, float bbox_lo[3], float bbox_hi[3]);
+// traversal records in leaf order (order: device) and shading records in primitive order
+int device_records(const MeshArrays& A, const BundleRec* bundles, const int32_t* order, int64_t ntris,
+                   TriRec* tris, ShadeRec* shade);
 constexpr int kWorkSlots = 256;
 unsigned long long* next_work_counter(bg_scene* s);
 void scene_launch_setup(bg_scene* s);

@@ -201,9 +201,18 @@ def raycast_c2(ctx, nrays=1 << 24, reps=5):
             "bytes_per_ray": bpr, "achieved_gbs": bpr * nrays / (ms * 1e-3) / 1e9}
         del dr, res, sub
     gs.close()
-    # device LBVH build (Morton order) of the same soup: build time and traversal with the looser tree
+    # the device builders (LBVH: Morton order; PLOC: clustering over it) on the
+    # same soup: build time and traversal speed of their trees
+    for builder, name in ((1, "device_lbvh"), (2, "device_ploc")):
+        out[name] = _device_build_traversal(ctx, builder, nrays, reps)
+    return out
+
+
+def _device_build_traversal(ctx, builder, nrays, reps):
+    import torch
+    from banshee_b200 import capi, scenes
     t0 = time.perf_counter()
-    gl = capi.GpuScene(ctx, scenes.soup(1 << 20, seed=1), builder=1)
+    gl = capi.GpuScene(ctx, scenes.soup(1 << 20, seed=1), builder=builder)
     lb = {"build_ms": gl.info()["build_ms"], "build_wall_s": time.perf_counter() - t0}
     for width in (4, 8):
         gl.set_node_width(width)
@@ -223,8 +232,7 @@ def raycast_c2(ctx, nrays=1 << 24, reps=5):
             lb["layout%d_%s_closest_mrays_per_s" % (width, kind)] = nrays / (e0.elapsed_time(e1) / reps) / 1e3
             del dr, res
     gl.close()
-    out["device_lbvh"] = lb
-    return out
+    return lb
 
 
 def cornell_c1(ctx, ref_seconds_cap=60.0):

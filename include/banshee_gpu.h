@@ -148,7 +148,9 @@ typedef struct bg_build_opts {
     int32_t max_leaf_size;  /* triangles per leaf, 1..16 (0 = default 4)*/
     int32_t sah_bins;       /* binned-SAH bins (0 = default 32)         */
     int32_t builder;        /* 0 = host binned SAH; 1 = device LBVH
-                               (Morton order, faster build, looser tree)  */
+                               (Morton order, faster build, looser tree);
+                               2 = device PLOC (nearest-neighbour
+                               clustering over the Morton order, radius 16) */
 } bg_build_opts;
 
 typedef struct bg_scene_info {
@@ -163,12 +165,13 @@ typedef struct bg_scene_info {
     int32_t nmeshes;
     int32_t nmaterials;
     int32_t nlights;
-    double  build_ms;       /* host build + upload time                   */
+    double  build_ms;       /* whole commit (wall time)                   */
     int32_t node_width;     /* active node layout: 4 or 8                  */
     int32_t node_widths;    /* layouts built: 4 | 8                        */
-    double  bvh_ms;         /* of build_ms: tree build + wide collapses    */
-    double  records_ms;     /*              triangle / shading records     */
-    double  upload_ms;      /*              device allocation and upload   */
+    double  bvh_ms;         /* of build_ms: world boxes, tree build and
+                               wide collapses                             */
+    double  records_ms;     /*   triangle / shading records (device)      */
+    double  upload_ms;      /*   validation and mesh-array upload         */
 } bg_scene_info;
 
 /* ---------------------------------------------------------------- tracing */

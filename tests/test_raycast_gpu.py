@@ -178,13 +178,15 @@ def test_layout_info_and_work(width, ctx):
         gs.set_node_width(2)
 
 
+@pytest.mark.parametrize("builder", [1, 2], ids=["lbvh", "ploc"])
 @pytest.mark.parametrize("kind", ["incoherent", "coherent"])
-def test_device_builder_parity(width, ctx, oracle_built, kind):
-    """The device LBVH builder changes only the tree: closest hits stay bit-exact
-    with the oracle (reference Bvh) and any-hit bits exact, on both layouts."""
+def test_device_builder_parity(width, ctx, oracle_built, kind, builder):
+    """The device builders (LBVH, PLOC) change only the tree: closest hits stay
+    bit-exact with the oracle (reference Bvh) and any-hit bits exact, on both
+    layouts."""
     from banshee_b200 import capi
     sc = scenes.soup(100_000, seed=21)
-    gs = capi.GpuScene(ctx, sc, builder=1)
+    gs = capi.GpuScene(ctx, sc, builder=builder)
     gs.set_node_width(width)
     o = oracle_built.Oracle(sc)
     rays = scenes.soup_rays(1 << 16, kind, seed=22)
@@ -200,15 +202,78 @@ def test_device_builder_parity(width, ctx, oracle_built, kind):
     assert gs.error_flags() == 0
 
 
-def test_device_builder_golden_cornell(width, ctx):
+@pytest.mark.parametrize("builder", [1, 2], ids=["lbvh", "ploc"])
+def test_device_builder_golden_cornell(width, ctx, builder):
     from banshee_b200 import capi
     from tests.golden.make_golden import CORNELL
     g = np.load(os.path.join(GOLD, "raycast_cornell.npz"))
-    gs = capi.GpuScene(ctx, scenes.cornell(**CORNELL), builder=1)
+    gs = capi.GpuScene(ctx, scenes.cornell(**CORNELL), builder=builder)
     gs.set_node_width(width)
     got = gs.intersect_closest_host(g["rays"])
     assert (got["primid"] == g["hits"]["primid"]).all()
     assert (_bits(got["t"]) == _bits(g["hits"]["t"])).all()
+
+
+def _degenerate_soup(seed):
+    """Soup with the cases a Morton-order build meets: 30% exact duplicates,
+    500 copies of one triangle (identical Morton codes), 5% zero-area
+    (collinear) triangles and a second, transformed mesh."""
+    from banshee_b200.scene import Mesh
+    rng = np.random.default_rng(seed)
+    sc = scenes.soup(20_000, seed=seed)
+    m = sc.meshes[0]
+    v = m.vertices.reshape(-1, 3, 3).copy()
+    nf = v.shape[0]
+    dup = rng.choice(nf, size=nf * 3 // 10, replace=False)
+    v[dup] = v[rng.integers(0, nf, size=dup.shape[0])]
+    v[:500] = v[500]
+    col = rng.choice(np.arange(501, nf), size=nf // 20, replace=False)
+    v[col, 2] = 0.5 * (v[col, 0] + v[col, 1])
+    m.vertices = np.ascontiguousarray(v.reshape(-1, 3))
+    m2 = Mesh(m.vertices[:3000].copy(), m.normals[:1000].copy(), m.vidx[:1000].copy(), m.nidx[:1000].copy(),
+              np.zeros(1000, np.int32))
+    m2.set_transform(np.array([[0.5, 0, 0, 0.2], [0, 0.5, 0, 0.3], [0, 0, 0.5, 0.1], [0, 0, 0, 1]]))
+    sc.meshes.append(m2)
+    return sc
+
+
+@pytest.mark.parametrize("builder", [0, 1, 2], ids=["sah", "lbvh", "ploc"])
+def test_builders_degenerate_soup(width, ctx, oracle_built, builder):
+    """Duplicates, identical Morton codes, zero-area triangles and a transformed
+    bundle: hits stay exact (ties classified) and any-hit bits identical, for
+    every builder and layout."""
+    from banshee_b200 import capi
+    sc = _degenerate_soup(41)
+    gs = capi.GpuScene(ctx, sc, builder=builder)
+    gs.set_node_width(width)
+    o = oracle_built.Oracle(sc)
+    rays = scenes.soup_rays(1 << 15, "incoherent", seed=42)
+    want = o.intersect_closest(rays)
+    got = gs.intersect_closest_host(rays)
+    ties, bad = classify(o, rays, got, want)
+    assert not bad, bad[:10]
+    assert (_bits(got["t"]) == _bits(want["t"])).all()
+    arays = scenes.soup_rays(1 << 15, "incoherent", seed=43, any_hit=True)
+    assert (gs.intersect_any_host(arays) == o.intersect_any(arays)).all()
+    assert gs.error_flags() == 0
+
+
+@pytest.mark.parametrize("ntris", [2, 3, 5, 17])
+@pytest.mark.parametrize("builder", [1, 2], ids=["lbvh", "ploc"])
+def test_device_builders_tiny_scenes(width, ctx, oracle_built, builder, ntris):
+    """A root that is itself cheaper as one leaf is still opened into a node."""
+    from banshee_b200 import capi
+    sc = scenes.soup(ntris, seed=50 + ntris)
+    gs = capi.GpuScene(ctx, sc, builder=builder)
+    gs.set_node_width(width)
+    o = oracle_built.Oracle(sc)
+    rays = scenes.soup_rays(4096, "coherent", seed=51)
+    want = o.intersect_closest(rays)
+    got = gs.intersect_closest_host(rays)
+    assert (got["primid"] == want["primid"]).all()
+    assert (_bits(got["t"]) == _bits(want["t"])).all()
+    info = gs.info()
+    assert info["ntriangles"] == ntris and info["nnodes"] >= 1
 
 
 def test_traversal_work_guard_vs_reference_bvh(width, ctx, oracle_built):
