@@ -47,6 +47,50 @@ void DevBuf::release() {
     bytes = 0;
 }
 
+static cudaMemPool_t scratch_pool(int device) {
+    static std::mutex mu;
+    static std::vector<cudaMemPool_t> pools;
+    std::lock_guard<std::mutex> lk(mu);
+    if (device < 0) return nullptr;
+    if (size_t(device) >= pools.size()) pools.resize(size_t(device) + 1, nullptr);
+    if (!pools[size_t(device)]) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        cudaMemPool_t p = nullptr;
+        if (cudaMemPoolCreate(&p, &props) != cudaSuccess) { cudaGetLastError(); return nullptr; }
+        uint64_t keep = kScratchKeepBytes;
+        cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+        pools[size_t(device)] = p;
+    }
+    return pools[size_t(device)];
+}
+
+int ScratchBuf::ensure(size_t need) {
+    if (need <= bytes && ptr) return BG_OK;
+    release();
+    int dev = 0;
+    BG_CUDA(cudaGetDevice(&dev));
+    cudaMemPool_t pool = scratch_pool(dev);
+    if (!pool) return set_error(BG_ERR_CUDA, "scratch memory pool unavailable on device %d", dev);
+    const size_t want = std::max<size_t>(need, 256);
+    cudaError_t e = cudaMallocFromPoolAsync(&ptr, want, pool, 0);
+    if (e != cudaSuccess) {
+        ptr = nullptr;
+        cudaGetLastError();
+        return set_error(BG_ERR_OOM, "scratch allocation (%zu bytes) failed: %s", want, cudaGetErrorString(e));
+    }
+    bytes = want;
+    return BG_OK;
+}
+
+void ScratchBuf::release() {
+    if (ptr) cudaFreeAsync(ptr, 0);
+    ptr = nullptr;
+    bytes = 0;
+}
+
 // ------------------------------------------------------------ trace kernel
 // Persistent threads with per-lane dynamic fetch: lanes whose ray finished
 // take new ray indices from one global counter with a single warp-aggregated
@@ -314,11 +358,7 @@ static int commit_scene(bg_scene* s, const bg_build_opts* opts) {
     const auto tb0 = std::chrono::steady_clock::now();
     // world-space triangle bounds (Mesh::GetShapeWorldBounds, primitive/mesh.cpp:263-283)
     if ((rc = device_world_boxes(A, s->bundles.as<BundleRec>(), ntris, s->bbox_lo, s->bbox_hi))) return rc;
-    DevBuf order_d;
-    struct OrderRelease {
-        DevBuf& b;
-        ~OrderRelease() { b.release(); }
-    } order_release{order_d};
+    ScratchBuf order_d;
     if ((rc = order_d.ensure(size_t(ntris) * 4))) return rc;
     int64_t nn4 = 0, nn8 = 0;
     int ms4 = 0, md4 = 0, ms8 = 0, md8 = 0;

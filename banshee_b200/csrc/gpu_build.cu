@@ -192,8 +192,11 @@ __device__ __forceinline__ bool tie_before(int i, int j, int k) {   // is pair (
     return lj < lk;
 }
 
-__global__ void k_ploc_nn(const int32_t* __restrict__ cl, int m, const float* __restrict__ box,
-                          int32_t* __restrict__ nn) {
+// The cluster count m lives on the device (written by the compaction), so the
+// rounds run back to back; m_bound >= m sizes the launches and CUB passes.
+__global__ void k_ploc_nn(const int32_t* __restrict__ cl, const int* __restrict__ m_dev,
+                          const float* __restrict__ box, int32_t* __restrict__ nn) {
+    const int m = *m_dev;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
         const float* bi = box + 6 * size_t(cl[i]);
         float best = FLT_MAX;
@@ -209,9 +212,11 @@ __global__ void k_ploc_nn(const int32_t* __restrict__ cl, int m, const float* __
 }
 
 // leader of a mutual pair (the lower index) creates the merged node
-__global__ void k_ploc_flags(const int32_t* __restrict__ nn, int m, int32_t* __restrict__ lead,
-                             int32_t* __restrict__ keep) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+__global__ void k_ploc_flags(const int32_t* __restrict__ nn, const int* __restrict__ m_dev, int m_bound,
+                             int32_t* __restrict__ lead, int32_t* __restrict__ keep) {
+    const int m = *m_dev;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m_bound; i += gridDim.x * blockDim.x) {
+        if (i >= m) { lead[i] = 0; keep[i] = 0; continue; }
         const int j = nn[i];
         const bool mutual = j >= 0 && nn[j] == i;
         lead[i] = (mutual && i < j) ? 1 : 0;
@@ -219,10 +224,12 @@ __global__ void k_ploc_flags(const int32_t* __restrict__ nn, int m, int32_t* __r
     }
 }
 
-__global__ void k_ploc_merge(int32_t* __restrict__ cl, const int32_t* __restrict__ nn, int m,
-                             const int32_t* __restrict__ lead, const int32_t* __restrict__ lead_scan, int32_t base,
-                             float* __restrict__ box, int32_t* __restrict__ left, int32_t* __restrict__ right,
-                             int32_t* __restrict__ parent) {
+__global__ void k_ploc_merge(int32_t* __restrict__ cl, const int32_t* __restrict__ nn, const int* __restrict__ m_dev,
+                             const int32_t* __restrict__ lead, const int32_t* __restrict__ lead_scan,
+                             const int32_t* __restrict__ base_dev, float* __restrict__ box, int32_t* __restrict__ left,
+                             int32_t* __restrict__ right, int32_t* __restrict__ parent) {
+    const int m = *m_dev;
+    const int32_t base = *base_dev;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
         if (!lead[i]) continue;
         const int j = nn[i];
@@ -238,6 +245,12 @@ __global__ void k_ploc_merge(int32_t* __restrict__ cl, const int32_t* __restrict
         parent[b] = node;
         cl[i] = node;
     }
+}
+
+// next free node index += this round's merges
+__global__ void k_ploc_advance(int32_t* __restrict__ base_dev, const int32_t* __restrict__ lead_scan,
+                               const int32_t* __restrict__ lead, int m_bound) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) *base_dev += lead_scan[m_bound - 1] + lead[m_bound - 1];
 }
 
 // ---------------------------------------------------------------- bottom-up SAH
@@ -429,8 +442,7 @@ template <int W>
 int run_collapse(CollapseArgs A, int32_t root, int capacity, int32_t* order, DevBuf& nodes, WideOut& r) {
     const size_t node_bytes = W == 4 ? sizeof(WideNode4) : sizeof(QNode8);
     struct Scratch {
-        DevBuf items0, items1, ctr, out;
-        ~Scratch() { items0.release(); items1.release(); ctr.release(); out.release(); }
+        ScratchBuf items0, items1, ctr, out;
     } S;
     int rc;
     if ((rc = S.items0.ensure(size_t(capacity) * sizeof(CItem))) ||
@@ -482,13 +494,8 @@ int gpu_build_bvh(const float* lo, const float* hi, int64_t n, int builder, cons
     if (n > (int64_t(1) << 29)) return set_error(BG_ERR_UNSUPPORTED, "device build: too many triangles");
     if (builder != 1 && builder != 2) return set_error(BG_ERR_INVALID_ARG, "device builder %d", builder);
     struct Scratch {
-        DevBuf cb, keys, keys2, idx, sorted, left, right, parent, box, cnt, cost, mk, visits, nopen, tmp;
-        DevBuf cl, cl2, nn, lead, scan, keep, nsel;
-        ~Scratch() {
-            for (DevBuf* b : {&cb, &keys, &keys2, &idx, &sorted, &left, &right, &parent, &box, &cnt, &cost, &mk,
-                              &visits, &nopen, &tmp, &cl, &cl2, &nn, &lead, &scan, &keep, &nsel})
-                b->release();
-        }
+        ScratchBuf cb, keys, keys2, idx, sorted, left, right, parent, box, cnt, cost, mk, visits, nopen, tmp;
+        ScratchBuf cl, cl2, nn, lead, scan, keep, nsel;
     } S;
     const size_t N = size_t(n), NN = 2 * N - 1;
     int rc;
@@ -532,35 +539,41 @@ int gpu_build_bvh(const float* lo, const float* hi, int64_t n, int builder, cons
                                       S.parent.as<int32_t>());
         BG_CUDA(cudaGetLastError());
     } else {
-        int m = int(n);
-        int32_t next_node = int32_t(n);
+        int* m_dev = S.nsel.as<int>();              // [0] clusters (written by the compaction), [1] next node
+        int32_t* base_dev = S.nsel.as<int32_t>() + 1;
+        const int32_t init_mb[2] = {int32_t(n), int32_t(n)};
+        BG_CUDA(cudaMemcpy(S.nsel.ptr, init_mb, sizeof(init_mb), cudaMemcpyHostToDevice));
         int32_t* cl = S.cl.as<int32_t>();
         int32_t* cl2 = S.cl2.as<int32_t>();
-        // every round merges at least one pair (the smallest pair is mutual),
-        // so the loop ends after < n rounds
-        while (m > 1) {
-            const int g = std::min(kBGrid, (m + kBT - 1) / kBT);
-            k_ploc_nn<<<g, kBT>>>(cl, m, S.box.as<float>(), S.nn.as<int32_t>());
-            k_ploc_flags<<<g, kBT>>>(S.nn.as<int32_t>(), m, S.lead.as<int32_t>(), S.keep.as<int32_t>());
-            tbytes = tb;
-            BG_CUDA(cub::DeviceScan::ExclusiveSum(S.tmp.ptr, tbytes, S.lead.as<int32_t>(), S.scan.as<int32_t>(), m));
-            int32_t last[2] = {0, 0};
-            BG_CUDA(cudaMemcpy(&last[0], S.scan.as<int32_t>() + (m - 1), 4, cudaMemcpyDeviceToHost));
-            BG_CUDA(cudaMemcpy(&last[1], S.lead.as<int32_t>() + (m - 1), 4, cudaMemcpyDeviceToHost));
-            const int32_t merges = last[0] + last[1];
-            if (merges <= 0) return set_error(BG_ERR_STATE, "device PLOC build made no progress");
-            k_ploc_merge<<<g, kBT>>>(cl, S.nn.as<int32_t>(), m, S.lead.as<int32_t>(), S.scan.as<int32_t>(),
-                                     next_node, S.box.as<float>(), S.left.as<int32_t>(), S.right.as<int32_t>(),
-                                     S.parent.as<int32_t>());
-            next_node += merges;
-            tbytes = tb;
-            BG_CUDA(cub::DeviceSelect::Flagged(S.tmp.ptr, tbytes, cl, S.keep.as<int32_t>(), cl2,
-                                               S.nsel.as<int32_t>(), m));
-            int32_t msel = 0;
-            BG_CUDA(cudaMemcpy(&msel, S.nsel.ptr, 4, cudaMemcpyDeviceToHost));
-            m = msel;
-            std::swap(cl, cl2);
+        // every round merges at least one pair (the smallest pair is mutual), so
+        // m falls by at least one per round while above 1; the host reads m
+        // every kPlocCheck rounds to shrink the launch bound and to stop
+        constexpr int kPlocCheck = 4;
+        int m_bound = int(n);
+        while (m_bound > 1) {
+            for (int r = 0; r < kPlocCheck; ++r) {
+                const int g = std::min(kBGrid, (m_bound + kBT - 1) / kBT);
+                k_ploc_nn<<<g, kBT>>>(cl, m_dev, S.box.as<float>(), S.nn.as<int32_t>());
+                k_ploc_flags<<<g, kBT>>>(S.nn.as<int32_t>(), m_dev, m_bound, S.lead.as<int32_t>(), S.keep.as<int32_t>());
+                tbytes = tb;
+                BG_CUDA(cub::DeviceScan::ExclusiveSum(S.tmp.ptr, tbytes, S.lead.as<int32_t>(), S.scan.as<int32_t>(),
+                                                      m_bound));
+                k_ploc_merge<<<g, kBT>>>(cl, S.nn.as<int32_t>(), m_dev, S.lead.as<int32_t>(), S.scan.as<int32_t>(),
+                                         base_dev, S.box.as<float>(), S.left.as<int32_t>(), S.right.as<int32_t>(),
+                                         S.parent.as<int32_t>());
+                k_ploc_advance<<<1, 32>>>(base_dev, S.scan.as<int32_t>(), S.lead.as<int32_t>(), m_bound);
+                tbytes = tb;
+                BG_CUDA(cub::DeviceSelect::Flagged(S.tmp.ptr, tbytes, cl, S.keep.as<int32_t>(), cl2, m_dev, m_bound));
+                std::swap(cl, cl2);
+            }
+            BG_CUDA(cudaGetLastError());
+            int m = 0;
+            BG_CUDA(cudaMemcpy(&m, m_dev, sizeof(int), cudaMemcpyDeviceToHost));
+            if (m >= m_bound) return set_error(BG_ERR_STATE, "device PLOC build made no progress");
+            m_bound = m;
         }
+        int32_t next_node = 0;
+        BG_CUDA(cudaMemcpy(&next_node, base_dev, sizeof(int32_t), cudaMemcpyDeviceToHost));
         if (next_node != int32_t(NN)) return set_error(BG_ERR_STATE, "device PLOC build: %d nodes", next_node);
         BG_CUDA(cudaMemcpy(&root, cl, 4, cudaMemcpyDeviceToHost));
     }

@@ -43,6 +43,20 @@ struct DevBuf {
     template <class T> T* as() const { return static_cast<T*>(ptr); }
 };
 
+// Scratch of one synchronous call (a commit's build buffers): drawn from a
+// per-device memory pool on the legacy default stream, so repeated commits
+// reuse memory instead of calling cudaMalloc / cudaFree each time.  Every use
+// must be on the legacy stream; the pool keeps up to kScratchKeepBytes.
+struct ScratchBuf {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    int ensure(size_t need);
+    void release();
+    ~ScratchBuf() { release(); }
+    template <class T> T* as() const { return static_cast<T*>(ptr); }
+};
+constexpr size_t kScratchKeepBytes = size_t(4) << 30;
+
 struct RenderState;   // render.cu
 void render_state_free(RenderState* rs);
 
@@ -100,8 +114,7 @@ int gpu_build_bvh(const float* lo, const float* hi, int64_t n, int builder, cons
 // vertex, normal and uv arrays and per-face index arrays concatenated, with
 // each face's bundle, and the world-space triangle boxes.
 struct MeshArrays {
-    DevBuf verts, normals, uvs, vi, ni, ti, mat, offs, bundle, lo, hi, bbox;
-    ~MeshArrays();
+    ScratchBuf verts, normals, uvs, vi, ni, ti, mat, offs, bundle, lo, hi, bbox;
 };
 int upload_mesh_arrays(const std::vector<MeshHost>& meshes, int64_t ntris, MeshArrays& A);
 // world boxes into A.lo / A.hi (Mesh::GetShapeWorldBounds) and the scene bounds of their finite values

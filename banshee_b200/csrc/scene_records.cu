@@ -142,10 +142,6 @@ int grid_for(int64_t n) { return int(std::max<int64_t>(1, std::min<int64_t>(kRGr
 
 }  // namespace
 
-MeshArrays::~MeshArrays() {
-    for (DevBuf* b : {&verts, &normals, &uvs, &vi, &ni, &ti, &mat, &offs, &bundle, &lo, &hi, &bbox}) b->release();
-}
-
 int upload_mesh_arrays(const std::vector<MeshHost>& meshes, int64_t ntris, MeshArrays& A) {
     const int nm = int(meshes.size());
     std::vector<MeshOff> offs(static_cast<size_t>(nm));
@@ -167,7 +163,7 @@ int upload_mesh_arrays(const std::vector<MeshHost>& meshes, int64_t ntris, MeshA
         (rc = A.bundle.ensure(F * 4)) || (rc = A.lo.ensure(F * 12)) || (rc = A.hi.ensure(F * 12)) ||
         (rc = A.bbox.ensure(6 * sizeof(unsigned int))))
         return rc;
-    auto put = [](DevBuf& dst, int64_t at, const void* src, size_t bytes) -> int {
+    auto put = [](ScratchBuf& dst, int64_t at, const void* src, size_t bytes) -> int {
         if (bytes == 0) return BG_OK;
         BG_CUDA(cudaMemcpy(static_cast<char*>(dst.ptr) + at, src, bytes, cudaMemcpyHostToDevice));
         return BG_OK;

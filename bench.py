@@ -272,49 +272,53 @@ def batch_c4(ctx, nscenes=64, seed=7, timed_frames=1, rank=0, world=1, dist=None
     """C4: 64 procedural scenes (triangles log-uniform in [1e4, 5e5], resolutions from
     {256^2, 512^2, 1024x768}, 16..128 spp each) traced together by one batch: one set of
     queues, persistent kernels, one pass graph; autotuned node width / block / wavefront
-    sizes.  On N GPUs each rank takes every N-th scene (no exchange); time = max over ranks."""
+    sizes.  Each builder (host binned SAH, device LBVH, device PLOC) builds the scenes
+    (wall time, scene generation excluded) and the batch renders its trees; the headline
+    fields are the host-SAH row.  On N GPUs each rank takes every N-th scene (no
+    exchange); times are the max over ranks."""
     import torch
     from banshee_b200 import capi, multigpu, scenes
     t0 = time.perf_counter()
     all_items = scenes.batch(nscenes, seed=seed)
+    gen_s = time.perf_counter() - t0
     items = multigpu.shard(all_items, rank, world)
-    gss = [capi.GpuScene(ctx, sc) for sc, _ in items]
-    batch = capi.Batch(ctx, gss)
-    build_s = time.perf_counter() - t0
-    for g in gss:
-        g.close()
-    # the same scenes built by the device LBVH builder (build time only; the batch renders the SAH trees)
-    t1 = time.perf_counter()
-    for sc, _ in items:
-        capi.GpuScene(ctx, sc, builder=1).close()
-    lbvh_build_s = time.perf_counter() - t1
     bufs, jobs = [], []
     for k, (sc, spp) in enumerate(items):
         acc = torch.zeros((sc.height, sc.width, 4), dtype=torch.float32, device="cuda")
         bufs.append(acc)
-        jobs.append(dict(scene=k, width=sc.width, height=sc.height, spp=spp, seed=1, camera=None,
+        jobs.append(dict(scene=k, width=sc.width, height=sc.height, spp=spp, seed=1, camera=sc.camera_desc(),
                          accum_dev=acc.data_ptr()))
-    for k, (sc, _) in enumerate(items):
-        jobs[k]["camera"] = sc.camera_desc()
-    tune = batch.autotune(jobs, probe_spp=2, maxdepth=MAXDEPTH)
-    for b in bufs:
-        b.zero_()
-    samples = sum(sc.width * sc.height * spp for sc, spp in items)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    e0.record()
-    for _ in range(timed_frames):
-        batch.render(jobs, maxdepth=MAXDEPTH)
-    e1.record()
-    torch.cuda.synchronize()
-    ms = multigpu.max_over_ranks(e0.elapsed_time(e1) / timed_frames, dist, device="cuda")
-    info = batch.info()
-    batch.close()
     samples = sum(sc.width * sc.height * spp for sc, spp in all_items)
+    rows = {}
+    for builder, name in ((0, "host_sah"), (1, "device_lbvh"), (2, "device_ploc")):
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        gss = [capi.GpuScene(ctx, sc, builder=builder) for sc, _ in items]
+        batch = capi.Batch(ctx, gss)
+        torch.cuda.synchronize()
+        build_s = multigpu.max_over_ranks(time.perf_counter() - t1, dist, device="cuda")
+        for g in gss:
+            g.close()
+        tune = batch.autotune(jobs, probe_spp=2, maxdepth=MAXDEPTH)
+        for b in bufs:
+            b.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(timed_frames):
+            batch.render(jobs, maxdepth=MAXDEPTH)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = multigpu.max_over_ranks(e0.elapsed_time(e1) / timed_frames, dist, device="cuda")
+        info = batch.info()
+        batch.close()
+        rows[name] = {"build_s": build_s, "ms": ms, "msamples_per_s": samples / ms / 1e3,
+                      "build_plus_frame_s": build_s + ms / 1e3, "node_width": info["node_width"], "autotune": tune}
+    head = rows["host_sah"]
     return {"scenes": nscenes, "triangles_total": sum(sc.ntriangles for sc, _ in all_items),
-            "camera_samples": samples, "scenes_per_rank": len(items), "node_width": info["node_width"],
-            "ms": ms, "msamples_per_s": samples / ms / 1e3, "autotune": tune, "build_s": build_s,
-            "build_s_device_lbvh": lbvh_build_s,
+            "camera_samples": samples, "scenes_per_rank": len(items), "node_width": head["node_width"],
+            "ms": head["ms"], "msamples_per_s": head["msamples_per_s"], "autotune": head["autotune"],
+            "build_s": head["build_s"], "scene_generation_s": gen_s, "by_builder": rows,
             "resolutions": sorted({"%dx%d" % (sc.width, sc.height) for sc, _ in all_items}),
             "spp_range": [min(s for _, s in all_items), max(s for _, s in all_items)],
             "triangle_range": [min(sc.ntriangles for sc, _ in all_items),
