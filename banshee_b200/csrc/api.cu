@@ -529,6 +529,8 @@ int bg_scene_destroy(bg_scene* s) {
                       &s->host_rays, &s->host_out})
         b->release();
     if (s->render) render_state_free(s->render);
+    if (s->ev_accum) cudaEventDestroy(s->ev_accum);
+    if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
     delete s;
     return BG_OK;
 }

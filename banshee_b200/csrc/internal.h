@@ -92,6 +92,10 @@ struct bg_scene {
     int64_t nnodes4 = 0, nnodes8 = 0;
     int max_stack4 = 0, max_stack8 = 0, max_depth4 = 0, max_depth8 = 0;
     bool owns_buffers = true;
+    // bg_render_host: the accumulation buffer's upload runs on copy_stream and
+    // overlaps the pass; the pass's accumulate waits for ev_accum
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t ev_accum = nullptr;
 };
 
 namespace bg {

@@ -92,7 +92,7 @@ struct RenderState {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     cudaGraphNode_t gen_node = nullptr, acc_node = nullptr;
-    int64_t graph_key[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    int64_t graph_key[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
 };
 
 void render_state_free(RenderState* rs) {
@@ -785,6 +785,8 @@ static int enqueue_pass(bg_scene* s, RenderState* rs, cudaStream_t st, const Pas
         cur = 1 - cur;
         pass_queues(rs, cur, c.batched, Q);
     }
+    // the accumulation buffer may still be arriving from the host (bg_render_host)
+    if (s->ev_accum) BG_CUDA(cudaStreamWaitEvent(st, s->ev_accum, cudaEventWaitExternal));
     k_accumulate<<<nb, kShadeThreads, 0, st>>>(P, c.segs, c.nseg, c.npix);
     if (ins) ++ins->launches;
     BG_CUDA(cudaGetLastError());
@@ -796,8 +798,8 @@ static int enqueue_pass(bg_scene* s, RenderState* rs, cudaStream_t st, const Pas
 static int pass_graph(bg_scene* s, RenderState* rs, const PassCfg& c) {
     uint32_t aob;
     memcpy(&aob, &c.ao_radius, sizeof(aob));
-    const int64_t key[8] = {c.maxdepth, c.kind, c.batched ? 1 : 0, rs->kmax, int64_t(rs->cap), s->tune_threads,
-                            s->dev.width, int64_t(aob)};
+    const int64_t key[9] = {c.maxdepth, c.kind, c.batched ? 1 : 0, rs->kmax, int64_t(rs->cap), s->tune_threads,
+                            s->dev.width, int64_t(aob), s->ev_accum ? 1 : 0};
     if (rs->exec && memcmp(key, rs->graph_key, sizeof(key)) == 0) return BG_OK;
     if (rs->exec) { cudaGraphExecDestroy(rs->exec); rs->exec = nullptr; }
     if (rs->graph) { cudaGraphDestroy(rs->graph); rs->graph = nullptr; }
@@ -1226,9 +1228,15 @@ extern "C" int bg_render_host(bg_scene* s, const bg_camera_desc* cam, const bg_t
     int rc = s->host_out.ensure(bytes);   // staging shared with the host ray casts (both hold the scene lock)
     if (rc) return rc;
     float4* d = s->host_out.as<float4>();
-    BG_CUDA(cudaMemcpy(d, accum, bytes, cudaMemcpyHostToDevice));
+    if (!s->copy_stream) {
+        BG_CUDA(cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking));
+        BG_CUDA(cudaEventCreateWithFlags(&s->ev_accum, cudaEventDisableTiming));
+    }
+    // upload on the copy stream, overlapping the pass; only accumulate waits for it
+    BG_CUDA(cudaMemcpyAsync(d, accum, bytes, cudaMemcpyHostToDevice, s->copy_stream));
+    BG_CUDA(cudaEventRecord(s->ev_accum, s->copy_stream));
     rc = render_impl(s, nullptr, cam, tr, sm, W, H, d, stats, 0);
-    if (rc) return rc;
+    if (rc) { cudaStreamSynchronize(s->copy_stream); return rc; }
     BG_CUDA(cudaMemcpy(accum, d, bytes, cudaMemcpyDeviceToHost));
     unsigned flags = 0;
     BG_CUDA(cudaMemcpy(&flags, s->err.ptr, sizeof(unsigned), cudaMemcpyDeviceToHost));
