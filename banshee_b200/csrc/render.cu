@@ -89,6 +89,10 @@ struct RenderState {
     // CUDA graph of one pass, replayed on an internal stream
     cudaStream_t gstream = nullptr;
     cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+    // side streams of a pass: the next bounce's extension trace (fstream) and
+    // this bounce's MIS trace + resolve (mstream), with fork / join events
+    cudaStream_t fstream = nullptr, mstream = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_mjoin = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     cudaGraphNode_t gen_node = nullptr, acc_node = nullptr;
@@ -105,6 +109,11 @@ void render_state_free(RenderState* rs) {
     if (rs->ev_in) cudaEventDestroy(rs->ev_in);
     if (rs->ev_out) cudaEventDestroy(rs->ev_out);
     if (rs->gstream) cudaStreamDestroy(rs->gstream);
+    if (rs->ev_fork) cudaEventDestroy(rs->ev_fork);
+    if (rs->ev_join) cudaEventDestroy(rs->ev_join);
+    if (rs->fstream) cudaStreamDestroy(rs->fstream);
+    if (rs->ev_mjoin) cudaEventDestroy(rs->ev_mjoin);
+    if (rs->mstream) cudaStreamDestroy(rs->mstream);
     for (DevBuf* b : {&rs->ext_rays[0], &rs->ext_rays[1], &rs->ext_path[0], &rs->ext_path[1], &rs->ext_hits,
                       &rs->sh_rays, &rs->sh_contrib, &rs->sh_slot, &rs->sh_occ, &rs->mis_rays, &rs->mis_a, &rs->mis_b,
                       &rs->mis_c, &rs->mis_hits, &rs->end_path, &rs->counts, &rs->st_key, &rs->st_cnt, &rs->st_rng,
@@ -654,6 +663,11 @@ static int ensure_state(bg_scene* s, int64_t cap, int maxL) {
     BG_CUDA(cudaStreamCreateWithFlags(&rs->gstream, cudaStreamNonBlocking));
     BG_CUDA(cudaEventCreateWithFlags(&rs->ev_in, cudaEventDisableTiming));
     BG_CUDA(cudaEventCreateWithFlags(&rs->ev_out, cudaEventDisableTiming));
+    BG_CUDA(cudaStreamCreateWithFlags(&rs->fstream, cudaStreamNonBlocking));
+    BG_CUDA(cudaEventCreateWithFlags(&rs->ev_fork, cudaEventDisableTiming));
+    BG_CUDA(cudaEventCreateWithFlags(&rs->ev_join, cudaEventDisableTiming));
+    BG_CUDA(cudaStreamCreateWithFlags(&rs->mstream, cudaStreamNonBlocking));
+    BG_CUDA(cudaEventCreateWithFlags(&rs->ev_mjoin, cudaEventDisableTiming));
     return BG_OK;
 }
 
@@ -741,13 +755,24 @@ static int enqueue_pass(bg_scene* s, RenderState* rs, cudaStream_t st, const Pas
     if (ins) ++ins->launches;
     bg_hit* cnt_hits = rs->cnt_out.as<bg_hit>();
     uint8_t* cnt_occ = rs->cnt_out.as<uint8_t>();
-    for (int b = 0; b < std::max(1, c.maxdepth); ++b) {
+    // Without instrumentation, the extension trace of bounce b + 1 runs on a
+    // second stream beside bounce b's shadow and MIS traces, resolves and
+    // finalize: it reads only the queue that shade(b) wrote and the hit buffer
+    // shade(b) has finished with; the MIS trace and its resolve run on a third
+    // stream beside the shadow trace.  The deep, nearly empty bounces are latency
+    // chains (one ray's traversal is dozens of dependent node loads), so
+    // running two chains side by side shortens the pass.
+    const bool fork = ins == nullptr && rs->fstream != nullptr && rs->mstream != nullptr;
+    const int depth = std::max(1, c.maxdepth);
+    for (int b = 0; b < depth; ++b) {
         unsigned long long* wk = rs->work.as<unsigned long long>() + 6 * b;
         BG_CUDA(cudaMemsetAsync(Q.n_ext_out, 0, sizeof(int), st));
         BG_CUDA(cudaMemsetAsync(cnt + kCntSh, 0, 3 * sizeof(int), st));
-        if (ins) ins->mark(0);
-        if ((rc = launch_trace(s, false, Q.ext_rays_in, 0, Q.n_ext_in, Q.ext_hits, nullptr, st, nullptr, 1, wk, Q.ext_root_in))) return rc;
-        if (ins) { ins->mark(0); ++ins->launches; ++ins->launches_extend; }
+        if (!fork || b == 0) {
+            if (ins) ins->mark(0);
+            if ((rc = launch_trace(s, false, Q.ext_rays_in, 0, Q.n_ext_in, Q.ext_hits, nullptr, st, nullptr, 1, wk, Q.ext_root_in))) return rc;
+            if (ins) { ins->mark(0); ++ins->launches; ++ins->launches_extend; }
+        }
         if (ins && ins->count_trav) {
             if ((rc = launch_trace(s, false, Q.ext_rays_in, 0, Q.n_ext_in, cnt_hits, nullptr, st, Q.totals + 3, 64, wk + 1, Q.ext_root_in))) return rc;
             ++ins->launches;
@@ -760,9 +785,30 @@ static int enqueue_pass(bg_scene* s, RenderState* rs, cudaStream_t st, const Pas
         else if (c.cache) k_shade<BG_TRACER_GI, true><<<nb, kShadeThreads, 0, st>>>(s->dev, A, P, Q);
         else k_shade<BG_TRACER_GI, false><<<nb, kShadeThreads, 0, st>>>(s->dev, A, P, Q);
         if (ins) { ++ins->launches; ins->mark(1); }
+        const bool forked = fork && b + 1 < depth;
+        if (forked) {
+            Queues Qn;
+            pass_queues(rs, 1 - cur, c.batched, Qn);
+            BG_CUDA(cudaEventRecord(rs->ev_fork, st));
+            BG_CUDA(cudaStreamWaitEvent(rs->fstream, rs->ev_fork, 0));
+            if ((rc = launch_trace(s, false, Qn.ext_rays_in, 0, Qn.n_ext_in, Qn.ext_hits, nullptr, rs->fstream, nullptr, 1,
+                                   wk + 6, Qn.ext_root_in)))
+                return rc;
+            BG_CUDA(cudaEventRecord(rs->ev_join, rs->fstream));
+        }
+        if (fork) {   // MIS trace and its resolve beside the shadow trace (they write different slots)
+            if (!forked) BG_CUDA(cudaEventRecord(rs->ev_fork, st));
+            BG_CUDA(cudaStreamWaitEvent(rs->mstream, rs->ev_fork, 0));
+            if ((rc = launch_trace(s, false, Q.mis_rays, 0, Q.n_mis, Q.mis_hits, nullptr, rs->mstream, nullptr, 1, wk + 3,
+                                   Q.mis_root)))
+                return rc;
+            k_resolve_mis<<<nb, kShadeThreads, 0, rs->mstream>>>(s->dev, P, Q);
+            BG_CUDA(cudaEventRecord(rs->ev_mjoin, rs->mstream));
+        }
         if ((rc = launch_trace(s, true, Q.sh_rays, 0, Q.n_sh, nullptr, Q.sh_occ, st, nullptr, 1, wk + 2, Q.sh_root))) return rc;
         if (ins) { ins->mark(1); ins->mark(2); }
-        if ((rc = launch_trace(s, false, Q.mis_rays, 0, Q.n_mis, Q.mis_hits, nullptr, st, nullptr, 1, wk + 3, Q.mis_root))) return rc;
+        if (!fork && (rc = launch_trace(s, false, Q.mis_rays, 0, Q.n_mis, Q.mis_hits, nullptr, st, nullptr, 1, wk + 3, Q.mis_root)))
+            return rc;
         if (ins) { ins->mark(2); ins->launches += 2; }
         if (ins && ins->count_trav) {
             if ((rc = launch_trace(s, true, Q.sh_rays, 0, Q.n_sh, nullptr, cnt_occ, st, Q.totals + 6, 64, wk + 4, Q.sh_root))) return rc;
@@ -770,7 +816,8 @@ static int enqueue_pass(bg_scene* s, RenderState* rs, cudaStream_t st, const Pas
             ins->launches += 2;
         }
         k_resolve_shadow<<<nb, kShadeThreads, 0, st>>>(P, Q);
-        k_resolve_mis<<<nb, kShadeThreads, 0, st>>>(s->dev, P, Q);
+        if (fork) BG_CUDA(cudaStreamWaitEvent(st, rs->ev_mjoin, 0));
+        else k_resolve_mis<<<nb, kShadeThreads, 0, st>>>(s->dev, P, Q);
         if (c.cache && b == c.cache_depth) {
             // rendering paths that ended here: encode, infer, add throughput * prediction
             if (ins) ins->mark(3);
@@ -782,6 +829,7 @@ static int enqueue_pass(bg_scene* s, RenderState* rs, cudaStream_t st, const Pas
         }
         k_finalize<<<nb, kShadeThreads, 0, st>>>(P, Q, rs->kmax, c.maxdepth, c.cache ? c.train_stride : 0, c.train_phase);
         if (ins) ins->launches += 3;
+        if (forked) BG_CUDA(cudaStreamWaitEvent(st, rs->ev_join, 0));
         cur = 1 - cur;
         pass_queues(rs, cur, c.batched, Q);
     }
