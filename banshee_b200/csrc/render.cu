@@ -755,14 +755,15 @@ static int enqueue_pass(bg_scene* s, RenderState* rs, cudaStream_t st, const Pas
     if (ins) ++ins->launches;
     bg_hit* cnt_hits = rs->cnt_out.as<bg_hit>();
     uint8_t* cnt_occ = rs->cnt_out.as<uint8_t>();
-    // Without instrumentation, the extension trace of bounce b + 1 runs on a
+    // Without phase timing or traversal counting, the extension trace of bounce b + 1 runs on a
     // second stream beside bounce b's shadow and MIS traces, resolves and
     // finalize: it reads only the queue that shade(b) wrote and the hit buffer
     // shade(b) has finished with; the MIS trace and its resolve run on a third
     // stream beside the shadow trace.  The deep, nearly empty bounces are latency
     // chains (one ray's traversal is dozens of dependent node loads), so
     // running two chains side by side shortens the pass.
-    const bool fork = ins == nullptr && rs->fstream != nullptr && rs->mstream != nullptr;
+    const bool fork = (ins == nullptr || (!ins->time_phases && !ins->count_trav)) && rs->fstream != nullptr &&
+                      rs->mstream != nullptr;
     const int depth = std::max(1, c.maxdepth);
     for (int b = 0; b < depth; ++b) {
         unsigned long long* wk = rs->work.as<unsigned long long>() + 6 * b;
@@ -795,6 +796,7 @@ static int enqueue_pass(bg_scene* s, RenderState* rs, cudaStream_t st, const Pas
                                    wk + 6, Qn.ext_root_in)))
                 return rc;
             BG_CUDA(cudaEventRecord(rs->ev_join, rs->fstream));
+            if (ins) { ++ins->launches; ++ins->launches_extend; }
         }
         if (fork) {   // MIS trace and its resolve beside the shadow trace (they write different slots)
             if (!forked) BG_CUDA(cudaEventRecord(rs->ev_fork, st));
@@ -834,7 +836,8 @@ static int enqueue_pass(bg_scene* s, RenderState* rs, cudaStream_t st, const Pas
         pass_queues(rs, cur, c.batched, Q);
     }
     // the accumulation buffer may still be arriving from the host (bg_render_host)
-    if (s->ev_accum) BG_CUDA(cudaStreamWaitEvent(st, s->ev_accum, cudaEventWaitExternal));
+    // (captured into the pass graph as an event-wait node; a plain wait otherwise)
+    if (s->ev_accum) BG_CUDA(cudaStreamWaitEvent(st, s->ev_accum, ins ? 0u : unsigned(cudaEventWaitExternal)));
     k_accumulate<<<nb, kShadeThreads, 0, st>>>(P, c.segs, c.nseg, c.npix);
     if (ins) ++ins->launches;
     BG_CUDA(cudaGetLastError());

@@ -105,6 +105,32 @@ def test_graph_replay_matches_direct_launches(ctx):
     assert gs.error_flags() == 0
 
 
+@pytest.mark.parametrize("flags", [0, 1, 3])
+def test_host_entry_overlapped_upload_then_every_launch_path(ctx, flags):
+    """bg_render_host uploads the accumulation buffer on a copy stream that
+    only the pass's accumulate waits for.  Progressive host frames, then device
+    renders replayed from the graph, launched one by one (statistics) and
+    instrumented (phase timing / traversal counting), all give the bits of one
+    direct render of the same samples."""
+    import torch
+    from banshee_b200 import capi
+    sc = scenes.production(96, 54, nterrain=48, nspheres=12, sphere_seg=12, seed=5)
+    gs = capi.GpuScene(ctx, sc)
+    host = np.zeros((54, 96, 4), dtype=np.float32)
+    for k in range(3):
+        host = gs.render_host(96, 54, 1, seed=6, sample_offset=k, maxdepth=8, accum=host)
+    dev = torch.zeros((54, 96, 4), dtype=torch.float32, device="cuda")
+    for k in range(3):
+        gs.render(dev.data_ptr(), 96, 54, 1, seed=6, sample_offset=k, maxdepth=8, stats=(k == 1), flags=flags)
+    one = torch.zeros_like(dev)
+    gs.render(one.data_ptr(), 96, 54, 3, seed=6, maxdepth=8, stats=False)
+    torch.cuda.synchronize()
+    want = one.cpu().numpy().view(np.uint32)
+    assert (dev.cpu().numpy().view(np.uint32) == want).all()
+    assert (host.view(np.uint32) == want).all()
+    assert gs.error_flags() == 0
+
+
 def test_device_render_entry_point(ctx):
     import torch
     from banshee_b200 import capi
