@@ -101,7 +101,7 @@ class CacheDesc(C.Structure):
                 ("max_resolution", C.c_int32), ("train_paths", C.c_int32), ("cache_depth", C.c_int32),
                 ("train_batch", C.c_int32), ("train_steps", C.c_int32), ("learning_rate", C.c_float),
                 ("bbox_min", C.c_float * 3), ("bbox_max", C.c_float * 3), ("seed", C.c_uint64),
-                ("mlp_kernel", C.c_int32), ("reserved", C.c_int32)]
+                ("mlp_kernel", C.c_int32), ("train_suffix", C.c_int32)]
 
 
 class BatchJob(C.Structure):

@@ -256,8 +256,10 @@ class RadianceCache:
 
     def __init__(self, gscene, log2_table_size=19, base_resolution=16, max_resolution=2048, train_paths=65536,
                  cache_depth=2, train_batch=16384, train_steps=4, learning_rate=1e-2, bbox=None, seed=1,
-                 mlp_kernel=0):
-        """mlp_kernel: inference on tcgen05 with TMEM accumulators (0) or on mma.sync (1)."""
+                 mlp_kernel=0, train_suffix=0):
+        """mlp_kernel: inference on tcgen05 with TMEM accumulators (0) or on mma.sync (1).
+        train_suffix: 0 = training paths run to maxdepth; k > 0 = they end into the
+        cache k bounces after cache_depth (self-training)."""
         d = abi.CacheDesc()
         d.levels = 16
         d.log2_table_size = log2_table_size
@@ -273,6 +275,7 @@ class RadianceCache:
             d.bbox_max[:] = list(bbox[1])
         d.seed = seed
         d.mlp_kernel = mlp_kernel
+        d.train_suffix = train_suffix
         self.gs = gscene
         self.h = _vp()
         check(lib().bg_cache_create(gscene.h, C.byref(d), C.byref(self.h)))

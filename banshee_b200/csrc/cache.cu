@@ -591,6 +591,7 @@ int nrc_train_step(bg_cache* c, const float* feat, const float4* target, const i
 int nrc_prepare(bg_cache* c, int64_t rows) { return cache_scratch(c, rows); }
 const bg_cache_desc* nrc_desc(const bg_cache* c) { return &c->desc; }
 int64_t nrc_next_frame(bg_cache* c) { return c->frame++; }
+int64_t nrc_frame(const bg_cache* c) { return c->frame; }
 bg_scene* nrc_scene(const bg_cache* c) { return c->scene; }
 
 }  // namespace bg
@@ -649,6 +650,10 @@ int bg_cache_create(bg_scene* s, const bg_cache_desc* d, bg_cache** out) {
     if (c->desc.mlp_kernel != 0 && c->desc.mlp_kernel != 1) {
         bg_cache_destroy(c);
         return set_error(BG_ERR_INVALID_ARG, "mlp_kernel %d: 0 (tcgen05) or 1 (mma.sync)", d->mlp_kernel);
+    }
+    if (c->desc.train_suffix < 0) {
+        bg_cache_destroy(c);
+        return set_error(BG_ERR_INVALID_ARG, "train_suffix %d < 0", d->train_suffix);
     }
     cudaFuncSetAttribute(k_nrc_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, kInferSmem);
     cudaFuncSetAttribute(k_nrc_infer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);

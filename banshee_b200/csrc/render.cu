@@ -38,6 +38,7 @@ int nrc_train_step(bg_cache* c, const float* feat, const float4* target, const i
                    cudaStream_t st);
 const bg_cache_desc* nrc_desc(const bg_cache* c);
 int64_t nrc_next_frame(bg_cache* c);
+int64_t nrc_frame(const bg_cache* c);   // frames rendered so far
 bg_scene* nrc_scene(const bg_cache* c);
 
 __global__ void k_clamp_count(int* n, int cap) {
@@ -76,7 +77,14 @@ struct RenderState {
     DevBuf work;       // persistent-kernel work counters of the pass (6 per bounce)
     // radiance-cache mode: cache queries, training-path vertex records, training samples
     DevBuf q_feat, q_path, q_thr, q_out, rec, tr_feat, tr_target;
-    int64_t q_cap = 0, tr_cap = 0;
+    int64_t q_cap = 0, tr_cap = 0;       // tr_cap: rows per training set
+    int tr_set = 0;                      // training set this frame writes
+    // rows of the other set wait to be trained at the start of the next frame
+    // of the same cache (pending_frame: that cache's frame index which wrote them)
+    bg_cache* pending_cache = nullptr;
+    int64_t pending_frame = -1;
+    cudaStream_t tstream = nullptr;      // training of the previous frame's rows
+    cudaEvent_t ev_tstart = nullptr, ev_train = nullptr;
     // segment table of the pass in flight: int header {nseg, total} + SegRec[kMaxSegs]
     DevBuf segs, jobs;
     int njobs_cap = 0;
@@ -112,6 +120,9 @@ void render_state_free(RenderState* rs) {
     if (rs->ev_fork) cudaEventDestroy(rs->ev_fork);
     if (rs->ev_join) cudaEventDestroy(rs->ev_join);
     if (rs->fstream) cudaStreamDestroy(rs->fstream);
+    if (rs->ev_tstart) cudaEventDestroy(rs->ev_tstart);
+    if (rs->ev_train) cudaEventDestroy(rs->ev_train);
+    if (rs->tstream) cudaStreamDestroy(rs->tstream);
     if (rs->ev_mjoin) cudaEventDestroy(rs->ev_mjoin);
     if (rs->mstream) cudaStreamDestroy(rs->mstream);
     for (DevBuf* b : {&rs->ext_rays[0], &rs->ext_rays[1], &rs->ext_path[0], &rs->ext_path[1], &rs->ext_hits,
@@ -126,6 +137,9 @@ void render_state_free(RenderState* rs) {
 }
 
 enum : int { kCntExt0 = 0, kCntExt1 = 1, kCntSh = 2, kCntMis = 3, kCntEnd = 4, kCntQuery = 5, kCntTrain = 6 };
+// training rows alternate between two halves of tr_feat / tr_target (counters
+// kCntTrain + set): a frame writes one while the previous frame's are trained on
+constexpr int kCntTrainSets = 2;
 enum : unsigned { kFlagNoClamp = 1u, kFlagTrain = 2u };   // bits 8..15: recorded vertices of a training path
 
 struct PathState {
@@ -241,6 +255,7 @@ __device__ __forceinline__ v3 gather_pending(const PathState& P, int kmax, int p
 struct ShadeArgs {
     int bounce, maxdepth, kind, kmax, batched;
     int cache_depth;              // -1: plain tracer
+    int train_end;                // training paths end into the cache here (-1: they run to maxdepth)
     int train_stride, train_phase;
     float ao_radius;              // BG_TRACER_AO
 };
@@ -408,8 +423,11 @@ k_shade(DevScene S, ShadeArgs A, PathState P, Queues Q) {
                 if (KIND == BG_TRACER_GI) rad = add(rad, emissive_le(M, h.n, wo));   // gitracer.cpp:61-68
                 if (KIND == BG_TRACER_DI) flags |= kFlagNoClamp;                    // ditracer.cpp:29-32
                 end = true;
-            } else if ((CACHE && A.cache_depth >= 0) && !train && A.bounce == A.cache_depth) {
-                // the rendering path ends into the radiance cache at this vertex
+            } else if ((CACHE && A.cache_depth >= 0) &&
+                       ((!train && A.bounce == A.cache_depth) || (train && A.bounce == A.train_end))) {
+                // the rendering path ends into the radiance cache at this vertex; so
+                // does a training path at the end of its suffix (self-training: its
+                // recorded vertices learn from the cache's own prediction here)
                 float4 f[4];
                 cache_features(h, wo, M, f);
                 int q = warp_push(Q.n_query);
@@ -664,6 +682,9 @@ static int ensure_state(bg_scene* s, int64_t cap, int maxL) {
     BG_CUDA(cudaEventCreateWithFlags(&rs->ev_in, cudaEventDisableTiming));
     BG_CUDA(cudaEventCreateWithFlags(&rs->ev_out, cudaEventDisableTiming));
     BG_CUDA(cudaStreamCreateWithFlags(&rs->fstream, cudaStreamNonBlocking));
+    BG_CUDA(cudaStreamCreateWithFlags(&rs->tstream, cudaStreamNonBlocking));
+    BG_CUDA(cudaEventCreateWithFlags(&rs->ev_tstart, cudaEventDisableTiming));
+    BG_CUDA(cudaEventCreateWithFlags(&rs->ev_train, cudaEventDisableTiming));
     BG_CUDA(cudaEventCreateWithFlags(&rs->ev_fork, cudaEventDisableTiming));
     BG_CUDA(cudaEventCreateWithFlags(&rs->ev_join, cudaEventDisableTiming));
     BG_CUDA(cudaStreamCreateWithFlags(&rs->mstream, cudaStreamNonBlocking));
@@ -695,7 +716,8 @@ struct PassCfg {
     int maxdepth, kind;
     bool batched;
     bg_cache* cache;           // radiance-cache mode when non-null
-    int cache_depth, train_stride, train_phase;
+    int cache_depth, train_end, train_stride, train_phase;
+    bool wait_train;           // the first query stage waits for RenderState::ev_train
     float ao_radius;
 };
 
@@ -715,8 +737,9 @@ static void pass_queues(RenderState* rs, int c, bool batched, Queues& Q) {
     Q.n_ext_out = cnt + (c ? kCntExt0 : kCntExt1);
     Q.q_feat = rs->q_feat.as<float4>(); Q.q_path = rs->q_path.as<int>(); Q.q_thr = rs->q_thr.as<float4>();
     Q.n_query = cnt + kCntQuery;
-    Q.tr_feat = rs->tr_feat.as<float4>(); Q.tr_target = rs->tr_target.as<float4>();
-    Q.n_train = cnt + kCntTrain;
+    Q.tr_feat = rs->tr_feat.as<float4>() + size_t(rs->tr_set) * rs->tr_cap * 4;
+    Q.tr_target = rs->tr_target.as<float4>() + size_t(rs->tr_set) * rs->tr_cap;
+    Q.n_train = cnt + kCntTrain + rs->tr_set;
     Q.tr_cap = int(rs->tr_cap);
     Q.ext_root_in = batched ? rs->ext_root[c].as<int>() : nullptr;
     Q.ext_root_out = batched ? rs->ext_root[1 - c].as<int>() : nullptr;
@@ -779,8 +802,11 @@ static int enqueue_pass(bg_scene* s, RenderState* rs, cudaStream_t st, const Pas
             ++ins->launches;
         }
         ShadeArgs A{b, c.maxdepth, c.kind, rs->kmax, c.batched ? 1 : 0, c.cache ? c.cache_depth : -1,
-                    c.cache ? c.train_stride : 0, c.train_phase, c.ao_radius};
-        if (c.cache && b == c.cache_depth) BG_CUDA(cudaMemsetAsync(Q.n_query, 0, sizeof(int), st));
+                    c.cache ? c.train_end : -1, c.cache ? c.train_stride : 0, c.train_phase, c.ao_radius};
+        const bool query_here = c.cache && (b == c.cache_depth || b == c.train_end);
+        if (query_here) BG_CUDA(cudaMemsetAsync(Q.n_query, 0, sizeof(int), st));
+        // the network the queries read is the one the previous frame's rows trained
+        if (c.cache && c.wait_train && b == c.cache_depth) BG_CUDA(cudaStreamWaitEvent(st, rs->ev_train, 0));
         if (c.kind == BG_TRACER_DI) k_shade<BG_TRACER_DI, false><<<nb, kShadeThreads, 0, st>>>(s->dev, A, P, Q);
         else if (c.kind == BG_TRACER_AO) k_shade<BG_TRACER_AO, false><<<nb, kShadeThreads, 0, st>>>(s->dev, A, P, Q);
         else if (c.cache) k_shade<BG_TRACER_GI, true><<<nb, kShadeThreads, 0, st>>>(s->dev, A, P, Q);
@@ -820,8 +846,8 @@ static int enqueue_pass(bg_scene* s, RenderState* rs, cudaStream_t st, const Pas
         k_resolve_shadow<<<nb, kShadeThreads, 0, st>>>(P, Q);
         if (fork) BG_CUDA(cudaStreamWaitEvent(st, rs->ev_mjoin, 0));
         else k_resolve_mis<<<nb, kShadeThreads, 0, st>>>(s->dev, P, Q);
-        if (c.cache && b == c.cache_depth) {
-            // rendering paths that ended here: encode, infer, add throughput * prediction
+        if (query_here) {
+            // paths that ended into the cache here: encode, infer, add throughput * prediction
             if (ins) ins->mark(3);
             float4* qo = rs->q_out.as<float4>();
             if ((rc = nrc_encode(c.cache, rs->q_feat.as<float>(), Q.n_query, 0, 0, 0, st))) return rc;
@@ -1053,12 +1079,16 @@ int render_jobs(bg_scene* s, bg_cache* cache, const std::vector<JobSpec>& jobs, 
         cudaEventRecord(ev0, st);
     }
     // radiance-cache mode: training-path selection and buffers
-    int cache_depth = -1, stride = 0, phase = 0, tsteps = 0, tbatch = 0;
+    int cache_depth = -1, train_end = -1, stride = 0, phase = 0, tsteps = 0, tbatch = 0;
+    bool train_prev = false, wait_train = false;
     if (cache) {
         const bg_cache_desc* cd = nrc_desc(cache);
         if (tr->kind != BG_TRACER_GI) return set_error(BG_ERR_UNSUPPORTED, "the radiance cache serves GiTracer only");
         cache_depth = cd->cache_depth;
         if (cache_depth < 0 || cache_depth >= std::max(1, maxdepth)) return set_error(BG_ERR_INVALID_ARG, "cache_depth %d outside [0, maxdepth)", cache_depth);
+        if (cd->train_suffix < 0) return set_error(BG_ERR_INVALID_ARG, "train_suffix %d < 0", cd->train_suffix);
+        if (cd->train_suffix > 0 && cache_depth + cd->train_suffix < std::max(1, maxdepth))
+            train_end = cache_depth + cd->train_suffix;
         const int64_t tp = std::max<int64_t>(1, cd->train_paths);
         stride = int(std::max<int64_t>(1, std::min<int64_t>(total_samples / tp, int64_t(1) << 24)));
         phase = int(nrc_next_frame(cache) % stride);
@@ -1074,11 +1104,42 @@ int render_jobs(bg_scene* s, bg_cache* cache, const std::vector<JobSpec>& jobs, 
         }
         if ((rc = rs->rec.ensure(size_t(tpaths_pass) * maxdepth * 6 * 16))) return rc;
         if (rs->tr_cap < tr_cap) {
-            if ((rc = rs->tr_feat.ensure(size_t(tr_cap) * 64)) || (rc = rs->tr_target.ensure(size_t(tr_cap) * 16))) return rc;
+            if ((rc = rs->tr_feat.ensure(size_t(tr_cap) * 64 * kCntTrainSets)) ||
+                (rc = rs->tr_target.ensure(size_t(tr_cap) * 16 * kCntTrainSets)))
+                return rc;
             rs->tr_cap = tr_cap;
+            rs->pending_cache = nullptr;             // the sets were reallocated
         }
         if ((rc = nrc_prepare(cache, std::max<int64_t>(cap, tbatch)))) return rc;
-        BG_CUDA(cudaMemsetAsync(rs->counts.as<int>() + kCntTrain, 0, sizeof(int), st));
+        // Online training is one frame behind: this frame's training rows go to
+        // one set while the previous frame's rows (the other set) are trained on
+        // a side stream, beside this frame's first bounces, which do not read
+        // the cache; the first query stage waits for that training.
+        const int64_t frame = nrc_frame(cache) - 1;
+        train_prev = tsteps > 0 && rs->pending_cache == cache && rs->pending_frame == frame - 1;
+        rs->tr_set ^= 1;
+        int* ntr_prev = rs->counts.as<int>() + kCntTrain + (rs->tr_set ^ 1);
+        if (train_prev) {
+            const float* feat = rs->tr_feat.as<float>() + size_t(rs->tr_set ^ 1) * rs->tr_cap * 16;
+            const float4* target = rs->tr_target.as<float4>() + size_t(rs->tr_set ^ 1) * rs->tr_cap;
+            const bool side = !ins.time_phases;
+            cudaStream_t ts = side ? rs->tstream : st;
+            if (side) {
+                BG_CUDA(cudaEventRecord(rs->ev_tstart, st));
+                BG_CUDA(cudaStreamWaitEvent(ts, rs->ev_tstart, 0));
+            }
+            ins.mark(4);
+            k_clamp_count<<<1, 1, 0, ts>>>(ntr_prev, int(rs->tr_cap));
+            for (int i = 0; i < tsteps; ++i)
+                if ((rc = nrc_train_step(cache, feat, target, ntr_prev, i * tbatch, tbatch, true, ts))) return rc;
+            ins.launches += 1 + 11 * tsteps;
+            ins.mark(4);
+            if (side) BG_CUDA(cudaEventRecord(rs->ev_train, ts));
+            wait_train = side;
+        }
+        BG_CUDA(cudaMemsetAsync(rs->counts.as<int>() + kCntTrain + rs->tr_set, 0, sizeof(int), st));
+        rs->pending_cache = cache;
+        rs->pending_frame = frame;
     }
     int64_t done_samples = 0;
     for (int p = 0; p < npass; ++p) {
@@ -1091,31 +1152,22 @@ int render_jobs(bg_scene* s, bg_cache* cache, const std::vector<JobSpec>& jobs, 
             c.total += segs[size_t(q)].np * segs[size_t(q)].ns;
             c.npix += segs[size_t(q)].np;
         }
-        c.maxdepth = maxdepth;
+        // with a training suffix no path continues past train_end
+        c.maxdepth = train_end >= 0 ? train_end + 1 : maxdepth;
         c.kind = tr->kind;
         c.ao_radius = tr->kind == BG_TRACER_AO ? tr->ao_radius : 0.f;
         c.batched = batched;
         c.cache = cache;
         c.cache_depth = cache_depth;
+        c.train_end = train_end;
+        c.wait_train = wait_train && p == 0;
         c.train_stride = stride;
         c.train_phase = phase;
         rc = use_graph ? launch_pass_graph(s, rs, c) : enqueue_pass(s, rs, st, c, &ins);
         if (rc) return rc;
         done_samples += c.total;
     }
-    if (cache && tsteps > 0) {
-        // online training on this frame's samples (gradients + Adam per step)
-        int* ntr = rs->counts.as<int>() + kCntTrain;
-        ins.mark(4);
-        k_clamp_count<<<1, 1, 0, st>>>(ntr, int(rs->tr_cap));
-        for (int i = 0; i < tsteps; ++i) {
-            if ((rc = nrc_train_step(cache, rs->tr_feat.as<float>(), rs->tr_target.as<float4>(), ntr, i * tbatch, tbatch,
-                                     true, st)))
-                return rc;
-        }
-        ins.launches += 1 + 11 * tsteps;
-        ins.mark(4);
-    }
+    if (wait_train) BG_CUDA(cudaStreamWaitEvent(st, rs->ev_train, 0));   // the call's work ends with the training
     if (use_graph) {
         BG_CUDA(cudaEventRecord(rs->ev_out, rs->gstream));
         BG_CUDA(cudaStreamWaitEvent(st, rs->ev_out, 0));

@@ -402,7 +402,10 @@ typedef struct bg_cache_desc {
     uint64_t seed;             /* parameter initialisation                     */
     int32_t mlp_kernel;        /* inference and training: 0 = tcgen05 (TMEM
                                   accumulators), 1 = mma.sync (registers)      */
-    int32_t reserved;
+    int32_t train_suffix;      /* 0: training paths run to maxdepth (unbiased
+                                  targets); k > 0: they end into the cache k
+                                  bounces after cache_depth (self-training, the
+                                  pass stops there)                             */
 } bg_cache_desc;
 
 /* Query record: 16 floats per row = position (3), outgoing direction (3),
