@@ -437,8 +437,9 @@ k_shade(DevScene S, ShadeArgs A, PathState P, Queues Q) {
                 Q.q_thr[q] = make_float4(thr.x, thr.y, thr.z, 0.f);
                 end = true;
             } else {
-                if ((CACHE && A.cache_depth >= 0) && train) {
+                if ((CACHE && A.cache_depth >= 0) && train && A.bounce >= A.cache_depth) {
                     // training path: remember the vertex, its throughput and the radiance so far
+                    // (from cache_depth on: the depths at which the cache is queried)
                     const int t = (path + A.train_phase) / A.train_stride;
                     float4* rr = P.rec + (size_t(t) * A.maxdepth + A.bounce) * 6;
                     float4 f[4];
@@ -554,7 +555,7 @@ k_resolve_mis(DevScene S, PathState P, Queues Q) {
 }
 
 __global__ void __launch_bounds__(kShadeThreads)
-k_finalize(PathState P, Queues Q, int kmax, int maxdepth, int train_stride, int train_phase) {
+k_finalize(PathState P, Queues Q, int kmax, int maxdepth, int train_stride, int train_phase, int train_from) {
     const int n = *Q.n_end;
     const int nthreads = gridDim.x * blockDim.x;
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += nthreads) {
@@ -567,7 +568,7 @@ k_finalize(PathState P, Queues Q, int kmax, int maxdepth, int train_stride, int 
             // one training sample per recorded vertex: radiance gathered from that
             // vertex on, divided by the throughput that reached it
             const int t = (path + train_phase) / train_stride;
-            for (int k = 0; k < nv; ++k) {
+            for (int k = train_from; k < nv; ++k) {
                 const float4* rr = P.rec + (size_t(t) * maxdepth + k) * 6;
                 const float4 tk = rr[4], rb = rr[5];
                 if (!(tk.x > 1e-6f && tk.y > 1e-6f && tk.z > 1e-6f)) continue;
@@ -855,7 +856,8 @@ static int enqueue_pass(bg_scene* s, RenderState* rs, cudaStream_t st, const Pas
             k_cache_resolve<<<nb, kShadeThreads, 0, st>>>(P, Q, qo);
             if (ins) { ins->launches += 3; ins->mark(3); }
         }
-        k_finalize<<<nb, kShadeThreads, 0, st>>>(P, Q, rs->kmax, c.maxdepth, c.cache ? c.train_stride : 0, c.train_phase);
+        k_finalize<<<nb, kShadeThreads, 0, st>>>(P, Q, rs->kmax, c.maxdepth, c.cache ? c.train_stride : 0, c.train_phase,
+                                                 c.cache ? c.cache_depth : 0);
         if (ins) ins->launches += 3;
         if (forked) BG_CUDA(cudaStreamWaitEvent(st, rs->ev_join, 0));
         cur = 1 - cur;

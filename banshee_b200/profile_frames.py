@@ -8,7 +8,8 @@ c3: the 6.09M-triangle production scene at 1920x1080, plain GiTracer(8), one
     camera sample per pixel per frame; k_trace launches per bounce are, in
     order, extension (closest hit), shadow (any hit), MIS (closest hit).
 c5: the same scene through the radiance cache (2^19-entry hash grid levels,
-    65,536 training paths per frame, paths ended after 2 bounces).
+    65,536 training paths per frame ending into the cache one bounce after the
+    rendering paths, which end after 2 bounces; training one frame behind).
 c2: the 1M-triangle soup, 16M incoherent closest-hit rays, one
     bg_intersect_closest call per frame.
 Prints one JSON line with the CUDA-event time per frame.
@@ -48,8 +49,9 @@ def main():
     else:
         acc = torch.zeros((1080, 1920, 4), dtype=torch.float32, device="cuda")
         if args.workload == "c5":
-            cache = capi.RadianceCache(gs, log2_table_size=19, train_paths=65536, cache_depth=2, train_batch=16384,
-                                       train_steps=1)
+            cache = capi.RadianceCache(gs, log2_table_size=19, base_resolution=16, max_resolution=2048,
+                                       train_paths=65536, cache_depth=2, train_batch=65536, train_steps=1,
+                                       learning_rate=1e-2, train_suffix=1)
 
             def frame(f):
                 cache.render(acc.data_ptr(), 1920, 1080, 1, seed=1, sample_offset=f, maxdepth=8)

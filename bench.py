@@ -341,7 +341,7 @@ def time_to_relmse(gs, sc, args, target=1e-3):
                                                stats=False),
                         WIDTH, HEIGHT, Wc, Hc, gt, args.conv_seconds, 100000, target=target, every=4)
     cache = capi.RadianceCache(gs, log2_table_size=19, base_resolution=16, max_resolution=2048, train_paths=65536,
-                               cache_depth=2, train_batch=65536, train_steps=1, learning_rate=1e-2)
+                               cache_depth=2, train_batch=65536, train_steps=1, learning_rate=1e-2, train_suffix=1)
     cached = CV.converge(lambda p, f: cache.render(p, WIDTH, HEIGHT, 1, seed=SEED, sample_offset=f,
                                                    maxdepth=MAXDEPTH),
                          WIDTH, HEIGHT, Wc, Hc, gt, args.conv_seconds, 100000, target=target, every=4)
@@ -368,8 +368,9 @@ def time_to_relmse(gs, sc, args, target=1e-3):
             "reference": "plain GiTracer(8), float64 accumulation of 256-spp chunks",
             "relmse": "mean over pixels and channels of (x - ref)^2 / (ref^2 + 0.01)",
             "cache_config": "hash grid 16 levels x 2 features, 2^19 entries/level, res 16..2048; MLP 64x5 bf16; "
-                            "Adam lr 1e-2; 65536 training paths/frame, one Adam step over up to 65536 of their vertices; paths end into "
-                            "the cache after 2 bounces",
+                            "Adam lr 1e-2; 65536 training paths/frame; rendering paths end into the cache after 2 bounces, "
+                            "training paths one bounce later (self-training); one Adam step per frame over up to 65536 "
+                            "training vertices from depth 2 on, trained one frame behind beside the next frame's first bounces",
             "plain": summ(plain), "cache": summ(cached), "cache_over_plain_time": ratio,
             "perfect_cache_bound": {
                 "what": "plain tracer truncated after 2 bounces (max depth 2) against its own reference: the "
