@@ -592,6 +592,7 @@ int nrc_prepare(bg_cache* c, int64_t rows) { return cache_scratch(c, rows); }
 const bg_cache_desc* nrc_desc(const bg_cache* c) { return &c->desc; }
 int64_t nrc_next_frame(bg_cache* c) { return c->frame++; }
 int64_t nrc_frame(const bg_cache* c) { return c->frame; }
+const void* nrc_rows_ptr(const bg_cache* c) { return c->X.ptr; }
 bg_scene* nrc_scene(const bg_cache* c) { return c->scene; }
 
 }  // namespace bg

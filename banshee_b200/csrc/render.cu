@@ -39,6 +39,7 @@ int nrc_train_step(bg_cache* c, const float* feat, const float4* target, const i
 const bg_cache_desc* nrc_desc(const bg_cache* c);
 int64_t nrc_next_frame(bg_cache* c);
 int64_t nrc_frame(const bg_cache* c);   // frames rendered so far
+const void* nrc_rows_ptr(const bg_cache* c);   // the encoded-rows buffer (changes when it grows)
 bg_scene* nrc_scene(const bg_cache* c);
 
 __global__ void k_clamp_count(int* n, int cap) {
@@ -47,6 +48,7 @@ __global__ void k_clamp_count(int* n, int cap) {
 
 constexpr int kShadeThreads = 128;
 constexpr int kMaxBounceCounters = 6 * 1024;   // 6 work counters per bounce, maxdepth <= 1024
+constexpr int kGraphKey = 16;                    // int64 fields identifying a captured pass
 
 
 // A pass segment: `ns` samples of pixels [p0, p0 + np) of job `job`, as paths
@@ -101,10 +103,15 @@ struct RenderState {
     // this bounce's MIS trace + resolve (mstream), with fork / join events
     cudaStream_t fstream = nullptr, mstream = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_mjoin = nullptr;
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
-    cudaGraphNode_t gen_node = nullptr, acc_node = nullptr;
-    int64_t graph_key[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    // captured passes, two kept (a cached render alternates its training-row sets)
+    struct PassGraph {
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        cudaGraphNode_t gen_node = nullptr, acc_node = nullptr;
+        int64_t key[kGraphKey] = {};
+        uint64_t used = 0;
+    } graphs[2];
+    uint64_t graph_clock = 0;
 };
 
 void render_state_free(RenderState* rs) {
@@ -112,8 +119,10 @@ void render_state_free(RenderState* rs) {
         if (rs->tab_ev[i]) { cudaEventSynchronize(rs->tab_ev[i]); cudaEventDestroy(rs->tab_ev[i]); }
         if (rs->host_tab[i]) cudaFreeHost(rs->host_tab[i]);
     }
-    if (rs->exec) cudaGraphExecDestroy(rs->exec);
-    if (rs->graph) cudaGraphDestroy(rs->graph);
+    for (auto& pg : rs->graphs) {
+        if (pg.exec) cudaGraphExecDestroy(pg.exec);
+        if (pg.graph) cudaGraphDestroy(pg.graph);
+    }
     if (rs->ev_in) cudaEventDestroy(rs->ev_in);
     if (rs->ev_out) cudaEventDestroy(rs->ev_out);
     if (rs->gstream) cudaStreamDestroy(rs->gstream);
@@ -256,7 +265,7 @@ struct ShadeArgs {
     int bounce, maxdepth, kind, kmax, batched;
     int cache_depth;              // -1: plain tracer
     int train_end;                // training paths end into the cache here (-1: they run to maxdepth)
-    int train_stride, train_phase;
+    int train_stride;
     float ao_radius;              // BG_TRACER_AO
 };
 
@@ -440,7 +449,7 @@ k_shade(DevScene S, ShadeArgs A, PathState P, Queues Q) {
                 if ((CACHE && A.cache_depth >= 0) && train && A.bounce >= A.cache_depth) {
                     // training path: remember the vertex, its throughput and the radiance so far
                     // (from cache_depth on: the depths at which the cache is queried)
-                    const int t = (path + A.train_phase) / A.train_stride;
+                    const int t = path / A.train_stride;   // training paths are train_stride apart
                     float4* rr = P.rec + (size_t(t) * A.maxdepth + A.bounce) * 6;
                     float4 f[4];
                     cache_features(h, wo, M, f);
@@ -555,7 +564,7 @@ k_resolve_mis(DevScene S, PathState P, Queues Q) {
 }
 
 __global__ void __launch_bounds__(kShadeThreads)
-k_finalize(PathState P, Queues Q, int kmax, int maxdepth, int train_stride, int train_phase, int train_from) {
+k_finalize(PathState P, Queues Q, int kmax, int maxdepth, int train_stride, int train_from) {
     const int n = *Q.n_end;
     const int nthreads = gridDim.x * blockDim.x;
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += nthreads) {
@@ -567,7 +576,7 @@ k_finalize(PathState P, Queues Q, int kmax, int maxdepth, int train_stride, int 
         if ((fl & kFlagTrain) && nv > 0 && train_stride > 0) {
             // one training sample per recorded vertex: radiance gathered from that
             // vertex on, divided by the throughput that reached it
-            const int t = (path + train_phase) / train_stride;
+            const int t = path / train_stride;
             for (int k = train_from; k < nv; ++k) {
                 const float4* rr = P.rec + (size_t(t) * maxdepth + k) * 6;
                 const float4 tk = rr[4], rb = rr[5];
@@ -803,11 +812,12 @@ static int enqueue_pass(bg_scene* s, RenderState* rs, cudaStream_t st, const Pas
             ++ins->launches;
         }
         ShadeArgs A{b, c.maxdepth, c.kind, rs->kmax, c.batched ? 1 : 0, c.cache ? c.cache_depth : -1,
-                    c.cache ? c.train_end : -1, c.cache ? c.train_stride : 0, c.train_phase, c.ao_radius};
+                    c.cache ? c.train_end : -1, c.cache ? c.train_stride : 0, c.ao_radius};
         const bool query_here = c.cache && (b == c.cache_depth || b == c.train_end);
         if (query_here) BG_CUDA(cudaMemsetAsync(Q.n_query, 0, sizeof(int), st));
         // the network the queries read is the one the previous frame's rows trained
-        if (c.cache && c.wait_train && b == c.cache_depth) BG_CUDA(cudaStreamWaitEvent(st, rs->ev_train, 0));
+        if (c.cache && (c.wait_train || !ins) && b == c.cache_depth)
+            BG_CUDA(cudaStreamWaitEvent(st, rs->ev_train, ins ? 0u : unsigned(cudaEventWaitExternal)));
         if (c.kind == BG_TRACER_DI) k_shade<BG_TRACER_DI, false><<<nb, kShadeThreads, 0, st>>>(s->dev, A, P, Q);
         else if (c.kind == BG_TRACER_AO) k_shade<BG_TRACER_AO, false><<<nb, kShadeThreads, 0, st>>>(s->dev, A, P, Q);
         else if (c.cache) k_shade<BG_TRACER_GI, true><<<nb, kShadeThreads, 0, st>>>(s->dev, A, P, Q);
@@ -856,7 +866,7 @@ static int enqueue_pass(bg_scene* s, RenderState* rs, cudaStream_t st, const Pas
             k_cache_resolve<<<nb, kShadeThreads, 0, st>>>(P, Q, qo);
             if (ins) { ins->launches += 3; ins->mark(3); }
         }
-        k_finalize<<<nb, kShadeThreads, 0, st>>>(P, Q, rs->kmax, c.maxdepth, c.cache ? c.train_stride : 0, c.train_phase,
+        k_finalize<<<nb, kShadeThreads, 0, st>>>(P, Q, rs->kmax, c.maxdepth, c.cache ? c.train_stride : 0,
                                                  c.cache ? c.cache_depth : 0);
         if (ins) ins->launches += 3;
         if (forked) BG_CUDA(cudaStreamWaitEvent(st, rs->ev_join, 0));
@@ -873,63 +883,77 @@ static int enqueue_pass(bg_scene* s, RenderState* rs, cudaStream_t st, const Pas
 }
 
 // Captures one pass into a CUDA graph (once per bounce-loop shape) and finds
-// the two kernel nodes whose arguments (the segment slice) change per pass.
-static int pass_graph(bg_scene* s, RenderState* rs, const PassCfg& c) {
+// the two kernel nodes whose arguments (the segment slice, the training-path
+// phase) change per pass.
+static int pass_graph(bg_scene* s, RenderState* rs, const PassCfg& c, RenderState::PassGraph*& out) {
     uint32_t aob;
     memcpy(&aob, &c.ao_radius, sizeof(aob));
-    const int64_t key[9] = {c.maxdepth, c.kind, c.batched ? 1 : 0, rs->kmax, int64_t(rs->cap), s->tune_threads,
-                            s->dev.width, int64_t(aob), s->ev_accum ? 1 : 0};
-    if (rs->exec && memcmp(key, rs->graph_key, sizeof(key)) == 0) return BG_OK;
-    if (rs->exec) { cudaGraphExecDestroy(rs->exec); rs->exec = nullptr; }
-    if (rs->graph) { cudaGraphDestroy(rs->graph); rs->graph = nullptr; }
+    const int64_t key[kGraphKey] = {c.maxdepth, c.kind, c.batched ? 1 : 0, rs->kmax, int64_t(rs->cap), s->tune_threads,
+                                    s->dev.width, int64_t(aob), s->ev_accum ? 1 : 0,
+                                    int64_t(reinterpret_cast<uintptr_t>(c.cache)),
+                                    c.cache ? int64_t(reinterpret_cast<uintptr_t>(nrc_rows_ptr(c.cache))) : 0,
+                                    c.cache ? c.cache_depth : -1, c.cache ? c.train_end : -1,
+                                    c.cache ? c.train_stride : 0, c.cache ? rs->tr_set : 0,
+                                    c.cache ? int64_t(reinterpret_cast<uintptr_t>(rs->tr_feat.ptr)) : 0};
+    ++rs->graph_clock;
+    for (auto& pg : rs->graphs)
+        if (pg.exec && memcmp(key, pg.key, sizeof(key)) == 0) { pg.used = rs->graph_clock; out = &pg; return BG_OK; }
+    RenderState::PassGraph* pg = &rs->graphs[0];
+    for (auto& q : rs->graphs)
+        if (!q.exec || q.used < pg->used) pg = &q;       // an empty slot or the least recently used
+    if (pg->exec) { cudaGraphExecDestroy(pg->exec); pg->exec = nullptr; }
+    if (pg->graph) { cudaGraphDestroy(pg->graph); pg->graph = nullptr; }
     BG_CUDA(cudaStreamBeginCapture(rs->gstream, cudaStreamCaptureModeThreadLocal));
     int rc = enqueue_pass(s, rs, rs->gstream, c, nullptr);
     cudaGraph_t g = nullptr;
     cudaError_t e = cudaStreamEndCapture(rs->gstream, &g);
     if (rc) { if (g) cudaGraphDestroy(g); return rc; }
     if (e != cudaSuccess) return set_error(BG_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
-    rs->graph = g;
+    pg->graph = g;
     size_t nn = 0;
     BG_CUDA(cudaGraphGetNodes(g, nullptr, &nn));
     std::vector<cudaGraphNode_t> nodes(nn);
     BG_CUDA(cudaGraphGetNodes(g, nodes.data(), &nn));
-    rs->gen_node = rs->acc_node = nullptr;
+    pg->gen_node = pg->acc_node = nullptr;
     for (cudaGraphNode_t n : nodes) {
         cudaGraphNodeType t;
         BG_CUDA(cudaGraphNodeGetType(n, &t));
         if (t != cudaGraphNodeTypeKernel) continue;
         cudaKernelNodeParams kp;
         BG_CUDA(cudaGraphKernelNodeGetParams(n, &kp));
-        if (kp.func == reinterpret_cast<void*>(k_generate)) rs->gen_node = n;
-        if (kp.func == reinterpret_cast<void*>(k_accumulate)) rs->acc_node = n;
+        if (kp.func == reinterpret_cast<void*>(k_generate)) pg->gen_node = n;
+        if (kp.func == reinterpret_cast<void*>(k_accumulate)) pg->acc_node = n;
     }
-    if (!rs->gen_node || !rs->acc_node) return set_error(BG_ERR_STATE, "pass graph: kernel nodes not found");
-    BG_CUDA(cudaGraphInstantiate(&rs->exec, g, 0));
-    memcpy(rs->graph_key, key, sizeof(key));
+    if (!pg->gen_node || !pg->acc_node) return set_error(BG_ERR_STATE, "pass graph: kernel nodes not found");
+    BG_CUDA(cudaGraphInstantiate(&pg->exec, g, 0));
+    memcpy(pg->key, key, sizeof(key));
+    pg->used = rs->graph_clock;
+    out = pg;
     return BG_OK;
 }
 
 static int launch_pass_graph(bg_scene* s, RenderState* rs, const PassCfg& c) {
-    int rc = pass_graph(s, rs, c);
+    RenderState::PassGraph* pg = nullptr;
+    int rc = pass_graph(s, rs, c, pg);
     if (rc) return rc;
     PathState P = path_state(rs);
     Queues Q;
     pass_queues(rs, 0, c.batched, Q);
     const SegRec* segs = c.segs;
     int nseg = c.nseg, total = c.total, npix = c.npix;
-    int tstride = 0, tphase = 0;
+    int tstride = c.cache ? c.train_stride : 0, tphase = c.cache ? c.train_phase : 0;
     void* gargs[] = {&segs, &nseg, &total, &P, &Q, &tstride, &tphase};
     cudaKernelNodeParams kp;
-    BG_CUDA(cudaGraphKernelNodeGetParams(rs->gen_node, &kp));
+    BG_CUDA(cudaGraphKernelNodeGetParams(pg->gen_node, &kp));
     kp.kernelParams = gargs;
     kp.extra = nullptr;
-    BG_CUDA(cudaGraphExecKernelNodeSetParams(rs->exec, rs->gen_node, &kp));
+    BG_CUDA(cudaGraphExecKernelNodeSetParams(pg->exec, pg->gen_node, &kp));
     void* aargs[] = {&P, &segs, &nseg, &npix};
-    BG_CUDA(cudaGraphKernelNodeGetParams(rs->acc_node, &kp));
+    BG_CUDA(cudaGraphKernelNodeGetParams(pg->acc_node, &kp));
     kp.kernelParams = aargs;
     kp.extra = nullptr;
-    BG_CUDA(cudaGraphExecKernelNodeSetParams(rs->exec, rs->acc_node, &kp));
-    BG_CUDA(cudaGraphLaunch(rs->exec, rs->gstream));
+    BG_CUDA(cudaGraphExecKernelNodeSetParams(pg->exec, pg->acc_node, &kp));
+    BG_CUDA(cudaGraphLaunch(pg->exec, rs->gstream));
     return BG_OK;
 }
 
@@ -1037,11 +1061,12 @@ int render_jobs(bg_scene* s, bg_cache* cache, const std::vector<JobSpec>& jobs, 
     std::vector<JobRec> jrec(jobs.size());
     for (size_t j = 0; j < jobs.size(); ++j) jrec[j] = jobs[j].rec;
 
-    // Graph replay unless statistics were asked for, the cache is in use, or
-    // the caller's stream is capturing.
+    // Graph replay unless statistics were asked for or the caller's stream is
+    // capturing (cached renders too: the frame's training-path phase is a
+    // parameter of the generate node, the rest of the pass is frame-invariant).
     cudaStreamCaptureStatus cap_st = cudaStreamCaptureStatusNone;
     BG_CUDA(cudaStreamIsCapturing(st, &cap_st));
-    const bool use_graph = !stats && !cache && cap_st == cudaStreamCaptureStatusNone;
+    const bool use_graph = !stats && cap_st == cudaStreamCaptureStatusNone;
     cudaStream_t ws = use_graph ? rs->gstream : st;
     if (use_graph) {
         BG_CUDA(cudaEventRecord(rs->ev_in, st));
@@ -1139,6 +1164,8 @@ int render_jobs(bg_scene* s, bg_cache* cache, const std::vector<JobSpec>& jobs, 
             if (side) BG_CUDA(cudaEventRecord(rs->ev_train, ts));
             wait_train = side;
         }
+        // a replayed pass always holds the wait on ev_train: without training this frame it waits on nothing new
+        if (use_graph && !wait_train) BG_CUDA(cudaEventRecord(rs->ev_train, st));
         BG_CUDA(cudaMemsetAsync(rs->counts.as<int>() + kCntTrain + rs->tr_set, 0, sizeof(int), st));
         rs->pending_cache = cache;
         rs->pending_frame = frame;
