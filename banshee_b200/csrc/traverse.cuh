@@ -12,7 +12,8 @@
 //     4e-7 on the exit distance (more than the 2*gamma(3) rounding bound of
 //     (lo - o) * (1/d)), so no box that holds an accepted triangle is culled.
 // Children are visited nearest-first; stack entries keep their entry distance
-// and are culled against the current closest hit when popped.
+// and are culled against the current closest hit, widened by the same slack,
+// when popped.
 #pragma once
 
 #include "device_common.cuh"
@@ -226,7 +227,8 @@ template <bool ANY, class STACK>
 __device__ __forceinline__ bool trav_pop(TravState& s, const STACK& stack, int& item) {
     while (s.sp > 0) {
         const int2 e = stack.get(--s.sp);
-        if (!ANY && __int_as_float(e.y) > s.best) continue;
+        // the entry distance carries the box test's rounding: cull with its slack
+        if (!ANY && __int_as_float(e.y) > s.best + fabsf(s.best) * kBoxSlack) continue;
         item = e.x;
         return true;
     }
