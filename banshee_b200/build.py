@@ -16,7 +16,7 @@ LIB = os.path.join(HERE, "libbanshee_gpu.so")
 CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 
-CU_SOURCES = ["api.cu", "render.cu", "cache.cu", "batch.cu", "gpu_build.cu", "scene_records.cu"]
+CU_SOURCES = ["api.cu", "render.cu", "cache.cu", "batch.cu", "gpu_build.cu", "sah_build.cu", "scene_records.cu"]
 CXX_SOURCES = ["bvh_build.cpp", "image.cpp"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false",

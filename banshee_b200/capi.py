@@ -133,7 +133,7 @@ class GpuScene:
     def __init__(self, ctx, scene, node_width=0, max_leaf=4, bins=32, builder=0):
         """node_width: 4 (128-byte nodes), 8 (96-byte compressed nodes) or 0 (both
         built; the active one is chosen with set_node_width).  builder: 0 = host
-        binned SAH, 1 = device LBVH, 2 = device PLOC."""
+        binned SAH, 1 = device LBVH, 2 = device PLOC, 3 = device binned SAH."""
         self.ctx = ctx
         self.scene = scene
         self.h = _vp()

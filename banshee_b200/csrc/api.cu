@@ -340,8 +340,9 @@ static int commit_scene(bg_scene* s, const bg_build_opts* opts) {
             return set_error(BG_ERR_UNSUPPORTED, "node_width %d: supported widths are 4 and 8 (0: both)", want_width);
         if (opts->max_leaf_size) bp.max_leaf = opts->max_leaf_size;
         if (opts->sah_bins) bp.bins = opts->sah_bins;
-        if (opts->builder < 0 || opts->builder > 2)
-            return set_error(BG_ERR_INVALID_ARG, "builder %d: 0 (host SAH), 1 (device LBVH) or 2 (device PLOC)",
+        if (opts->builder < 0 || opts->builder > 3)
+            return set_error(BG_ERR_INVALID_ARG,
+                             "builder %d: 0 (host SAH), 1 (device LBVH), 2 (device PLOC) or 3 (device SAH)",
                              opts->builder);
     }
     const int device_build = (opts && ntris >= 2) ? opts->builder : 0;

@@ -492,7 +492,7 @@ int gpu_build_bvh(const float* lo, const float* hi, int64_t n, int builder, cons
                   DevBuf& nodes4, DevBuf& nodes8, DeviceBvh& out) {
     if (n < 2) return set_error(BG_ERR_INVALID_ARG, "device build needs at least 2 triangles");
     if (n > (int64_t(1) << 29)) return set_error(BG_ERR_UNSUPPORTED, "device build: too many triangles");
-    if (builder != 1 && builder != 2) return set_error(BG_ERR_INVALID_ARG, "device builder %d", builder);
+    if (builder < 1 || builder > 3) return set_error(BG_ERR_INVALID_ARG, "device builder %d", builder);
     struct Scratch {
         ScratchBuf cb, keys, keys2, idx, sorted, left, right, parent, box, cnt, cost, mk, visits, nopen, tmp;
         ScratchBuf cl, cl2, nn, lead, scan, keep, nsel;
@@ -510,72 +510,81 @@ int gpu_build_bvh(const float* lo, const float* hi, int64_t n, int builder, cons
          (rc = S.lead.ensure(N * 4)) || (rc = S.scan.ensure(N * 4)) || (rc = S.keep.ensure(N * 4)) ||
          (rc = S.nsel.ensure(8))))
         return rc;
-    const unsigned int init[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
-    BG_CUDA(cudaMemcpy(S.cb.ptr, init, sizeof(init), cudaMemcpyHostToDevice));
     const int blocks = int(std::min<int64_t>(kBGrid, (n + kBT - 1) / kBT));
-    k_centroid_bounds<<<blocks, kBT>>>(lo, hi, n, S.cb.as<unsigned int>());
-    k_morton<<<blocks, kBT>>>(lo, hi, n, S.cb.as<unsigned int>(), S.keys.as<uint64_t>(), S.idx.as<int32_t>());
-    BG_CUDA(cudaGetLastError());
-    size_t b1 = 0, b2 = 0, b3 = 0;
-    BG_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, b1, S.keys.as<uint64_t>(), S.keys2.as<uint64_t>(),
-                                            S.idx.as<int32_t>(), S.sorted.as<int32_t>(), int(n), 0, 63));
-    if (builder == 2) {
-        BG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, b2, S.lead.as<int32_t>(), S.scan.as<int32_t>(), int(n)));
-        BG_CUDA(cub::DeviceSelect::Flagged(nullptr, b3, S.cl.as<int32_t>(), S.keep.as<int32_t>(),
-                                           S.cl2.as<int32_t>(), S.nsel.as<int32_t>(), int(n)));
-    }
-    const size_t tb = std::max(b1, std::max(b2, b3));
-    if ((rc = S.tmp.ensure(tb))) return rc;
-    size_t tbytes = tb;
-    BG_CUDA(cub::DeviceRadixSort::SortPairs(S.tmp.ptr, tbytes, S.keys.as<uint64_t>(), S.keys2.as<uint64_t>(),
-                                            S.idx.as<int32_t>(), S.sorted.as<int32_t>(), int(n), 0, 63));
-    BG_CUDA(cudaMemset(S.parent.ptr, 0xff, NN * 4));
-    k_leaf_boxes<<<blocks, kBT>>>(lo, hi, S.sorted.as<int32_t>(), n, S.box.as<float>(),
-                                  builder == 2 ? S.cl.as<int32_t>() : nullptr);
-    BG_CUDA(cudaGetLastError());
     int32_t root = int32_t(n);
-    if (builder == 1) {
-        k_radix_tree<<<blocks, kBT>>>(S.keys2.as<uint64_t>(), n, S.left.as<int32_t>(), S.right.as<int32_t>(),
-                                      S.parent.as<int32_t>());
+    if (builder == 3) {
+        // top-down binned SAH on the device (sah_build.cu): tree and final order
+        if ((rc = sah_binary_tree(lo, hi, n, S.sorted.as<int32_t>(), S.left.as<int32_t>(), S.right.as<int32_t>(),
+                                  S.parent.as<int32_t>())))
+            return rc;
+        k_leaf_boxes<<<blocks, kBT>>>(lo, hi, S.sorted.as<int32_t>(), n, S.box.as<float>(), nullptr);
         BG_CUDA(cudaGetLastError());
     } else {
-        int* m_dev = S.nsel.as<int>();              // [0] clusters (written by the compaction), [1] next node
-        int32_t* base_dev = S.nsel.as<int32_t>() + 1;
-        const int32_t init_mb[2] = {int32_t(n), int32_t(n)};
-        BG_CUDA(cudaMemcpy(S.nsel.ptr, init_mb, sizeof(init_mb), cudaMemcpyHostToDevice));
-        int32_t* cl = S.cl.as<int32_t>();
-        int32_t* cl2 = S.cl2.as<int32_t>();
-        // every round merges at least one pair (the smallest pair is mutual), so
-        // m falls by at least one per round while above 1; the host reads m
-        // every kPlocCheck rounds to shrink the launch bound and to stop
-        constexpr int kPlocCheck = 4;
-        int m_bound = int(n);
-        while (m_bound > 1) {
-            for (int r = 0; r < kPlocCheck; ++r) {
-                const int g = std::min(kBGrid, (m_bound + kBT - 1) / kBT);
-                k_ploc_nn<<<g, kBT>>>(cl, m_dev, S.box.as<float>(), S.nn.as<int32_t>());
-                k_ploc_flags<<<g, kBT>>>(S.nn.as<int32_t>(), m_dev, m_bound, S.lead.as<int32_t>(), S.keep.as<int32_t>());
-                tbytes = tb;
-                BG_CUDA(cub::DeviceScan::ExclusiveSum(S.tmp.ptr, tbytes, S.lead.as<int32_t>(), S.scan.as<int32_t>(),
-                                                      m_bound));
-                k_ploc_merge<<<g, kBT>>>(cl, S.nn.as<int32_t>(), m_dev, S.lead.as<int32_t>(), S.scan.as<int32_t>(),
-                                         base_dev, S.box.as<float>(), S.left.as<int32_t>(), S.right.as<int32_t>(),
-                                         S.parent.as<int32_t>());
-                k_ploc_advance<<<1, 32>>>(base_dev, S.scan.as<int32_t>(), S.lead.as<int32_t>(), m_bound);
-                tbytes = tb;
-                BG_CUDA(cub::DeviceSelect::Flagged(S.tmp.ptr, tbytes, cl, S.keep.as<int32_t>(), cl2, m_dev, m_bound));
-                std::swap(cl, cl2);
-            }
-            BG_CUDA(cudaGetLastError());
-            int m = 0;
-            BG_CUDA(cudaMemcpy(&m, m_dev, sizeof(int), cudaMemcpyDeviceToHost));
-            if (m >= m_bound) return set_error(BG_ERR_STATE, "device PLOC build made no progress");
-            m_bound = m;
+        const unsigned int init[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
+        BG_CUDA(cudaMemcpy(S.cb.ptr, init, sizeof(init), cudaMemcpyHostToDevice));
+        k_centroid_bounds<<<blocks, kBT>>>(lo, hi, n, S.cb.as<unsigned int>());
+        k_morton<<<blocks, kBT>>>(lo, hi, n, S.cb.as<unsigned int>(), S.keys.as<uint64_t>(), S.idx.as<int32_t>());
+        BG_CUDA(cudaGetLastError());
+        size_t b1 = 0, b2 = 0, b3 = 0;
+        BG_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, b1, S.keys.as<uint64_t>(), S.keys2.as<uint64_t>(),
+                                                S.idx.as<int32_t>(), S.sorted.as<int32_t>(), int(n), 0, 63));
+        if (builder == 2) {
+            BG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, b2, S.lead.as<int32_t>(), S.scan.as<int32_t>(), int(n)));
+            BG_CUDA(cub::DeviceSelect::Flagged(nullptr, b3, S.cl.as<int32_t>(), S.keep.as<int32_t>(),
+                                               S.cl2.as<int32_t>(), S.nsel.as<int32_t>(), int(n)));
         }
-        int32_t next_node = 0;
-        BG_CUDA(cudaMemcpy(&next_node, base_dev, sizeof(int32_t), cudaMemcpyDeviceToHost));
-        if (next_node != int32_t(NN)) return set_error(BG_ERR_STATE, "device PLOC build: %d nodes", next_node);
-        BG_CUDA(cudaMemcpy(&root, cl, 4, cudaMemcpyDeviceToHost));
+        const size_t tb = std::max(b1, std::max(b2, b3));
+        if ((rc = S.tmp.ensure(tb))) return rc;
+        size_t tbytes = tb;
+        BG_CUDA(cub::DeviceRadixSort::SortPairs(S.tmp.ptr, tbytes, S.keys.as<uint64_t>(), S.keys2.as<uint64_t>(),
+                                                S.idx.as<int32_t>(), S.sorted.as<int32_t>(), int(n), 0, 63));
+        BG_CUDA(cudaMemset(S.parent.ptr, 0xff, NN * 4));
+        k_leaf_boxes<<<blocks, kBT>>>(lo, hi, S.sorted.as<int32_t>(), n, S.box.as<float>(),
+                                      builder == 2 ? S.cl.as<int32_t>() : nullptr);
+        BG_CUDA(cudaGetLastError());
+        if (builder == 1) {
+            k_radix_tree<<<blocks, kBT>>>(S.keys2.as<uint64_t>(), n, S.left.as<int32_t>(), S.right.as<int32_t>(),
+                                          S.parent.as<int32_t>());
+            BG_CUDA(cudaGetLastError());
+        } else {
+            int* m_dev = S.nsel.as<int>();              // [0] clusters (written by the compaction), [1] next node
+            int32_t* base_dev = S.nsel.as<int32_t>() + 1;
+            const int32_t init_mb[2] = {int32_t(n), int32_t(n)};
+            BG_CUDA(cudaMemcpy(S.nsel.ptr, init_mb, sizeof(init_mb), cudaMemcpyHostToDevice));
+            int32_t* cl = S.cl.as<int32_t>();
+            int32_t* cl2 = S.cl2.as<int32_t>();
+            // every round merges at least one pair (the smallest pair is mutual), so
+            // m falls by at least one per round while above 1; the host reads m
+            // every kPlocCheck rounds to shrink the launch bound and to stop
+            constexpr int kPlocCheck = 4;
+            int m_bound = int(n);
+            while (m_bound > 1) {
+                for (int r = 0; r < kPlocCheck; ++r) {
+                    const int g = std::min(kBGrid, (m_bound + kBT - 1) / kBT);
+                    k_ploc_nn<<<g, kBT>>>(cl, m_dev, S.box.as<float>(), S.nn.as<int32_t>());
+                    k_ploc_flags<<<g, kBT>>>(S.nn.as<int32_t>(), m_dev, m_bound, S.lead.as<int32_t>(), S.keep.as<int32_t>());
+                    tbytes = tb;
+                    BG_CUDA(cub::DeviceScan::ExclusiveSum(S.tmp.ptr, tbytes, S.lead.as<int32_t>(), S.scan.as<int32_t>(),
+                                                          m_bound));
+                    k_ploc_merge<<<g, kBT>>>(cl, S.nn.as<int32_t>(), m_dev, S.lead.as<int32_t>(), S.scan.as<int32_t>(),
+                                             base_dev, S.box.as<float>(), S.left.as<int32_t>(), S.right.as<int32_t>(),
+                                             S.parent.as<int32_t>());
+                    k_ploc_advance<<<1, 32>>>(base_dev, S.scan.as<int32_t>(), S.lead.as<int32_t>(), m_bound);
+                    tbytes = tb;
+                    BG_CUDA(cub::DeviceSelect::Flagged(S.tmp.ptr, tbytes, cl, S.keep.as<int32_t>(), cl2, m_dev, m_bound));
+                    std::swap(cl, cl2);
+                }
+                BG_CUDA(cudaGetLastError());
+                int m = 0;
+                BG_CUDA(cudaMemcpy(&m, m_dev, sizeof(int), cudaMemcpyDeviceToHost));
+                if (m >= m_bound) return set_error(BG_ERR_STATE, "device PLOC build made no progress");
+                m_bound = m;
+            }
+            int32_t next_node = 0;
+            BG_CUDA(cudaMemcpy(&next_node, base_dev, sizeof(int32_t), cudaMemcpyDeviceToHost));
+            if (next_node != int32_t(NN)) return set_error(BG_ERR_STATE, "device PLOC build: %d nodes", next_node);
+            BG_CUDA(cudaMemcpy(&root, cl, 4, cudaMemcpyDeviceToHost));
+        }
     }
     BG_CUDA(cudaMemset(S.visits.ptr, 0, NN * 4));
     BG_CUDA(cudaMemset(S.nopen.ptr, 0, 2 * sizeof(int)));

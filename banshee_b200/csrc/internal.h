@@ -113,6 +113,11 @@ struct DeviceBvh {
 };
 int gpu_build_bvh(const float* lo, const float* hi, int64_t n, int builder, const BuildParams& bp, int32_t* order,
                   DevBuf& nodes4, DevBuf& nodes8, DeviceBvh& out);
+// Top-down binned-SAH binary tree on the device (sah_build.cu), in gpu_build.cu's
+// numbering: sorted[p] = triangle at final position p (leaf p), internal nodes
+// n .. 2n-2 with the root n; left / right / parent of 2n - 1 entries.
+int sah_binary_tree(const float* lo, const float* hi, int64_t n, int32_t* sorted, int32_t* left, int32_t* right,
+                    int32_t* parent);
 
 // One commit's mesh arrays on the device (scene_records.cu): the meshes'
 // vertex, normal and uv arrays and per-face index arrays concatenated, with

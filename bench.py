@@ -203,7 +203,7 @@ def raycast_c2(ctx, nrays=1 << 24, reps=5):
     gs.close()
     # the device builders (LBVH: Morton order; PLOC: clustering over it) on the
     # same soup: build time and traversal speed of their trees
-    for builder, name in ((1, "device_lbvh"), (2, "device_ploc")):
+    for builder, name in ((1, "device_lbvh"), (2, "device_ploc"), (3, "device_sah")):
         out[name] = _device_build_traversal(ctx, builder, nrays, reps)
     return out
 
@@ -272,7 +272,7 @@ def batch_c4(ctx, nscenes=64, seed=7, timed_frames=1, rank=0, world=1, dist=None
     """C4: 64 procedural scenes (triangles log-uniform in [1e4, 5e5], resolutions from
     {256^2, 512^2, 1024x768}, 16..128 spp each) traced together by one batch: one set of
     queues, persistent kernels, one pass graph; autotuned node width / block / wavefront
-    sizes.  Each builder (host binned SAH, device LBVH, device PLOC) builds the scenes
+    sizes.  Each builder (host binned SAH, device LBVH, PLOC and binned SAH) builds the scenes
     (wall time, scene generation excluded) and the batch renders its trees; the headline
     fields are the host-SAH row.  On N GPUs each rank takes every N-th scene (no
     exchange); times are the max over ranks."""
@@ -290,7 +290,7 @@ def batch_c4(ctx, nscenes=64, seed=7, timed_frames=1, rank=0, world=1, dist=None
                          accum_dev=acc.data_ptr()))
     samples = sum(sc.width * sc.height * spp for sc, spp in all_items)
     rows = {}
-    for builder, name in ((0, "host_sah"), (1, "device_lbvh"), (2, "device_ploc")):
+    for builder, name in ((0, "host_sah"), (1, "device_lbvh"), (2, "device_ploc"), (3, "device_sah")):
         torch.cuda.synchronize()
         t1 = time.perf_counter()
         gss = [capi.GpuScene(ctx, sc, builder=builder) for sc, _ in items]

@@ -150,7 +150,8 @@ typedef struct bg_build_opts {
     int32_t builder;        /* 0 = host binned SAH; 1 = device LBVH
                                (Morton order, faster build, looser tree);
                                2 = device PLOC (nearest-neighbour
-                               clustering over the Morton order, radius 16) */
+                               clustering over the Morton order, radius 16);
+                               3 = device binned SAH (top-down, 32 bins) */
 } bg_build_opts;
 
 typedef struct bg_scene_info {

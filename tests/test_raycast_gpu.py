@@ -178,12 +178,12 @@ def test_layout_info_and_work(width, ctx):
         gs.set_node_width(2)
 
 
-@pytest.mark.parametrize("builder", [1, 2], ids=["lbvh", "ploc"])
+@pytest.mark.parametrize("builder", [1, 2, 3], ids=["lbvh", "ploc", "dsah"])
 @pytest.mark.parametrize("kind", ["incoherent", "coherent"])
 def test_device_builder_parity(width, ctx, oracle_built, kind, builder):
-    """The device builders (LBVH, PLOC) change only the tree: closest hits stay
-    bit-exact with the oracle (reference Bvh) and any-hit bits exact, on both
-    layouts."""
+    """The device builders (LBVH, PLOC, binned SAH) change only the tree:
+    closest hits stay bit-exact with the oracle (reference Bvh) and any-hit
+    bits exact, on both layouts."""
     from banshee_b200 import capi
     sc = scenes.soup(100_000, seed=21)
     gs = capi.GpuScene(ctx, sc, builder=builder)
@@ -202,7 +202,7 @@ def test_device_builder_parity(width, ctx, oracle_built, kind, builder):
     assert gs.error_flags() == 0
 
 
-@pytest.mark.parametrize("builder", [1, 2], ids=["lbvh", "ploc"])
+@pytest.mark.parametrize("builder", [1, 2, 3], ids=["lbvh", "ploc", "dsah"])
 def test_device_builder_golden_cornell(width, ctx, builder):
     from banshee_b200 import capi
     from tests.golden.make_golden import CORNELL
@@ -237,7 +237,7 @@ def _degenerate_soup(seed):
     return sc
 
 
-@pytest.mark.parametrize("builder", [0, 1, 2], ids=["sah", "lbvh", "ploc"])
+@pytest.mark.parametrize("builder", [0, 1, 2, 3], ids=["sah", "lbvh", "ploc", "dsah"])
 def test_builders_degenerate_soup(width, ctx, oracle_built, builder):
     """Duplicates, identical Morton codes, zero-area triangles and a transformed
     bundle: hits stay exact (ties classified) and any-hit bits identical, for
@@ -259,7 +259,7 @@ def test_builders_degenerate_soup(width, ctx, oracle_built, builder):
 
 
 @pytest.mark.parametrize("ntris", [2, 3, 5, 17])
-@pytest.mark.parametrize("builder", [1, 2], ids=["lbvh", "ploc"])
+@pytest.mark.parametrize("builder", [1, 2, 3], ids=["lbvh", "ploc", "dsah"])
 def test_device_builders_tiny_scenes(width, ctx, oracle_built, builder, ntris):
     """A root that is itself cheaper as one leaf is still opened into a node."""
     from banshee_b200 import capi
