@@ -816,7 +816,9 @@ static int enqueue_pass(bg_scene* s, RenderState* rs, cudaStream_t st, const Pas
         const bool query_here = c.cache && (b == c.cache_depth || b == c.train_end);
         if (query_here) BG_CUDA(cudaMemsetAsync(Q.n_query, 0, sizeof(int), st));
         // the network the queries read is the one the previous frame's rows trained
-        if (c.cache && (c.wait_train || !ins) && b == c.cache_depth)
+        // (with side streams the wait sits on the query's own stream, below)
+        const bool wait_here = c.cache && (c.wait_train || !ins) && b == c.cache_depth;
+        if (wait_here && !fork)
             BG_CUDA(cudaStreamWaitEvent(st, rs->ev_train, ins ? 0u : unsigned(cudaEventWaitExternal)));
         if (c.kind == BG_TRACER_DI) k_shade<BG_TRACER_DI, false><<<nb, kShadeThreads, 0, st>>>(s->dev, A, P, Q);
         else if (c.kind == BG_TRACER_AO) k_shade<BG_TRACER_AO, false><<<nb, kShadeThreads, 0, st>>>(s->dev, A, P, Q);
@@ -842,6 +844,15 @@ static int enqueue_pass(bg_scene* s, RenderState* rs, cudaStream_t st, const Pas
                                    Q.mis_root)))
                 return rc;
             k_resolve_mis<<<nb, kShadeThreads, 0, rs->mstream>>>(s->dev, P, Q);
+            if (query_here) {   // the cache query too: it adds to P.rad of ended paths, the resolves write P.slots
+                if (wait_here)
+                    BG_CUDA(cudaStreamWaitEvent(rs->mstream, rs->ev_train, ins ? 0u : unsigned(cudaEventWaitExternal)));
+                float4* qo = rs->q_out.as<float4>();
+                if ((rc = nrc_encode(c.cache, rs->q_feat.as<float>(), Q.n_query, 0, 0, 0, rs->mstream))) return rc;
+                if ((rc = nrc_infer(c.cache, Q.n_query, 0, qo, rs->mstream))) return rc;
+                k_cache_resolve<<<nb, kShadeThreads, 0, rs->mstream>>>(P, Q, qo);
+                if (ins) ins->launches += 3;
+            }
             BG_CUDA(cudaEventRecord(rs->ev_mjoin, rs->mstream));
         }
         if ((rc = launch_trace(s, true, Q.sh_rays, 0, Q.n_sh, nullptr, Q.sh_occ, st, nullptr, 1, wk + 2, Q.sh_root))) return rc;
@@ -857,7 +868,7 @@ static int enqueue_pass(bg_scene* s, RenderState* rs, cudaStream_t st, const Pas
         k_resolve_shadow<<<nb, kShadeThreads, 0, st>>>(P, Q);
         if (fork) BG_CUDA(cudaStreamWaitEvent(st, rs->ev_mjoin, 0));
         else k_resolve_mis<<<nb, kShadeThreads, 0, st>>>(s->dev, P, Q);
-        if (query_here) {
+        if (query_here && !fork) {
             // paths that ended into the cache here: encode, infer, add throughput * prediction
             if (ins) ins->mark(3);
             float4* qo = rs->q_out.as<float4>();
