@@ -457,6 +457,38 @@ __global__ void __launch_bounds__(256) k_nrc_adam(float* __restrict__ p, float* 
     }
 }
 
+// Adam over the hash grid, four parameters per thread.  A quad whose gradient
+// and both moments are zero (table entries no sample has reached yet, among
+// them the unused tails of the densely indexed coarse levels) is left as it
+// is: the update would change none of its values.
+__global__ void __launch_bounds__(256) k_nrc_adam4(float4* __restrict__ p, float4* __restrict__ g,
+                                                   float4* __restrict__ m, float4* __restrict__ v, int64_t n4,
+                                                   const int* step, float lr, float b1, float b2, float eps) {
+    const int t = *step;
+    const float c1 = 1.f / (1.f - powf(b1, float(t))), c2 = 1.f / (1.f - powf(b2, float(t)));
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n4; i += int64_t(gridDim.x) * blockDim.x) {
+        const float4 gi = g[i], mi = m[i], vi = v[i];
+        if (gi.x == 0.f && gi.y == 0.f && gi.z == 0.f && gi.w == 0.f && mi.x == 0.f && mi.y == 0.f && mi.z == 0.f &&
+            mi.w == 0.f && vi.x == 0.f && vi.y == 0.f && vi.z == 0.f && vi.w == 0.f)
+            continue;
+        float4 pi = p[i], mo, vo;
+        const float ga[4] = {gi.x, gi.y, gi.z, gi.w}, ma[4] = {mi.x, mi.y, mi.z, mi.w}, va[4] = {vi.x, vi.y, vi.z, vi.w};
+        float pa[4] = {pi.x, pi.y, pi.z, pi.w}, mn[4], vn[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            mn[k] = b1 * ma[k] + (1.f - b1) * ga[k];
+            vn[k] = b2 * va[k] + (1.f - b2) * ga[k] * ga[k];
+            pa[k] = pa[k] - lr * (mn[k] * c1) / (sqrtf(vn[k] * c2) + eps);
+        }
+        mo = make_float4(mn[0], mn[1], mn[2], mn[3]);
+        vo = make_float4(vn[0], vn[1], vn[2], vn[3]);
+        m[i] = mo;
+        v[i] = vo;
+        p[i] = make_float4(pa[0], pa[1], pa[2], pa[3]);
+        g[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+}
+
 __global__ void k_nrc_to_bf16(const float* __restrict__ p, __nv_bfloat16* __restrict__ out, int n) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = __float2bfloat16_rn(p[i]);
 }
@@ -580,9 +612,16 @@ int nrc_train_step(bg_cache* c, const float* feat, const float4* target, const i
         k_nrc_adam<<<c->sms * 4, 256, 0, st>>>(c->w.as<float>(), dW, c->w_m.as<float>(), c->w_v.as<float>(), kNrcParams,
                                                c->step.as<int>(), c->dev.lr, c->dev.beta1, c->dev.beta2, c->dev.eps,
                                                c->wb.as<__nv_bfloat16>());
-        k_nrc_adam<<<c->sms * 8, 256, 0, st>>>(c->grid.as<float>(), c->grid_grad.as<float>(), c->grid_m.as<float>(),
-                                               c->grid_v.as<float>(), grid_params(c), c->step.as<int>(), c->dev.lr,
-                                               c->dev.beta1, c->dev.beta2, c->dev.eps, nullptr);
+        const int64_t gp = grid_params(c);
+        if (gp % 4 == 0)
+            k_nrc_adam4<<<c->sms * 8, 256, 0, st>>>(c->grid.as<float4>(), c->grid_grad.as<float4>(),
+                                                    c->grid_m.as<float4>(), c->grid_v.as<float4>(), gp / 4,
+                                                    c->step.as<int>(), c->dev.lr, c->dev.beta1, c->dev.beta2,
+                                                    c->dev.eps);
+        else
+            k_nrc_adam<<<c->sms * 8, 256, 0, st>>>(c->grid.as<float>(), c->grid_grad.as<float>(), c->grid_m.as<float>(),
+                                                   c->grid_v.as<float>(), gp, c->step.as<int>(), c->dev.lr,
+                                                   c->dev.beta1, c->dev.beta2, c->dev.eps, nullptr);
         BG_CUDA(cudaGetLastError());
     }
     return BG_OK;

@@ -340,8 +340,20 @@ def time_to_relmse(gs, sc, args, target=1e-3):
     plain = CV.converge(lambda p, f: gs.render(p, WIDTH, HEIGHT, 1, seed=SEED, sample_offset=f, maxdepth=MAXDEPTH,
                                                stats=False),
                         WIDTH, HEIGHT, Wc, Hc, gt, args.conv_seconds, 100000, target=target, every=4)
-    cache = capi.RadianceCache(gs, log2_table_size=19, base_resolution=16, max_resolution=2048, train_paths=65536,
-                               cache_depth=2, train_batch=65536, train_steps=1, learning_rate=1e-2, train_suffix=1)
+    cache_cfg = dict(log2_table_size=19, base_resolution=16, max_resolution=2048, train_paths=65536, cache_depth=2,
+                     train_batch=65536, train_steps=1, learning_rate=1e-2, train_suffix=1)
+    # warm the process as the plain tracer's timing is warm: a throwaway cache
+    # renders a few frames (kernel modules loaded, scratch memory pooled); the
+    # timed cache then starts untrained
+    import torch
+    warm = capi.RadianceCache(gs, **cache_cfg)
+    wbuf = torch.zeros((HEIGHT, WIDTH, 4), dtype=torch.float32, device="cuda")
+    for f in range(4):
+        warm.render(wbuf.data_ptr(), WIDTH, HEIGHT, 1, seed=SEED, sample_offset=f, maxdepth=MAXDEPTH)
+    torch.cuda.synchronize()
+    warm.close()
+    del wbuf
+    cache = capi.RadianceCache(gs, **cache_cfg)
     cached = CV.converge(lambda p, f: cache.render(p, WIDTH, HEIGHT, 1, seed=SEED, sample_offset=f,
                                                    maxdepth=MAXDEPTH),
                          WIDTH, HEIGHT, Wc, Hc, gt, args.conv_seconds, 100000, target=target, every=4)
