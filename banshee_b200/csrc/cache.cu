@@ -429,8 +429,7 @@ __global__ void __launch_bounds__(128) k_nrc_grid_bwd(NrcDev C, const float* __r
                 const float w = (dx ? g.fx : 1.f - g.fx) * (dy ? g.fy : 1.f - g.fy) * (dz ? g.fz : 1.f - g.fz);
                 const uint32_t idx = grid_index(C, l, g.x0 + dx, g.y0 + dy, g.z0 + dz);
                 float* dst = C.grid_grad + (size_t(l) << C.log2_T) * 2 + size_t(idx) * 2;
-                atomicAdd(dst, w * g0);
-                atomicAdd(dst + 1, w * g1);
+                atomicAdd(reinterpret_cast<float2*>(dst), make_float2(w * g0, w * g1));   // both features, one vector atomic
             }
         }
     }
