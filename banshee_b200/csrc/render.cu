@@ -146,6 +146,9 @@ void render_state_free(RenderState* rs) {
 }
 
 enum : int { kCntExt0 = 0, kCntExt1 = 1, kCntSh = 2, kCntMis = 3, kCntEnd = 4, kCntQuery = 5, kCntTrain = 6 };
+// shadow / MIS / ended-path counters of the odd bounces when direct light is
+// resolved one bounce late (the even bounces use kCntSh..kCntEnd)
+constexpr int kCntSh1 = 8;
 // training rows alternate between two halves of tr_feat / tr_target (counters
 // kCntTrain + set): a frame writes one while the previous frame's are trained on
 constexpr int kCntTrainSets = 2;
@@ -178,6 +181,14 @@ struct Queues {
     int* ext_root_in; int* ext_root_out; int* sh_root; int* mis_root; // per-ray roots, batched only
     const JobRec* jobs;
 };
+
+// With direct light resolved one bounce late, a path's DI slots and DI
+// throughput alternate between two halves by bounce parity, and rad.w packs the
+// pending slot counts of both (bits 0-15: even bounces, 16-31: odd bounces).
+__device__ __forceinline__ int pend_get(int packed, int h) { return (packed >> (16 * h)) & 0xffff; }
+__device__ __forceinline__ int pend_set(int packed, int h, int v) {
+    return int((unsigned(packed) & ~(0xffffu << (16 * h))) | (unsigned(v) << (16 * h)));
+}
 
 // Warp-aggregated slot allocation: one atomicAdd per converged group of lanes.
 __device__ __forceinline__ int warp_push(int* counter) {
@@ -246,13 +257,14 @@ k_generate(const SegRec* __restrict__ segs, int nseg, int total, PathState P, Qu
     if (blockIdx.x == 0 && threadIdx.x == 0) *Q.n_ext_in = total;
 }
 
-// Adds the pending direct-light slots of path `path` into its radiance in light
-// order: di = ls + bs per light (GetDi), radiance += (throughput * di) * mult.
-__device__ __forceinline__ v3 gather_pending(const PathState& P, int kmax, int path, v3 rad, int pending) {
+// Adds the pending direct-light slots of a path (slots from `slot0`, DI
+// throughput at `di`) into its radiance in light order: di = ls + bs per light
+// (GetDi), radiance += (throughput * di) * mult.
+__device__ __forceinline__ v3 gather_pending(const PathState& P, size_t slot0, size_t di, v3 rad, int pending) {
     if (pending == 0) return rad;
-    float4 dt = P.dithr[path];
+    float4 dt = P.dithr[di];
     v3 thr = mk(dt.x, dt.y, dt.z);
-    const float4* sl = P.slots + size_t(path) * kmax;
+    const float4* sl = P.slots + slot0;
     for (int j = 0; j < pending; j += 2) {
         float4 a = sl[j], b = sl[j + 1];
         v3 di = add(mk(a.x, a.y, a.z), mk(b.x, b.y, b.z));
@@ -267,6 +279,8 @@ struct ShadeArgs {
     int train_end;                // training paths end into the cache here (-1: they run to maxdepth)
     int train_stride;
     float ao_radius;              // BG_TRACER_AO
+    int defer;                    // direct light resolved one bounce late (slot halves by bounce parity)
+    int cap;                      // paths per pass (size of one slot half / 2 kmax)
 };
 
 // Radiance-cache query record of a surface point: position, outgoing
@@ -363,7 +377,13 @@ template <int KIND, bool CACHE>
 __global__ void __launch_bounds__(kShadeThreads, 8)   // 64 registers (measured: 8 > 7 > 10 > 6 blocks / SM)
 k_shade(DevScene S, ShadeArgs A, PathState P, Queues Q) {
     const int n = *Q.n_ext_in;
+    if (blockIdx.x == 0 && threadIdx.x == 0) Q.totals[0] += (unsigned long long)n;
     const int nthreads = gridDim.x * blockDim.x;
+    // deferred mode: this bounce's DI goes to half h, which held the DI of bounce
+    // - 2 (gathered first); half 1 - h (bounce - 1) is still being resolved
+    const int h = A.bounce & 1;
+    const size_t shalf = A.defer ? size_t(h) * size_t(A.cap) * size_t(A.kmax) : 0;
+    const size_t dhalf = A.defer ? size_t(h) * size_t(A.cap) : 0;
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += nthreads) {
         const int path = Q.ext_path_in[e];
         const bg_hit hit = Q.ext_hits[e];
@@ -371,7 +391,9 @@ k_shade(DevScene S, ShadeArgs A, PathState P, Queues Q) {
         const v3 d = mk(rd.x, rd.y, rd.z);
         float4 r4 = P.rad[path];
         v3 rad = mk(r4.x, r4.y, r4.z);
-        rad = gather_pending(P, A.kmax, path, rad, __float_as_int(r4.w));
+        const int packed = __float_as_int(r4.w);
+        rad = gather_pending(P, shalf + size_t(path) * A.kmax, dhalf + path, rad,
+                             A.defer ? pend_get(packed, h) : packed);
         const JobRec J = Q.jobs[P.flags[path] >> 16];
         const int root = A.batched ? J.root : -1;
         unsigned flags = 0u;
@@ -415,7 +437,7 @@ k_shade(DevScene S, ShadeArgs A, PathState P, Queues Q) {
                 float ax, ay;
                 sample2d(lr, ax, ay);
                 const v3 dir = map_to_hemisphere(h.n, ax, ay, 1.f);
-                const int base = path * A.kmax;
+                const int base = int(shalf) + path * A.kmax;
                 P.slots[size_t(base)] = make_float4(0.f, 0.f, 0.f, 0.f);
                 P.slots[size_t(base) + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
                 const int k = warp_push(Q.n_sh);
@@ -423,7 +445,7 @@ k_shade(DevScene S, ShadeArgs A, PathState P, Queues Q) {
                 Q.sh_contrib[k] = make_float4(1.f, 1.f, 1.f, 0.f);
                 Q.sh_slot[k] = base;
                 if (root >= 0) Q.sh_root[k] = root;
-                P.dithr[path] = make_float4(1.f, 1.f, 1.f, 1.f);
+                P.dithr[dhalf + path] = make_float4(1.f, 1.f, 1.f, 1.f);
                 pending = 2;
                 flags |= kFlagNoClamp;
                 P.rng[path] = make_uint4(lr.z, lr.w, br.z, br.w);
@@ -460,7 +482,7 @@ k_shade(DevScene S, ShadeArgs A, PathState P, Queues Q) {
                     flags = (flags & ~0xff00u) | (unsigned(A.bounce + 1) << 8);
                 }
                 unsigned cnt = P.cnt[path];
-                const int base = path * A.kmax;
+                const int base = int(shalf) + path * A.kmax;
                 // bounce 0: every light, weight 1; later: one light picked by rand(), weight L
                 // (gitracer.cpp:72-84)
                 int first = J.light0, nl = J.nlights;
@@ -473,7 +495,7 @@ k_shade(DevScene S, ShadeArgs A, PathState P, Queues Q) {
                 pending = 2 * nl;
                 for (int j = 0; j < pending; ++j) P.slots[size_t(base) + j] = make_float4(0.f, 0.f, 0.f, 0.f);
                 for (int i = 0; i < nl; ++i) emit_di(S, Q, first + i, h, M, wo, lr, br, base + 2 * i, path, root);
-                P.dithr[path] = make_float4(thr.x, thr.y, thr.z, mult);
+                P.dithr[dhalf + path] = make_float4(thr.x, thr.y, thr.z, mult);
                 if (KIND == BG_TRACER_DI) {
                     flags |= kFlagNoClamp;
                     end = true;
@@ -509,7 +531,7 @@ k_shade(DevScene S, ShadeArgs A, PathState P, Queues Q) {
                 P.rng[path] = make_uint4(lr.z, lr.w, br.z, br.w);
             }
         }
-        P.rad[path] = make_float4(rad.x, rad.y, rad.z, __int_as_float(pending));
+        P.rad[path] = make_float4(rad.x, rad.y, rad.z, __int_as_float(A.defer ? pend_set(packed, h, pending) : pending));
         if (hit.primid < 0) flags |= P.flags[path];
         P.flags[path] = flags;
         if (end) {
@@ -527,7 +549,6 @@ k_resolve_shadow(PathState P, Queues Q) {
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += nthreads)
         if (!Q.sh_occ[e]) P.slots[Q.sh_slot[e]] = Q.sh_contrib[e];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
-        Q.totals[0] += (unsigned long long)*Q.n_ext_in;
         Q.totals[1] += (unsigned long long)n;
         Q.totals[2] += (unsigned long long)*Q.n_mis;
     }
@@ -564,13 +585,24 @@ k_resolve_mis(DevScene S, PathState P, Queues Q) {
 }
 
 __global__ void __launch_bounds__(kShadeThreads)
-k_finalize(PathState P, Queues Q, int kmax, int maxdepth, int train_stride, int train_from) {
+k_finalize(PathState P, Queues Q, int kmax, int maxdepth, int train_stride, int train_from, int bounce, int defer,
+           int cap) {
     const int n = *Q.n_end;
     const int nthreads = gridDim.x * blockDim.x;
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += nthreads) {
         const int path = Q.end_path[e];
         float4 r4 = P.rad[path];
-        v3 rad = gather_pending(P, kmax, path, mk(r4.x, r4.y, r4.z), __float_as_int(r4.w));
+        const int packed = __float_as_int(r4.w);
+        v3 rad = mk(r4.x, r4.y, r4.z);
+        if (defer) {   // the previous bounce's DI, then this bounce's
+            const int h = bounce & 1, g = h ^ 1;
+            rad = gather_pending(P, size_t(g) * cap * kmax + size_t(path) * kmax, size_t(g) * cap + path, rad,
+                                 pend_get(packed, g));
+            rad = gather_pending(P, size_t(h) * cap * kmax + size_t(path) * kmax, size_t(h) * cap + path, rad,
+                                 pend_get(packed, h));
+        } else {
+            rad = gather_pending(P, size_t(path) * kmax, size_t(path), rad, packed);
+        }
         const unsigned fl = P.flags[path];
         const int nv = int((fl >> 8) & 0xffu);
         if ((fl & kFlagTrain) && nv > 0 && train_stride > 0) {
@@ -669,19 +701,23 @@ static int ensure_state(bg_scene* s, int64_t cap, int maxL) {
             (rc = rs->ext_root[k].ensure(C * 4)))
             return rc;
     }
+    // shadow / MIS / ended-path queues, DI slots and DI throughput come in two
+    // halves (bounce parity) for passes that resolve direct light one bounce late
+    if (C * size_t(rs->kmax) * 2 >= (size_t(1) << 31))
+        return set_error(BG_ERR_UNSUPPORTED, "paths per pass x light slots too large (%zu x %d)", C, rs->kmax);
     if ((rc = rs->ext_hits.ensure(C * 16)) ||
-        (rc = rs->sh_rays.ensure(C * 2 * L * 32)) || (rc = rs->sh_contrib.ensure(C * 2 * L * 16)) ||
-        (rc = rs->sh_slot.ensure(C * 2 * L * 4)) || (rc = rs->sh_occ.ensure(C * 2 * L)) ||
-        (rc = rs->sh_root.ensure(C * 2 * L * 4)) ||
-        (rc = rs->mis_rays.ensure(C * L * 32)) || (rc = rs->mis_a.ensure(C * L * 16)) ||
-        (rc = rs->mis_b.ensure(C * L * 16)) || (rc = rs->mis_c.ensure(C * L * 16)) ||
-        (rc = rs->mis_hits.ensure(C * L * 16)) || (rc = rs->mis_root.ensure(C * L * 4)) ||
-        (rc = rs->end_path.ensure(C * 4)) ||
+        (rc = rs->sh_rays.ensure(2 * C * 2 * L * 32)) || (rc = rs->sh_contrib.ensure(2 * C * 2 * L * 16)) ||
+        (rc = rs->sh_slot.ensure(2 * C * 2 * L * 4)) || (rc = rs->sh_occ.ensure(2 * C * 2 * L)) ||
+        (rc = rs->sh_root.ensure(2 * C * 2 * L * 4)) ||
+        (rc = rs->mis_rays.ensure(2 * C * L * 32)) || (rc = rs->mis_a.ensure(2 * C * L * 16)) ||
+        (rc = rs->mis_b.ensure(2 * C * L * 16)) || (rc = rs->mis_c.ensure(2 * C * L * 16)) ||
+        (rc = rs->mis_hits.ensure(2 * C * L * 16)) || (rc = rs->mis_root.ensure(2 * C * L * 4)) ||
+        (rc = rs->end_path.ensure(2 * C * 4)) ||
         (rc = rs->counts.ensure(256)) ||
         (rc = rs->st_key.ensure(C * 8)) || (rc = rs->st_cnt.ensure(C * 4)) || (rc = rs->st_rng.ensure(C * 16)) ||
         (rc = rs->st_bs.ensure(C * 8)) || (rc = rs->st_thr.ensure(C * 16)) || (rc = rs->st_rad.ensure(C * 16)) ||
-        (rc = rs->st_dithr.ensure(C * 16)) || (rc = rs->st_flags.ensure(C * 4)) ||
-        (rc = rs->slots.ensure(C * rs->kmax * 16)) || (rc = rs->sample_rad.ensure(C * 16)) ||
+        (rc = rs->st_dithr.ensure(2 * C * 16)) || (rc = rs->st_flags.ensure(C * 4)) ||
+        (rc = rs->slots.ensure(2 * C * rs->kmax * 16)) || (rc = rs->sample_rad.ensure(C * 16)) ||
         (rc = rs->cnt_out.ensure((C * 2 * L / 64 + 64) * 16)) ||
         (rc = rs->work.ensure(size_t(kMaxBounceCounters) * 8)))
         return rc;
@@ -731,15 +767,21 @@ struct PassCfg {
     float ao_radius;
 };
 
-static void pass_queues(RenderState* rs, int c, bool batched, Queues& Q) {
+// Queue pointers of a bounce: extension queue `c` in, 1 - c out; shadow, MIS
+// and ended-path queues and their counters of parity `par`.
+static void pass_queues(RenderState* rs, int c, bool batched, Queues& Q, int par = 0) {
     int* cnt = rs->counts.as<int>();
+    const size_t C = size_t(rs->cap), L = size_t(rs->nlights);
+    const size_t sh = par ? C * 2 * L : 0, mi = par ? C * L : 0;   // entries before this parity's half
     Q.ext_hits = rs->ext_hits.as<bg_hit>();
-    Q.sh_rays = rs->sh_rays.as<float4>(); Q.sh_contrib = rs->sh_contrib.as<float4>();
-    Q.sh_slot = rs->sh_slot.as<int>(); Q.sh_occ = rs->sh_occ.as<uint8_t>();
-    Q.mis_rays = rs->mis_rays.as<float4>(); Q.mis_a = rs->mis_a.as<float4>(); Q.mis_b = rs->mis_b.as<float4>();
-    Q.mis_c = rs->mis_c.as<int4>(); Q.mis_hits = rs->mis_hits.as<bg_hit>();
-    Q.end_path = rs->end_path.as<int>();
-    Q.n_sh = cnt + kCntSh; Q.n_mis = cnt + kCntMis; Q.n_end = cnt + kCntEnd;
+    Q.sh_rays = rs->sh_rays.as<float4>() + 2 * sh; Q.sh_contrib = rs->sh_contrib.as<float4>() + sh;
+    Q.sh_slot = rs->sh_slot.as<int>() + sh; Q.sh_occ = rs->sh_occ.as<uint8_t>() + sh;
+    Q.mis_rays = rs->mis_rays.as<float4>() + 2 * mi; Q.mis_a = rs->mis_a.as<float4>() + mi;
+    Q.mis_b = rs->mis_b.as<float4>() + mi;
+    Q.mis_c = rs->mis_c.as<int4>() + mi; Q.mis_hits = rs->mis_hits.as<bg_hit>() + mi;
+    Q.end_path = rs->end_path.as<int>() + (par ? C : 0);
+    const int c0 = par ? kCntSh1 : kCntSh;
+    Q.n_sh = cnt + c0; Q.n_mis = cnt + c0 + 1; Q.n_end = cnt + c0 + 2;
     Q.totals = reinterpret_cast<unsigned long long*>(rs->counts.as<char>() + 64);
     Q.ext_rays_in = rs->ext_rays[c].as<float4>(); Q.ext_path_in = rs->ext_path[c].as<int>();
     Q.ext_rays_out = rs->ext_rays[1 - c].as<float4>(); Q.ext_path_out = rs->ext_path[1 - c].as<int>();
@@ -753,8 +795,8 @@ static void pass_queues(RenderState* rs, int c, bool batched, Queues& Q) {
     Q.tr_cap = int(rs->tr_cap);
     Q.ext_root_in = batched ? rs->ext_root[c].as<int>() : nullptr;
     Q.ext_root_out = batched ? rs->ext_root[1 - c].as<int>() : nullptr;
-    Q.sh_root = batched ? rs->sh_root.as<int>() : nullptr;
-    Q.mis_root = batched ? rs->mis_root.as<int>() : nullptr;
+    Q.sh_root = batched ? rs->sh_root.as<int>() + sh : nullptr;
+    Q.mis_root = batched ? rs->mis_root.as<int>() + mi : nullptr;
     Q.jobs = rs->jobs.as<JobRec>();
 }
 
@@ -798,7 +840,58 @@ static int enqueue_pass(bg_scene* s, RenderState* rs, cudaStream_t st, const Pas
     const bool fork = (ins == nullptr || (!ins->time_phases && !ins->count_trav)) && rs->fstream != nullptr &&
                       rs->mstream != nullptr;
     const int depth = std::max(1, c.maxdepth);
-    for (int b = 0; b < depth; ++b) {
+    if (fork && !c.cache) {
+        // Direct light resolved one bounce late.  Shade(b) gathers the DI of
+        // bounce b - 2 and writes its own into the slot half of parity b, so the
+        // main stream runs extension trace -> shade -> extension trace -> ...
+        // while a side stream traces bounce b's shadow and MIS rays, resolves
+        // them and finalizes the paths that ended at b; shade(b + 2) waits for
+        // that.  Radiance is summed in the same order (every bounce's DI in turn,
+        // and nothing else is added after bounce 0), so images are unchanged.
+        cudaStream_t ds = rs->mstream;
+        cudaEvent_t evd[2] = {rs->ev_join, rs->ev_mjoin};
+        for (int b = 0; b < depth; ++b) {
+            const int par = b & 1;
+            unsigned long long* wk = rs->work.as<unsigned long long>() + 6 * b;
+            pass_queues(rs, cur, c.batched, Q, par);
+            if (b >= 2) BG_CUDA(cudaStreamWaitEvent(st, evd[par], 0));   // bounce b - 2's side work is done
+            BG_CUDA(cudaMemsetAsync(Q.n_ext_out, 0, sizeof(int), st));
+            BG_CUDA(cudaMemsetAsync(cnt + (par ? kCntSh1 : kCntSh), 0, 3 * sizeof(int), st));
+            if (b == 0) {
+                if ((rc = launch_trace(s, false, Q.ext_rays_in, 0, Q.n_ext_in, Q.ext_hits, nullptr, st, nullptr, 1, wk,
+                                       Q.ext_root_in)))
+                    return rc;
+                if (ins) { ++ins->launches; ++ins->launches_extend; }
+            }
+            ShadeArgs A{b, c.maxdepth, c.kind, rs->kmax, c.batched ? 1 : 0, -1, -1, 0, c.ao_radius, 1, int(rs->cap)};
+            if (c.kind == BG_TRACER_DI) k_shade<BG_TRACER_DI, false><<<nb, kShadeThreads, 0, st>>>(s->dev, A, P, Q);
+            else if (c.kind == BG_TRACER_AO) k_shade<BG_TRACER_AO, false><<<nb, kShadeThreads, 0, st>>>(s->dev, A, P, Q);
+            else k_shade<BG_TRACER_GI, false><<<nb, kShadeThreads, 0, st>>>(s->dev, A, P, Q);
+            BG_CUDA(cudaEventRecord(rs->ev_fork, st));
+            BG_CUDA(cudaStreamWaitEvent(ds, rs->ev_fork, 0));
+            if ((rc = launch_trace(s, true, Q.sh_rays, 0, Q.n_sh, nullptr, Q.sh_occ, ds, nullptr, 1, wk + 2, Q.sh_root)))
+                return rc;
+            if ((rc = launch_trace(s, false, Q.mis_rays, 0, Q.n_mis, Q.mis_hits, nullptr, ds, nullptr, 1, wk + 3,
+                                   Q.mis_root)))
+                return rc;
+            k_resolve_shadow<<<nb, kShadeThreads, 0, ds>>>(P, Q);
+            k_resolve_mis<<<nb, kShadeThreads, 0, ds>>>(s->dev, P, Q);
+            k_finalize<<<nb, kShadeThreads, 0, ds>>>(P, Q, rs->kmax, c.maxdepth, 0, 0, b, 1, int(rs->cap));
+            BG_CUDA(cudaEventRecord(evd[par], ds));
+            if (ins) ins->launches += 6;
+            if (b + 1 < depth) {
+                cur = 1 - cur;
+                Queues Qn;
+                pass_queues(rs, cur, c.batched, Qn, par ^ 1);
+                if ((rc = launch_trace(s, false, Qn.ext_rays_in, 0, Qn.n_ext_in, Qn.ext_hits, nullptr, st, nullptr, 1,
+                                       wk + 6, Qn.ext_root_in)))
+                    return rc;
+                if (ins) { ++ins->launches; ++ins->launches_extend; }
+            }
+        }
+        BG_CUDA(cudaStreamWaitEvent(st, evd[(depth - 1) & 1], 0));   // the side stream is in bounce order
+    }
+    for (int b = 0; b < depth && !(fork && !c.cache); ++b) {
         unsigned long long* wk = rs->work.as<unsigned long long>() + 6 * b;
         BG_CUDA(cudaMemsetAsync(Q.n_ext_out, 0, sizeof(int), st));
         BG_CUDA(cudaMemsetAsync(cnt + kCntSh, 0, 3 * sizeof(int), st));
@@ -812,7 +905,7 @@ static int enqueue_pass(bg_scene* s, RenderState* rs, cudaStream_t st, const Pas
             ++ins->launches;
         }
         ShadeArgs A{b, c.maxdepth, c.kind, rs->kmax, c.batched ? 1 : 0, c.cache ? c.cache_depth : -1,
-                    c.cache ? c.train_end : -1, c.cache ? c.train_stride : 0, c.ao_radius};
+                    c.cache ? c.train_end : -1, c.cache ? c.train_stride : 0, c.ao_radius, 0, int(rs->cap)};
         const bool query_here = c.cache && (b == c.cache_depth || b == c.train_end);
         if (query_here) BG_CUDA(cudaMemsetAsync(Q.n_query, 0, sizeof(int), st));
         // the network the queries read is the one the previous frame's rows trained
@@ -878,7 +971,7 @@ static int enqueue_pass(bg_scene* s, RenderState* rs, cudaStream_t st, const Pas
             if (ins) { ins->launches += 3; ins->mark(3); }
         }
         k_finalize<<<nb, kShadeThreads, 0, st>>>(P, Q, rs->kmax, c.maxdepth, c.cache ? c.train_stride : 0,
-                                                 c.cache ? c.cache_depth : 0);
+                                                 c.cache ? c.cache_depth : 0, b, 0, int(rs->cap));
         if (ins) ins->launches += 3;
         if (forked) BG_CUDA(cudaStreamWaitEvent(st, rs->ev_join, 0));
         cur = 1 - cur;
