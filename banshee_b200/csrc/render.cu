@@ -223,11 +223,22 @@ k_generate(const SegRec* __restrict__ segs, int nseg, int total, PathState P, Qu
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += nthreads) {
         const SegRec& G = segs[find_seg(segs, nseg, i)];
         const CamDev& cam = G.cam;
+        const int W = G.W, H = G.H;
         const int li = i - G.path0;
         const int sl = li / G.np;
-        const int pix = G.p0 + (li - sl * G.np);
+        // queue slot i holds the sample of pixel offset `off` of its slice: slices of
+        // whole rows are laid out in 8 x 4 pixel tiles (one warp's 32 rays), row
+        // groups of 4 in turn, rows beyond the last full group in row order; the
+        // path index stays the pixel's, so only the ray order changes
+        int off = li - sl * G.np;
+        if (W % 8 == 0 && G.p0 % W == 0 && G.np % W == 0 && off < (G.np / (4 * W)) * 4 * W) {
+            const int rg = off / (4 * W), rem = off - rg * 4 * W;
+            const int tc = rem >> 5, w = rem & 31;
+            off = (4 * rg + (w >> 3)) * W + 8 * tc + (w & 7);
+        }
+        const int pix = G.p0 + off;
+        const int path = G.path0 + sl * G.np + off;
         const uint32_t s = uint32_t(G.s0 + sl);
-        const int W = G.W, H = G.H;
         const uint64_t key = keyed_key(G.seed, uint32_t(pix), s);
         McRng img{keyed_rand(key, 0), keyed_rand(key, 1)};
         McRng lr{keyed_rand(key, 2), keyed_rand(key, 3)};
@@ -243,16 +254,16 @@ k_generate(const SegRec* __restrict__ segs, int nseg, int total, PathState P, Qu
                                  muls(mk(cam.right[0], cam.right[1], cam.right[2]), cx)),
                              muls(mk(cam.up[0], cam.up[1], cam.up[2]), cy)));
         put_ray(Q.ext_rays_in, i, mk(cam.p[0], cam.p[1], cam.p[2]), cam.znear, d, cam.zfar);
-        Q.ext_path_in[i] = i;
+        Q.ext_path_in[i] = path;
         if (Q.ext_root_in) Q.ext_root_in[i] = Q.jobs[G.job].root;
-        P.key[i] = key;
-        P.cnt[i] = 6u;
-        P.rng[i] = make_uint4(lr.z, lr.w, br.z, br.w);
-        P.thr[i] = make_float4(1.f, 1.f, 1.f, 0.f);
-        P.rad[i] = make_float4(0.f, 0.f, 0.f, __int_as_float(0));
-        P.flags[i] = ((train_stride > 0 && (i + train_phase) % train_stride == 0) ? kFlagTrain : 0u) |
-                     (unsigned(G.job) << 16);
-        P.sample_rad[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        P.key[path] = key;
+        P.cnt[path] = 6u;
+        P.rng[path] = make_uint4(lr.z, lr.w, br.z, br.w);
+        P.thr[path] = make_float4(1.f, 1.f, 1.f, 0.f);
+        P.rad[path] = make_float4(0.f, 0.f, 0.f, __int_as_float(0));
+        P.flags[path] = ((train_stride > 0 && (path + train_phase) % train_stride == 0) ? kFlagTrain : 0u) |
+                        (unsigned(G.job) << 16);
+        P.sample_rad[path] = make_float4(0.f, 0.f, 0.f, 0.f);
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) *Q.n_ext_in = total;
 }
@@ -1086,7 +1097,6 @@ static void plan_passes(const std::vector<JobSpec>& jobs, int64_t cap, std::vect
                     SegRec g{};
                     g.cam = J.cam; g.accum = J.accum; g.seed = J.seed; g.job = int(j);
                     g.skind = J.skind; g.grid = J.grid;
-                g.skind = J.skind; g.grid = J.grid;
                     g.np = int(std::min<int64_t>(cap, npix - p0)); g.ns = 1; g.p0 = int(p0); g.s0 = J.soff + s;
                     g.W = J.W; g.H = J.H;
                     all.push_back(g);
