@@ -276,7 +276,6 @@ int bg_batch_autotune(bg_batch* b, const bg_batch_job* jobs, int32_t njobs, cons
     if (M.dev.nodes) widths.push_back(4);
     if (M.dev.nodes8) widths.push_back(8);
     const int threads[2] = {128, 256};
-    const int64_t paths[4] = {int64_t(1) << 19, int64_t(1) << 20, int64_t(1) << 21, int64_t(1) << 22};
     float best = 1e30f;
     int best_t = 128, best_w = M.dev.width;
     int64_t best_p = int64_t(1) << 21;
@@ -288,12 +287,21 @@ int bg_batch_autotune(bg_batch* b, const bg_batch_job* jobs, int32_t njobs, cons
     for (int w : widths) {
         M.dev.width = w;
         if ((rc = batch_jobs(b, jobs, njobs, js, std::max(1, probe_spp)))) break;   // roots of this layout
+        int64_t probe_samples = 0;
+        for (const JobSpec& J : js) probe_samples += int64_t(J.W) * J.H * J.spp;
         for (int t : threads) {
-            for (int64_t p : paths) {
+            for (int pi = 0; pi < kPassCandidates && pass_candidate_needed(pi, probe_samples); ++pi) {
+                const int64_t p = pass_candidate(pi);
                 M.tune_threads = t;
                 M.tune_paths = p;
                 // first call warms the graph and buffers for this candidate, the second is timed
-                if ((rc = render_jobs(&M, nullptr, js, tracer, nullptr, st, true))) break;
+                if ((rc = render_jobs(&M, nullptr, js, tracer, nullptr, st, true))) {
+                    if (rc == BG_ERR_OOM && pi > 0) {   // no room for passes this large: keep the smaller
+                        cudaGetLastError();
+                        rc = BG_OK;
+                    }
+                    break;
+                }
                 BG_CUDA(cudaEventRecord(e0, st));
                 if ((rc = render_jobs(&M, nullptr, js, tracer, nullptr, st, true))) break;
                 BG_CUDA(cudaEventRecord(e1, st));

@@ -696,12 +696,7 @@ CamDev make_camera(const bg_camera_desc* c) {
     return k;
 }
 
-static int ensure_state(bg_scene* s, int64_t cap, int maxL) {
-    RenderState* rs = s->render;
-    const int L = std::max(1, maxL);
-    if (rs && rs->cap >= cap && rs->nlights == L) return BG_OK;
-    if (rs) render_state_free(rs);
-    rs = s->render = new RenderState();
+static int alloc_state(bg_scene* s, RenderState* rs, int64_t cap, int L) {
     rs->cap = cap;
     rs->nlights = L;
     rs->kmax = 2 * L;
@@ -747,6 +742,21 @@ static int ensure_state(bg_scene* s, int64_t cap, int maxL) {
     BG_CUDA(cudaStreamCreateWithFlags(&rs->mstream, cudaStreamNonBlocking));
     BG_CUDA(cudaEventCreateWithFlags(&rs->ev_mjoin, cudaEventDisableTiming));
     return BG_OK;
+}
+
+// Path state and queues for passes of `cap` paths with up to maxL lights per
+// job; a failed allocation leaves no state behind (the next call starts over).
+static int ensure_state(bg_scene* s, int64_t cap, int maxL) {
+    const int L = std::max(1, maxL);
+    if (s->render && s->render->cap >= cap && s->render->nlights == L) return BG_OK;
+    if (s->render) render_state_free(s->render);
+    s->render = new RenderState();
+    const int rc = alloc_state(s, s->render, cap, L);
+    if (rc) {
+        render_state_free(s->render);
+        s->render = nullptr;
+    }
+    return rc;
 }
 
 struct Instr {
@@ -1388,7 +1398,7 @@ static int scene_autotune(bg_scene* s, const bg_camera_desc* cam, const bg_trace
     if (s->dev.nodes) widths.push_back(4);
     if (s->dev.nodes8) widths.push_back(8);
     const int threads[2] = {128, 256};
-    const int64_t paths[4] = {int64_t(1) << 19, int64_t(1) << 20, int64_t(1) << 21, int64_t(1) << 22};
+    const int64_t probe_samples = int64_t(W) * H * std::max(1, probe_spp);
     bg_sampler_desc sm = {BG_SAMPLER_RANDOM, std::max(1, probe_spp), 1, 0, 0};
     float best = 1e30f;
     int best_t = 128, best_w = s->dev.width, tried = 0, rc = BG_OK;
@@ -1399,11 +1409,18 @@ static int scene_autotune(bg_scene* s, const bg_camera_desc* cam, const bg_trace
     for (int w : widths) {
         s->dev.width = w;
         for (int t : threads) {
-            for (int64_t p : paths) {
+            for (int pi = 0; pi < kPassCandidates && pass_candidate_needed(pi, probe_samples); ++pi) {
+                const int64_t p = pass_candidate(pi);
                 s->tune_threads = t;
                 s->tune_paths = p;
                 // the first render warms the graph and buffers of this candidate, the second is timed
-                if ((rc = render_impl(s, nullptr, cam, tr, &sm, W, H, accum, nullptr, st))) break;
+                if ((rc = render_impl(s, nullptr, cam, tr, &sm, W, H, accum, nullptr, st))) {
+                    if (rc == BG_ERR_OOM && pi > 0) {   // no room for passes this large: keep the smaller
+                        cudaGetLastError();
+                        rc = BG_OK;
+                    }
+                    break;
+                }
                 BG_CUDA(cudaEventRecord(e0, st));
                 if ((rc = render_impl(s, nullptr, cam, tr, &sm, W, H, accum, nullptr, st))) break;
                 BG_CUDA(cudaEventRecord(e1, st));

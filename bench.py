@@ -30,11 +30,12 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 WIDTH, HEIGHT, MAXDEPTH, SEED = 1920, 1080, 8, 1
+SPP = 8   # camera samples per pixel per step: the 256-spp image in 32 steps
 METRIC = "Msamples/s at 1080p"
 WORKLOAD = ("C3 plain wavefront GI tracer: seeded fBm terrain (1024^2 grid) + 200 UV spheres "
             "(20k triangles each, own transforms) = 6.09M triangles, GGX (70%) / Lambert materials, "
             "sun + constant environment, 1920x1080, GiTracer maxdepth 8 with Russian roulette after bounce 3, "
-            "1 camera sample per pixel per step")
+            "8 camera samples per pixel per step (one render call; the 256-spp image in 32 steps)")
 
 
 def peaks():
@@ -393,7 +394,7 @@ def time_to_relmse(gs, sc, args, target=1e-3):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=150)
+    ap.add_argument("--steps", type=int, default=60)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="bounded CPU-baseline sample (seconds)")
@@ -432,13 +433,13 @@ def main():
     acc = torch.zeros((HEIGHT, WIDTH, 4), dtype=torch.float32, device="cuda")
     npix = WIDTH * HEIGHT
     # the framework's autotuner picks node layout, traversal block size and paths per pass
-    tune = gs.autotune(acc.data_ptr(), WIDTH, HEIGHT, probe_spp=1, maxdepth=MAXDEPTH, stream=stream.cuda_stream)
+    tune = gs.autotune(acc.data_ptr(), WIDTH, HEIGHT, probe_spp=SPP, maxdepth=MAXDEPTH, stream=stream.cuda_stream)
     acc.zero_()
     info = gs.info()
 
     def step(i, stats=False, flags=0):
-        return gs.render(acc.data_ptr(), WIDTH, HEIGHT, 1, seed=SEED,
-                         sample_offset=multigpu.sample_offset(i, rank, world), tracer=abi.BG_TRACER_GI,
+        return gs.render(acc.data_ptr(), WIDTH, HEIGHT, SPP, seed=SEED,
+                         sample_offset=multigpu.sample_offset(i, rank, world, SPP), tracer=abi.BG_TRACER_GI,
                          maxdepth=MAXDEPTH, stream=stream.cuda_stream, flags=flags, stats=stats)
 
     def exchange():
@@ -472,7 +473,7 @@ def main():
     clocks.stop()
     clocks.window(w0, w1 + 0.05)
     ms = multigpu.max_over_ranks(ms, dist, device="cuda")
-    samples_total = world * npix * args.steps
+    samples_total = world * npix * SPP * args.steps
     value = samples_total / (ms * 1e-3) / 1e6
     flags_err = gs.error_flags()
 
@@ -516,16 +517,16 @@ def main():
     host_np = host.numpy()
     ek = max(3, min(args.steps, 10))
     for i in range(2):
-        gs.render_host(WIDTH, HEIGHT, 1, seed=SEED, sample_offset=i, maxdepth=MAXDEPTH, accum=host_np)
+        gs.render_host(WIDTH, HEIGHT, SPP, seed=SEED, sample_offset=i * SPP, maxdepth=MAXDEPTH, accum=host_np)
     if dist is not None:
         dist.barrier()
     t0 = time.perf_counter()
     for i in range(ek):
-        gs.render_host(WIDTH, HEIGHT, 1, seed=SEED, sample_offset=multigpu.sample_offset(2 + i, rank, world),
+        gs.render_host(WIDTH, HEIGHT, SPP, seed=SEED, sample_offset=multigpu.sample_offset(2 + i, rank, world, SPP),
                        maxdepth=MAXDEPTH, accum=host_np)
     e2e_s = time.perf_counter() - t0
     e2e_s = multigpu.max_over_ranks(e2e_s, dist, device="cuda")
-    e2e_value = world * npix * ek / e2e_s / 1e6
+    e2e_value = world * npix * SPP * ek / e2e_s / 1e6
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -553,12 +554,12 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
             "config": {"workload": WORKLOAD, "triangles": info["ntriangles"], "resolution": [WIDTH, HEIGHT],
-                       "spp_per_step": 1, "maxdepth": MAXDEPTH, "parallelism": "dp%d (samples)" % world,
+                       "spp_per_step": SPP, "maxdepth": MAXDEPTH, "parallelism": "dp%d (samples)" % world,
                        "l2": "inputs larger than L2: scene %.2f GB resident in HBM (126 MB L2)"
                              % ((info["node_bytes"] + info["tri_bytes"] + info["shade_bytes"]) / 1e9),
                        "scene_build_s": t_scene, "autotune": tune},
             "mrays_per_s": world * rays_per_step * args.steps / (ms * 1e-3) / 1e6,
-            "rays_per_sample": rays_per_step / npix,
+            "rays_per_sample": rays_per_step / (npix * SPP),
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "Msamples/s", "h2d_bytes_per_step": npix * 16,

@@ -353,10 +353,14 @@ int bg_batch_info(bg_batch* batch, bg_scene_info* info);
 int bg_batch_render(bg_batch* batch, const bg_batch_job* jobs, int32_t njobs, const bg_tracer_desc* tracer,
                     bg_render_stats* stats, void* stream);
 /* Times node layouts {4-wide, 8-wide compressed} (those every scene built) x
- * traversal block sizes {128, 256} x paths per pass {2^19 .. 2^22} on
+ * traversal block sizes {128, 256} x paths per pass {2^19 .. 2^24} on
  * the jobs with spp capped at probe_spp and keeps the fastest for later
- * bg_batch_render calls.  The jobs' accumulation buffers receive the probe
- * samples: clear them before the real render.  Synchronises. */
+ * bg_batch_render calls.  A pass size is skipped when the probe's samples fit
+ * in half of it (it would run the same passes as the size before), and the
+ * sizes end at the first one whose buffers do not fit in device memory.
+ * result->candidates counts the configurations timed.  The jobs'
+ * accumulation buffers receive the probe samples: clear them before the real
+ * render.  Synchronises. */
 int bg_batch_autotune(bg_batch* batch, const bg_batch_job* jobs, int32_t njobs, const bg_tracer_desc* tracer,
                       int32_t probe_spp, bg_tune_result* result, void* stream);
 int bg_batch_destroy(bg_batch* batch);

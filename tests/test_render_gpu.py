@@ -212,8 +212,9 @@ def test_scene_autotune_keeps_images_bit_identical(ctx):
     probe = torch.zeros((45, 80, 4), dtype=torch.float32, device="cuda")
     res = gs.autotune(probe.data_ptr(), 80, 45, probe_spp=1, maxdepth=8)
     torch.cuda.synchronize()
-    assert res["candidates"] == 16 and res["node_width"] in (4, 8) and res["trace_threads"] in (128, 256)
+    # node widths x block sizes x one pass size: 3,600 probe samples fit in 2^19 / 2
+    assert res["candidates"] == 4 and res["node_width"] in (4, 8) and res["trace_threads"] in (128, 256)
     assert gs.info()["node_width"] == res["node_width"]
-    assert (probe.cpu().numpy()[..., 3] == 32).all()       # 16 candidates x 2 probe renders x 1 spp
+    assert (probe.cpu().numpy()[..., 3] == 8).all()        # 4 candidates x 2 probe renders x 1 spp
     after = gs.render_host(80, 45, 6, seed=4, maxdepth=8)
     assert (before.view(np.uint32) == after.view(np.uint32)).all()
