@@ -1170,6 +1170,9 @@ int render_jobs(bg_scene* s, bg_cache* cache, const std::vector<JobSpec>& jobs, 
     }
     const int64_t target = s->tune_paths > 0 ? s->tune_paths : (int64_t(1) << 21);   // paths per pass
     int64_t cap = std::max<int64_t>(1, std::min<int64_t>(target, std::max<int64_t>(total_samples, 1)));
+    // at most 2^26 DI slots (2 per light) per pass, which bounds the shadow / MIS
+    // queues too (about 16 GB at the bound): scenes with many lights get smaller passes
+    cap = std::max<int64_t>(1, std::min<int64_t>(cap, (int64_t(1) << 26) / (2 * std::max(1, maxL))));
     int rc = ensure_state(s, cap, maxL);
     if (rc) return rc;
     RenderState* rs = s->render;   // buffers may be larger than this call's pass size

@@ -330,7 +330,9 @@ def time_to_relmse(gs, sc, args, target=1e-3):
     """Second half of the metric: wall (GPU) time for the radiance-cache tracer and
     the plain tracer to reach relMSE 1e-3 on a centred 240x136 window of the 1080p
     frame, against a plain render of that window at args.gt_spp spp accumulated in
-    float64.  Both tracers render full 1080p frames, 1 spp per frame."""
+    float64.  Both tracers render full 1080p frames, 1 spp per frame (the cache
+    trains once per frame); the plain tracer is also timed at SPP samples per call,
+    its throughput configuration."""
     from banshee_b200 import capi
     from banshee_b200 import convergence as CV
     Wc, Hc = 240, 136
@@ -341,6 +343,10 @@ def time_to_relmse(gs, sc, args, target=1e-3):
     plain = CV.converge(lambda p, f: gs.render(p, WIDTH, HEIGHT, 1, seed=SEED, sample_offset=f, maxdepth=MAXDEPTH,
                                                stats=False),
                         WIDTH, HEIGHT, Wc, Hc, gt, args.conv_seconds, 100000, target=target, every=4)
+    # the plain tracer at its bench configuration too: SPP samples per render call
+    plain_spp = CV.converge(lambda p, f: gs.render(p, WIDTH, HEIGHT, SPP, seed=SEED, sample_offset=f * SPP,
+                                                   maxdepth=MAXDEPTH, stats=False),
+                            WIDTH, HEIGHT, Wc, Hc, gt, args.conv_seconds, 100000, target=target, every=1)
     cache_cfg = dict(log2_table_size=19, base_resolution=16, max_resolution=2048, train_paths=65536, cache_depth=2,
                      train_batch=65536, train_steps=1, learning_rate=1e-2, train_suffix=1)
     # warm the process as the plain tracer's timing is warm: a throwaway cache
@@ -376,6 +382,7 @@ def time_to_relmse(gs, sc, args, target=1e-3):
                 "curve": [[round(t, 4), n, float("%.4g" % e)] for t, n, e in r["curve"][::max(1, len(r["curve"]) // 12)]]}
 
     ratio = (cached["t_target"] / plain["t_target"]) if (cached["t_target"] and plain["t_target"]) else None
+    ratio_spp = (cached["t_target"] / plain_spp["t_target"]) if (cached["t_target"] and plain_spp["t_target"]) else None
     bound = (trunc["t_target"] / plain["t_target"]) if (trunc["t_target"] and plain["t_target"]) else None
     return {"target_relmse": target, "window": [Wc, Hc], "reference_spp": args.gt_spp, "reference_seconds": gt_s,
             "reference": "plain GiTracer(8), float64 accumulation of 256-spp chunks",
@@ -385,6 +392,8 @@ def time_to_relmse(gs, sc, args, target=1e-3):
                             "training paths one bounce later (self-training); one Adam step per frame over up to 65536 "
                             "training vertices from depth 2 on, trained one frame behind beside the next frame's first bounces",
             "plain": summ(plain), "cache": summ(cached), "cache_over_plain_time": ratio,
+            "plain_spp_per_call": {"spp_per_call": SPP, **summ(plain_spp)},
+            "cache_over_plain_spp_per_call_time": ratio_spp,
             "perfect_cache_bound": {
                 "what": "plain tracer truncated after 2 bounces (max depth 2) against its own reference: the "
                         "time-to-target of a free, exact cache ending paths there",
