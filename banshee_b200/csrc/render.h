@@ -33,7 +33,7 @@ struct JobSpec {       // host-side job description
 
 // Paths-per-pass candidates of the autotuners: 2^19 .. 2^24.  Larger passes
 // amortise the deep bounces, which hold few paths and take about the same time
-// whatever the pass size (2^24 paths hold about 22 GB of state).  A candidate
+// whatever the pass size (2^24 paths hold about 20 GB of state with 2 lights).  A candidate
 // is skipped when the probe fits in half of it: it would run the same passes
 // as the one before.
 constexpr int kPassCandidates = 6;

@@ -370,7 +370,7 @@ int bg_batch_destroy(bg_batch* batch);
  * for later bg_render / bg_render_host calls of this scene.  Passes are sized
  * for the probe: calls with more samples than probe_spp use the same pass
  * size.  The path state and queues of a pass stay allocated with the scene,
- * about 1.3 KB per path with 2 lights (22 GB at 2^24 paths).  No counterpart
+ * about 1.2 KB per path with 2 lights (20 GB at 2^24 paths).  No counterpart
  * in the reference.  Synchronises. */
 int bg_scene_autotune(bg_scene* scene, const bg_camera_desc* camera, const bg_tracer_desc* tracer,
                       int32_t probe_spp, int32_t width, int32_t height, float* accum_rgbw_dev,
