@@ -100,8 +100,9 @@ template <bool ANY, bool COUNT, int THREADS = kTraceThreads, int WIDTH = 4>
 __global__ void __launch_bounds__(THREADS, 1024 / THREADS)
 k_trace(DevScene S, const float4* __restrict__ rays, int64_t n_static, const int* __restrict__ n_dev,
         bg_hit* __restrict__ hits, uint8_t* __restrict__ occ, unsigned long long* __restrict__ work,
-        unsigned long long* __restrict__ counters, int stride, const int* __restrict__ roots) {
+        unsigned long long* __restrict__ counters, int stride, const int* __restrict__ roots, ShadowResolve res) {
     // roots (optional): per-ray root node, for rays of several scenes merged into one
+    // res.slots (any hit, optional): visible rays store their contribution in their slot
     // COUNT: instrumented replay of rays 0, stride, 2*stride, ... (outputs compacted)
     const int64_t n_all = n_dev ? int64_t(*n_dev) : n_static;
     const int64_t n = COUNT ? (n_all + stride - 1) / stride : n_all;
@@ -142,7 +143,8 @@ k_trace(DevScene S, const float4* __restrict__ rays, int64_t n_static, const int
         if (active) {
             if (trav_steps<ANY, COUNT, WIDTH>(S, s, stack, kRefillSteps, cnt)) {
                 if (ANY) {
-                    occ[ridx] = s.prim >= 0 ? 1 : 0;
+                    if (!res.slots) occ[ridx] = s.prim >= 0 ? 1 : 0;
+                    else if (s.prim < 0) res.slots[__ldg(res.slot_of + ridx)] = __ldg(res.contrib + ridx);
                 } else {
                     bg_hit h;
                     h.t = s.prim >= 0 ? s.best : s.r.tmax;
@@ -201,35 +203,37 @@ unsigned long long* next_work_counter(bg_scene* s) {
 template <int WIDTH>
 static void launch_width(bg_scene* s, bool any_hit, const float4* rays, int64_t n_static, const int* n_dev,
                          bg_hit* hits, uint8_t* occ, cudaStream_t st, unsigned long long* counters, int stride,
-                         unsigned long long* w, const int* roots) {
+                         unsigned long long* w, const int* roots,
+                         ShadowResolve res = ShadowResolve{nullptr, nullptr, nullptr}) {
     const int wi = WIDTH == 8 ? 1 : 0;
     const DevScene& d = s->dev;
     if (counters) {
         if (any_hit)
-            k_trace<true, true, 128, WIDTH><<<s->trace_blocks[wi][1][1][0], 128, 0, st>>>(d, rays, n_static, n_dev, hits, occ, w, counters, stride, roots);
+            k_trace<true, true, 128, WIDTH><<<s->trace_blocks[wi][1][1][0], 128, 0, st>>>(d, rays, n_static, n_dev, hits, occ, w, counters, stride, roots, res);
         else
-            k_trace<false, true, 128, WIDTH><<<s->trace_blocks[wi][0][1][0], 128, 0, st>>>(d, rays, n_static, n_dev, hits, occ, w, counters, stride, roots);
+            k_trace<false, true, 128, WIDTH><<<s->trace_blocks[wi][0][1][0], 128, 0, st>>>(d, rays, n_static, n_dev, hits, occ, w, counters, stride, roots, res);
     } else if (s->tune_threads == 256) {
         if (any_hit)
-            k_trace<true, false, 256, WIDTH><<<s->trace_blocks[wi][1][0][1], 256, 0, st>>>(d, rays, n_static, n_dev, hits, occ, w, nullptr, 1, roots);
+            k_trace<true, false, 256, WIDTH><<<s->trace_blocks[wi][1][0][1], 256, 0, st>>>(d, rays, n_static, n_dev, hits, occ, w, nullptr, 1, roots, res);
         else
-            k_trace<false, false, 256, WIDTH><<<s->trace_blocks[wi][0][0][1], 256, 0, st>>>(d, rays, n_static, n_dev, hits, occ, w, nullptr, 1, roots);
+            k_trace<false, false, 256, WIDTH><<<s->trace_blocks[wi][0][0][1], 256, 0, st>>>(d, rays, n_static, n_dev, hits, occ, w, nullptr, 1, roots, res);
     } else if (any_hit) {
-        k_trace<true, false, 128, WIDTH><<<s->trace_blocks[wi][1][0][0], 128, 0, st>>>(d, rays, n_static, n_dev, hits, occ, w, nullptr, 1, roots);
+        k_trace<true, false, 128, WIDTH><<<s->trace_blocks[wi][1][0][0], 128, 0, st>>>(d, rays, n_static, n_dev, hits, occ, w, nullptr, 1, roots, res);
     } else {
-        k_trace<false, false, 128, WIDTH><<<s->trace_blocks[wi][0][0][0], 128, 0, st>>>(d, rays, n_static, n_dev, hits, occ, w, nullptr, 1, roots);
+        k_trace<false, false, 128, WIDTH><<<s->trace_blocks[wi][0][0][0], 128, 0, st>>>(d, rays, n_static, n_dev, hits, occ, w, nullptr, 1, roots, res);
     }
 }
 
 int launch_trace(bg_scene* s, bool any_hit, const float4* rays, int64_t n_static, const int* n_dev,
                  bg_hit* hits, uint8_t* occ, cudaStream_t st, unsigned long long* counters, int stride,
-                 unsigned long long* work, const int* roots) {
+                 unsigned long long* work, const int* roots, const ShadowResolve* resolve) {
     unsigned long long* w = work ? work : next_work_counter(s);
     BG_CUDA(cudaMemsetAsync(w, 0, sizeof(unsigned long long), st));
+    const ShadowResolve res = (any_hit && resolve && !counters) ? *resolve : ShadowResolve{nullptr, nullptr, nullptr};
     if (s->dev.width == 8)
-        launch_width<8>(s, any_hit, rays, n_static, n_dev, hits, occ, st, counters, stride, w, roots);
+        launch_width<8>(s, any_hit, rays, n_static, n_dev, hits, occ, st, counters, stride, w, roots, res);
     else
-        launch_width<4>(s, any_hit, rays, n_static, n_dev, hits, occ, st, counters, stride, w, roots);
+        launch_width<4>(s, any_hit, rays, n_static, n_dev, hits, occ, st, counters, stride, w, roots, res);
     BG_CUDA(cudaGetLastError());
     return BG_OK;
 }

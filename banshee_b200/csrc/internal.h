@@ -134,7 +134,15 @@ int device_records(const MeshArrays& A, const BundleRec* bundles, const int32_t*
 constexpr int kWorkSlots = 256;
 unsigned long long* next_work_counter(bg_scene* s);
 void scene_launch_setup(bg_scene* s);
+// Shadow-ray resolve fused into an any-hit trace: a ray that finds no occluder
+// stores contrib[i] into slots[slot_of[i]] instead of writing an occlusion byte.
+struct ShadowResolve {
+    const float4* contrib;
+    const int* slot_of;
+    float4* slots;
+};
 int launch_trace(bg_scene* s, bool any_hit, const float4* rays, int64_t n_static, const int* n_dev,
                  bg_hit* hits, uint8_t* occ, cudaStream_t st, unsigned long long* counters = nullptr,
-                 int stride = 1, unsigned long long* work = nullptr, const int* roots = nullptr);
+                 int stride = 1, unsigned long long* work = nullptr, const int* roots = nullptr,
+                 const ShadowResolve* resolve = nullptr);
 }  // namespace bg

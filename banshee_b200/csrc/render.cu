@@ -69,7 +69,7 @@ struct RenderState {
     int kmax = 0;      // DI slots per path
     int nlights = 0;
     DevBuf ext_rays[2], ext_path[2], ext_hits;
-    DevBuf sh_rays, sh_contrib, sh_slot, sh_occ;
+    DevBuf sh_rays, sh_contrib, sh_slot;
     DevBuf mis_rays, mis_a, mis_b, mis_c, mis_hits;
     DevBuf end_path;
     DevBuf counts;     // int: ext[0], ext[1], sh, mis, end ; u64 totals at +64 bytes
@@ -135,7 +135,7 @@ void render_state_free(RenderState* rs) {
     if (rs->ev_mjoin) cudaEventDestroy(rs->ev_mjoin);
     if (rs->mstream) cudaStreamDestroy(rs->mstream);
     for (DevBuf* b : {&rs->ext_rays[0], &rs->ext_rays[1], &rs->ext_path[0], &rs->ext_path[1], &rs->ext_hits,
-                      &rs->sh_rays, &rs->sh_contrib, &rs->sh_slot, &rs->sh_occ, &rs->mis_rays, &rs->mis_a, &rs->mis_b,
+                      &rs->sh_rays, &rs->sh_contrib, &rs->sh_slot, &rs->mis_rays, &rs->mis_a, &rs->mis_b,
                       &rs->mis_c, &rs->mis_hits, &rs->end_path, &rs->counts, &rs->st_key, &rs->st_cnt, &rs->st_rng,
                       &rs->st_bs, &rs->st_thr, &rs->st_rad, &rs->st_dithr, &rs->st_flags, &rs->slots,
                       &rs->sample_rad, &rs->cnt_out, &rs->work, &rs->q_feat, &rs->q_path, &rs->q_thr,
@@ -171,7 +171,7 @@ struct PathState {
 struct Queues {
     float4* ext_rays_in; int* ext_path_in; bg_hit* ext_hits;
     float4* ext_rays_out; int* ext_path_out;
-    float4* sh_rays; float4* sh_contrib; int* sh_slot; uint8_t* sh_occ;
+    float4* sh_rays; float4* sh_contrib; int* sh_slot;
     float4* mis_rays; float4* mis_a; float4* mis_b; int4* mis_c; bg_hit* mis_hits;
     int* end_path;
     int* n_ext_in; int* n_ext_out; int* n_sh; int* n_mis; int* n_end;
@@ -552,19 +552,6 @@ k_shade(DevScene S, ShadeArgs A, PathState P, Queues Q) {
     }
 }
 
-// Visible light-sample / environment terms land in their slot.
-__global__ void __launch_bounds__(kShadeThreads)
-k_resolve_shadow(PathState P, Queues Q) {
-    const int n = *Q.n_sh;
-    const int nthreads = gridDim.x * blockDim.x;
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += nthreads)
-        if (!Q.sh_occ[e]) P.slots[Q.sh_slot[e]] = Q.sh_contrib[e];
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        Q.totals[1] += (unsigned long long)n;
-        Q.totals[2] += (unsigned long long)*Q.n_mis;
-    }
-}
-
 // BSDF-sampled rays towards area lights: the closest hit must be on a bundle
 // whose (last registered) area light is this one, front facing
 // (ditracer.cpp:199-220).
@@ -572,6 +559,10 @@ __global__ void __launch_bounds__(kShadeThreads)
 k_resolve_mis(DevScene S, PathState P, Queues Q) {
     const int n = *Q.n_mis;
     const int nthreads = gridDim.x * blockDim.x;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        Q.totals[1] += (unsigned long long)*Q.n_sh;
+        Q.totals[2] += (unsigned long long)n;
+    }
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += nthreads) {
         const bg_hit hit = Q.mis_hits[e];
         if (hit.primid < 0) continue;   // area lights emit nothing on a miss
@@ -713,7 +704,7 @@ static int alloc_state(bg_scene* s, RenderState* rs, int64_t cap, int L) {
         return set_error(BG_ERR_UNSUPPORTED, "paths per pass x light slots too large (%zu x %d)", C, rs->kmax);
     if ((rc = rs->ext_hits.ensure(C * 16)) ||
         (rc = rs->sh_rays.ensure(2 * C * 2 * L * 32)) || (rc = rs->sh_contrib.ensure(2 * C * 2 * L * 16)) ||
-        (rc = rs->sh_slot.ensure(2 * C * 2 * L * 4)) || (rc = rs->sh_occ.ensure(2 * C * 2 * L)) ||
+        (rc = rs->sh_slot.ensure(2 * C * 2 * L * 4)) ||
         (rc = rs->sh_root.ensure(2 * C * 2 * L * 4)) ||
         (rc = rs->mis_rays.ensure(2 * C * L * 32)) || (rc = rs->mis_a.ensure(2 * C * L * 16)) ||
         (rc = rs->mis_b.ensure(2 * C * L * 16)) || (rc = rs->mis_c.ensure(2 * C * L * 16)) ||
@@ -796,7 +787,7 @@ static void pass_queues(RenderState* rs, int c, bool batched, Queues& Q, int par
     const size_t sh = par ? C * 2 * L : 0, mi = par ? C * L : 0;   // entries before this parity's half
     Q.ext_hits = rs->ext_hits.as<bg_hit>();
     Q.sh_rays = rs->sh_rays.as<float4>() + 2 * sh; Q.sh_contrib = rs->sh_contrib.as<float4>() + sh;
-    Q.sh_slot = rs->sh_slot.as<int>() + sh; Q.sh_occ = rs->sh_occ.as<uint8_t>() + sh;
+    Q.sh_slot = rs->sh_slot.as<int>() + sh;
     Q.mis_rays = rs->mis_rays.as<float4>() + 2 * mi; Q.mis_a = rs->mis_a.as<float4>() + mi;
     Q.mis_b = rs->mis_b.as<float4>() + mi;
     Q.mis_c = rs->mis_c.as<int4>() + mi; Q.mis_hits = rs->mis_hits.as<bg_hit>() + mi;
@@ -890,16 +881,17 @@ static int enqueue_pass(bg_scene* s, RenderState* rs, cudaStream_t st, const Pas
             else k_shade<BG_TRACER_GI, false><<<nb, kShadeThreads, 0, st>>>(s->dev, A, P, Q);
             BG_CUDA(cudaEventRecord(rs->ev_fork, st));
             BG_CUDA(cudaStreamWaitEvent(ds, rs->ev_fork, 0));
-            if ((rc = launch_trace(s, true, Q.sh_rays, 0, Q.n_sh, nullptr, Q.sh_occ, ds, nullptr, 1, wk + 2, Q.sh_root)))
+            const ShadowResolve sr{Q.sh_contrib, Q.sh_slot, P.slots};
+            if ((rc = launch_trace(s, true, Q.sh_rays, 0, Q.n_sh, nullptr, nullptr, ds, nullptr, 1, wk + 2, Q.sh_root,
+                                   &sr)))
                 return rc;
             if ((rc = launch_trace(s, false, Q.mis_rays, 0, Q.n_mis, Q.mis_hits, nullptr, ds, nullptr, 1, wk + 3,
                                    Q.mis_root)))
                 return rc;
-            k_resolve_shadow<<<nb, kShadeThreads, 0, ds>>>(P, Q);
             k_resolve_mis<<<nb, kShadeThreads, 0, ds>>>(s->dev, P, Q);
             k_finalize<<<nb, kShadeThreads, 0, ds>>>(P, Q, rs->kmax, c.maxdepth, 0, 0, b, 1, int(rs->cap));
             BG_CUDA(cudaEventRecord(evd[par], ds));
-            if (ins) ins->launches += 6;
+            if (ins) ins->launches += 5;
             if (b + 1 < depth) {
                 cur = 1 - cur;
                 Queues Qn;
@@ -969,7 +961,9 @@ static int enqueue_pass(bg_scene* s, RenderState* rs, cudaStream_t st, const Pas
             }
             BG_CUDA(cudaEventRecord(rs->ev_mjoin, rs->mstream));
         }
-        if ((rc = launch_trace(s, true, Q.sh_rays, 0, Q.n_sh, nullptr, Q.sh_occ, st, nullptr, 1, wk + 2, Q.sh_root))) return rc;
+        const ShadowResolve sr{Q.sh_contrib, Q.sh_slot, P.slots};   // visible rays land in their slot
+        if ((rc = launch_trace(s, true, Q.sh_rays, 0, Q.n_sh, nullptr, nullptr, st, nullptr, 1, wk + 2, Q.sh_root, &sr)))
+            return rc;
         if (ins) { ins->mark(1); ins->mark(2); }
         if (!fork && (rc = launch_trace(s, false, Q.mis_rays, 0, Q.n_mis, Q.mis_hits, nullptr, st, nullptr, 1, wk + 3, Q.mis_root)))
             return rc;
@@ -979,7 +973,6 @@ static int enqueue_pass(bg_scene* s, RenderState* rs, cudaStream_t st, const Pas
             if ((rc = launch_trace(s, false, Q.mis_rays, 0, Q.n_mis, cnt_hits, nullptr, st, Q.totals + 9, 64, wk + 5, Q.mis_root))) return rc;
             ins->launches += 2;
         }
-        k_resolve_shadow<<<nb, kShadeThreads, 0, st>>>(P, Q);
         if (fork) BG_CUDA(cudaStreamWaitEvent(st, rs->ev_mjoin, 0));
         else k_resolve_mis<<<nb, kShadeThreads, 0, st>>>(s->dev, P, Q);
         if (query_here && !fork) {
@@ -993,7 +986,7 @@ static int enqueue_pass(bg_scene* s, RenderState* rs, cudaStream_t st, const Pas
         }
         k_finalize<<<nb, kShadeThreads, 0, st>>>(P, Q, rs->kmax, c.maxdepth, c.cache ? c.train_stride : 0,
                                                  c.cache ? c.cache_depth : 0, b, 0, int(rs->cap));
-        if (ins) ins->launches += 3;
+        if (ins) ins->launches += 2;
         if (forked) BG_CUDA(cudaStreamWaitEvent(st, rs->ev_join, 0));
         cur = 1 - cur;
         pass_queues(rs, cur, c.batched, Q);
