@@ -522,6 +522,30 @@ def main():
                       "instrumented replay of every 64th ray of each extension queue",
     }
     rays_per_step = st_plain["rays_closest"] + st_plain["rays_any"]
+    # every k_trace launch of the step (extension, shadow any-hit, MIS): the
+    # traversal kernel's whole share of the step; a shadow ray also reads its
+    # slot index and contribution (20 B), a closest-hit ray writes a 16 B hit
+    any_rays = st_plain["rays_any"]
+    mis_rays = st_plain["rays_closest"] - ext_rays
+
+    def per_ray(kind, extra):
+        n = max(1, st["sub_rays_" + kind])
+        nodes, tris = st["sub_nodes_" + kind] / n, st["sub_tris_" + kind] / n
+        return 32 + extra + node_b * nodes + tri_b * tris, nodes, tris
+
+    any_b, any_nodes, any_tris = per_ray("any", 20)
+    mis_b, _, _ = per_ray("mis", 16) if st["sub_rays_mis"] > 0 else (bytes_per_ray, 0, 0)
+    all_bytes = ext_bytes + any_rays * any_b + mis_rays * mis_b
+    all_ms = st_plain["ms_extend"] + st_plain["ms_shadow"] + st_plain["ms_mis"]
+    all_achieved = all_bytes / (all_ms * 1e-3) / 1e9
+    roofline_all = {
+        "kernel": "k_trace, every launch of one step (extension + shadow any-hit + MIS)",
+        "bound": "hbm", "achieved": all_achieved, "peak": peak, "unit": "GB/s", "frac": all_achieved / peak,
+        "peak_source": peak_src, "traffic": None,
+        "rays": {"extension": ext_rays, "any": any_rays, "mis": mis_rays},
+        "bytes_per_any_ray": any_b, "nodes_per_any_ray": any_nodes, "tris_per_any_ray": any_tris,
+        "ms": all_ms,
+    }
 
     # e2e through the public host-buffer entry point (pinned host accumulation buffer)
     host = torch.zeros((HEIGHT, WIDTH, 4), dtype=torch.float32, pin_memory=True)
@@ -572,6 +596,7 @@ def main():
             "mrays_per_s": world * rays_per_step * args.steps / (ms * 1e-3) / 1e6,
             "rays_per_sample": rays_per_step / (npix * SPP),
             "roofline": roofline,
+            "roofline_traversal_all": roofline_all,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "Msamples/s", "h2d_bytes_per_step": npix * 16,
                     "d2h_bytes_per_step": npix * 16, "api": "bg_render_host (pinned host RGBW buffer)"},
