@@ -5,8 +5,9 @@
   python -m banshee_b200.profile_frames --workload c2 [--width 8]
 
 c3: the 6.09M-triangle production scene at 1920x1080, plain GiTracer(8), one
-    camera sample per pixel per frame; k_trace launches per bounce are, in
-    order, extension (closest hit), shadow (any hit), MIS (closest hit).
+    camera sample per pixel per frame (one pass of 2^21 paths, 128-thread
+    traversal blocks: no autotuning); k_trace launches per bounce are, in
+    capture order, extension (closest hit), shadow (any hit), MIS (closest hit).
 c5: the same scene through the radiance cache (2^19-entry hash grid levels,
     65,536 training paths per frame ending into the cache one bounce after the
     rendering paths, which end after 2 bounces; training one frame behind).
