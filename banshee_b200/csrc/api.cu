@@ -94,8 +94,9 @@ void ScratchBuf::release() {
 // ------------------------------------------------------------ trace kernel
 // Persistent threads with per-lane dynamic fetch: lanes whose ray finished
 // take new ray indices from one global counter with a single warp-aggregated
-// atomicAdd, every kRefillSteps traversal steps.  Termination: the counter is
-// monotone and every ray finishes after at most one visit per node.
+// atomicAdd, every kRefillStepsClosest / kRefillStepsAny traversal steps.
+// Termination: the counter is monotone and every ray finishes after at most
+// one visit per node.
 template <bool ANY, bool COUNT, int THREADS = kTraceThreads, int WIDTH = 4>
 __global__ void __launch_bounds__(THREADS, 1024 / THREADS)
 k_trace(DevScene S, const float4* __restrict__ rays, int64_t n_static, const int* __restrict__ n_dev,
@@ -141,7 +142,7 @@ k_trace(DevScene S, const float4* __restrict__ rays, int64_t n_static, const int
         }
         if (!__any_sync(0xffffffffu, active)) break;
         if (active) {
-            if (trav_steps<ANY, COUNT, WIDTH>(S, s, stack, kRefillSteps, cnt)) {
+            if (trav_steps<ANY, COUNT, WIDTH>(S, s, stack, ANY ? kRefillStepsAny : kRefillStepsClosest, cnt)) {
                 if (ANY) {
                     if (!res.slots) occ[ridx] = s.prim >= 0 ? 1 : 0;
                     else if (s.prim < 0) res.slots[__ldg(res.slot_of + ridx)] = __ldg(res.contrib + ridx);
