@@ -101,7 +101,7 @@ class CacheDesc(C.Structure):
                 ("max_resolution", C.c_int32), ("train_paths", C.c_int32), ("cache_depth", C.c_int32),
                 ("train_batch", C.c_int32), ("train_steps", C.c_int32), ("learning_rate", C.c_float),
                 ("bbox_min", C.c_float * 3), ("bbox_max", C.c_float * 3), ("seed", C.c_uint64),
-                ("mlp_kernel", C.c_int32), ("train_suffix", C.c_int32)]
+                ("mlp_kernel", C.c_int32), ("train_suffix", C.c_int32), ("wait_polls", C.c_int32)]
 
 
 class BatchJob(C.Structure):
@@ -120,3 +120,7 @@ def fptr(a):
 
 def iptr(a):
     return a.ctypes.data_as(_ip) if a is not None else None
+
+
+class AllocStats(C.Structure):
+    _fields_ = [("calls", C.c_int64), ("bytes", C.c_int64), ("refused", C.c_int64), ("budget", C.c_int64)]

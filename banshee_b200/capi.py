@@ -80,6 +80,8 @@ def lib():
             "bg_cache_train": [_vp, _vp, _vp, _i64, _i32, C.POINTER(C.c_float), _vp],
             "bg_cache_params": [_vp, _vp, _vp, _vp, _vp],
             "bg_cache_set_params": [_vp, _vp, _vp],
+            "bg_alloc_limit": [_i64],
+            "bg_alloc_stats_get": [C.POINTER(abi.AllocStats)],
             "bg_render_cached": [_vp, _vp, C.POINTER(abi.CameraDesc), C.POINTER(abi.TracerDesc),
                                  C.POINTER(abi.SamplerDesc), _i32, _i32, _vp, C.POINTER(abi.RenderStats), _vp],
         }
@@ -102,6 +104,19 @@ def _stream_handle(stream):
         import torch
         return torch.cuda.current_stream().cuda_stream
     return int(stream)
+
+
+def alloc_limit(nbytes):
+    """bg_alloc_limit: allow `nbytes` more bytes of library allocations from now
+    on (None or a negative value removes the cap)."""
+    check(lib().bg_alloc_limit(-1 if nbytes is None else int(nbytes)))
+
+
+def alloc_stats():
+    """bg_alloc_stats_get: allocations made / bytes / refused by the cap / budget left."""
+    st = abi.AllocStats()
+    check(lib().bg_alloc_stats_get(C.byref(st)))
+    return {k: getattr(st, k) for k, _ in abi.AllocStats._fields_}
 
 
 class Context:
@@ -130,10 +145,11 @@ class Context:
 class GpuScene:
     """A committed scene on the device: World::Commit + the Intersectable surface."""
 
-    def __init__(self, ctx, scene, node_width=0, max_leaf=4, bins=32, builder=0):
+    def __init__(self, ctx, scene, node_width=0, max_leaf=4, bins=32, builder=0, commit=True):
         """node_width: 4 (128-byte nodes), 8 (96-byte compressed nodes) or 0 (both
         built; the active one is chosen with set_node_width).  builder: 0 = host
-        binned SAH, 1 = device LBVH, 2 = device PLOC, 3 = device binned SAH."""
+        binned SAH, 1 = device LBVH, 2 = device PLOC, 3 = device binned SAH.
+        commit=False leaves the scene assembled but uncommitted (commit())."""
         self.ctx = ctx
         self.scene = scene
         self.h = _vp()
@@ -152,8 +168,13 @@ class GpuScene:
             check(L.bg_scene_add_light(self.h, C.byref(d), None))
         bg = (C.c_float * 3)(*scene.bgcolor)
         check(L.bg_scene_set_background(self.h, bg))
-        opts = abi.BuildOpts(node_width, max_leaf, bins, builder)
-        check(L.bg_scene_commit(self.h, C.byref(opts)))
+        self._opts = abi.BuildOpts(node_width, max_leaf, bins, builder)
+        if commit:
+            self.commit()
+
+    def commit(self):
+        """bg_scene_commit with the build options given at construction."""
+        check(lib().bg_scene_commit(self.h, C.byref(self._opts)))
 
     def info(self):
         i = abi.SceneInfo()
@@ -256,10 +277,11 @@ class RadianceCache:
 
     def __init__(self, gscene, log2_table_size=19, base_resolution=16, max_resolution=2048, train_paths=65536,
                  cache_depth=2, train_batch=16384, train_steps=4, learning_rate=1e-2, bbox=None, seed=1,
-                 mlp_kernel=0, train_suffix=0):
+                 mlp_kernel=0, train_suffix=0, wait_polls=0):
         """mlp_kernel: inference on tcgen05 with TMEM accumulators (0) or on mma.sync (1).
         train_suffix: 0 = training paths run to maxdepth; k > 0 = they end into the
-        cache k bounces after cache_depth (self-training)."""
+        cache k bounces after cache_depth (self-training).  wait_polls: budget of
+        the tcgen05 kernels' bounded mbarrier waits (0 = default)."""
         d = abi.CacheDesc()
         d.levels = 16
         d.log2_table_size = log2_table_size
@@ -276,6 +298,7 @@ class RadianceCache:
         d.seed = seed
         d.mlp_kernel = mlp_kernel
         d.train_suffix = train_suffix
+        d.wait_polls = wait_polls
         self.gs = gscene
         self.h = _vp()
         check(lib().bg_cache_create(gscene.h, C.byref(d), C.byref(self.h)))

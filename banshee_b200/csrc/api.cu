@@ -26,10 +26,32 @@ int set_error(int code, const char* fmt, ...) {
     return code;
 }
 
+// Allocation accounting and the optional cap (bg_alloc_limit): every device
+// and pinned-host allocation the library makes is charged here first.
+static std::mutex g_alloc_mu;
+static int64_t g_alloc_budget = -1;   // bytes still allowed; < 0 = no cap
+static int64_t g_alloc_calls = 0, g_alloc_bytes = 0, g_alloc_refused = 0;
+
+bool alloc_charge(size_t bytes) {
+    std::lock_guard<std::mutex> lk(g_alloc_mu);
+    if (g_alloc_budget >= 0) {
+        if (int64_t(bytes) > g_alloc_budget) {
+            ++g_alloc_refused;
+            return false;
+        }
+        g_alloc_budget -= int64_t(bytes);
+    }
+    ++g_alloc_calls;
+    g_alloc_bytes += int64_t(bytes);
+    return true;
+}
+
 int DevBuf::ensure(size_t need) {
     if (need <= bytes && ptr) return BG_OK;
     release();
     size_t want = std::max<size_t>(need, 256);
+    if (!alloc_charge(want))
+        return set_error(BG_ERR_OOM, "device allocation of %zu bytes refused: over the library's allocation limit", want);
     cudaError_t e = cudaMalloc(&ptr, want);
     if (e != cudaSuccess) {
         ptr = nullptr;
@@ -75,6 +97,8 @@ int ScratchBuf::ensure(size_t need) {
     cudaMemPool_t pool = scratch_pool(dev);
     if (!pool) return set_error(BG_ERR_CUDA, "scratch memory pool unavailable on device %d", dev);
     const size_t want = std::max<size_t>(need, 256);
+    if (!alloc_charge(want))
+        return set_error(BG_ERR_OOM, "scratch allocation of %zu bytes refused: over the library's allocation limit", want);
     cudaError_t e = cudaMallocFromPoolAsync(&ptr, want, pool, 0);
     if (e != cudaSuccess) {
         ptr = nullptr;
@@ -483,6 +507,22 @@ int bg_version(int32_t* major, int32_t* minor) {
     return BG_OK;
 }
 
+int bg_alloc_limit(int64_t bytes) {
+    std::lock_guard<std::mutex> lk(g_alloc_mu);
+    g_alloc_budget = bytes < 0 ? -1 : bytes;
+    return BG_OK;
+}
+
+int bg_alloc_stats_get(bg_alloc_stats* out) {
+    if (!out) return set_error(BG_ERR_INVALID_ARG, "out is NULL");
+    std::lock_guard<std::mutex> lk(g_alloc_mu);
+    out->calls = g_alloc_calls;
+    out->bytes = g_alloc_bytes;
+    out->refused = g_alloc_refused;
+    out->budget = g_alloc_budget;
+    return BG_OK;
+}
+
 int bg_ctx_create(int32_t device, bg_ctx** out) {
     if (!out) return set_error(BG_ERR_INVALID_ARG, "out is NULL");
     *out = nullptr;
@@ -507,7 +547,7 @@ int bg_ctx_create(int32_t device, bg_ctx** out) {
 }
 
 int bg_ctx_destroy(bg_ctx* ctx) {
-    delete ctx;
+    ctx_release(ctx);   // freed once its scenes and batches are gone too
     return BG_OK;
 }
 
@@ -523,21 +563,26 @@ int bg_scene_create(bg_ctx* ctx, bg_scene** out) {
     bg_scene* s = new (std::nothrow) bg_scene();
     if (!s) return set_error(BG_ERR_OOM, "host allocation failed");
     s->ctx = ctx;
+    ctx_retain(ctx);
     *out = s;
     return BG_OK;
 }
 
 int bg_scene_destroy(bg_scene* s) {
     if (!s) return BG_OK;
-    cudaSetDevice(s->ctx->device);
-    cudaDeviceSynchronize();
-    for (DevBuf* b : {&s->nodes, &s->nodes8, &s->tris, &s->shade, &s->bundles, &s->mats_d, &s->lights_d, &s->err, &s->work,
-                      &s->host_rays, &s->host_out})
-        b->release();
-    if (s->render) render_state_free(s->render);
-    if (s->ev_accum) cudaEventDestroy(s->ev_accum);
-    if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
-    delete s;
+    bg_ctx* ctx = s->ctx;
+    {
+        DeviceGuard dg(ctx->device);
+        cudaDeviceSynchronize();
+        for (DevBuf* b : {&s->nodes, &s->nodes8, &s->tris, &s->shade, &s->bundles, &s->mats_d, &s->lights_d, &s->err,
+                          &s->work, &s->host_rays, &s->host_out})
+            b->release();
+        if (s->render) render_state_free(s->render);
+        if (s->ev_accum) cudaEventDestroy(s->ev_accum);
+        if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
+        delete s;
+    }
+    ctx_release(ctx);
     return BG_OK;
 }
 
@@ -638,7 +683,17 @@ int bg_scene_commit(bg_scene* s, const bg_build_opts* opts) {
     std::lock_guard<std::mutex> lk(s->mu);
     if (s->committed) return set_error(BG_ERR_STATE, "scene already committed");
     BG_CUDA(cudaSetDevice(s->ctx->device));
-    return commit_scene(s, opts);
+    const int rc = commit_scene(s, opts);
+    if (rc != BG_OK) {
+        // a failed commit keeps nothing on the device: the scene stays
+        // uncommitted and may be committed again (e.g. after memory is freed)
+        for (DevBuf* b : {&s->nodes, &s->nodes8, &s->tris, &s->shade, &s->bundles, &s->mats_d, &s->lights_d, &s->err,
+                          &s->work})
+            b->release();
+        s->dev = DevScene{};
+        s->nnodes4 = s->nnodes8 = 0;
+    }
+    return rc;
 }
 
 int bg_scene_info_get(bg_scene* s, bg_scene_info* info) {
@@ -716,11 +771,26 @@ int bg_intersect_any_host(bg_scene* s, const bg_ray* rays, uint8_t* occ, int64_t
     return host_cast(s, rays, occ, n, true);
 }
 
+}  // extern "C"
+
+// A replay whose traversal stack overflowed undercounts: report it as the
+// *_host casts do (the scene's device error word, read synchronously).
+static int counts_overflow_check(bg_scene* s) {
+    unsigned flags = 0;
+    BG_CUDA(cudaMemcpy(&flags, s->err.ptr, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    if (flags & BG_FLAG_STACK_OVERFLOW) return set_error(BG_ERR_OVERFLOW, "traversal stack overflow during the replay");
+    return BG_OK;
+}
+
+extern "C" {
+
 int bg_traversal_counts(bg_scene* s, const bg_ray* rays, int64_t n, int32_t any_hit, uint64_t* nodes,
                         uint64_t* triangles, void* stream) {
     int rc;
     if ((rc = check_scene(s)) || (rc = check_rays(rays, nodes, n))) return rc;
     if (!triangles) return set_error(BG_ERR_INVALID_ARG, "triangles is NULL");
+    DeviceGuard dg(s->ctx->device);
+    if (dg.err != cudaSuccess) return set_error(BG_ERR_CUDA, "traversal counts: %s", cudaGetErrorString(dg.err));
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     DevBuf tmp;
     if ((rc = tmp.ensure(256 + (any_hit ? size_t(n) : size_t(n) * sizeof(bg_hit))))) return rc;
@@ -739,7 +809,7 @@ int bg_traversal_counts(bg_scene* s, const bg_ray* rays, int64_t n, int32_t any_
     if (e != cudaSuccess) return set_error(BG_ERR_CUDA, "traversal counts: %s", cudaGetErrorString(e));
     *nodes = h[1];
     *triangles = h[2];
-    return BG_OK;
+    return counts_overflow_check(s);
 }
 
 }  // extern "C"
@@ -760,7 +830,9 @@ int bg_traversal_counts(bg_scene* s, const bg_ray* rays, int64_t n, int32_t any_
 // The array lives in every CUDA context that loads this library, from module
 // load until exit.  Its device address is looked up once per device with
 // cudaGetSymbolAddress, by the first call on that device, with that device
-// current; make that first call before any stream capture.  All calls share the
+// current; make that first call before any stream capture.  Every call makes
+// the scene's device current for its own work and gives the calling thread's
+// current device back before it returns.  All calls share the
 // array and it keeps the last call's contents: each call clears the counters it
 // uses, and calls whose work overlaps on the GPU (different streams, or
 // different host threads) race on the same memory.
@@ -776,11 +848,9 @@ static int noalloc_scratch(int device, unsigned char** out) {
     if (device < 0 || device >= 64) return set_error(BG_ERR_INVALID_ARG, "device %d out of range for the static scratch", device);
     std::lock_guard<std::mutex> lk(g_noalloc_mu);
     if (!g_noalloc_ptr[device]) {
-        int cur = -1;
-        cudaError_t e = cudaGetDevice(&cur);
-        if (e == cudaSuccess && cur != device) e = cudaSetDevice(device);
+        // the caller has made `device` current (DeviceGuard)
         void* p = nullptr;
-        if (e == cudaSuccess) e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess) {
             cudaGetLastError();
             return set_error(BG_ERR_CUDA, "cudaGetSymbolAddress(static scratch) failed: %s", cudaGetErrorString(e));
@@ -805,6 +875,9 @@ extern "C" int bg_traversal_counts_noalloc(bg_scene* s, const bg_ray* rays, int6
                          "bg_traversal_counts_noalloc: %lld rays exceed the %lld-ray limit of its %zu-byte static "
                          "scratch (%s); split the rays or use bg_traversal_counts",
                          (long long)n, (long long)max_rays, kNoAllocScratchBytes, any_hit ? "any hit" : "closest hit");
+    DeviceGuard dg(s->ctx->device);   // the scene's device for this call; the caller's comes back after
+    if (dg.err != cudaSuccess)
+        return set_error(BG_ERR_CUDA, "bg_traversal_counts_noalloc: %s", cudaGetErrorString(dg.err));
     unsigned char* base = nullptr;
     if ((rc = noalloc_scratch(s->ctx->device, &base))) return rc;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -829,5 +902,5 @@ extern "C" int bg_traversal_counts_noalloc(bg_scene* s, const bg_ray* rays, int6
     if (e != cudaSuccess) return set_error(BG_ERR_CUDA, "bg_traversal_counts_noalloc: %s", cudaGetErrorString(e));
     *nodes = h[1];
     *triangles = h[2];
-    return BG_OK;
+    return counts_overflow_check(s);
 }

@@ -90,6 +90,7 @@ int bg_batch_create(bg_ctx* ctx, bg_batch** out) {
     bg_batch* b = new bg_batch();
     b->ctx = ctx;
     b->merged.ctx = ctx;
+    ctx_retain(ctx);
     *out = b;
     return BG_OK;
 }
@@ -337,14 +338,18 @@ int bg_batch_autotune(bg_batch* b, const bg_batch_job* jobs, int32_t njobs, cons
 
 int bg_batch_destroy(bg_batch* b) {
     if (!b) return BG_OK;
-    bg_scene& M = b->merged;
-    if (M.ctx) cudaSetDevice(M.ctx->device);
-    cudaDeviceSynchronize();
-    for (DevBuf* d : {&M.nodes, &M.tris, &M.shade, &M.bundles, &M.mats_d, &M.lights_d, &M.err, &M.work,
-                      &M.host_rays, &M.host_out})
-        d->release();
-    if (M.render) { render_state_free(M.render); M.render = nullptr; }
-    delete b;
+    bg_ctx* ctx = b->ctx;
+    {
+        bg_scene& M = b->merged;
+        DeviceGuard dg(ctx->device);
+        cudaDeviceSynchronize();
+        for (DevBuf* d : {&M.nodes, &M.nodes8, &M.tris, &M.shade, &M.bundles, &M.mats_d, &M.lights_d, &M.err, &M.work,
+                          &M.host_rays, &M.host_out})
+            d->release();
+        if (M.render) { render_state_free(M.render); M.render = nullptr; }
+        delete b;
+    }
+    ctx_release(ctx);
     return BG_OK;
 }
 

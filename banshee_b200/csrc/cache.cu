@@ -504,14 +504,19 @@ struct bg_cache {
     int64_t cap = 0;
     int sms = 0;
     int64_t frame = 0;
+    uint64_t id = 0;          // unique over the process (captured passes key on it)
+    uint64_t buf_epoch = 0;   // a fresh process-unique value whenever the scratch moves
 };
 
 namespace bg {
 
 static int64_t grid_params(const bg_cache* c) { return int64_t(kNrcLevels) * (int64_t(1) << c->dev.log2_T) * kNrcFeat; }
 
+static std::atomic<uint64_t> g_cache_ids{1};
+
 static int cache_scratch(bg_cache* c, int64_t rows) {
     if (rows <= c->cap) return BG_OK;
+    c->buf_epoch = g_cache_ids.fetch_add(1);
     int rc;
     const size_t R = size_t(rows);
     if ((rc = c->X.ensure(R * kNrcIn * 2)) || (rc = c->H.ensure(5 * R * 64 * 2)) || (rc = c->DZ.ensure(5 * R * 64 * 2)) ||
@@ -630,7 +635,8 @@ int nrc_prepare(bg_cache* c, int64_t rows) { return cache_scratch(c, rows); }
 const bg_cache_desc* nrc_desc(const bg_cache* c) { return &c->desc; }
 int64_t nrc_next_frame(bg_cache* c) { return c->frame++; }
 int64_t nrc_frame(const bg_cache* c) { return c->frame; }
-const void* nrc_rows_ptr(const bg_cache* c) { return c->X.ptr; }
+uint64_t nrc_id(const bg_cache* c) { return c->id; }
+uint64_t nrc_buf_epoch(const bg_cache* c) { return c->buf_epoch; }
 bg_scene* nrc_scene(const bg_cache* c) { return c->scene; }
 
 }  // namespace bg
@@ -649,6 +655,7 @@ int bg_cache_create(bg_scene* s, const bg_cache_desc* d, bg_cache** out) {
     *out = nullptr;
     bg_cache* c = new bg_cache();
     c->scene = s;
+    c->id = g_cache_ids.fetch_add(1);
     c->desc = *d;
     if (c->desc.train_paths <= 0) c->desc.train_paths = 65536;
     if (c->desc.train_batch <= 0) c->desc.train_batch = 16384;
@@ -668,6 +675,11 @@ int bg_cache_create(bg_scene* s, const bg_cache_desc* d, bg_cache** out) {
         D.bscale[k] = 1.f / (ext * 1.002f);
     }
     D.lr = d->learning_rate > 0.f ? d->learning_rate : 1e-2f;
+    if (d->wait_polls < 0) {
+        delete c;
+        return set_error(BG_ERR_INVALID_ARG, "wait_polls %d < 0", d->wait_polls);
+    }
+    D.wait_polls = uint32_t(d->wait_polls);
     D.beta1 = 0.9f;
     D.beta2 = 0.99f;
     D.eps = 1e-15f;

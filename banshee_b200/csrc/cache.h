@@ -54,6 +54,7 @@ struct NrcDev {
     __nv_bfloat16* wb;         // bf16 copy used by the kernels
     float lr, beta1, beta2, eps;
     int* step;                 // Adam step counter (device)
+    uint32_t wait_polls;       // tcgen05 mbarrier wait budget (0 = default)
 };
 
 }  // namespace bg

@@ -34,6 +34,10 @@ struct MeshHost {
     int nfaces = 0;
 };
 
+// Charges an allocation against the library's optional cap (bg_alloc_limit)
+// and counts it; false = refused (report BG_ERR_OOM without calling CUDA).
+bool alloc_charge(size_t bytes);
+
 // Device buffer that grows on demand (never shrinks until freed).
 struct DevBuf {
     void* ptr = nullptr;
@@ -57,16 +61,45 @@ struct ScratchBuf {
 };
 constexpr size_t kScratchKeepBytes = size_t(4) << 30;
 
+// Makes `device` current for the lifetime of the guard and gives the caller's
+// current device back afterwards (entry points that must run on the scene's
+// device whatever the calling thread had selected).
+struct DeviceGuard {
+    int prev = -1;
+    cudaError_t err = cudaSuccess;
+    explicit DeviceGuard(int device) {
+        err = cudaGetDevice(&prev);
+        if (err == cudaSuccess && prev != device) err = cudaSetDevice(device);
+        else if (err == cudaSuccess) prev = -1;   // already current: nothing to restore
+    }
+    ~DeviceGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+    DeviceGuard(const DeviceGuard&) = delete;
+    DeviceGuard& operator=(const DeviceGuard&) = delete;
+};
+
 struct RenderState;   // render.cu
 void render_state_free(RenderState* rs);
 
 }  // namespace bg
 
+// A context lives until bg_ctx_destroy has been called AND every scene and
+// batch created on it is destroyed (each holds a reference), so objects may be
+// destroyed in any order.
 struct bg_ctx {
     int device = 0;
     int num_sms = 0;
     size_t l2_bytes = 0;
+    std::atomic<int> refs{1};   // the creator's reference + one per live scene / batch
 };
+
+namespace bg {
+inline void ctx_retain(bg_ctx* c) { c->refs.fetch_add(1); }
+inline void ctx_release(bg_ctx* c) {
+    if (c && c->refs.fetch_sub(1) == 1) delete c;
+}
+}  // namespace bg
 
 struct bg_scene {
     bg_ctx* ctx = nullptr;

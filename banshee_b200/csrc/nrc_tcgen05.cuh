@@ -12,8 +12,10 @@
 //     instruction) and commits to an mbarrier; every thread then reads its own
 //     accumulator row (TMEM lane = tile row) with tcgen05.ld, applies ReLU,
 //     rounds to bf16 and writes the next layer's A row.
-// Waits on the mbarrier are bounded: on timeout the kernel raises
-// BG_FLAG_TIMEOUT, stops, releases its tensor memory and returns.
+// Waits on the mbarrier are bounded (NrcDev::wait_polls polls, 0 = the
+// default of 2^24): on timeout the kernel raises BG_FLAG_TIMEOUT, stops, gives
+// its outstanding MMA group one more wait with the default bound, releases
+// its tensor memory and returns.
 #pragma once
 
 #include <cuda_bf16.h>
@@ -66,10 +68,18 @@ __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
-// true once the phase of parity `phase` of the mbarrier has completed; false after kTcWaitLimit polls
-__device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t phase) {
-    for (uint32_t it = 0; it < kTcWaitLimit; ++it) {
-        uint32_t done;
+// true once the phase of parity `phase` of the mbarrier has completed; false
+// after `polls` polls (0 = kTcWaitLimit).  The first poll is a non-blocking
+// test_wait, the rest are try_wait (which may suspend the thread briefly), so
+// a budget of one poll gives up at once unless the phase is already complete.
+__device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t phase, uint32_t polls = 0) {
+    const uint32_t limit = polls ? polls : kTcWaitLimit;
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done) : "r"(bar), "r"(phase) : "memory");
+    if (done) return true;
+    for (uint32_t it = 1; it < limit; ++it) {
         asm volatile(
             "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
             : "=r"(done) : "r"(bar), "r"(phase) : "memory");
@@ -165,7 +175,7 @@ __global__ void __launch_bounds__(128, 2) k_nrc_infer_tc(NrcDev C, const __nv_bf
                            s > 0 ? 1u : 0u);
                 tc_commit(bar);
             }
-            if (!tc_wait(bar, phase)) {
+            if (!tc_wait(bar, phase, C.wait_polls)) {
                 atomicOr(errflags, BG_FLAG_TIMEOUT);
                 abort_flag = 1;
             }
@@ -286,7 +296,7 @@ __global__ void __launch_bounds__(128, 2) k_nrc_train_tc(NrcDev C, TcTrainArgs T
                        s > 0 ? 1u : 0u);
             tc_commit(bar);
         }
-        if (!tc_wait(bar, phase)) {
+        if (!tc_wait(bar, phase, C.wait_polls)) {
             atomicOr(errflags, BG_FLAG_TIMEOUT);
             abort_flag = 1;
         }

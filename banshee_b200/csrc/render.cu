@@ -39,7 +39,8 @@ int nrc_train_step(bg_cache* c, const float* feat, const float4* target, const i
 const bg_cache_desc* nrc_desc(const bg_cache* c);
 int64_t nrc_next_frame(bg_cache* c);
 int64_t nrc_frame(const bg_cache* c);   // frames rendered so far
-const void* nrc_rows_ptr(const bg_cache* c);   // the encoded-rows buffer (changes when it grows)
+uint64_t nrc_id(const bg_cache* c);          // unique over the process, never reused
+uint64_t nrc_buf_epoch(const bg_cache* c);   // changes whenever the cache's scratch is reallocated
 bg_scene* nrc_scene(const bg_cache* c);
 
 __global__ void k_clamp_count(int* n, int cap) {
@@ -83,7 +84,11 @@ struct RenderState {
     int tr_set = 0;                      // training set this frame writes
     // rows of the other set wait to be trained at the start of the next frame
     // of the same cache (pending_frame: that cache's frame index which wrote them)
-    bg_cache* pending_cache = nullptr;
+    uint64_t pending_cache = 0;         // id (nrc_id) of the cache whose training rows are pending
+    // bumped whenever a buffer that captured passes bake in is reallocated
+    // (segment / job tables, cache-mode queues and training sets): graphs
+    // captured before then hold stale pointers and must not be replayed
+    uint64_t buf_epoch = 0;
     int64_t pending_frame = -1;
     cudaStream_t tstream = nullptr;      // training of the previous frame's rows
     cudaEvent_t ev_tstart = nullptr, ev_train = nullptr;
@@ -687,6 +692,15 @@ CamDev make_camera(const bg_camera_desc* c) {
     return k;
 }
 
+// DevBuf::ensure that bumps the render state's buffer epoch when the buffer
+// moves, so no captured pass is replayed with the old address.
+static int ensure_tracked(RenderState* rs, DevBuf& b, size_t need) {
+    const void* before = b.ptr;
+    const int rc = b.ensure(need);
+    if (b.ptr != before) ++rs->buf_epoch;
+    return rc;
+}
+
 static int alloc_state(bg_scene* s, RenderState* rs, int64_t cap, int L) {
     rs->cap = cap;
     rs->nlights = L;
@@ -1008,11 +1022,11 @@ static int pass_graph(bg_scene* s, RenderState* rs, const PassCfg& c, RenderStat
     memcpy(&aob, &c.ao_radius, sizeof(aob));
     const int64_t key[kGraphKey] = {c.maxdepth, c.kind, c.batched ? 1 : 0, rs->kmax, int64_t(rs->cap), s->tune_threads,
                                     s->dev.width, int64_t(aob), s->ev_accum ? 1 : 0,
-                                    int64_t(reinterpret_cast<uintptr_t>(c.cache)),
-                                    c.cache ? int64_t(reinterpret_cast<uintptr_t>(nrc_rows_ptr(c.cache))) : 0,
+                                    c.cache ? int64_t(nrc_id(c.cache)) : 0,
+                                    c.cache ? int64_t(nrc_buf_epoch(c.cache)) : 0,
                                     c.cache ? c.cache_depth : -1, c.cache ? c.train_end : -1,
                                     c.cache ? c.train_stride : 0, c.cache ? rs->tr_set : 0,
-                                    c.cache ? int64_t(reinterpret_cast<uintptr_t>(rs->tr_feat.ptr)) : 0};
+                                    int64_t(rs->buf_epoch)};
     ++rs->graph_clock;
     for (auto& pg : rs->graphs)
         if (pg.exec && memcmp(key, pg.key, sizeof(key)) == 0) { pg.used = rs->graph_clock; out = &pg; return BG_OK; }
@@ -1176,8 +1190,9 @@ int render_jobs(bg_scene* s, bg_cache* cache, const std::vector<JobSpec>& jobs, 
     std::vector<int> pass_begin;
     plan_passes(jobs, cap, segs, pass_begin);
     const int npass = int(pass_begin.size()) - 1;
-    if ((rc = rs->segs.ensure(std::max<size_t>(1, segs.size()) * sizeof(SegRec)))) return rc;
-    if ((rc = rs->jobs.ensure(jobs.size() * sizeof(JobRec)))) return rc;
+    if ((rc = ensure_tracked(rs, rs->segs, std::max<size_t>(1, segs.size()) * sizeof(SegRec))) ||
+        (rc = ensure_tracked(rs, rs->jobs, jobs.size() * sizeof(JobRec))))
+        return rc;
     std::vector<JobRec> jrec(jobs.size());
     for (size_t j = 0; j < jobs.size(); ++j) jrec[j] = jobs[j].rec;
 
@@ -1202,6 +1217,9 @@ int render_jobs(bg_scene* s, bg_cache* cache, const std::vector<JobSpec>& jobs, 
             if (rs->host_tab[i]) cudaFreeHost(rs->host_tab[i]);
             rs->host_tab[i] = nullptr;
             rs->host_tab_bytes[i] = 0;
+            if (!alloc_charge((sb + jb) * 2))
+                return set_error(BG_ERR_OOM, "pinned staging of %zu bytes refused: over the library's allocation limit",
+                                 (sb + jb) * 2);
             BG_CUDA(cudaMallocHost(&rs->host_tab[i], (sb + jb) * 2));
             rs->host_tab_bytes[i] = (sb + jb) * 2;
         }
@@ -1244,18 +1262,20 @@ int render_jobs(bg_scene* s, bg_cache* cache, const std::vector<JobSpec>& jobs, 
         const int64_t tpaths_pass = cap / stride + 2;
         const int64_t tr_cap = (total_samples / stride + 2 * npass + 2) * maxdepth;
         if (rs->q_cap < cap) {
-            if ((rc = rs->q_feat.ensure(size_t(cap) * 64)) || (rc = rs->q_path.ensure(size_t(cap) * 4)) ||
-                (rc = rs->q_thr.ensure(size_t(cap) * 16)) || (rc = rs->q_out.ensure(size_t(cap) * 16)))
+            if ((rc = ensure_tracked(rs, rs->q_feat, size_t(cap) * 64)) ||
+                (rc = ensure_tracked(rs, rs->q_path, size_t(cap) * 4)) ||
+                (rc = ensure_tracked(rs, rs->q_thr, size_t(cap) * 16)) ||
+                (rc = ensure_tracked(rs, rs->q_out, size_t(cap) * 16)))
                 return rc;
             rs->q_cap = cap;
         }
-        if ((rc = rs->rec.ensure(size_t(tpaths_pass) * maxdepth * 6 * 16))) return rc;
+        if ((rc = ensure_tracked(rs, rs->rec, size_t(tpaths_pass) * maxdepth * 6 * 16))) return rc;
         if (rs->tr_cap < tr_cap) {
-            if ((rc = rs->tr_feat.ensure(size_t(tr_cap) * 64 * kCntTrainSets)) ||
-                (rc = rs->tr_target.ensure(size_t(tr_cap) * 16 * kCntTrainSets)))
+            if ((rc = ensure_tracked(rs, rs->tr_feat, size_t(tr_cap) * 64 * kCntTrainSets)) ||
+                (rc = ensure_tracked(rs, rs->tr_target, size_t(tr_cap) * 16 * kCntTrainSets)))
                 return rc;
             rs->tr_cap = tr_cap;
-            rs->pending_cache = nullptr;             // the sets were reallocated
+            rs->pending_cache = 0;                   // the sets were reallocated
         }
         if ((rc = nrc_prepare(cache, std::max<int64_t>(cap, tbatch)))) return rc;
         // Online training is one frame behind: this frame's training rows go to
@@ -1263,7 +1283,7 @@ int render_jobs(bg_scene* s, bg_cache* cache, const std::vector<JobSpec>& jobs, 
         // a side stream, beside this frame's first bounces, which do not read
         // the cache; the first query stage waits for that training.
         const int64_t frame = nrc_frame(cache) - 1;
-        train_prev = tsteps > 0 && rs->pending_cache == cache && rs->pending_frame == frame - 1;
+        train_prev = tsteps > 0 && rs->pending_cache == nrc_id(cache) && rs->pending_frame == frame - 1;
         rs->tr_set ^= 1;
         int* ntr_prev = rs->counts.as<int>() + kCntTrain + (rs->tr_set ^ 1);
         if (train_prev) {
@@ -1287,7 +1307,7 @@ int render_jobs(bg_scene* s, bg_cache* cache, const std::vector<JobSpec>& jobs, 
         // a replayed pass always holds the wait on ev_train: without training this frame it waits on nothing new
         if (use_graph && !wait_train) BG_CUDA(cudaEventRecord(rs->ev_train, st));
         BG_CUDA(cudaMemsetAsync(rs->counts.as<int>() + kCntTrain + rs->tr_set, 0, sizeof(int), st));
-        rs->pending_cache = cache;
+        rs->pending_cache = nrc_id(cache);
         rs->pending_frame = frame;
     }
     int64_t done_samples = 0;

@@ -127,10 +127,13 @@ def soup(ntris=1 << 20, seed=1):
     return sc
 
 
-def soup_rays(nrays=1 << 24, kind="incoherent", seed=2, any_hit=False):
+def soup_rays(nrays=1 << 24, kind="incoherent", seed=2, any_hit=False, tmax_range=(0.0, 1.0)):
     """C2 rays.  coherent: a pinhole grid of sqrt(n) x sqrt(n) rays from (0.5,0.5,2.5)
     at the cube centre; incoherent: origins U[0,1]^3, directions uniform on S^2.
-    tmin = 0; tmax = FLT_MAX for closest-hit sets, U[0,1] for any-hit sets."""
+    tmin = 0; tmax = FLT_MAX for closest-hit sets, U[tmax_range] (default U[0,1],
+    the config's shadow interval) for any-hit sets.  Coherent rays start 1.5
+    units in front of the cube, so coherent any-hit rays with tmax in [0,1]
+    end before reaching it; tmax_range=(1.5, 2.5) makes them end inside it."""
     rng = np.random.default_rng(seed)
     rays = np.zeros(nrays, dtype=abi.RAY_DTYPE)
     if kind == "coherent":
@@ -151,7 +154,11 @@ def soup_rays(nrays=1 << 24, kind="incoherent", seed=2, any_hit=False):
         d /= np.linalg.norm(d, axis=1, keepdims=True)
         rays["d"] = d.astype(np.float32)
     rays["tmin"] = 0.0
-    rays["tmax"] = rng.random(nrays).astype(np.float32) if any_hit else FLT_MAX
+    if any_hit:
+        lo, hi = tmax_range
+        rays["tmax"] = (lo + (hi - lo) * rng.random(nrays)).astype(np.float32)
+    else:
+        rays["tmax"] = FLT_MAX
     return rays
 
 

@@ -8,8 +8,9 @@ One step = one pass of the hot path over one batch: every pixel of a
 after bounce 3) on the seeded 6.09M-triangle production scene (fBm terrain +
 200 transformed UV spheres, GGX / Lambert, sun + constant environment).
 Prints ONE JSON line (rank 0).  N > 1 runs under torchrun, one rank per GPU:
-each rank traces its own samples of the frame (weak scaling) and the ranks sum
-their RGBW accumulation buffers with one NCCL all-reduce per step.
+each rank traces its own samples of the frame (weak scaling) into a per-step
+RGBW buffer; one NCCL all-reduce per step sums the ranks' step buffers, and the
+sum is added once into the running image.
 
 --impl reference times Banshee's own CPU tracer (the reference sources compiled
 unmodified in oracle/_ref) on the box's host cores on a bounded sample of the
@@ -124,7 +125,26 @@ def cpu_baseline_reference(scene, seconds, rows_per_call=8, nthreads=0, warm=Tru
         y += 1
     dt = time.perf_counter() - t0
     ref.close()
-    return samples / dt / 1e6, dt, samples, (nthreads or ncores)
+    return samples / dt / 1e6, dt, samples, (nthreads or ncores), acc
+
+
+def c3_rows_parity(gs, cpu_acc):
+    """relMSE of the GPU's 1-spp frame (sample 0 of every pixel, the same keyed
+    samples) against the rows the reference CPU tracer rendered for the CPU
+    baseline (a row it rendered k times holds k copies of sample 0)."""
+    import torch
+    from banshee_b200.metrics import mean_image, relmse
+    rows = np.nonzero(cpu_acc[:, 0, 3] > 0)[0]
+    frame = torch.zeros((HEIGHT, WIDTH, 4), dtype=torch.float32, device="cuda")
+    gs.render(frame.data_ptr(), WIDTH, HEIGHT, 1, seed=SEED, sample_offset=0, maxdepth=MAXDEPTH, stats=False)
+    torch.cuda.synchronize()
+    got = frame.cpu().numpy()[rows]
+    want = cpu_acc[rows]
+    return {"rows": int(rows.size), "pixels": int(rows.size * WIDTH),
+            "relmse": float(relmse(mean_image(got), mean_image(want))),
+            "counts_ok": bool((want[..., 3] == want[:, :1, 3]).all() and (got[..., 3] == 1).all()),
+            "error_flags": gs.error_flags(),
+            "what": "GPU 1-spp frame vs Banshee's own CPU tracer (oracle/_ref) on the CPU-baseline rows, same keyed samples"}
 
 
 def run_reference_arm(args, rank):
@@ -174,12 +194,20 @@ def raycast_c2(ctx, nrays=1 << 24, reps=5):
     gs = capi.GpuScene(ctx, scenes.soup(1 << 20, seed=1))
     info = gs.info()
     out = {"triangles": info["ntriangles"], "rays_per_set": nrays, "build_ms": info["build_ms"]}
-    for width, kind, anyhit in [(w, k, a) for w in (4, 8) for k in ("coherent", "incoherent") for a in (False, True)]:
+    # the config's four sets, plus coherent shadow rays whose interval ends
+    # inside the soup: the config's coherent any-hit set (tmax U[0,1] from 1.5
+    # units in front of the cube) is culled at the root and does no work
+    sets = [("coherent", False, None), ("coherent", True, None), ("incoherent", False, None),
+            ("incoherent", True, None), ("coherent", True, (1.5, 2.5))]
+    out["coherent_any_note"] = ("degenerate by construction: rays start 1.5 units in front of the cube and end "
+                                "within 1 unit, so every ray is culled at the root (1 node, 0 triangles); "
+                                "coherent_shadow_any uses tmax U[1.5,2.5], ending inside the soup")
+    for width, (kind, anyhit, trange) in [(w, st) for w in (4, 8) for st in sets]:
         gs.set_node_width(width)
         info = gs.info()
         lay = out.setdefault("layout%d" % width, {"node_width": width, "bvh_nodes": info["nnodes"],
                                                    "node_bytes": info["node_stride"]})
-        rays = scenes.soup_rays(nrays, kind, seed=2, any_hit=anyhit)
+        rays = scenes.soup_rays(nrays, kind, seed=2, any_hit=anyhit, **({"tmax_range": trange} if trange else {}))
         dr = torch.from_numpy(rays.view(np.uint8)).cuda()
         res = torch.zeros(nrays * (1 if anyhit else 16), dtype=torch.uint8, device="cuda")
         fn = gs.intersect_any if anyhit else gs.intersect_closest
@@ -197,9 +225,11 @@ def raycast_c2(ctx, nrays=1 << 24, reps=5):
         nodes, tris = gs.traversal_counts(sub.data_ptr(), sub.numel() // 32, anyhit)
         nsub = sub.numel() // 32
         bpr = 32 + (1 if anyhit else 16) + info["node_stride"] * nodes / nsub + 48 * tris / nsub
-        lay[kind + ("_any" if anyhit else "_closest")] = {
-            "mrays_per_s": nrays / ms / 1e3, "ms": ms, "nodes_per_ray": nodes / nsub, "tris_per_ray": tris / nsub,
-            "bytes_per_ray": bpr, "achieved_gbs": bpr * nrays / (ms * 1e-3) / 1e9}
+        name = ("coherent_shadow" if trange else kind) + ("_any" if anyhit else "_closest")
+        lay[name] = {
+            "mrays_per_s": round(nrays / ms / 1e3, 1), "ms": round(ms, 3), "nodes_per_ray": round(nodes / nsub, 2),
+            "tris_per_ray": round(tris / nsub, 2), "bytes_per_ray": round(bpr, 1),
+            "achieved_gbs": round(bpr * nrays / (ms * 1e-3) / 1e9, 1)}
         del dr, res, sub
     gs.close()
     # the device builders (LBVH: Morton order; PLOC: clustering over it) on the
@@ -272,14 +302,15 @@ def cornell_c1(ctx, ref_seconds_cap=60.0):
     return out
 
 
-def batch_c4(ctx, nscenes=64, seed=7, timed_frames=1, rank=0, world=1, dist=None):
+def batch_c4(ctx, nscenes=64, seed=7, timed_frames=1, rank=0, world=1, dist=None, builders=((3, "device_sah"),)):
     """C4: 64 procedural scenes (triangles log-uniform in [1e4, 5e5], resolutions from
     {256^2, 512^2, 1024x768}, 16..128 spp each) traced together by one batch: one set of
     queues, persistent kernels, one pass graph; autotuned node width / block / wavefront
-    sizes.  Each builder (host binned SAH, device LBVH, PLOC and binned SAH) builds the scenes
-    (wall time, scene generation excluded) and the batch renders its trees; the headline
-    fields are the host-SAH row.  On N GPUs each rank takes every N-th scene (no
-    exchange); times are the max over ranks."""
+    sizes.  Each builder in `builders` (default: the device binned SAH; --c4-all-builders
+    adds host binned SAH, device LBVH and PLOC) builds the scenes (wall time, scene
+    generation excluded) and the batch renders its trees; the headline fields are the first
+    builder's row.  On N GPUs each rank takes every N-th scene (no exchange); times are the
+    max over ranks."""
     import torch
     from banshee_b200 import capi, multigpu, scenes
     t0 = time.perf_counter()
@@ -294,7 +325,7 @@ def batch_c4(ctx, nscenes=64, seed=7, timed_frames=1, rank=0, world=1, dist=None
                          accum_dev=acc.data_ptr()))
     samples = sum(sc.width * sc.height * spp for sc, spp in all_items)
     rows = {}
-    for builder, name in ((0, "host_sah"), (1, "device_lbvh"), (2, "device_ploc"), (3, "device_sah")):
+    for builder, name in builders:
         torch.cuda.synchronize()
         t1 = time.perf_counter()
         gss = [capi.GpuScene(ctx, sc, builder=builder) for sc, _ in items]
@@ -318,9 +349,10 @@ def batch_c4(ctx, nscenes=64, seed=7, timed_frames=1, rank=0, world=1, dist=None
         batch.close()
         rows[name] = {"build_s": build_s, "ms": ms, "msamples_per_s": samples / ms / 1e3,
                       "build_plus_frame_s": build_s + ms / 1e3, "node_width": info["node_width"], "autotune": tune}
-    head = rows["host_sah"]
+    head = rows[builders[0][1]]
     return {"scenes": nscenes, "triangles_total": sum(sc.ntriangles for sc, _ in all_items),
-            "camera_samples": samples, "scenes_per_rank": len(items), "node_width": head["node_width"],
+            "camera_samples": samples, "scenes_per_rank": len(items), "builder": builders[0][1],
+            "node_width": head["node_width"],
             "ms": head["ms"], "msamples_per_s": head["msamples_per_s"], "autotune": head["autotune"],
             "build_s": head["build_s"], "scene_generation_s": gen_s, "by_builder": rows,
             "resolutions": sorted({"%dx%d" % (sc.width, sc.height) for sc, _ in all_items}),
@@ -397,10 +429,40 @@ def time_to_relmse(gs, sc, args, target=1e-3):
             "plain": summ(plain), "cache": summ(cached), "cache_over_plain_time": ratio,
             "plain_spp_per_call": {"spp_per_call": SPP, **summ(plain_spp)},
             "cache_over_plain_spp_per_call_time": ratio_spp,
+            "summary_cache_over_plain_1spp": ratio, "summary_cache_over_plain_best": ratio_spp,
+            "summary_truncation_bound": bound,
             "perfect_cache_bound": {
                 "what": "plain tracer truncated after 2 bounces (max depth 2) against its own reference: the "
                         "time-to-target of a free, exact cache ending paths there",
                 "reference_seconds": gt2_s, **summ(trunc), "over_plain_time": bound}}
+
+
+def summary(line):
+    """A few numbers per config, kept short so the end of the JSON line carries them."""
+    def g(d, *ks):
+        for k in ks:
+            if not isinstance(d, dict) or d.get(k) is None:
+                return None
+            d = d[k]
+        return round(d, 6) if isinstance(d, float) else d
+    out = {"c3_msamples_per_s": g(line, "value"), "c3_e2e_msamples_per_s": g(line, "e2e", "value"),
+           "c3_parity_relmse": g(line, "c3_parity", "relmse"), "c3_parity_pixels": g(line, "c3_parity", "pixels"),
+           "traversal_frac_hbm": g(line, "roofline", "frac"), "error_flags": line.get("error_flags")}
+    c2 = line.get("raycast_c2")
+    if c2:
+        for w in (4, 8):
+            for k in ("coherent_closest", "incoherent_closest", "incoherent_any", "coherent_shadow_any"):
+                out["c2_w%d_%s_mrays" % (w, k)] = g(c2, "layout%d" % w, k, "mrays_per_s")
+    out["c1_msamples_per_s"] = g(line, "cornell_c1", "gpu_msamples_per_s")
+    out["c1_relmse_vs_reference"] = g(line, "cornell_c1", "relmse_gpu_vs_reference")
+    out["c4_msamples_per_s"] = g(line, "batch_c4", "msamples_per_s")
+    out["c4_autotune"] = [g(line, "batch_c4", "autotune", k) for k in ("node_width", "trace_threads", "paths_per_pass")]
+    rt = line.get("relmse_time")
+    if rt:
+        for k, v in rt.items():
+            if k.startswith("summary_"):
+                out["c5_" + k[len("summary_"):]] = v
+    return out
 
 
 def main():
@@ -414,7 +476,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-cache", action="store_true", help="skip the time-to-relMSE measurement")
     ap.add_argument("--no-extra", action="store_true", help="skip the C1 / C2 sections")
-    ap.add_argument("--c4", action="store_true", help="also run the 64-scene batch (C4)")
+    ap.add_argument("--no-c4", action="store_true", help="skip the 64-scene batch (C4)")
+    ap.add_argument("--c4-all-builders", action="store_true", help="C4 with every BVH builder, not only device SAH")
     ap.add_argument("--gt-spp", type=int, default=65536, help="reference spp of the relMSE window")
     ap.add_argument("--conv-seconds", type=float, default=20.0, help="time budget per tracer for time-to-relMSE")
     args = ap.parse_args()
@@ -449,13 +512,18 @@ def main():
     acc.zero_()
     info = gs.info()
 
+    # N = 1: steps render straight into acc.  N > 1: each step renders this
+    # rank's samples into a zeroed step buffer, one all-reduce sums the ranks'
+    # step buffers and the sum is added once into acc
+    frame = multigpu.StepExchange(acc, dist)
+
     def step(i, stats=False, flags=0):
-        return gs.render(acc.data_ptr(), WIDTH, HEIGHT, SPP, seed=SEED,
+        return gs.render(frame.target.data_ptr(), WIDTH, HEIGHT, SPP, seed=SEED,
                          sample_offset=multigpu.sample_offset(i, rank, world, SPP), tracer=abi.BG_TRACER_GI,
                          maxdepth=MAXDEPTH, stream=stream.cuda_stream, flags=flags, stats=stats)
 
     def exchange():
-        multigpu.combine(acc, dist)
+        frame.end_step()
 
     # warm-up (untimed)
     for i in range(args.warmup):
@@ -567,12 +635,14 @@ def main():
     e2e_value = world * npix * SPP * ek / e2e_s / 1e6
 
     cpu = None
+    c3_parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            v, dt, n, cores = cpu_baseline_reference(sc, args.cpu_seconds)
+            v, dt, n, cores, cpu_acc = cpu_baseline_reference(sc, args.cpu_seconds)
             cpu = {"value": v, "unit": "Msamples/s", "cores": cores, "kind": "reference",
                    "sample": "%d camera samples (%d rows x %d px x 1 spp) in %.1f s with %d threads"
                              % (n, n // WIDTH, WIDTH, dt, cores)}
+            c3_parity = c3_rows_parity(gs, cpu_acc)
         except Exception as exc:   # the checker library may be absent
             cpu = {"value": None, "unit": "Msamples/s", "cores": 0, "kind": "reference",
                    "sample": "unavailable: %s" % exc}
@@ -584,7 +654,11 @@ def main():
         gs.close()
         c2 = raycast_c2(ctx)
         c1 = cornell_c1(ctx)
-    c4 = batch_c4(ctx, rank=rank, world=world, dist=dist) if args.c4 else None
+    c4 = None
+    if not args.no_c4:
+        blds = (((3, "device_sah"), (0, "host_sah"), (1, "device_lbvh"), (2, "device_ploc")) if args.c4_all_builders
+                else ((3, "device_sah"),))
+        c4 = batch_c4(ctx, rank=rank, world=world, dist=dist, builders=blds)
 
     if rank == 0:
         line = {
@@ -608,12 +682,15 @@ def main():
             "error_flags": flags_err,
             "phase_ms": {"extend": st_plain["ms_extend"], "shadow": st_plain["ms_shadow"],
                          "mis": st_plain["ms_mis"], "shade_and_rest": st_plain["ms_shade"]},
-            "relmse_time": cache_res,
             "raycast_c2": c2,
             "cornell_c1": c1,
             "batch_c4": c4,
+            "relmse_time": cache_res,
+            "c3_parity": c3_parity,
         }
+        line["summary"] = summary(line)     # last key: the short record of every config
         print(json.dumps(line), flush=True)
+        print("summary: " + json.dumps(line["summary"]), file=sys.stderr, flush=True)
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()

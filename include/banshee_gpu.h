@@ -253,6 +253,25 @@ typedef struct bg_render_stats {
 const char* bg_last_error(void);
 int bg_version(int32_t* major, int32_t* minor);
 
+/* Allocation accounting.  Every device allocation the library makes (scene,
+ * tree, wavefront state, cache, build scratch) and its pinned host staging is
+ * counted, and may be capped: bg_alloc_limit(bytes) allows `bytes` more bytes
+ * from this call on, process-wide (bytes < 0 removes the cap).  An allocation
+ * past the cap fails without calling CUDA, exactly as a failed cudaMalloc does:
+ * the entry point returns BG_ERR_OOM and keeps no partial state (a scene whose
+ * commit failed stays uncommitted and holds no device memory; a render whose
+ * path state could not be allocated holds none either).  For out-of-memory
+ * tests and for applications that give the library a fixed budget.  No
+ * counterpart in the reference. */
+typedef struct bg_alloc_stats {
+    int64_t calls;          /* allocations made since load                 */
+    int64_t bytes;          /* bytes of those allocations                   */
+    int64_t refused;        /* allocations refused by the cap               */
+    int64_t budget;         /* bytes still allowed, -1 = no cap             */
+} bg_alloc_stats;
+int bg_alloc_limit(int64_t bytes);
+int bg_alloc_stats_get(bg_alloc_stats* out);
+
 int bg_ctx_create(int32_t device, bg_ctx** out);
 int bg_ctx_destroy(bg_ctx* ctx);
 int bg_ctx_sync(bg_ctx* ctx);
@@ -286,7 +305,10 @@ int bg_intersect_closest_host(bg_scene* scene, const bg_ray* rays, bg_hit* hits,
 int bg_intersect_any_host(bg_scene* scene, const bg_ray* rays, uint8_t* occluded, int64_t n);
 
 /* Instrumented replay of the same traversal: total nodes fetched and
- * triangles tested over the n rays (the per-ray byte model of the roofline). */
+ * triangles tested over the n rays (the per-ray byte model of the roofline).
+ * Runs on the scene's device and gives the calling thread's current device
+ * back; synchronous on `stream`.  A replay whose traversal stack overflowed
+ * returns BG_ERR_OVERFLOW (the counts would be short). */
 int bg_traversal_counts(bg_scene* scene, const bg_ray* rays_dev, int64_t n, int32_t any_hit,
                         uint64_t* nodes, uint64_t* triangles, void* stream);
 /* Same counts as bg_traversal_counts, for callers that cannot let the library
@@ -298,7 +320,9 @@ int bg_traversal_counts(bg_scene* scene, const bg_ray* rays_dev, int64_t n, int3
  * 16,776,960 for any hit (larger n returns BG_ERR_INVALID_ARG).  The first
  * call on a device looks up the array's address; make it before any stream
  * capture.  Calls share the array: calls that overlap on the GPU race.
- * Synchronous on `stream`. */
+ * Like bg_traversal_counts it runs on the scene's device, gives the calling
+ * thread's current device back, is synchronous on `stream` and returns
+ * BG_ERR_OVERFLOW when the replay's traversal stack overflowed. */
 int bg_traversal_counts_noalloc(bg_scene* scene, const bg_ray* rays_dev, int64_t n, int32_t any_hit,
                                 uint64_t* nodes, uint64_t* triangles, void* stream);
 
@@ -414,6 +438,11 @@ typedef struct bg_cache_desc {
                                   targets); k > 0: they end into the cache k
                                   bounces after cache_depth (self-training, the
                                   pass stops there)                             */
+    int32_t wait_polls;        /* mlp_kernel 0: polls of each bounded mbarrier
+                                  wait before the kernel gives up, raises
+                                  BG_FLAG_TIMEOUT and returns (0 = 2^24).  A
+                                  budget of 1 makes every wait give up at once:
+                                  a test of the timeout path.                   */
 } bg_cache_desc;
 
 /* Query record: 16 floats per row = position (3), outgoing direction (3),

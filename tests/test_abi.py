@@ -47,3 +47,15 @@ def test_errors_without_device_or_arguments(libso):
         assert b"device" in libso.bg_last_error()
     assert libso.bg_scene_create(None, None) == -1
     assert libso.bg_intersect_closest(None, None, None, 0, None) == -1
+
+
+def test_allocation_cap_bookkeeping_without_device():
+    """bg_alloc_limit / bg_alloc_stats_get are plain host bookkeeping."""
+    from banshee_b200 import capi
+    capi.alloc_limit(12345)
+    try:
+        assert capi.alloc_stats()["budget"] == 12345
+    finally:
+        capi.alloc_limit(None)
+    st = capi.alloc_stats()
+    assert st["budget"] == -1 and st["calls"] >= 0 and st["refused"] >= 0

@@ -3,7 +3,8 @@
 Each rank renders its share of the samples (sample_offset = (step * N + rank) *
 spp) with the CPU oracle standing in for its GPU, the ranks all-reduce their
 accumulation buffers, and the result must equal one process rendering every
-sample (up to float summation order).  A second test makes one rank leave
+sample (up to float summation order).  The exchange runs after every step, as
+the bench's does, and every pixel's sample count must be exact after each one.  A second test makes one rank leave
 before the collective: the other must get an error from the process-group
 timeout instead of hanging.
 """
@@ -30,15 +31,19 @@ def _worker_render(rank, world, port, steps, out_path):
     dist = multigpu.init("gloo", timeout_s=60)
     sc = scenes.cornell(16, 16)
     o = Oracle(sc)
-    acc = np.zeros((16, 16, 4), np.float32)
+    total = torch.zeros((16, 16, 4), dtype=torch.float32)
+    ex = multigpu.StepExchange(total, dist)
     for step in range(steps):
-        o.render(spp=1, seed=5, maxdepth=5, sample_offset=multigpu.sample_offset(step, rank, world), accum=acc,
-                 nthreads=1)
-    t = torch.from_numpy(acc)
-    multigpu.combine(t, dist)
+        # each step renders this rank's samples into the step buffer, then the
+        # ranks exchange and the running total grows by that step only
+        o.render(spp=1, seed=5, maxdepth=5, sample_offset=multigpu.sample_offset(step, rank, world),
+                 accum=ex.target.numpy(), nthreads=1)
+        ex.end_step()
+        # after step k every pixel holds exactly (k + 1) * world samples
+        assert (total[..., 3] == float((step + 1) * world)).all(), (step, total[..., 3].unique())
     ms = multigpu.max_over_ranks(10.0 * (rank + 1), dist)
     if rank == 0:
-        np.save(out_path, t.numpy())
+        np.save(out_path, total.numpy())
         with open(out_path + ".ms", "w") as f:
             f.write(str(ms))
     dist.barrier()
@@ -68,7 +73,7 @@ def test_sharded_render_equals_single_process(tmp_path, oracle_built):
     from banshee_b200 import scenes
     from oracle.oracle import Oracle
     out = str(tmp_path / "acc.npy")
-    world, steps = 2, 3
+    world, steps = 2, 4
     mp.start_processes(_worker_render, args=(world, _free_port(), steps, out), nprocs=world, start_method="spawn")
     got = np.load(out)
     ref = Oracle(scenes.cornell(16, 16)).render(spp=world * steps, seed=5, maxdepth=5, nthreads=1)

@@ -7,7 +7,9 @@ disturb.  It must give the same node and triangle counts as
 bg_traversal_counts (integer counts of the same traversal: exact equality), on
 two calls in a row (the static scratch keeps the previous call's contents, so
 the second call checks that the counters are cleared), and reject ray counts
-beyond its static scratch with a clear error.  Kept in a file of its own that
+beyond its static scratch with a clear error.  With the library's allocation
+cap at zero (bg_alloc_limit) it must still work -- it allocates nothing --
+while the allocating entry point is refused.  Kept in a file of its own that
 is collected last.
 """
 import numpy as np
@@ -50,3 +52,33 @@ def test_noalloc_rejects_sizes_beyond_its_scratch():
     with pytest.raises(capi.BansheeError) as ei:
         gs.traversal_counts_noalloc(buf.data_ptr(), limit + 1, any_hit=False)
     assert ei.value.code == -1 and "limit" in str(ei.value)
+
+
+def test_noalloc_allocates_nothing():
+    """Under a zero allocation cap the allocation-free entry point still gives
+    the allocating entry point's counts, the allocation counter does not move,
+    and the allocating entry point is refused with BG_ERR_OOM."""
+    import torch
+    from banshee_b200 import capi, scenes
+
+    ctx = capi.Context(0)
+    gs = capi.GpuScene(ctx, scenes.soup(20_000, seed=5))
+    rays = scenes.soup_rays(1 << 16, "coherent", seed=6)
+    dr = torch.from_numpy(rays.view(np.uint8)).cuda()
+    torch.cuda.synchronize()
+    want = gs.traversal_counts(dr.data_ptr(), rays.shape[0])
+    gs.traversal_counts_noalloc(dr.data_ptr(), rays.shape[0])       # the device's scratch address is looked up
+    before = capi.alloc_stats()
+    capi.alloc_limit(0)
+    try:
+        for _ in range(2):
+            assert gs.traversal_counts_noalloc(dr.data_ptr(), rays.shape[0]) == want
+        after = capi.alloc_stats()
+        assert after["calls"] == before["calls"] and after["bytes"] == before["bytes"]
+        with pytest.raises(capi.BansheeError) as ei:
+            gs.traversal_counts(dr.data_ptr(), rays.shape[0])
+        assert ei.value.code == -3                                   # BG_ERR_OOM
+        assert capi.alloc_stats()["refused"] == after["refused"] + 1
+    finally:
+        capi.alloc_limit(None)
+    assert gs.traversal_counts(dr.data_ptr(), rays.shape[0]) == want
