@@ -57,7 +57,10 @@ class CameraDesc(C.Structure):
 
 class BuildOpts(C.Structure):
     _fields_ = [("node_width", C.c_int32), ("max_leaf_size", C.c_int32),
-                ("sah_bins", C.c_int32), ("builder", C.c_int32)]
+                ("sah_bins", C.c_int32), ("builder", C.c_int32), ("intersect", C.c_int32)]
+
+
+BG_INTERSECT_REFERENCE, BG_INTERSECT_WATERTIGHT = 0, 1
 
 
 class SceneInfo(C.Structure):

@@ -145,11 +145,13 @@ class Context:
 class GpuScene:
     """A committed scene on the device: World::Commit + the Intersectable surface."""
 
-    def __init__(self, ctx, scene, node_width=0, max_leaf=4, bins=32, builder=0, commit=True):
+    def __init__(self, ctx, scene, node_width=0, max_leaf=4, bins=32, builder=0, commit=True, intersect=0):
         """node_width: 4 (128-byte nodes), 8 (96-byte compressed nodes) or 0 (both
         built; the active one is chosen with set_node_width).  builder: 0 = host
         binned SAH, 1 = device LBVH, 2 = device PLOC, 3 = device binned SAH.
-        commit=False leaves the scene assembled but uncommitted (commit())."""
+        commit=False leaves the scene assembled but uncommitted (commit()).
+        intersect: 0 = the reference's Moller-Trumbore (bit-exact hits),
+        1 = the watertight test."""
         self.ctx = ctx
         self.scene = scene
         self.h = _vp()
@@ -168,7 +170,7 @@ class GpuScene:
             check(L.bg_scene_add_light(self.h, C.byref(d), None))
         bg = (C.c_float * 3)(*scene.bgcolor)
         check(L.bg_scene_set_background(self.h, bg))
-        self._opts = abi.BuildOpts(node_width, max_leaf, bins, builder)
+        self._opts = abi.BuildOpts(node_width, max_leaf, bins, builder, intersect)
         if commit:
             self.commit()
 

@@ -85,3 +85,68 @@ def converge(render_frame, W, H, Wc, Hc, gt, max_seconds, max_frames, target=1e-
             break
     return {"curve": curve, "t_target": t_target, "frames": curve[-1][1] if curve else 0,
             "final_relmse": curve[-1][2] if curve else None, "seconds": t}
+
+
+# ---------------------------------------------------------------- full frame
+def converge_frame(render_frame, W, H, gt, gt_var, max_seconds, max_frames, target=1e-3, every=1):
+    """Full-frame version of converge(): relMSE of the whole W x H image against
+    the float64 reference `gt` (H, W, 3, a device tensor, in the accumulation
+    buffer's row order) with the reference's own variance `gt_var` subtracted
+    (groundtruth.relmse_vs).  The time is the CUDA-event time of the render
+    calls only; the error evaluation runs outside it."""
+    import torch
+    from .groundtruth import relmse_vs
+    acc = torch.zeros((H, W, 4), dtype=torch.float32, device="cuda")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t = 0.0
+    curve = []
+    t_target = None
+    for f in range(max_frames):
+        e0.record()
+        render_frame(acc.data_ptr(), f)
+        e1.record()
+        torch.cuda.synchronize()
+        t += e0.elapsed_time(e1) * 1e-3
+        if (f + 1) % every == 0 or f + 1 == max_frames:
+            img = acc[..., :3].double() / acc[..., 3:4].double().clamp(min=1.0)
+            _, e = relmse_vs(img, gt, gt_var)
+            curve.append((t, f + 1, e))
+            if e <= target and t_target is None:
+                if len(curve) >= 2 and curve[-2][2] > target:
+                    (ta, _, ea), (tb, _, eb) = curve[-2], curve[-1]
+                    w = (math.log(ea) - math.log(target)) / max(math.log(ea) - math.log(eb), 1e-12)
+                    t_target = ta + w * (tb - ta)
+                else:
+                    t_target = t
+                break
+        if t > max_seconds:
+            break
+    return {"curve": curve, "t_target": t_target, "frames": curve[-1][1] if curve else 0,
+            "final_relmse": curve[-1][2] if curve else None, "seconds": t}
+
+
+def bias_floor(render_frame, W, H, gt, gt_var, frames, first_frame=0):
+    """Error floor of a (possibly biased) renderer: renders `frames` frames
+    (render_frame(acc_ptr, frame_index), frame indices from first_frame) into
+    two buffers by frame parity and splits the relMSE of their combined image
+    against the reference into its noise (the halves' difference estimates the
+    image's own variance) and the rest, the squared bias:
+        relmse = bias^2 + Var(image) + Var(reference).
+    Returns dict(relmse, image_noise, reference_noise, bias_floor)."""
+    import torch
+    from .metrics import RELMSE_EPS
+    halves = [torch.zeros((H, W, 4), dtype=torch.float32, device="cuda") for _ in range(2)]
+    for f in range(frames):
+        render_frame(halves[f & 1].data_ptr(), first_frame + f)
+    torch.cuda.synchronize()
+    a, b = (x.double() for x in halves)
+    ma = a[..., :3] / a[..., 3:4].clamp(min=1.0)
+    mb = b[..., :3] / b[..., 3:4].clamp(min=1.0)
+    tot = a + b
+    m = tot[..., :3] / tot[..., 3:4].clamp(min=1.0)
+    w = 1.0 / (gt * gt + RELMSE_EPS)
+    raw = float(((m - gt) ** 2 * w).mean())
+    noise = float(((ma - mb) ** 2 / 4.0 * w).mean())
+    ref_noise = float((gt_var * w).mean())
+    return {"frames": frames, "relmse": raw, "image_noise": noise, "reference_noise": ref_noise,
+            "bias_floor": raw - noise - ref_noise}

@@ -121,7 +121,7 @@ void ScratchBuf::release() {
 // atomicAdd, every kRefillStepsClosest / kRefillStepsAny traversal steps.
 // Termination: the counter is monotone and every ray finishes after at most
 // one visit per node.
-template <bool ANY, bool COUNT, int THREADS = kTraceThreads, int WIDTH = 4>
+template <bool ANY, bool COUNT, int THREADS = kTraceThreads, int WIDTH = 4, bool WT = false>
 __global__ void __launch_bounds__(THREADS, 1024 / THREADS)
 k_trace(DevScene S, const float4* __restrict__ rays, int64_t n_static, const int* __restrict__ n_dev,
         bg_hit* __restrict__ hits, uint8_t* __restrict__ occ, unsigned long long* __restrict__ work,
@@ -136,7 +136,7 @@ k_trace(DevScene S, const float4* __restrict__ rays, int64_t n_static, const int
     int2 lstack[stack_entries<WIDTH>() - kSm];
     __shared__ int2 sstack[kSm > 0 ? kSm : 1][THREADS];
     const RayStack<kSm> stack{&sstack[0][threadIdx.x], lstack, THREADS};
-    TravState s;
+    TravState<WT> s;
     Counters cnt{0ull, 0ull, 0ull};
     int64_t ridx = -1;
     bool active = false, exhausted = false;
@@ -196,28 +196,34 @@ k_trace(DevScene S, const float4* __restrict__ rays, int64_t n_static, const int
     }
 }
 
-template <bool ANY, bool COUNT, int THREADS, int WIDTH>
+template <bool ANY, bool COUNT, int THREADS, int WIDTH, bool WT>
 static int trace_blocks(bg_scene* s) {
     int nb = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_trace<ANY, COUNT, THREADS, WIDTH>, THREADS, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_trace<ANY, COUNT, THREADS, WIDTH, WT>, THREADS, 0);
     if (nb < 1) nb = 1;
     return nb * s->ctx->num_sms;
 }
 
-// Grid sizes of every traversal variant: [width 4/8][any][count][128/256 threads].
-template <int WIDTH>
+// Grid sizes of every traversal variant of the scene's intersection test:
+// [width 4/8][any][count][128/256 threads].
+template <int WIDTH, bool WT>
 static void setup_width(bg_scene* s, int w) {
-    s->trace_blocks[w][0][0][0] = trace_blocks<false, false, 128, WIDTH>(s);
-    s->trace_blocks[w][1][0][0] = trace_blocks<true, false, 128, WIDTH>(s);
-    s->trace_blocks[w][0][1][0] = trace_blocks<false, true, 128, WIDTH>(s);
-    s->trace_blocks[w][1][1][0] = trace_blocks<true, true, 128, WIDTH>(s);
-    s->trace_blocks[w][0][0][1] = trace_blocks<false, false, 256, WIDTH>(s);
-    s->trace_blocks[w][1][0][1] = trace_blocks<true, false, 256, WIDTH>(s);
+    s->trace_blocks[w][0][0][0] = trace_blocks<false, false, 128, WIDTH, WT>(s);
+    s->trace_blocks[w][1][0][0] = trace_blocks<true, false, 128, WIDTH, WT>(s);
+    s->trace_blocks[w][0][1][0] = trace_blocks<false, true, 128, WIDTH, WT>(s);
+    s->trace_blocks[w][1][1][0] = trace_blocks<true, true, 128, WIDTH, WT>(s);
+    s->trace_blocks[w][0][0][1] = trace_blocks<false, false, 256, WIDTH, WT>(s);
+    s->trace_blocks[w][1][0][1] = trace_blocks<true, false, 256, WIDTH, WT>(s);
 }
 
 void scene_launch_setup(bg_scene* s) {
-    setup_width<4>(s, 0);
-    setup_width<8>(s, 1);
+    if (s->dev.watertight) {
+        setup_width<4, true>(s, 0);
+        setup_width<8, true>(s, 1);
+    } else {
+        setup_width<4, false>(s, 0);
+        setup_width<8, false>(s, 1);
+    }
 }
 
 unsigned long long* next_work_counter(bg_scene* s) {
@@ -225,28 +231,46 @@ unsigned long long* next_work_counter(bg_scene* s) {
     return s->work.as<unsigned long long>() + slot;
 }
 
-template <int WIDTH>
+template <int WIDTH, bool WT>
 static void launch_width(bg_scene* s, bool any_hit, const float4* rays, int64_t n_static, const int* n_dev,
                          bg_hit* hits, uint8_t* occ, cudaStream_t st, unsigned long long* counters, int stride,
                          unsigned long long* w, const int* roots,
                          ShadowResolve res = ShadowResolve{nullptr, nullptr, nullptr}) {
     const int wi = WIDTH == 8 ? 1 : 0;
     const DevScene& d = s->dev;
+    // a static count smaller than the persistent grid (a few rays of a *_host
+    // call) gets only the blocks it can use
+    auto grid = [&](int blocks, int threads) {
+        if (n_dev || n_static <= 0) return blocks;
+        const int64_t rays_n = counters ? (n_static + stride - 1) / stride : n_static;
+        return int(std::max<int64_t>(1, std::min<int64_t>(blocks, (rays_n + threads - 1) / threads)));
+    };
     if (counters) {
         if (any_hit)
-            k_trace<true, true, 128, WIDTH><<<s->trace_blocks[wi][1][1][0], 128, 0, st>>>(d, rays, n_static, n_dev, hits, occ, w, counters, stride, roots, res);
+            k_trace<true, true, 128, WIDTH, WT><<<grid(s->trace_blocks[wi][1][1][0], 128), 128, 0, st>>>(d, rays, n_static, n_dev, hits, occ, w, counters, stride, roots, res);
         else
-            k_trace<false, true, 128, WIDTH><<<s->trace_blocks[wi][0][1][0], 128, 0, st>>>(d, rays, n_static, n_dev, hits, occ, w, counters, stride, roots, res);
+            k_trace<false, true, 128, WIDTH, WT><<<grid(s->trace_blocks[wi][0][1][0], 128), 128, 0, st>>>(d, rays, n_static, n_dev, hits, occ, w, counters, stride, roots, res);
     } else if (s->tune_threads == 256) {
         if (any_hit)
-            k_trace<true, false, 256, WIDTH><<<s->trace_blocks[wi][1][0][1], 256, 0, st>>>(d, rays, n_static, n_dev, hits, occ, w, nullptr, 1, roots, res);
+            k_trace<true, false, 256, WIDTH, WT><<<grid(s->trace_blocks[wi][1][0][1], 256), 256, 0, st>>>(d, rays, n_static, n_dev, hits, occ, w, nullptr, 1, roots, res);
         else
-            k_trace<false, false, 256, WIDTH><<<s->trace_blocks[wi][0][0][1], 256, 0, st>>>(d, rays, n_static, n_dev, hits, occ, w, nullptr, 1, roots, res);
+            k_trace<false, false, 256, WIDTH, WT><<<grid(s->trace_blocks[wi][0][0][1], 256), 256, 0, st>>>(d, rays, n_static, n_dev, hits, occ, w, nullptr, 1, roots, res);
     } else if (any_hit) {
-        k_trace<true, false, 128, WIDTH><<<s->trace_blocks[wi][1][0][0], 128, 0, st>>>(d, rays, n_static, n_dev, hits, occ, w, nullptr, 1, roots, res);
+        k_trace<true, false, 128, WIDTH, WT><<<grid(s->trace_blocks[wi][1][0][0], 128), 128, 0, st>>>(d, rays, n_static, n_dev, hits, occ, w, nullptr, 1, roots, res);
     } else {
-        k_trace<false, false, 128, WIDTH><<<s->trace_blocks[wi][0][0][0], 128, 0, st>>>(d, rays, n_static, n_dev, hits, occ, w, nullptr, 1, roots, res);
+        k_trace<false, false, 128, WIDTH, WT><<<grid(s->trace_blocks[wi][0][0][0], 128), 128, 0, st>>>(d, rays, n_static, n_dev, hits, occ, w, nullptr, 1, roots, res);
     }
+}
+
+// The traversal kernel of the scene's node layout and intersection test.
+static void launch_layout(bg_scene* s, bool any_hit, const float4* rays, int64_t n_static, const int* n_dev,
+                          bg_hit* hits, uint8_t* occ, cudaStream_t st, unsigned long long* counters, int stride,
+                          unsigned long long* w, const int* roots, ShadowResolve res) {
+    const bool w8 = s->dev.width == 8, wt = s->dev.watertight != 0;
+    if (w8 && wt) launch_width<8, true>(s, any_hit, rays, n_static, n_dev, hits, occ, st, counters, stride, w, roots, res);
+    else if (w8) launch_width<8, false>(s, any_hit, rays, n_static, n_dev, hits, occ, st, counters, stride, w, roots, res);
+    else if (wt) launch_width<4, true>(s, any_hit, rays, n_static, n_dev, hits, occ, st, counters, stride, w, roots, res);
+    else launch_width<4, false>(s, any_hit, rays, n_static, n_dev, hits, occ, st, counters, stride, w, roots, res);
 }
 
 int launch_trace(bg_scene* s, bool any_hit, const float4* rays, int64_t n_static, const int* n_dev,
@@ -255,10 +279,7 @@ int launch_trace(bg_scene* s, bool any_hit, const float4* rays, int64_t n_static
     unsigned long long* w = work ? work : next_work_counter(s);
     BG_CUDA(cudaMemsetAsync(w, 0, sizeof(unsigned long long), st));
     const ShadowResolve res = (any_hit && resolve && !counters) ? *resolve : ShadowResolve{nullptr, nullptr, nullptr};
-    if (s->dev.width == 8)
-        launch_width<8>(s, any_hit, rays, n_static, n_dev, hits, occ, st, counters, stride, w, roots, res);
-    else
-        launch_width<4>(s, any_hit, rays, n_static, n_dev, hits, occ, st, counters, stride, w, roots, res);
+    launch_layout(s, any_hit, rays, n_static, n_dev, hits, occ, st, counters, stride, w, roots, res);
     BG_CUDA(cudaGetLastError());
     return BG_OK;
 }
@@ -369,6 +390,9 @@ static int commit_scene(bg_scene* s, const bg_build_opts* opts) {
             return set_error(BG_ERR_UNSUPPORTED, "node_width %d: supported widths are 4 and 8 (0: both)", want_width);
         if (opts->max_leaf_size) bp.max_leaf = opts->max_leaf_size;
         if (opts->sah_bins) bp.bins = opts->sah_bins;
+        if (opts->intersect != BG_INTERSECT_REFERENCE && opts->intersect != BG_INTERSECT_WATERTIGHT)
+            return set_error(BG_ERR_INVALID_ARG, "intersect %d: 0 (reference Moller-Trumbore) or 1 (watertight)",
+                             opts->intersect);
         if (opts->builder < 0 || opts->builder > 3)
             return set_error(BG_ERR_INVALID_ARG,
                              "builder %d: 0 (host SAH), 1 (device LBVH), 2 (device PLOC) or 3 (device SAH)",
@@ -428,8 +452,9 @@ static int commit_scene(bg_scene* s, const bg_build_opts* opts) {
     // traversal records in leaf order, shading records in primitive order
     if ((rc = s->tris.ensure(size_t(ntris) * sizeof(TriRec))) || (rc = s->shade.ensure(size_t(ntris) * sizeof(ShadeRec))))
         return rc;
+    const bool watertight = opts && opts->intersect == BG_INTERSECT_WATERTIGHT;
     if ((rc = device_records(A, s->bundles.as<BundleRec>(), order_d.as<int32_t>(), ntris, s->tris.as<TriRec>(),
-                             s->shade.as<ShadeRec>())))
+                             s->shade.as<ShadeRec>(), watertight)))
         return rc;
     const auto tb2 = std::chrono::steady_clock::now();
     if ((rc = s->mats_d.ensure(mats.size() * sizeof(MatRec))) ||
@@ -460,6 +485,9 @@ static int commit_scene(bg_scene* s, const bg_build_opts* opts) {
     d.nbundles = nm;
     d.nmats = nmat;
     d.nlights = int(lights.size());
+    d.has_area = 0;
+    for (const LightRec& L : lights) d.has_area |= L.type == BG_LIGHT_AREA ? 1 : 0;
+    d.watertight = watertight ? 1 : 0;
     d.bg[0] = s->bg[0]; d.bg[1] = s->bg[1]; d.bg[2] = s->bg[2];
     scene_launch_setup(s);
     auto t1 = std::chrono::steady_clock::now();
@@ -564,6 +592,8 @@ int bg_scene_create(bg_ctx* ctx, bg_scene** out) {
     if (!s) return set_error(BG_ERR_OOM, "host allocation failed");
     s->ctx = ctx;
     ctx_retain(ctx);
+    static std::atomic<uint64_t> next_uid{1};
+    s->uid = next_uid.fetch_add(1);
     *out = s;
     return BG_OK;
 }
@@ -744,24 +774,93 @@ int bg_intersect_any(bg_scene* s, const bg_ray* rays, uint8_t* occ, int64_t n, v
                         static_cast<cudaStream_t>(stream));
 }
 
+}  // extern "C"
+
+// Per-thread staging of the *_host ray casts.  Banshee's renderers call
+// World::Intersect from every thread of their pool (async/thread_pool.h:
+// 136-150, renderer/mt_imagerenderer.cpp:86), one ray at a time.  Each calling
+// thread gets its own stream, pinned host staging, device buffers and
+// persistent-kernel work counter per scene, so concurrent calls run side by
+// side on the GPU instead of queueing on the scene lock; a thread keeps the
+// staging of its last kStages scenes (least recently used replaced).
+namespace {
+struct CastStage {
+    uint64_t scene_uid = 0;
+    int device = -1;
+    uint64_t used = 0;
+    cudaStream_t st = nullptr;
+    DevBuf dev;                      // work counter (256 B) | rays | results
+    void* pinned = nullptr;          // rays | results | error word
+    size_t pinned_bytes = 0;
+    void release() {
+        if (st) cudaStreamSynchronize(st);
+        dev.release();
+        if (pinned) cudaFreeHost(pinned);
+        if (st) cudaStreamDestroy(st);
+        st = nullptr; pinned = nullptr; pinned_bytes = 0; scene_uid = 0; device = -1;
+    }
+    ~CastStage() { release(); }
+};
+constexpr int kStages = 4;
+thread_local CastStage t_stage[kStages];
+thread_local uint64_t t_stage_clock = 0;
+}  // namespace
+
+static CastStage* cast_stage(bg_scene* s) {
+    CastStage* pick = &t_stage[0];
+    for (CastStage& c : t_stage) {
+        if (c.scene_uid == s->uid && c.device == s->ctx->device) { pick = &c; break; }
+        if (c.used < pick->used) pick = &c;
+    }
+    if (pick->scene_uid != s->uid || pick->device != s->ctx->device) {
+        pick->release();
+        pick->scene_uid = s->uid;
+        pick->device = s->ctx->device;
+    }
+    pick->used = ++t_stage_clock;
+    return pick;
+}
+
 static int host_cast(bg_scene* s, const bg_ray* rays, void* out, int64_t n, bool any) {
     int rc;
     if ((rc = check_scene(s)) || (rc = check_rays(rays, out, n))) return rc;
     if (n == 0) return BG_OK;
-    std::lock_guard<std::mutex> lk(s->mu);
-    BG_CUDA(cudaSetDevice(s->ctx->device));
+    DeviceGuard dg(s->ctx->device);
+    if (dg.err != cudaSuccess) return set_error(BG_ERR_CUDA, "ray cast: %s", cudaGetErrorString(dg.err));
+    CastStage* c = cast_stage(s);
+    if (!c->st) BG_CUDA(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
     const size_t rb = size_t(n) * sizeof(bg_ray), ob = size_t(n) * (any ? 1 : sizeof(bg_hit));
-    if ((rc = s->host_rays.ensure(rb)) || (rc = s->host_out.ensure(ob))) return rc;
-    BG_CUDA(cudaMemcpy(s->host_rays.ptr, rays, rb, cudaMemcpyHostToDevice));
-    rc = launch_trace(s, any, s->host_rays.as<float4>(), n, nullptr, any ? nullptr : s->host_out.as<bg_hit>(),
-                      any ? s->host_out.as<uint8_t>() : nullptr, 0);
+    const size_t ob16 = (ob + 15) & ~size_t(15);
+    if ((rc = c->dev.ensure(256 + rb + ob16))) return rc;
+    if (c->pinned_bytes < rb + ob16 + 16) {
+        if (c->pinned) cudaFreeHost(c->pinned);
+        c->pinned = nullptr;
+        c->pinned_bytes = 0;
+        const size_t want = std::max<size_t>(rb + ob16 + 16, 4096);
+        if (!alloc_charge(want))
+            return set_error(BG_ERR_OOM, "pinned staging of %zu bytes refused: over the library's allocation limit", want);
+        BG_CUDA(cudaMallocHost(&c->pinned, want));
+        c->pinned_bytes = want;
+    }
+    char* hp = static_cast<char*>(c->pinned);
+    char* dp = c->dev.as<char>();
+    memcpy(hp, rays, rb);
+    BG_CUDA(cudaMemcpyAsync(dp + 256, hp, rb, cudaMemcpyHostToDevice, c->st));
+    rc = launch_trace(s, any, reinterpret_cast<const float4*>(dp + 256), n, nullptr,
+                      any ? nullptr : reinterpret_cast<bg_hit*>(dp + 256 + rb), any ? reinterpret_cast<uint8_t*>(dp + 256 + rb) : nullptr,
+                      c->st, nullptr, 1, reinterpret_cast<unsigned long long*>(dp));
     if (rc) return rc;
-    BG_CUDA(cudaMemcpy(out, s->host_out.ptr, ob, cudaMemcpyDeviceToHost));
+    BG_CUDA(cudaMemcpyAsync(hp + rb, dp + 256 + rb, ob, cudaMemcpyDeviceToHost, c->st));
+    BG_CUDA(cudaMemcpyAsync(hp + rb + ob16, s->err.ptr, sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
+    BG_CUDA(cudaStreamSynchronize(c->st));
+    memcpy(out, hp + rb, ob);
     unsigned flags = 0;
-    BG_CUDA(cudaMemcpy(&flags, s->err.ptr, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    memcpy(&flags, hp + rb + ob16, sizeof(unsigned));
     if (flags & BG_FLAG_STACK_OVERFLOW) return set_error(BG_ERR_OVERFLOW, "traversal stack overflow");
     return BG_OK;
 }
+
+extern "C" {
 
 int bg_intersect_closest_host(bg_scene* s, const bg_ray* rays, bg_hit* hits, int64_t n) {
     return host_cast(s, rays, hits, n, false);
@@ -888,12 +987,8 @@ extern "C" int bg_traversal_counts_noalloc(bg_scene* s, const bg_ray* rays, int6
     cudaError_t e = cudaMemsetAsync(base, 0, kNoAllocHeader, st);   // counters and work counter start at zero
     if (e == cudaSuccess && n > 0) {
         const float4* r4 = reinterpret_cast<const float4*>(rays);
-        if (s->dev.width == 8)
-            launch_width<8>(s, any_hit != 0, r4, n, nullptr, any_hit ? nullptr : hits, any_hit ? occ : nullptr, st,
-                            cnt, 1, work, nullptr);
-        else
-            launch_width<4>(s, any_hit != 0, r4, n, nullptr, any_hit ? nullptr : hits, any_hit ? occ : nullptr, st,
-                            cnt, 1, work, nullptr);
+        launch_layout(s, any_hit != 0, r4, n, nullptr, any_hit ? nullptr : hits, any_hit ? occ : nullptr, st, cnt, 1,
+                      work, nullptr, ShadowResolve{nullptr, nullptr, nullptr});
         e = cudaGetLastError();
     }
     unsigned long long h[3] = {0, 0, 0};

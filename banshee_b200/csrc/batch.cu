@@ -119,6 +119,9 @@ int bg_batch_commit(bg_batch* b) {
         all4 = all4 && s->dev.nodes; all8 = all8 && s->dev.nodes8;
     }
     if (!all4 && !all8) return set_error(BG_ERR_UNSUPPORTED, "the batch's scenes share no node layout");
+    for (bg_scene* s : b->scenes)
+        if (s->dev.watertight != b->scenes[0]->dev.watertight)
+            return set_error(BG_ERR_UNSUPPORTED, "the batch's scenes use different ray / triangle tests");
     if (!all4) nn = 0;
     if (!all8) nn8 = 0;
     if (nt > int64_t(kMaxLeafStart)) return set_error(BG_ERR_UNSUPPORTED, "batch of %lld triangles exceeds %d", (long long)nt, kMaxLeafStart);
@@ -200,6 +203,9 @@ int bg_batch_commit(bg_batch* b) {
     d.nbundles = int(nb);
     d.nmats = int(nm);
     d.nlights = int(nl);
+    d.has_area = 0;
+    for (bg_scene* s : b->scenes) d.has_area |= s->dev.has_area;
+    d.watertight = b->scenes[0]->dev.watertight;
     scene_launch_setup(&M);
     bg_scene_info& info = M.info;
     info.ntriangles = nt;

@@ -114,7 +114,8 @@ struct bg_scene {
     bg::DevBuf nodes, tris, shade, bundles, mats_d, lights_d, err;
     bg::DevBuf work;          // persistent-kernel work counters (scratch)
     std::atomic<unsigned> work_slot{0};
-    bg::DevBuf host_rays, host_out;   // staging for the *_host entry points
+    bg::DevBuf host_rays, host_out;   // staging of bg_render_host
+    uint64_t uid = 0;                 // unique over the process (per-thread ray-cast staging keys on it)
     bg::DevScene dev{};
     bg_scene_info info{};
     bg::RenderState* render = nullptr;
@@ -162,8 +163,9 @@ int upload_mesh_arrays(const std::vector<MeshHost>& meshes, int64_t ntris, MeshA
 // world boxes into A.lo / A.hi (Mesh::GetShapeWorldBounds) and the scene bounds of their finite values
 int device_world_boxes(MeshArrays& A, const BundleRec* bundles, int64_t ntris, float bbox_lo[3], float bbox_hi[3]);
 // traversal records in leaf order (order: device) and shading records in primitive order
+// vertices: the watertight test's records (p1, p2, p3) instead of (p1, e1, e2)
 int device_records(const MeshArrays& A, const BundleRec* bundles, const int32_t* order, int64_t ntris,
-                   TriRec* tris, ShadeRec* shade);
+                   TriRec* tris, ShadeRec* shade, bool vertices);
 constexpr int kWorkSlots = 256;
 unsigned long long* next_work_counter(bg_scene* s);
 void scene_launch_setup(bg_scene* s);

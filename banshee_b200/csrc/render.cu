@@ -73,6 +73,7 @@ struct RenderState {
     DevBuf sh_rays, sh_contrib, sh_slot;
     DevBuf mis_rays, mis_a, mis_b, mis_c, mis_hits;
     DevBuf end_path;
+    DevBuf cls;        // material-class lists of the extension queue: 3 x cap queue indices
     DevBuf counts;     // int: ext[0], ext[1], sh, mis, end ; u64 totals at +64 bytes
     DevBuf st_key, st_cnt, st_rng, st_bs, st_thr, st_rad, st_dithr, st_flags;
     DevBuf slots, sample_rad;
@@ -101,6 +102,7 @@ struct RenderState {
     int tab_i = 0;
     DevBuf ext_root[2], sh_root, mis_root;   // per-ray root node (batched renders)
     int blocks = 0;
+    int blocks_class = 0;   // grid of the material-class shading kernels
     // CUDA graph of one pass, replayed on an internal stream
     cudaStream_t gstream = nullptr;
     cudaEvent_t ev_in = nullptr, ev_out = nullptr;
@@ -145,12 +147,13 @@ void render_state_free(RenderState* rs) {
                       &rs->st_bs, &rs->st_thr, &rs->st_rad, &rs->st_dithr, &rs->st_flags, &rs->slots,
                       &rs->sample_rad, &rs->cnt_out, &rs->work, &rs->q_feat, &rs->q_path, &rs->q_thr,
                       &rs->q_out, &rs->rec, &rs->tr_feat, &rs->tr_target, &rs->segs, &rs->jobs,
-                      &rs->ext_root[0], &rs->ext_root[1], &rs->sh_root, &rs->mis_root})
+                      &rs->ext_root[0], &rs->ext_root[1], &rs->sh_root, &rs->mis_root, &rs->cls})
         b->release();
     delete rs;
 }
 
 enum : int { kCntExt0 = 0, kCntExt1 = 1, kCntSh = 2, kCntMis = 3, kCntEnd = 4, kCntQuery = 5, kCntTrain = 6 };
+constexpr int kCntCls = 12;   // three material-class counters (k_classify)
 // shadow / MIS / ended-path counters of the odd bounces when direct light is
 // resolved one bounce late (the even bounces use kCntSh..kCntEnd)
 constexpr int kCntSh1 = 8;
@@ -185,6 +188,7 @@ struct Queues {
     float4* tr_feat; float4* tr_target; int* n_train; int tr_cap;   // training samples
     int* ext_root_in; int* ext_root_out; int* sh_root; int* mis_root; // per-ray roots, batched only
     const JobRec* jobs;
+    int* n_cls; int* cls;                                            // material-class lists (k_classify)
 };
 
 // With direct light resolved one bounce late, a path's DI slots and DI
@@ -317,6 +321,9 @@ __device__ __forceinline__ void cache_features(const SHit& h, v3 wo, const MatRe
 }
 
 // One light's DirectIllumination terms (DiTracer::GetDi, ditracer.cpp:57-239, n = 1).
+// AREA = false: no light of the scene is an area light.  INL: BSDF and light
+// sampling inline (the material-class kernels) instead of out of line.
+template <bool AREA, bool INL>
 __device__ __forceinline__ void emit_di(const DevScene& S, const Queues& Q, int li, const SHit& h, const MatRec& M, v3 wo,
                                         McRng& lr, McRng& br, int slot0, int path, int root) {
     const LightRec L = load_light(S, li);
@@ -326,17 +333,17 @@ __device__ __forceinline__ void emit_di(const DevScene& S, const Queues& Q, int 
     const bool singular = light_singular(L);
     float lightpdf = 0.f, bsdfpdf = 0.f;
     v3 ldir;
-    v3 le = light_getsample(S, L, h, lx, ly, ldir, lightpdf);
+    v3 le = light_getsample<AREA, INL>(S, L, h, lx, ly, ldir, lightpdf);
     if (lightpdf > BG_MINPDF && sqnorm(le) > 0.f) {
         v3 wi = normalize(ldir);
         float dist = sqrtf(sqnorm(ldir));
-        v3 bsdf = mat_eval(M, h, wi, wo);
+        v3 bsdf = mat_eval<INL>(M, h, wi, wo);
         float c = fabsf(dot(h.n, wi));
         v3 ls;
         if (singular) {
             ls = muls(muls(mulv(le, bsdf), c), (1.f / lightpdf));
         } else {
-            bsdfpdf = mat_pdf(M, h, wi, wo);
+            bsdfpdf = mat_pdf<INL>(M, h, wi, wo);
             float w = power_heuristic(lightpdf, bsdfpdf);
             ls = muls(muls(muls(mulv(le, bsdf), c), w), (1.f / lightpdf));
         }
@@ -351,19 +358,19 @@ __device__ __forceinline__ void emit_di(const DevScene& S, const Queues& Q, int 
     if (!singular) {
         int type = 0;
         v3 wi;
-        v3 f = mat_sample(M, h, bx, by, wo, wi, bsdfpdf, type);
+        v3 f = mat_sample<INL>(M, h, bx, by, wo, wi, bsdfpdf, type);
         wi = normalize(wi);
         if (sqnorm(f) > 0.f && bsdfpdf > BG_MINPDF) {
             float w = 1.f;
             bool skip = false;
             if (!(type & kBsdfSpecular)) {
-                float lp = light_getpdf(S, L, h, wi);
+                float lp = light_getpdf<AREA>(S, L, h, wi);
                 if (lp < BG_MINPDF) skip = true;
                 else w = power_heuristic(bsdfpdf, lp);
             }
             if (!skip) {
                 float c = fabsf(dot(h.n, wi));
-                if (L.type == BG_LIGHT_ENVIRONMENT) {
+                if (!AREA || L.type == BG_LIGHT_ENVIRONMENT) {
                     // a hit anywhere gives 0 (no bundle points at this light); a miss gives GetLe
                     v3 lev = mk(L.env[0], L.env[1], L.env[2]);
                     v3 bs = muls(muls(muls(mulv(lev, f), c), w), (1.f / bsdfpdf));
@@ -387,20 +394,26 @@ __device__ __forceinline__ void emit_di(const DevScene& S, const Queues& Q, int 
     }
 }
 
-// One instantiation per tracer kind and cache mode keeps each kernel's code
-// (and its instruction-cache footprint) to what that configuration runs.
-template <int KIND, bool CACHE>
-__global__ void __launch_bounds__(kShadeThreads, 8)   // 64 registers (measured: 8 > 7 > 10 > 6 blocks / SM)
-k_shade(DevScene S, ShadeArgs A, PathState P, Queues Q) {
-    const int n = *Q.n_ext_in;
-    if (blockIdx.x == 0 && threadIdx.x == 0) Q.totals[0] += (unsigned long long)n;
-    const int nthreads = gridDim.x * blockDim.x;
+// One instantiation per tracer kind, cache mode and area-light presence keeps
+// each kernel's code (and its instruction-cache footprint and registers) to
+// what that configuration runs.
+//
+// MAT: the material class of the hits this kernel shades (kMatAny: any, the
+// type read per hit; BG_MAT_LAMBERT / BG_MAT_MICROFACET_GGX: only hits on that
+// material; kMatOther: misses and emissive hits).  A class kernel compiles
+// only its own BSDF, inline, so it needs fewer registers and no call frame.
+constexpr int kMatAny = -1;
+constexpr int kMatOther = BG_MAT_EMISSIVE;
+
+template <int KIND, bool CACHE, bool AREA, int MAT>
+__device__ __forceinline__ void shade_path(const DevScene& S, const ShadeArgs& A, const PathState& P, const Queues& Q,
+                                           int e) {
     // deferred mode: this bounce's DI goes to half h, which held the DI of bounce
     // - 2 (gathered first); half 1 - h (bounce - 1) is still being resolved
     const int h = A.bounce & 1;
     const size_t shalf = A.defer ? size_t(h) * size_t(A.cap) * size_t(A.kmax) : 0;
     const size_t dhalf = A.defer ? size_t(h) * size_t(A.cap) : 0;
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += nthreads) {
+    {
         const int path = Q.ext_path_in[e];
         const bg_hit hit = Q.ext_hits[e];
         const float4 rd = Q.ext_rays_in[2 * e + 1];
@@ -439,7 +452,8 @@ k_shade(DevScene S, ShadeArgs A, PathState P, Queues Q) {
             } else {
                 bs = P.bs[path];
             }
-            const MatRec M = load_mat(S, h.m);
+            MatRec M = load_mat(S, h.m);
+            if (MAT != kMatAny) M.type = MAT;   // a class kernel: the material type is a constant
             const v3 wo = neg(d);
             float4 t4 = P.thr[path];
             v3 thr = mk(t4.x, t4.y, t4.z);
@@ -510,7 +524,8 @@ k_shade(DevScene S, ShadeArgs A, PathState P, Queues Q) {
                 }
                 pending = 2 * nl;
                 for (int j = 0; j < pending; ++j) P.slots[size_t(base) + j] = make_float4(0.f, 0.f, 0.f, 0.f);
-                for (int i = 0; i < nl; ++i) emit_di(S, Q, first + i, h, M, wo, lr, br, base + 2 * i, path, root);
+                for (int i = 0; i < nl; ++i)
+                    emit_di<AREA, MAT != kMatAny>(S, Q, first + i, h, M, wo, lr, br, base + 2 * i, path, root);
                 P.dithr[dhalf + path] = make_float4(thr.x, thr.y, thr.z, mult);
                 if (KIND == BG_TRACER_DI) {
                     flags |= kFlagNoClamp;
@@ -520,7 +535,7 @@ k_shade(DevScene S, ShadeArgs A, PathState P, Queues Q) {
                     int type = 0;
                     float pdf = 0.f;
                     v3 wi;
-                    v3 f = mat_sample(M, h, bs.x, bs.y, wo, wi, pdf, type);
+                    v3 f = mat_sample<MAT != kMatAny>(M, h, bs.x, bs.y, wo, wi, pdf, type);
                     if (sqnorm(f) == 0.f || pdf < BG_MINPDF) {
                         end = true;
                     } else {
@@ -555,6 +570,118 @@ k_shade(DevScene S, ShadeArgs A, PathState P, Queues Q) {
             Q.end_path[k] = path;
         }
     }
+}
+
+// Every hit of the extension queue, material read per hit.
+template <int KIND, bool CACHE, bool AREA>
+__global__ void __launch_bounds__(kShadeThreads, 8)   // 64 registers (measured: 8 > 7 > 10 > 6 blocks / SM)
+k_shade(DevScene S, ShadeArgs A, PathState P, Queues Q) {
+    const int n = *Q.n_ext_in;
+    if (blockIdx.x == 0 && threadIdx.x == 0) Q.totals[0] += (unsigned long long)n;
+    const int nthreads = gridDim.x * blockDim.x;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += nthreads)
+        shade_path<KIND, CACHE, AREA, kMatAny>(S, A, P, Q, e);
+}
+
+// Splits the extension queue by material class: list c of Q.cls (entries
+// c * cap ..) receives the queue indices of the hits of class c (0 = misses and
+// emissive, 1 = Lambert, 2 = GGX), warp-aggregated, in queue order within a warp.
+__global__ void __launch_bounds__(kShadeThreads)
+k_classify(DevScene S, Queues Q, int cap) {
+    const int n = *Q.n_ext_in;
+    const int nthreads = gridDim.x * blockDim.x;
+    const unsigned lane = threadIdx.x & 31u;
+    for (int base = blockIdx.x * blockDim.x; base < n; base += nthreads) {
+        const int e = base + int(threadIdx.x);
+        int cls = -1;
+        if (e < n) {
+            const int prim = Q.ext_hits[e].primid;
+            cls = 0;
+            if (prim >= 0) {
+                const int m = __float_as_int(__ldg(reinterpret_cast<const float*>(S.shade + prim) + 7));
+                const int t = __ldg(&S.mats[m].type);
+                cls = t == BG_MAT_LAMBERT ? 1 : t == BG_MAT_MICROFACET_GGX ? 2 : 0;
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const unsigned m = __ballot_sync(0xffffffffu, cls == c);
+            if (m == 0) continue;
+            const int leader = __ffs(m) - 1;
+            int at = 0;
+            if (lane == unsigned(leader)) at = atomicAdd(Q.n_cls + c, __popc(m));
+            at = __shfl_sync(0xffffffffu, at, leader);
+            if (cls == c) Q.cls[size_t(c) * cap + at + __popc(m & ((1u << lane) - 1u))] = e;
+        }
+    }
+}
+
+// The hits of one material class (list MAT of k_classify).
+#ifndef BG_SHADE_CLASS_BLOCKS
+#define BG_SHADE_CLASS_BLOCKS 8
+#endif
+template <int KIND, bool CACHE, bool AREA, int MAT>
+__global__ void __launch_bounds__(kShadeThreads, BG_SHADE_CLASS_BLOCKS)
+k_shade_class(DevScene S, ShadeArgs A, PathState P, Queues Q) {
+    constexpr int c = MAT == BG_MAT_LAMBERT ? 1 : MAT == BG_MAT_MICROFACET_GGX ? 2 : 0;
+    const int n = Q.n_cls[c];
+    if (MAT == kMatOther && blockIdx.x == 0 && threadIdx.x == 0) Q.totals[0] += (unsigned long long)*Q.n_ext_in;
+    const int nthreads = gridDim.x * blockDim.x;
+    const int* list = Q.cls + size_t(c) * A.cap;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += nthreads)
+        shade_path<KIND, CACHE, AREA, MAT>(S, A, P, Q, list[i]);
+}
+
+#ifndef BG_SHADE_SPLIT
+#define BG_SHADE_SPLIT 1
+#endif
+
+// Material-class kernels of one configuration: classify, then misses and
+// emissive hits, Lambert hits and GGX hits, each by its own kernel.
+template <int KIND, bool CACHE, bool AREA>
+static int launch_shade_split(const DevScene& d, int nb, int nbc, cudaStream_t st, const ShadeArgs& A,
+                              const PathState& P, const Queues& Q) {
+    BG_CUDA(cudaMemsetAsync(Q.n_cls, 0, 3 * sizeof(int), st));
+    k_classify<<<nb, kShadeThreads, 0, st>>>(d, Q, A.cap);
+    k_shade_class<KIND, CACHE, AREA, kMatOther><<<nbc, kShadeThreads, 0, st>>>(d, A, P, Q);
+    k_shade_class<KIND, CACHE, AREA, BG_MAT_LAMBERT><<<nbc, kShadeThreads, 0, st>>>(d, A, P, Q);
+    k_shade_class<KIND, CACHE, AREA, BG_MAT_MICROFACET_GGX><<<nbc, kShadeThreads, 0, st>>>(d, A, P, Q);
+    return BG_OK;
+}
+
+// The shading kernel(s) for a tracer kind, cache mode and the scene's lights.
+// Returns the number of kernels launched (< 0: an error code).
+static int launch_shade(const DevScene& d, int kind, bool cache, int nb, int nbc, cudaStream_t st,
+                        const ShadeArgs& A, const PathState& P, const Queues& Q) {
+    const bool area = d.has_area != 0;
+    if (kind == BG_TRACER_AO) {
+        k_shade<BG_TRACER_AO, false, false><<<nb, kShadeThreads, 0, st>>>(d, A, P, Q);
+        return 1;
+    }
+    if (BG_SHADE_SPLIT) {
+        int rc;
+        if (kind == BG_TRACER_DI)
+            rc = area ? launch_shade_split<BG_TRACER_DI, false, true>(d, nb, nbc, st, A, P, Q)
+                      : launch_shade_split<BG_TRACER_DI, false, false>(d, nb, nbc, st, A, P, Q);
+        else if (cache)
+            rc = area ? launch_shade_split<BG_TRACER_GI, true, true>(d, nb, nbc, st, A, P, Q)
+                      : launch_shade_split<BG_TRACER_GI, true, false>(d, nb, nbc, st, A, P, Q);
+        else
+            rc = area ? launch_shade_split<BG_TRACER_GI, false, true>(d, nb, nbc, st, A, P, Q)
+                      : launch_shade_split<BG_TRACER_GI, false, false>(d, nb, nbc, st, A, P, Q);
+        return rc ? rc : 4;
+    }
+    if (kind == BG_TRACER_DI) {
+        if (area) k_shade<BG_TRACER_DI, false, true><<<nb, kShadeThreads, 0, st>>>(d, A, P, Q);
+        else k_shade<BG_TRACER_DI, false, false><<<nb, kShadeThreads, 0, st>>>(d, A, P, Q);
+    } else if (cache) {
+        if (area) k_shade<BG_TRACER_GI, true, true><<<nb, kShadeThreads, 0, st>>>(d, A, P, Q);
+        else k_shade<BG_TRACER_GI, true, false><<<nb, kShadeThreads, 0, st>>>(d, A, P, Q);
+    } else {
+        if (area) k_shade<BG_TRACER_GI, false, true><<<nb, kShadeThreads, 0, st>>>(d, A, P, Q);
+        else k_shade<BG_TRACER_GI, false, false><<<nb, kShadeThreads, 0, st>>>(d, A, P, Q);
+    }
+    return 1;
 }
 
 // BSDF-sampled rays towards area lights: the closest hit must be on a bundle
@@ -723,7 +850,7 @@ static int alloc_state(bg_scene* s, RenderState* rs, int64_t cap, int L) {
         (rc = rs->mis_rays.ensure(2 * C * L * 32)) || (rc = rs->mis_a.ensure(2 * C * L * 16)) ||
         (rc = rs->mis_b.ensure(2 * C * L * 16)) || (rc = rs->mis_c.ensure(2 * C * L * 16)) ||
         (rc = rs->mis_hits.ensure(2 * C * L * 16)) || (rc = rs->mis_root.ensure(2 * C * L * 4)) ||
-        (rc = rs->end_path.ensure(2 * C * 4)) ||
+        (rc = rs->end_path.ensure(2 * C * 4)) || (rc = rs->cls.ensure(3 * C * 4)) ||
         (rc = rs->counts.ensure(256)) ||
         (rc = rs->st_key.ensure(C * 8)) || (rc = rs->st_cnt.ensure(C * 4)) || (rc = rs->st_rng.ensure(C * 16)) ||
         (rc = rs->st_bs.ensure(C * 8)) || (rc = rs->st_thr.ensure(C * 16)) || (rc = rs->st_rad.ensure(C * 16)) ||
@@ -733,8 +860,12 @@ static int alloc_state(bg_scene* s, RenderState* rs, int64_t cap, int L) {
         (rc = rs->work.ensure(size_t(kMaxBounceCounters) * 8)))
         return rc;
     int nb = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_shade<BG_TRACER_GI, false>, kShadeThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_shade<BG_TRACER_GI, false, true>, kShadeThreads, 0);
     rs->blocks = std::max(1, nb) * s->ctx->num_sms;
+    nb = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_shade_class<BG_TRACER_GI, false, false, BG_MAT_MICROFACET_GGX>,
+                                                  kShadeThreads, 0);
+    rs->blocks_class = std::max(1, nb) * s->ctx->num_sms;
     BG_CUDA(cudaStreamCreateWithFlags(&rs->gstream, cudaStreamNonBlocking));
     BG_CUDA(cudaEventCreateWithFlags(&rs->ev_in, cudaEventDisableTiming));
     BG_CUDA(cudaEventCreateWithFlags(&rs->ev_out, cudaEventDisableTiming));
@@ -824,6 +955,8 @@ static void pass_queues(RenderState* rs, int c, bool batched, Queues& Q, int par
     Q.sh_root = batched ? rs->sh_root.as<int>() + sh : nullptr;
     Q.mis_root = batched ? rs->mis_root.as<int>() + mi : nullptr;
     Q.jobs = rs->jobs.as<JobRec>();
+    Q.n_cls = cnt + kCntCls;
+    Q.cls = rs->cls.as<int>();
 }
 
 static PathState path_state(RenderState* rs) {
@@ -890,22 +1023,25 @@ static int enqueue_pass(bg_scene* s, RenderState* rs, cudaStream_t st, const Pas
                 if (ins) { ++ins->launches; ++ins->launches_extend; }
             }
             ShadeArgs A{b, c.maxdepth, c.kind, rs->kmax, c.batched ? 1 : 0, -1, -1, 0, c.ao_radius, 1, int(rs->cap)};
-            if (c.kind == BG_TRACER_DI) k_shade<BG_TRACER_DI, false><<<nb, kShadeThreads, 0, st>>>(s->dev, A, P, Q);
-            else if (c.kind == BG_TRACER_AO) k_shade<BG_TRACER_AO, false><<<nb, kShadeThreads, 0, st>>>(s->dev, A, P, Q);
-            else k_shade<BG_TRACER_GI, false><<<nb, kShadeThreads, 0, st>>>(s->dev, A, P, Q);
+            const int nsh = launch_shade(s->dev, c.kind, false, nb, rs->blocks_class, st, A, P, Q);
+            if (nsh < 0) return nsh;
+            if (ins) ins->launches += nsh - 1;
             BG_CUDA(cudaEventRecord(rs->ev_fork, st));
             BG_CUDA(cudaStreamWaitEvent(ds, rs->ev_fork, 0));
             const ShadowResolve sr{Q.sh_contrib, Q.sh_slot, P.slots};
             if ((rc = launch_trace(s, true, Q.sh_rays, 0, Q.n_sh, nullptr, nullptr, ds, nullptr, 1, wk + 2, Q.sh_root,
                                    &sr)))
                 return rc;
-            if ((rc = launch_trace(s, false, Q.mis_rays, 0, Q.n_mis, Q.mis_hits, nullptr, ds, nullptr, 1, wk + 3,
-                                   Q.mis_root)))
-                return rc;
-            k_resolve_mis<<<nb, kShadeThreads, 0, ds>>>(s->dev, P, Q);
+            if (s->dev.has_area) {   // MIS rays go to area lights only (the queue is empty otherwise)
+                if ((rc = launch_trace(s, false, Q.mis_rays, 0, Q.n_mis, Q.mis_hits, nullptr, ds, nullptr, 1, wk + 3,
+                                       Q.mis_root)))
+                    return rc;
+                k_resolve_mis<<<nb, kShadeThreads, 0, ds>>>(s->dev, P, Q);
+                if (ins) ins->launches += 2;
+            }
             k_finalize<<<nb, kShadeThreads, 0, ds>>>(P, Q, rs->kmax, c.maxdepth, 0, 0, b, 1, int(rs->cap));
             BG_CUDA(cudaEventRecord(evd[par], ds));
-            if (ins) ins->launches += 5;
+            if (ins) ins->launches += 3;
             if (b + 1 < depth) {
                 cur = 1 - cur;
                 Queues Qn;
@@ -940,11 +1076,9 @@ static int enqueue_pass(bg_scene* s, RenderState* rs, cudaStream_t st, const Pas
         const bool wait_here = c.cache && (c.wait_train || !ins) && b == c.cache_depth;
         if (wait_here && !fork)
             BG_CUDA(cudaStreamWaitEvent(st, rs->ev_train, ins ? 0u : unsigned(cudaEventWaitExternal)));
-        if (c.kind == BG_TRACER_DI) k_shade<BG_TRACER_DI, false><<<nb, kShadeThreads, 0, st>>>(s->dev, A, P, Q);
-        else if (c.kind == BG_TRACER_AO) k_shade<BG_TRACER_AO, false><<<nb, kShadeThreads, 0, st>>>(s->dev, A, P, Q);
-        else if (c.cache) k_shade<BG_TRACER_GI, true><<<nb, kShadeThreads, 0, st>>>(s->dev, A, P, Q);
-        else k_shade<BG_TRACER_GI, false><<<nb, kShadeThreads, 0, st>>>(s->dev, A, P, Q);
-        if (ins) { ++ins->launches; ins->mark(1); }
+        const int nsh = launch_shade(s->dev, c.kind, c.cache != nullptr, nb, rs->blocks_class, st, A, P, Q);
+        if (nsh < 0) return nsh;
+        if (ins) { ins->launches += nsh; ins->mark(1); }
         const bool forked = fork && b + 1 < depth;
         if (forked) {
             Queues Qn;

@@ -92,14 +92,14 @@ __global__ void k_world_boxes(int64_t ntris, const int32_t* __restrict__ bundle,
 __global__ void k_tri_records(int64_t ntris, const int32_t* __restrict__ order, const int32_t* __restrict__ bundle,
                               const MeshOff* __restrict__ offs, const float* __restrict__ verts,
                               const int32_t* __restrict__ vi, const BundleRec* __restrict__ bundles,
-                              TriRec* __restrict__ tris) {
+                              TriRec* __restrict__ tris, int vertices) {
     for (int64_t k = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; k < ntris; k += int64_t(gridDim.x) * blockDim.x) {
         const int64_t t = order[k];
         const int b = bundle[t];
         const int64_t v0 = offs[b].v;
         const v3 p1 = load3(verts, v0 + vi[3 * t]), p2 = load3(verts, v0 + vi[3 * t + 1]),
                  p3 = load3(verts, v0 + vi[3 * t + 2]);
-        const v3 e1 = sub(p2, p1), e2 = sub(p3, p1);
+        const v3 e1 = vertices ? p2 : sub(p2, p1), e2 = vertices ? p3 : sub(p3, p1);
         const int bcode = bundles[b].identity ? -1 : b;
         TriRec r;
         r.v0 = make_float4(p1.x, p1.y, p1.z, __int_as_float(bcode));
@@ -202,9 +202,9 @@ int device_world_boxes(MeshArrays& A, const BundleRec* bundles, int64_t ntris, f
 }
 
 int device_records(const MeshArrays& A, const BundleRec* bundles, const int32_t* order, int64_t ntris, TriRec* tris,
-                   ShadeRec* shade) {
+                   ShadeRec* shade, bool vertices) {
     k_tri_records<<<grid_for(ntris), kRT>>>(ntris, order, A.bundle.as<int32_t>(), A.offs.as<MeshOff>(),
-                                            A.verts.as<float>(), A.vi.as<int32_t>(), bundles, tris);
+                                            A.verts.as<float>(), A.vi.as<int32_t>(), bundles, tris, vertices ? 1 : 0);
     k_shade_records<<<grid_for(ntris), kRT>>>(ntris, A.bundle.as<int32_t>(), A.offs.as<MeshOff>(), A.verts.as<float>(),
                                               A.normals.as<float>(), A.uvs.as<float>(), A.vi.as<int32_t>(),
                                               A.ni.as<int32_t>(), A.ti.as<int32_t>(), A.mat.as<int32_t>(), shade);

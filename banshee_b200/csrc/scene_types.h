@@ -16,9 +16,10 @@
 namespace bg {
 
 // Moller-Trumbore operands in object space: v0 = p1, e1 = p2 - p1, e2 = p3 - p1
-// (computed once on the host with the same float subtraction as
-// primitive/mesh.cpp:13-14).  v0.w = bundle index (int bits), e1.w = global
-// primitive id (int bits).
+// (computed once with the same float subtraction as primitive/mesh.cpp:13-14).
+// v0.w = bundle index (int bits), e1.w = global primitive id (int bits).  A
+// scene committed with the watertight test holds the vertices themselves:
+// v0 = p1, e1 = p2, e2 = p3 (same .w fields).
 struct alignas(16) TriRec {
     float4 v0, e1, e2;
 };
@@ -76,7 +77,9 @@ struct DevScene {
     int32_t nbundles, nmats, nlights;
     int32_t width;          // node layout traversed: 4 (nodes) or 8 (nodes8)
     float bg[3];
-    float pad2;
+    int32_t has_area;       // some light is an AreaLight (selects the shading variant)
+    int32_t watertight;     // tris hold (p1, p2, p3) for the watertight test, not (p1, e1, e2)
+    int32_t pad3;
 };
 
 }  // namespace bg

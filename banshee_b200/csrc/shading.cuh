@@ -98,7 +98,7 @@ __device__ __forceinline__ void fill_hit(const DevScene& S, int prim, float a, f
 }
 
 // map_to_hemisphere(n, s, e), math/mathutils.h:230-244
-__device__ __noinline__ v3 map_to_hemisphere(v3 n, float sx, float sy, float e) {
+__device__ __forceinline__ v3 map_to_hemisphere_body(v3 n, float sx, float sy, float e) {
     v3 u = orthovector(n);
     v3 v = cross(u, n);
     u = cross(n, v);
@@ -107,6 +107,12 @@ __device__ __noinline__ v3 map_to_hemisphere(v3 n, float sx, float sy, float e) 
     float costheta = powf(1.f - sy, 1.f / (e + 1.f));
     float sintheta = sqrtf(1.f - costheta * costheta);
     return normalize(add(add(muls(muls(u, sintheta), cospsi), muls(muls(v, sintheta), sinpsi)), muls(n, costheta)));
+}
+__device__ __noinline__ v3 map_to_hemisphere(v3 n, float sx, float sy, float e) { return map_to_hemisphere_body(n, sx, sy, e); }
+// INL: inline copy (the material-class shading kernels) or the shared out-of-line one
+template <bool INL>
+__device__ __forceinline__ v3 hemisphere(v3 n, float sx, float sy, float e) {
+    return INL ? map_to_hemisphere_body(n, sx, sy, e) : map_to_hemisphere(n, sx, sy, e);
 }
 
 __device__ __forceinline__ float power_heuristic(float fpdf, float gpdf) {
@@ -149,44 +155,76 @@ __device__ __forceinline__ float fresnel_dielectric(float etai, float etat, floa
     float rperp = ((ei * ndotwi) - (et * ndotwt)) / ((ei * ndotwi) + (et * ndotwt));
     return (rparl * rparl + rperp * rperp) * 0.5f;
 }
-__device__ __noinline__ v3 microfacet_eval(const MatRec& M, const SHit& h, v3 wi, v3 wo) {
-    float sameside = dot(wi, h.n) * dot(wo, h.n);
+// The out-of-line BSDF functions take and return values only (no reference to
+// the caller's hit record or material), so the caller's registers stay
+// registers across the call instead of being written to a local-memory frame.
+struct BsdfSample {
+    v3 f, wo;
+    float pdf;
+};
+
+// Microfacet::Evaluate (bsdf/microfacet.h:110-148) for the shading normal hn
+__device__ __forceinline__ v3 microfacet_eval_body(v3 ks, float eta, float a, v3 hn, v3 wi, v3 wo) {
+    float sameside = dot(wi, hn) * dot(wo, hn);
     if (sameside < 0.f) return mk(0.f, 0.f, 0.f);
-    v3 n = dot(h.n, wi) < 0.f ? neg(h.n) : h.n;
+    v3 n = dot(hn, wi) < 0.f ? neg(hn) : hn;
     float cos_o = dot(n, wo);
     float cos_i = dot(n, wi);
     if (cos_i == 0.f || cos_o == 0.f) return mk(0.f, 0.f, 0.f);
     v3 wh = normalize(add(wi, wo));
-    float F = fresnel_dielectric(1.f, M.eta, dot(wi, wh));
-    float G = ggx_G1(M.a, wi, wh, n) * ggx_G1(M.a, wo, wh, n);
-    return muls(mk(M.ks[0], M.ks[1], M.ks[2]), (ggx_D(M.a, wh, n) * G * F / (4.f * cos_i * cos_o)));
+    float F = fresnel_dielectric(1.f, eta, dot(wi, wh));
+    float G = ggx_G1(a, wi, wh, n) * ggx_G1(a, wo, wh, n);
+    return muls(ks, (ggx_D(a, wh, n) * G * F / (4.f * cos_i * cos_o)));
 }
-__device__ __noinline__ v3 microfacet_sample(const MatRec& M, const SHit& h, float sx, float sy, v3 wi, v3& wo, float& pdf) {
-    v3 n = h.n, du = h.dpdu, dv = h.dpdv;
-    if (dot(h.n, wi) < 0.f) { n = neg(n); du = neg(du); dv = neg(dv); }
-    float temp = atanf(M.a * sqrtf(sx) / sqrtf(1.f - sx));
+__device__ __noinline__ v3 microfacet_eval(v3 ks, float eta, float a, v3 hn, v3 wi, v3 wo) {
+    return microfacet_eval_body(ks, eta, a, hn, wi, wo);
+}
+// Microfacet::Sample + GgxDistribution::Sample (bsdf/microfacet.h:80-108,
+// bsdf/microfacet_distribution.h:236-262); the value is Evaluate on the
+// unflipped hit
+__device__ __forceinline__ BsdfSample microfacet_sample_body(v3 ks, float eta, float a, v3 hn, v3 hdu, v3 hdv, float sx, float sy,
+                                                     v3 wi) {
+    v3 n = hn, du = hdu, dv = hdv;
+    if (dot(hn, wi) < 0.f) { n = neg(n); du = neg(du); dv = neg(dv); }
+    float temp = atanf(a * sqrtf(sx) / sqrtf(1.f - sx));
     float theta = (float)((temp >= 0) ? temp : (temp + 2 * BG_PI));
     float costheta = cosf(theta);
     float sintheta = sqrtf(1.f - clamp_ref(costheta * costheta, 0.f, 1.f));
     float cosphi = cosf(2.f * BG_PI * sy);
     float sinphi = sinf(2.f * BG_PI * sy);
     v3 wh = normalize(add(add(muls(muls(du, sintheta), cosphi), muls(muls(dv, sintheta), sinphi)), muls(n, costheta)));
-    wo = add(neg(wi), muls(wh, 2.f * dot(wi, wh)));
-    pdf = ggx_pdf(M.a, n, wi, wo);
-    return microfacet_eval(M, h, wi, wo);
+    BsdfSample r;
+    r.wo = add(neg(wi), muls(wh, 2.f * dot(wi, wh)));
+    r.pdf = ggx_pdf(a, n, wi, r.wo);
+    r.f = microfacet_eval_body(ks, eta, a, hn, wi, r.wo);
+    return r;
 }
-__device__ __noinline__ float microfacet_pdf(const MatRec& M, const SHit& h, v3 wi, v3 wo) {
-    float sameside = dot(wi, h.n) * dot(wo, h.n);
+__device__ __noinline__ BsdfSample microfacet_sample(v3 ks, float eta, float a, v3 hn, v3 hdu, v3 hdv, float sx, float sy,
+                                                     v3 wi) {
+    return microfacet_sample_body(ks, eta, a, hn, hdu, hdv, sx, sy, wi);
+}
+// Microfacet::GetPdf (bsdf/microfacet.h:150-165)
+__device__ __forceinline__ float microfacet_pdf_body(float a, v3 hn, v3 wi, v3 wo) {
+    float sameside = dot(wi, hn) * dot(wo, hn);
     if (sameside < 0.f) return 0.f;
-    v3 n = dot(h.n, wi) < 0 ? neg(h.n) : h.n;
-    return ggx_pdf(M.a, n, wi, wo);
+    v3 n = dot(hn, wi) < 0 ? neg(hn) : hn;
+    return ggx_pdf(a, n, wi, wo);
 }
-__device__ __noinline__ v3 lambert_sample(const MatRec& M, const SHit& h, float sx, float sy, v3 wi, v3& wo, float& pdf) {
-    v3 n = dot(wi, h.ng) >= 0.f ? h.n : neg(h.n);
-    wo = map_to_hemisphere(n, sx, sy, 1.f);
+__device__ __noinline__ float microfacet_pdf(float a, v3 hn, v3 wi, v3 wo) {
+    return microfacet_pdf_body(a, hn, wi, wo);
+}
+// Lambert::Sample (bsdf/lambert.h:66-86)
+__device__ __forceinline__ BsdfSample lambert_sample_body(v3 kd, v3 hn, v3 ng, float sx, float sy, v3 wi) {
+    v3 n = dot(wi, ng) >= 0.f ? hn : neg(hn);
+    BsdfSample r;
+    r.wo = map_to_hemisphere_body(n, sx, sy, 1.f);
     float invpi = 1.f / BG_PI;
-    pdf = dot(n, wo) * invpi;
-    return muls(mk(M.kd[0], M.kd[1], M.kd[2]), invpi);
+    r.pdf = dot(n, r.wo) * invpi;
+    r.f = muls(kd, invpi);
+    return r;
+}
+__device__ __noinline__ BsdfSample lambert_sample(v3 kd, v3 hn, v3 ng, float sx, float sy, v3 wi) {
+    return lambert_sample_body(kd, hn, ng, sx, sy, wi);
 }
 __device__ __forceinline__ v3 lambert_eval(const MatRec& M, const SHit& h, v3 wi, v3 wo) {
     float sameside = dot(wi, h.ng) * dot(wo, h.ng);
@@ -219,21 +257,42 @@ __device__ __forceinline__ MatRec load_mat(const DevScene& S, int m) {
 }
 
 // SimpleMaterial / Emissive dispatch (material/simplematerial.h:54-70, emissive.h:55-81)
+template <bool INL = false>
 __device__ __forceinline__ v3 mat_sample(const MatRec& M, const SHit& h, float sx, float sy, v3 wi, v3& wo, float& pdf, int& type) {
-    if (M.type == BG_MAT_LAMBERT) { type = kBsdfReflection | kBsdfDiffuse; return lambert_sample(M, h, sx, sy, wi, wo, pdf); }
-    if (M.type == BG_MAT_MICROFACET_GGX) { type = kBsdfReflection | kBsdfGlossy; return microfacet_sample(M, h, sx, sy, wi, wo, pdf); }
+    if (M.type == BG_MAT_LAMBERT) {
+        type = kBsdfReflection | kBsdfDiffuse;
+        const v3 kd = mk(M.kd[0], M.kd[1], M.kd[2]);
+        const BsdfSample r = INL ? lambert_sample_body(kd, h.n, h.ng, sx, sy, wi) : lambert_sample(kd, h.n, h.ng, sx, sy, wi);
+        wo = r.wo;
+        pdf = r.pdf;
+        return r.f;
+    }
+    if (M.type == BG_MAT_MICROFACET_GGX) {
+        type = kBsdfReflection | kBsdfGlossy;
+        const v3 ks = mk(M.ks[0], M.ks[1], M.ks[2]);
+        const BsdfSample r = INL ? microfacet_sample_body(ks, M.eta, M.a, h.n, h.dpdu, h.dpdv, sx, sy, wi)
+                                 : microfacet_sample(ks, M.eta, M.a, h.n, h.dpdu, h.dpdv, sx, sy, wi);
+        wo = r.wo;
+        pdf = r.pdf;
+        return r.f;
+    }
     pdf = 0.f;
     wo = mk(0.f, 0.f, 0.f);
     return emissive_le(M, h.n, wi);
 }
+template <bool INL = false>
 __device__ __forceinline__ v3 mat_eval(const MatRec& M, const SHit& h, v3 wi, v3 wo) {
     if (M.type == BG_MAT_LAMBERT) return lambert_eval(M, h, wi, wo);
-    if (M.type == BG_MAT_MICROFACET_GGX) return microfacet_eval(M, h, wi, wo);
+    if (M.type == BG_MAT_MICROFACET_GGX) {
+        const v3 ks = mk(M.ks[0], M.ks[1], M.ks[2]);
+        return INL ? microfacet_eval_body(ks, M.eta, M.a, h.n, wi, wo) : microfacet_eval(ks, M.eta, M.a, h.n, wi, wo);
+    }
     return emissive_le(M, h.n, wi);
 }
+template <bool INL = false>
 __device__ __forceinline__ float mat_pdf(const MatRec& M, const SHit& h, v3 wi, v3 wo) {
     if (M.type == BG_MAT_LAMBERT) return lambert_pdf(h, wi, wo);
-    if (M.type == BG_MAT_MICROFACET_GGX) return microfacet_pdf(M, h, wi, wo);
+    if (M.type == BG_MAT_MICROFACET_GGX) return INL ? microfacet_pdf_body(M.a, h.n, wi, wo) : microfacet_pdf(M.a, h.n, wi, wo);
     return 0.f;
 }
 
@@ -310,21 +369,25 @@ __device__ __noinline__ float area_getpdf(const DevScene& S, const LightRec& L, 
 
 __device__ __forceinline__ bool light_singular(const LightRec& L) { return L.type == BG_LIGHT_DIRECTIONAL; }
 
+// AREA = false: the scene has no area light (the shading variant without the
+// area-light code; its lights are directional or environment lights).
+template <bool AREA, bool INL = false>
 __device__ __forceinline__ v3 light_getsample(const DevScene& S, const LightRec& L, const SHit& h, float sx, float sy, v3& d, float& pdf) {
-    if (L.type == BG_LIGHT_AREA) return area_getsample(S, L, h.p, sx, sy, d, pdf);
+    if (AREA && L.type == BG_LIGHT_AREA) return area_getsample(S, L, h.p, sx, sy, d, pdf);
     if (L.type == BG_LIGHT_DIRECTIONAL) {                       // directional_light.cpp:5-14
         d = muls(neg(mk(L.dir[0], L.dir[1], L.dir[2])), 100000000.f);
         pdf = 1.f;
         return mk(L.e[0], L.e[1], L.e[2]);
     }
     float invpi = 1.f / BG_PI;                                    // environment_light.cpp:8-33
-    d = map_to_hemisphere(h.n, sx, sy, 1.f);
+    d = hemisphere<INL>(h.n, sx, sy, 1.f);
     pdf = dot(h.n, d) * invpi;
     d = muls(d, 10000000.f);
     return mk(L.env[0], L.env[1], L.env[2]);
 }
+template <bool AREA>
 __device__ __forceinline__ float light_getpdf(const DevScene& S, const LightRec& L, const SHit& h, v3 w) {
-    if (L.type == BG_LIGHT_AREA) return area_getpdf(S, L, h.p, w);
+    if (AREA && L.type == BG_LIGHT_AREA) return area_getpdf(S, L, h.p, w);
     if (L.type == BG_LIGHT_DIRECTIONAL) return 0.f;
     return dot(h.n, normalize(w)) * (1.f / BG_PI);
 }

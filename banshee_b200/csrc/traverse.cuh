@@ -16,6 +16,8 @@
 // when popped.
 #pragma once
 
+#include <type_traits>
+
 #include "device_common.cuh"
 #include "scene_types.h"
 #include "../../include/banshee_gpu.h"
@@ -36,10 +38,18 @@ constexpr int kRefillStepsClosest = 24;
 constexpr int kRefillStepsAny = 16;
 constexpr float kBoxSlack = 4e-7f;
 
+#ifndef BG_BOX_FMA
+#define BG_BOX_FMA 1
+#endif
+
 struct Ray {
     v3 o, d, inv;
     float tmin, tmax;
     uint32_t oct;    // bit k set: direction component k is negative (sign of 1/d)
+#if BG_BOX_FMA
+    v3 oinv;         // o * inv, rounded: a slab distance is fmaf(P, inv, -oinv)
+    float eabs;      // bound on the absolute rounding error that adds: 2^-24 max |o * inv| (+ margin)
+#endif
 };
 
 __device__ __forceinline__ Ray make_ray(float4 a, float4 b) {
@@ -48,6 +58,10 @@ __device__ __forceinline__ Ray make_ray(float4 a, float4 b) {
     r.d = mk(b.x, b.y, b.z); r.tmax = b.w;
     r.inv = mk(1.f / r.d.x, 1.f / r.d.y, 1.f / r.d.z);
     r.oct = (signbit(r.inv.x) ? 1u : 0u) | (signbit(r.inv.y) ? 2u : 0u) | (signbit(r.inv.z) ? 4u : 0u);
+#if BG_BOX_FMA
+    r.oinv = mk(r.o.x * r.inv.x, r.o.y * r.inv.y, r.o.z * r.inv.z);
+    r.eabs = fmaxf(fmaxf(fabsf(r.oinv.x), fabsf(r.oinv.y)), fabsf(r.oinv.z)) * 6.0e-8f;
+#endif
     return r;
 }
 
@@ -70,21 +84,85 @@ __device__ __forceinline__ bool mt_test(v3 o, v3 d, v3 p1, v3 e1, v3 e2, float t
     return false;
 }
 
-struct ObjRay {          // ray in the object space of bundle `bundle`
+// ray in the object space of bundle `bundle`; with WT also the watertight
+// test's shear (Woop, Benthin and Wald, "Watertight Ray/Triangle
+// Intersection", JCGT 2(1), 2013): kz = the axis of the largest |d|, kx, ky
+// the next two (swapped when d[kz] < 0, keeping the winding), sx = d[kx] /
+// d[kz], sy = d[ky] / d[kz], sz = 1 / d[kz]
+struct ObjRay {
     int bundle;
     v3 o, d;
 };
+struct ObjRayWT : ObjRay {
+    int kx, ky, kz;
+    float sx, sy, sz;
+};
 
-__device__ __forceinline__ void obj_ray(const DevScene& S, const Ray& r, int b, ObjRay& c) {
+__device__ __forceinline__ float comp(v3 v, int k) { return k == 0 ? v.x : k == 1 ? v.y : v.z; }
+
+__device__ __forceinline__ void shear(ObjRay&) {}
+__device__ __forceinline__ void shear(ObjRayWT& c) {
+    const float ax = fabsf(c.d.x), ay = fabsf(c.d.y), az = fabsf(c.d.z);
+    c.kz = (ax >= ay && ax >= az) ? 0 : (ay >= az ? 1 : 2);
+    c.kx = c.kz == 2 ? 0 : c.kz + 1;
+    c.ky = c.kx == 2 ? 0 : c.kx + 1;
+    const float dz = comp(c.d, c.kz);
+    if (dz < 0.f) { const int t = c.kx; c.kx = c.ky; c.ky = t; }
+    c.sx = comp(c.d, c.kx) / dz;
+    c.sy = comp(c.d, c.ky) / dz;
+    c.sz = 1.f / dz;
+}
+
+template <class OR>
+__device__ __forceinline__ void obj_ray(const DevScene& S, const Ray& r, int b, OR& c) {
     if (b == c.bundle) return;
     c.bundle = b;
-    if (b < 0) { c.o = r.o; c.d = r.d; return; }
-    const float* mi = S.bundles[b].minv;
-    float m[12];
+    if (b < 0) {
+        c.o = r.o; c.d = r.d;
+    } else {
+        const float* mi = S.bundles[b].minv;
+        float m[12];
 #pragma unroll
-    for (int k = 0; k < 12; ++k) m[k] = __ldg(mi + k);
-    c.o = xf_point(m, r.o);
-    c.d = xf_vector(m, r.d);
+        for (int k = 0; k < 12; ++k) m[k] = __ldg(mi + k);
+        c.o = xf_point(m, r.o);
+        c.d = xf_vector(m, r.d);
+    }
+    shear(c);
+}
+
+// Watertight ray / triangle test (Woop, Benthin and Wald 2013) on the exact
+// vertices: the edge functions U, V, W of an edge are computed from the same
+// sheared vertex coordinates in both triangles that share it (and are exact
+// negatives of each other there), so no ray passes between them.  Edges are
+// inclusive; an edge function that comes out exactly 0 is recomputed in double
+// precision.  Returns t and the barycentrics of p2 (a) and p3 (b), as
+// Moller-Trumbore's b1, b2.
+__device__ __forceinline__ bool wt_test(const ObjRayWT& c, v3 p1, v3 p2, v3 p3, float tmin, float tmax, float& t,
+                                        float& a, float& b) {
+    const v3 A = sub(p1, c.o), B = sub(p2, c.o), C = sub(p3, c.o);
+    const float az = comp(A, c.kz), bz = comp(B, c.kz), cz = comp(C, c.kz);
+    const float ax = comp(A, c.kx) - c.sx * az, ay = comp(A, c.ky) - c.sy * az;
+    const float bx = comp(B, c.kx) - c.sx * bz, by = comp(B, c.ky) - c.sy * bz;
+    const float cx = comp(C, c.kx) - c.sx * cz, cy = comp(C, c.ky) - c.sy * cz;
+    float U = cx * by - cy * bx;
+    float V = ax * cy - ay * cx;
+    float W = bx * ay - by * ax;
+    if (U == 0.f || V == 0.f || W == 0.f) {
+        U = float(double(cx) * double(by) - double(cy) * double(bx));
+        V = float(double(ax) * double(cy) - double(ay) * double(cx));
+        W = float(double(bx) * double(ay) - double(by) * double(ax));
+    }
+    if ((U < 0.f || V < 0.f || W < 0.f) && (U > 0.f || V > 0.f || W > 0.f)) return false;
+    const float det = U + V + W;
+    if (det == 0.f) return false;
+    const float T = U * (c.sz * az) + V * (c.sz * bz) + W * (c.sz * cz);
+    const float rcp = 1.f / det;
+    const float tt = T * rcp;
+    if (!(tt > tmin && tt <= tmax)) return false;
+    t = tt;
+    a = V * rcp;
+    b = W * rcp;
+    return true;
 }
 
 // Test the 4 children of node `ni`; returns a hit mask and entry distances.
@@ -105,6 +183,17 @@ __device__ __forceinline__ uint32_t box4(const WideNode4* __restrict__ nodes, in
     uint32_t mask = 0;
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
+#if BG_BOX_FMA
+        float ax = fmaf(nxa[i], r.inv.x, -r.oinv.x);
+        float bx = fmaf(fxa[i], r.inv.x, -r.oinv.x);
+        float ay = fmaf(nya[i], r.inv.y, -r.oinv.y);
+        float by = fmaf(fya[i], r.inv.y, -r.oinv.y);
+        float az = fmaf(nza[i], r.inv.z, -r.oinv.z);
+        float bz = fmaf(fza[i], r.inv.z, -r.oinv.z);
+        float t0 = fmaxf(fmaxf(ax, ay), fmaxf(az, r.tmin)) - r.eabs;
+        float t1 = fminf(fminf(bx, by), fminf(bz, best));
+        t1 = fmaf(fabsf(t1), kBoxSlack, t1) + r.eabs;
+#else
         float ax = (nxa[i] - r.o.x) * r.inv.x;
         float bx = (fxa[i] - r.o.x) * r.inv.x;
         float ay = (nya[i] - r.o.y) * r.inv.y;
@@ -114,6 +203,7 @@ __device__ __forceinline__ uint32_t box4(const WideNode4* __restrict__ nodes, in
         float t0 = fmaxf(fmaxf(ax, ay), fmaxf(az, r.tmin));
         float t1 = fminf(fminf(bx, by), fminf(bz, best));
         t1 = t1 + fabsf(t1) * kBoxSlack;
+#endif
         tn[i] = t0;
         if (t0 <= t1) mask |= 1u << i;
     }
@@ -158,6 +248,17 @@ __device__ __forceinline__ uint32_t box8(const QNode8* __restrict__ nodes, int n
         const float fqy = __uint_as_float(__byte_perm(i < 4 ? qfy.x : qfy.y, 0x4B000000u, sel));
         const float nqz = __uint_as_float(__byte_perm(i < 4 ? qnz.x : qnz.y, 0x4B000000u, sel));
         const float fqz = __uint_as_float(__byte_perm(i < 4 ? qfz.x : qfz.y, 0x4B000000u, sel));
+#if BG_BOX_FMA
+        const float ax = fmaf(fmaf(nqx, sx, hd.x), r.inv.x, -r.oinv.x);
+        const float bx = fmaf(fmaf(fqx, sx, hd.x), r.inv.x, -r.oinv.x);
+        const float ay = fmaf(fmaf(nqy, sy, hd.y), r.inv.y, -r.oinv.y);
+        const float by = fmaf(fmaf(fqy, sy, hd.y), r.inv.y, -r.oinv.y);
+        const float az = fmaf(fmaf(nqz, sz, hd.z), r.inv.z, -r.oinv.z);
+        const float bz = fmaf(fmaf(fqz, sz, hd.z), r.inv.z, -r.oinv.z);
+        float t0 = fmaxf(fmaxf(ax, ay), fmaxf(az, r.tmin)) - r.eabs;
+        float t1 = fminf(fminf(bx, by), fminf(bz, best));
+        t1 = fmaf(fabsf(t1), kBoxSlack, t1) + r.eabs;
+#else
         const float ax = (fmaf(nqx, sx, hd.x) - r.o.x) * r.inv.x;
         const float bx = (fmaf(fqx, sx, hd.x) - r.o.x) * r.inv.x;
         const float ay = (fmaf(nqy, sy, hd.y) - r.o.y) * r.inv.y;
@@ -167,6 +268,7 @@ __device__ __forceinline__ uint32_t box8(const QNode8* __restrict__ nodes, int n
         float t0 = fmaxf(fmaxf(ax, ay), fmaxf(az, r.tmin));
         float t1 = fminf(fminf(bx, by), fminf(bz, best));
         t1 = t1 + fabsf(t1) * kBoxSlack;
+#endif
         tn[i] = t0;
         if (t0 <= t1) mask |= 1u << i;
     }
@@ -203,9 +305,10 @@ struct Counters {
 };
 
 // Per-lane traversal state kept across refill points.
+template <bool WT>
 struct TravState {
     Ray r;
-    ObjRay cache;
+    typename std::conditional<WT, ObjRayWT, ObjRay>::type cache;
     float best, u, v;
     int prim;
     int item;       // current node / leaf code; kNone when the stack must be popped
@@ -213,7 +316,8 @@ struct TravState {
 };
 constexpr int kNone = 0x7fffffff;   // == kEmptyChild
 
-__device__ __forceinline__ void trav_init(TravState& s, float4 a, float4 b) {
+template <class TS>
+__device__ __forceinline__ void trav_init(TS& s, float4 a, float4 b) {
     s.r = make_ray(a, b);
     s.cache.bundle = -2;
     s.best = s.r.tmax;
@@ -226,8 +330,8 @@ __device__ __forceinline__ void trav_init(TravState& s, float4 a, float4 b) {
 // Runs at most `steps` node / leaf visits.  Returns true when the ray is done.
 // Pops the next stack entry, skipping entries that start beyond the closest
 // hit; false when the stack is empty.
-template <bool ANY, class STACK>
-__device__ __forceinline__ bool trav_pop(TravState& s, const STACK& stack, int& item) {
+template <bool ANY, class STACK, class TS>
+__device__ __forceinline__ bool trav_pop(TS& s, const STACK& stack, int& item) {
     while (s.sp > 0) {
         const int2 e = stack.get(--s.sp);
         // the entry distance carries the box test's rounding: cull with its slack
@@ -240,8 +344,8 @@ __device__ __forceinline__ bool trav_pop(TravState& s, const STACK& stack, int& 
 
 // Visits internal node `item`: continues with the nearest hit child (s.item),
 // pushes the others.  False on stack overflow (error flag raised).
-template <bool COUNT, int WIDTH, class STACK>
-__device__ __forceinline__ bool trav_node(const DevScene& S, TravState& s, const STACK& stack, int item,
+template <bool COUNT, int WIDTH, class STACK, class TS>
+__device__ __forceinline__ bool trav_node(const DevScene& S, TS& s, const STACK& stack, int item,
                                           Counters& cnt) {
     if (COUNT) ++cnt.nodes;
     if (WIDTH == 8) {
@@ -306,8 +410,10 @@ __device__ __forceinline__ bool trav_node(const DevScene& S, TravState& s, const
 
 // Tests the triangles of leaf code `item` (bit 31 set, count-1 in bits 27..30,
 // first triangle in bits 0..26).  True when an any-hit query found its hit.
-template <bool ANY, bool COUNT>
-__device__ __forceinline__ bool trav_leaf(const DevScene& S, TravState& s, int item, Counters& cnt) {
+// WT: the scene's records hold the vertices (p1, p2, p3) and the test is the
+// watertight one; otherwise they hold (p1, e1, e2) for Moller-Trumbore.
+template <bool ANY, bool COUNT, bool WT>
+__device__ __forceinline__ bool trav_leaf(const DevScene& S, TravState<WT>& s, int item, Counters& cnt) {
     const uint32_t code = uint32_t(item);
     const int count = int((code >> kLeafStartBits) & 15u) + 1;
     const int start = int(code & uint32_t(kMaxLeafStart));
@@ -317,8 +423,14 @@ __device__ __forceinline__ bool trav_leaf(const DevScene& S, TravState& s, int i
         if (COUNT) ++cnt.tris;
         obj_ray(S, s.r, __float_as_int(v0.w), s.cache);
         float t, a, b;
-        if (mt_test(s.cache.o, s.cache.d, mk(v0.x, v0.y, v0.z), mk(e1.x, e1.y, e1.z), mk(e2.x, e2.y, e2.z),
-                    s.r.tmin, ANY ? s.r.tmax : s.best, t, a, b)) {
+        bool hit;
+        if constexpr (WT)
+            hit = wt_test(s.cache, mk(v0.x, v0.y, v0.z), mk(e1.x, e1.y, e1.z), mk(e2.x, e2.y, e2.z), s.r.tmin,
+                          ANY ? s.r.tmax : s.best, t, a, b);
+        else
+            hit = mt_test(s.cache.o, s.cache.d, mk(v0.x, v0.y, v0.z), mk(e1.x, e1.y, e1.z), mk(e2.x, e2.y, e2.z),
+                          s.r.tmin, ANY ? s.r.tmax : s.best, t, a, b);
+        if (hit) {
             s.prim = __float_as_int(e1.w);
             if (ANY) return true;
             s.best = t; s.u = a; s.v = b;
@@ -328,8 +440,11 @@ __device__ __forceinline__ bool trav_leaf(const DevScene& S, TravState& s, int i
 }
 
 // Runs at most `steps` node / leaf visits.  Returns true when the ray is done.
-template <bool ANY, bool COUNT, int WIDTH, class STACK>
-__device__ __forceinline__ bool trav_steps(const DevScene& S, TravState& s, const STACK& stack, int steps,
+// (Measured and rejected: node and leaf visits in two warp-wide phases,
+// with or without postponing a lane's leaf while others still descend: the
+// votes and the longer loops cost 2.5-4x on C2 and C3.)
+template <bool ANY, bool COUNT, int WIDTH, class STACK, bool WT>
+__device__ __forceinline__ bool trav_steps(const DevScene& S, TravState<WT>& s, const STACK& stack, int steps,
                                            Counters& cnt) {
     for (int it = 0; it < steps; ++it) {
         int item = s.item;

@@ -361,80 +361,111 @@ def batch_c4(ctx, nscenes=64, seed=7, timed_frames=1, rank=0, world=1, dist=None
                                max(sc.ntriangles for sc, _ in all_items)]}
 
 
+def _ground_truth(gs, args, maxdepth, spp, camera=None, width=WIDTH, height=HEIGHT, name="c3"):
+    """Plain GiTracer(maxdepth) render of the full frame at `spp` samples per pixel,
+    float64 accumulation of 256-spp chunks, checkpointed under --gt-cache (resumed
+    when the same reference was started before).  Returns (mean, variance of the
+    mean, seconds of this run, spp resumed from a checkpoint)."""
+    from banshee_b200 import groundtruth as GT
+    key = {"scene": name, "w": width, "h": height, "maxdepth": maxdepth, "seed": 7777, "spp": spp,
+           "triangles": gs.info()["ntriangles"]}
+    path = None
+    if args.gt_cache:
+        os.makedirs(args.gt_cache, exist_ok=True)
+        path = os.path.join(args.gt_cache, "gt_%s_d%d_%d.npz" % (name, maxdepth, spp))
+    start = {}
+    t0 = time.perf_counter()
+
+    def chunk(acc32, off, n):
+        start.setdefault("spp", off)
+        gs.render(acc32.data_ptr(), width, height, n, seed=7777, sample_offset=off, maxdepth=maxdepth, camera=camera,
+                  stats=False)
+
+    acc = GT.accumulate(chunk, height, width, spp, key, chunk=256, path=path, every=32)
+    import torch
+    torch.cuda.synchronize()
+    return acc.mean(), acc.mean_variance(), time.perf_counter() - t0, start.get("spp", spp)
+
+
+def _summ(r):
+    return {"seconds_to_target": r["t_target"], "frames": r["frames"], "final_relmse": r["final_relmse"],
+            "ms_per_frame": 1e3 * r["seconds"] / max(1, r["frames"]),
+            "curve": [[round(t, 4), n, float("%.4g" % e)] for t, n, e in r["curve"][::max(1, len(r["curve"]) // 12)]]}
+
+
+def _ratio(a, b):
+    return (a / b) if (a and b) else None
+
+
+CACHE_CFG = dict(log2_table_size=19, base_resolution=16, max_resolution=2048, train_paths=65536, cache_depth=2,
+                 train_batch=65536, train_steps=1, learning_rate=1e-2, train_suffix=1)
+CACHE_DESC = ("hash grid 16 levels x 2 features, 2^19 entries/level, res 16..2048; MLP 64x5 bf16; Adam lr 1e-2; "
+              "65536 training paths/frame; rendering paths end into the cache after 2 bounces, training paths one "
+              "bounce later (self-training); one Adam step per frame over up to 65536 training vertices from depth 2 "
+              "on, trained one frame behind beside the next frame's first bounces")
+
+
 def time_to_relmse(gs, sc, args, target=1e-3):
-    """Second half of the metric: wall (GPU) time for the radiance-cache tracer and
-    the plain tracer to reach relMSE 1e-3 on a centred 240x136 window of the 1080p
-    frame, against a plain render of that window at args.gt_spp spp accumulated in
-    float64.  Both tracers render full 1080p frames, 1 spp per frame (the cache
-    trains once per frame); the plain tracer is also timed at SPP samples per call,
-    its throughput configuration."""
+    """Second half of the metric, on the full 1920x1080 frame: GPU time for the
+    radiance-cache tracer and for the plain tracer to reach relMSE 1e-3 against a
+    plain GiTracer(8) render at args.gt_spp spp accumulated in float64 (the
+    reference's own noise, estimated from two halves, subtracted).  The plain
+    tracer runs at 1 spp per frame and at SPP per call (its throughput
+    configuration, the headline comparison); the cache renders 1 spp per frame
+    and trains once per frame.  The cache's bias floor is its error, after
+    convergence, once its image noise and the reference's are taken out.  The
+    bound for any cache that ends paths after 2 bounces is the plain tracer
+    truncated there (max depth 2) against its own float64 reference."""
+    import torch
     from banshee_b200 import capi
     from banshee_b200 import convergence as CV
-    Wc, Hc = 240, 136
-    wcam = CV.window_camera(sc.camera, WIDTH, HEIGHT, Wc, Hc)
-    t0 = time.perf_counter()
-    gt = CV.ground_truth(gs, Wc, Hc, args.gt_spp, MAXDEPTH, seed=7777, camera=wcam)
-    gt_s = time.perf_counter() - t0
-    plain = CV.converge(lambda p, f: gs.render(p, WIDTH, HEIGHT, 1, seed=SEED, sample_offset=f, maxdepth=MAXDEPTH,
-                                               stats=False),
-                        WIDTH, HEIGHT, Wc, Hc, gt, args.conv_seconds, 100000, target=target, every=4)
-    # the plain tracer at its bench configuration too: SPP samples per render call
-    plain_spp = CV.converge(lambda p, f: gs.render(p, WIDTH, HEIGHT, SPP, seed=SEED, sample_offset=f * SPP,
-                                                   maxdepth=MAXDEPTH, stats=False),
-                            WIDTH, HEIGHT, Wc, Hc, gt, args.conv_seconds, 100000, target=target, every=1)
-    cache_cfg = dict(log2_table_size=19, base_resolution=16, max_resolution=2048, train_paths=65536, cache_depth=2,
-                     train_batch=65536, train_steps=1, learning_rate=1e-2, train_suffix=1)
+    gt, gt_var, gt_s, gt_from = _ground_truth(gs, args, MAXDEPTH, args.gt_spp)
+    run = lambda fn, every: CV.converge_frame(fn, WIDTH, HEIGHT, gt, gt_var, args.conv_seconds, 100000,
+                                              target=target, every=every)
+    plain = run(lambda p, f: gs.render(p, WIDTH, HEIGHT, 1, seed=SEED, sample_offset=f, maxdepth=MAXDEPTH,
+                                       stats=False), 4)
+    plain_spp = run(lambda p, f: gs.render(p, WIDTH, HEIGHT, SPP, seed=SEED, sample_offset=f * SPP,
+                                           maxdepth=MAXDEPTH, stats=False), 1)
     # warm the process as the plain tracer's timing is warm: a throwaway cache
     # renders a few frames (kernel modules loaded, scratch memory pooled); the
     # timed cache then starts untrained
-    import torch
-    warm = capi.RadianceCache(gs, **cache_cfg)
+    warm = capi.RadianceCache(gs, **CACHE_CFG)
     wbuf = torch.zeros((HEIGHT, WIDTH, 4), dtype=torch.float32, device="cuda")
     for f in range(4):
         warm.render(wbuf.data_ptr(), WIDTH, HEIGHT, 1, seed=SEED, sample_offset=f, maxdepth=MAXDEPTH)
     torch.cuda.synchronize()
     warm.close()
     del wbuf
-    cache = capi.RadianceCache(gs, **cache_cfg)
-    cached = CV.converge(lambda p, f: cache.render(p, WIDTH, HEIGHT, 1, seed=SEED, sample_offset=f,
-                                                   maxdepth=MAXDEPTH),
-                         WIDTH, HEIGHT, Wc, Hc, gt, args.conv_seconds, 100000, target=target, every=4)
+    cache = capi.RadianceCache(gs, **CACHE_CFG)
+    render_cached = lambda p, f: cache.render(p, WIDTH, HEIGHT, 1, seed=SEED, sample_offset=f, maxdepth=MAXDEPTH)
+    cached = run(render_cached, 4)
+    # the cache keeps training while the floor is measured
+    floor = CV.bias_floor(render_cached, WIDTH, HEIGHT, gt, gt_var, args.floor_frames, first_frame=cached["frames"])
     cache.close()
-    # Bound for any cache that ends paths after 2 bounces: the plain tracer
-    # truncated there (max depth 2, nothing added at the 3rd vertex), judged
-    # against its own deep reference -- a perfect cache at zero cost would
-    # converge at this rate and frame time, no faster.
-    t0 = time.perf_counter()
-    gt2 = CV.ground_truth(gs, Wc, Hc, args.gt_spp, 2, seed=7777, camera=wcam)
-    gt2_s = time.perf_counter() - t0
-    trunc = CV.converge(lambda p, f: gs.render(p, WIDTH, HEIGHT, 1, seed=SEED, sample_offset=f, maxdepth=2,
-                                               stats=False),
-                        WIDTH, HEIGHT, Wc, Hc, gt2, args.conv_seconds, 100000, target=target, every=4)
-
-    def summ(r):
-        return {"seconds_to_target": r["t_target"], "frames": r["frames"], "final_relmse": r["final_relmse"],
-                "ms_per_frame": 1e3 * r["seconds"] / max(1, r["frames"]),
-                "curve": [[round(t, 4), n, float("%.4g" % e)] for t, n, e in r["curve"][::max(1, len(r["curve"]) // 12)]]}
-
-    ratio = (cached["t_target"] / plain["t_target"]) if (cached["t_target"] and plain["t_target"]) else None
-    ratio_spp = (cached["t_target"] / plain_spp["t_target"]) if (cached["t_target"] and plain_spp["t_target"]) else None
-    bound = (trunc["t_target"] / plain["t_target"]) if (trunc["t_target"] and plain["t_target"]) else None
-    return {"target_relmse": target, "window": [Wc, Hc], "reference_spp": args.gt_spp, "reference_seconds": gt_s,
-            "reference": "plain GiTracer(8), float64 accumulation of 256-spp chunks",
-            "relmse": "mean over pixels and channels of (x - ref)^2 / (ref^2 + 0.01)",
-            "cache_config": "hash grid 16 levels x 2 features, 2^19 entries/level, res 16..2048; MLP 64x5 bf16; "
-                            "Adam lr 1e-2; 65536 training paths/frame; rendering paths end into the cache after 2 bounces, "
-                            "training paths one bounce later (self-training); one Adam step per frame over up to 65536 "
-                            "training vertices from depth 2 on, trained one frame behind beside the next frame's first bounces",
-            "plain": summ(plain), "cache": summ(cached), "cache_over_plain_time": ratio,
-            "plain_spp_per_call": {"spp_per_call": SPP, **summ(plain_spp)},
-            "cache_over_plain_spp_per_call_time": ratio_spp,
-            "summary_cache_over_plain_1spp": ratio, "summary_cache_over_plain_best": ratio_spp,
-            "summary_truncation_bound": bound,
+    gt2, gt2_var, gt2_s, _ = _ground_truth(gs, args, 2, args.gt_spp_bound)
+    trunc = CV.converge_frame(lambda p, f: gs.render(p, WIDTH, HEIGHT, 1, seed=SEED, sample_offset=f, maxdepth=2,
+                                                     stats=False),
+                              WIDTH, HEIGHT, gt2, gt2_var, args.conv_seconds, 100000, target=target, every=4)
+    del gt, gt_var, gt2, gt2_var
+    ratio = _ratio(cached["t_target"], plain["t_target"])
+    ratio_spp = _ratio(cached["t_target"], plain_spp["t_target"])
+    bound = _ratio(trunc["t_target"], plain["t_target"])
+    return {"target_relmse": target, "frame": [WIDTH, HEIGHT], "reference_spp": args.gt_spp,
+            "reference_seconds": gt_s, "reference_resumed_from_spp": gt_from,
+            "reference": "plain GiTracer(8), full frame, float64 accumulation of 256-spp chunks in two halves",
+            "relmse": "mean over pixels and channels of (x - ref)^2 / (ref^2 + 0.01), minus the same mean of the "
+                      "reference's own variance (from its two halves)",
+            "cache_config": CACHE_DESC,
+            "plain": _summ(plain), "plain_spp_per_call": {"spp_per_call": SPP, **_summ(plain_spp)},
+            "cache": _summ(cached), "cache_bias_floor": floor,
+            "cache_over_plain_time": ratio, "cache_over_plain_spp_per_call_time": ratio_spp,
             "perfect_cache_bound": {
-                "what": "plain tracer truncated after 2 bounces (max depth 2) against its own reference: the "
-                        "time-to-target of a free, exact cache ending paths there",
-                "reference_seconds": gt2_s, **summ(trunc), "over_plain_time": bound}}
+                "what": "plain tracer truncated after 2 bounces (max depth 2) against its own reference at "
+                        "%d spp: the time-to-target of a free, exact cache ending paths there" % args.gt_spp_bound,
+                "reference_seconds": gt2_s, **_summ(trunc), "over_plain_time": bound},
+            "summary_cache_over_plain_best": ratio_spp, "summary_cache_over_plain_1spp": ratio,
+            "summary_bias_floor": floor["bias_floor"], "summary_truncation_bound": bound,
+            "summary_reference_spp": args.gt_spp}
 
 
 def summary(line):
@@ -478,7 +509,10 @@ def main():
     ap.add_argument("--no-extra", action="store_true", help="skip the C1 / C2 sections")
     ap.add_argument("--no-c4", action="store_true", help="skip the 64-scene batch (C4)")
     ap.add_argument("--c4-all-builders", action="store_true", help="C4 with every BVH builder, not only device SAH")
-    ap.add_argument("--gt-spp", type=int, default=65536, help="reference spp of the relMSE window")
+    ap.add_argument("--gt-spp", type=int, default=65536, help="spp of the float64 reference frame")
+    ap.add_argument("--gt-spp-bound", type=int, default=16384, help="spp of the depth-2 reference (the bound)")
+    ap.add_argument("--gt-cache", default=None, help="directory for reference checkpoints (resumed when present)")
+    ap.add_argument("--floor-frames", type=int, default=256, help="cache frames of the bias-floor measurement")
     ap.add_argument("--conv-seconds", type=float, default=20.0, help="time budget per tracer for time-to-relMSE")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -574,12 +608,20 @@ def main():
     achieved = ext_bytes / (ext_ms * 1e-3) / 1e9
     peak, peak_src = peaks()
     traffic = None
+    measured = {}
     prof = os.path.join(ROOT, "profiles", "traverse_extend_c3.json")
     if os.path.exists(prof):
         with open(prof) as f:
             p = json.load(f)
         if "dram_bytes_per_ray" in p:
             traffic = p["dram_bytes_per_ray"] * ext_rays / max(1, st_plain["launches_extend"])
+        # what the kernel really moves (ncu, one 1-spp frame, scaled by rays): the
+        # byte model above counts node and triangle bytes wherever they are served
+        # from; DRAM and L2 bytes and SIMT efficiency say where the time goes
+        for k in ("dram_bytes_per_ray", "l2_bytes_per_ray", "l2_pct_of_peak", "threads_per_instruction",
+                  "dram_pct_of_peak", "sm_pct_of_peak"):
+            if k in p:
+                measured[k] = p[k]
     roofline = {
         "kernel": "k_trace<closest> on the extension-ray queues (all bounces of one step)",
         "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
@@ -590,7 +632,9 @@ def main():
         "node_bytes": node_b, "tri_bytes": tri_b,
         "launches": st_plain["launches_extend"], "ms_extend": ext_ms, "ms_step": st_plain["ms_total"],
         "byte_model": "32 B ray + 16 B hit + node_bytes * nodes/ray + 48 B * triangles/ray, counts from an "
-                      "instrumented replay of every 64th ray of each extension queue",
+                      "instrumented replay of every 64th ray of each extension queue; frac counts those bytes "
+                      "wherever they are served from (mostly L1/L2), see ncu_measured",
+        "ncu_measured": measured or None,
     }
     rays_per_step = st_plain["rays_closest"] + st_plain["rays_any"]
     # every k_trace launch of the step (extension, shadow any-hit, MIS): the

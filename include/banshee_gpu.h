@@ -152,7 +152,19 @@ typedef struct bg_build_opts {
                                2 = device PLOC (nearest-neighbour
                                clustering over the Morton order, radius 16);
                                3 = device binned SAH (top-down, 32 bins) */
+    int32_t intersect;      /* ray / triangle test of every cast and render:
+                               BG_INTERSECT_REFERENCE (0) = Moller-Trumbore in
+                               the reference's operation order (primitive/
+                               mesh.cpp:7-45): hits bit-exact with Bvh::Intersect;
+                               BG_INTERSECT_WATERTIGHT (1) = watertight test
+                               (Woop, Benthin and Wald 2013): no ray passes
+                               between triangles that share an edge or a
+                               vertex; not in the reference, hits differ from
+                               Moller-Trumbore only at edges */
 } bg_build_opts;
+
+#define BG_INTERSECT_REFERENCE  0
+#define BG_INTERSECT_WATERTIGHT 1
 
 typedef struct bg_scene_info {
     int64_t ntriangles;
