@@ -176,6 +176,7 @@ k_trace(DevScene S, const float4* __restrict__ rays, int64_t n_static, const int
                     h.primid = s.prim;
                     h.u = s.u;
                     h.v = s.v;
+                    if (res.hit_class && s.prim >= 0) h.primid = s.prim | (s.cls << kClassShift);
                     reinterpret_cast<float4*>(hits)[ridx] = *reinterpret_cast<float4*>(&h);
                 }
                 active = false;
@@ -235,7 +236,7 @@ template <int WIDTH, bool WT>
 static void launch_width(bg_scene* s, bool any_hit, const float4* rays, int64_t n_static, const int* n_dev,
                          bg_hit* hits, uint8_t* occ, cudaStream_t st, unsigned long long* counters, int stride,
                          unsigned long long* w, const int* roots,
-                         ShadowResolve res = ShadowResolve{nullptr, nullptr, nullptr}) {
+                         ShadowResolve res = ShadowResolve{nullptr, nullptr, nullptr, 0}) {
     const int wi = WIDTH == 8 ? 1 : 0;
     const DevScene& d = s->dev;
     // a static count smaller than the persistent grid (a few rays of a *_host
@@ -278,7 +279,11 @@ int launch_trace(bg_scene* s, bool any_hit, const float4* rays, int64_t n_static
                  unsigned long long* work, const int* roots, const ShadowResolve* resolve) {
     unsigned long long* w = work ? work : next_work_counter(s);
     BG_CUDA(cudaMemsetAsync(w, 0, sizeof(unsigned long long), st));
-    const ShadowResolve res = (any_hit && resolve && !counters) ? *resolve : ShadowResolve{nullptr, nullptr, nullptr};
+    ShadowResolve res{nullptr, nullptr, nullptr, 0};
+    if (resolve && !counters) {
+        if (any_hit) res = *resolve;
+        else res.hit_class = resolve->hit_class;
+    }
     launch_layout(s, any_hit, rays, n_static, n_dev, hits, occ, st, counters, stride, w, roots, res);
     BG_CUDA(cudaGetLastError());
     return BG_OK;
@@ -453,8 +458,15 @@ static int commit_scene(bg_scene* s, const bg_build_opts* opts) {
     if ((rc = s->tris.ensure(size_t(ntris) * sizeof(TriRec))) || (rc = s->shade.ensure(size_t(ntris) * sizeof(ShadeRec))))
         return rc;
     const bool watertight = opts && opts->intersect == BG_INTERSECT_WATERTIGHT;
+    // material class per material (the renderer's shading split), stored with each triangle
+    std::vector<int32_t> mclass(std::max(nmat, 1), 0);
+    for (int i = 0; i < nmat; ++i)
+        mclass[i] = s->mats[i].type == BG_MAT_LAMBERT ? 1 : s->mats[i].type == BG_MAT_MICROFACET_GGX ? 2 : 0;
+    ScratchBuf mclass_d;
+    if ((rc = mclass_d.ensure(mclass.size() * 4))) return rc;
+    BG_CUDA(cudaMemcpy(mclass_d.ptr, mclass.data(), mclass.size() * 4, cudaMemcpyHostToDevice));
     if ((rc = device_records(A, s->bundles.as<BundleRec>(), order_d.as<int32_t>(), ntris, s->tris.as<TriRec>(),
-                             s->shade.as<ShadeRec>(), watertight)))
+                             s->shade.as<ShadeRec>(), watertight, mclass_d.as<int32_t>(), nmat)))
         return rc;
     const auto tb2 = std::chrono::steady_clock::now();
     if ((rc = s->mats_d.ensure(mats.size() * sizeof(MatRec))) ||
@@ -988,7 +1000,7 @@ extern "C" int bg_traversal_counts_noalloc(bg_scene* s, const bg_ray* rays, int6
     if (e == cudaSuccess && n > 0) {
         const float4* r4 = reinterpret_cast<const float4*>(rays);
         launch_layout(s, any_hit != 0, r4, n, nullptr, any_hit ? nullptr : hits, any_hit ? occ : nullptr, st, cnt, 1,
-                      work, nullptr, ShadowResolve{nullptr, nullptr, nullptr});
+                      work, nullptr, ShadowResolve{nullptr, nullptr, nullptr, 0});
         e = cudaGetLastError();
     }
     unsigned long long h[3] = {0, 0, 0};

@@ -159,22 +159,32 @@ int sah_binary_tree(const float* lo, const float* hi, int64_t n, int32_t* sorted
 struct MeshArrays {
     ScratchBuf verts, normals, uvs, vi, ni, ti, mat, offs, bundle, lo, hi, bbox;
 };
+// material class of a hit (bits 28-29 of a packed primid): 0 misses / emissive,
+// 1 Lambert, 2 GGX; primids stay below 2^27
+constexpr int kPrimMask = (1 << 28) - 1;
+constexpr int kClassShift = 28;
+
 int upload_mesh_arrays(const std::vector<MeshHost>& meshes, int64_t ntris, MeshArrays& A);
 // world boxes into A.lo / A.hi (Mesh::GetShapeWorldBounds) and the scene bounds of their finite values
 int device_world_boxes(MeshArrays& A, const BundleRec* bundles, int64_t ntris, float bbox_lo[3], float bbox_hi[3]);
 // traversal records in leaf order (order: device) and shading records in primitive order
 // vertices: the watertight test's records (p1, p2, p3) instead of (p1, e1, e2)
+// mat_class: class per material index (0 other, 1 Lambert, 2 GGX), stored in TriRec e2.w
 int device_records(const MeshArrays& A, const BundleRec* bundles, const int32_t* order, int64_t ntris,
-                   TriRec* tris, ShadeRec* shade, bool vertices);
+                   TriRec* tris, ShadeRec* shade, bool vertices, const int32_t* mat_class, int nmat);
 constexpr int kWorkSlots = 256;
 unsigned long long* next_work_counter(bg_scene* s);
 void scene_launch_setup(bg_scene* s);
-// Shadow-ray resolve fused into an any-hit trace: a ray that finds no occluder
-// stores contrib[i] into slots[slot_of[i]] instead of writing an occlusion byte.
+// Extras of a traversal launch.  Any hit: the shadow-ray resolve fused into the
+// trace (a ray that finds no occluder stores contrib[i] into slots[slot_of[i]]
+// instead of writing an occlusion byte).  Closest hit: hit_class != 0 packs the
+// material class of the hit triangle into bits 28-29 of the written primid
+// (the renderer's extension queues; see kPrimMask).
 struct ShadowResolve {
     const float4* contrib;
     const int* slot_of;
     float4* slots;
+    int hit_class;
 };
 int launch_trace(bg_scene* s, bool any_hit, const float4* rays, int64_t n_static, const int* n_dev,
                  bg_hit* hits, uint8_t* occ, cudaStream_t st, unsigned long long* counters = nullptr,

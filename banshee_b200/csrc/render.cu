@@ -154,6 +154,8 @@ void render_state_free(RenderState* rs) {
 
 enum : int { kCntExt0 = 0, kCntExt1 = 1, kCntSh = 2, kCntMis = 3, kCntEnd = 4, kCntQuery = 5, kCntTrain = 6 };
 constexpr int kCntCls = 12;   // three material-class counters (k_classify)
+// extension traces write the material class of each hit into its primid
+static const ShadowResolve kExtTrace{nullptr, nullptr, nullptr, 1};
 // shadow / MIS / ended-path counters of the odd bounces when direct light is
 // resolved one bounce late (the even bounces use kCntSh..kCntEnd)
 constexpr int kCntSh1 = 8;
@@ -415,7 +417,8 @@ __device__ __forceinline__ void shade_path(const DevScene& S, const ShadeArgs& A
     const size_t dhalf = A.defer ? size_t(h) * size_t(A.cap) : 0;
     {
         const int path = Q.ext_path_in[e];
-        const bg_hit hit = Q.ext_hits[e];
+        bg_hit hit = Q.ext_hits[e];
+        if (hit.primid >= 0) hit.primid &= kPrimMask;   // the material class rides in bits 28-29
         const float4 rd = Q.ext_rays_in[2 * e + 1];
         const v3 d = mk(rd.x, rd.y, rd.z);
         float4 r4 = P.rad[path];
@@ -585,40 +588,56 @@ k_shade(DevScene S, ShadeArgs A, PathState P, Queues Q) {
 
 // Splits the extension queue by material class: list c of Q.cls (entries
 // c * cap ..) receives the queue indices of the hits of class c (0 = misses and
-// emissive, 1 = Lambert, 2 = GGX), warp-aggregated, in queue order within a warp.
-__global__ void __launch_bounds__(kShadeThreads)
-k_classify(DevScene S, Queues Q, int cap) {
+// emissive, 1 = Lambert, 2 = GGX), in queue order within a block.  The class
+// comes with the hit (bits 28-29 of primid, written by the extension trace
+// from TriRec e2.w), so this reads 16 bytes per ray and makes three atomics
+// per block of kClassifyThreads rays.
+constexpr int kClassifyThreads = 512;
+__global__ void __launch_bounds__(kClassifyThreads)
+k_classify(Queues Q, int cap) {
+    __shared__ int wcount[kClassifyThreads / 32][3];
+    __shared__ int base[3];
     const int n = *Q.n_ext_in;
-    const int nthreads = gridDim.x * blockDim.x;
-    const unsigned lane = threadIdx.x & 31u;
-    for (int base = blockIdx.x * blockDim.x; base < n; base += nthreads) {
-        const int e = base + int(threadIdx.x);
+    const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    for (int start = blockIdx.x * kClassifyThreads; start < n; start += gridDim.x * kClassifyThreads) {
+        const int e = start + int(threadIdx.x);
         int cls = -1;
         if (e < n) {
             const int prim = Q.ext_hits[e].primid;
-            cls = 0;
-            if (prim >= 0) {
-                const int m = __float_as_int(__ldg(reinterpret_cast<const float*>(S.shade + prim) + 7));
-                const int t = __ldg(&S.mats[m].type);
-                cls = t == BG_MAT_LAMBERT ? 1 : t == BG_MAT_MICROFACET_GGX ? 2 : 0;
-            }
+            cls = prim < 0 ? 0 : (prim >> kClassShift) & 3;
         }
+        unsigned m[3];
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            const unsigned m = __ballot_sync(0xffffffffu, cls == c);
-            if (m == 0) continue;
-            const int leader = __ffs(m) - 1;
-            int at = 0;
-            if (lane == unsigned(leader)) at = atomicAdd(Q.n_cls + c, __popc(m));
-            at = __shfl_sync(0xffffffffu, at, leader);
-            if (cls == c) Q.cls[size_t(c) * cap + at + __popc(m & ((1u << lane) - 1u))] = e;
+            m[c] = __ballot_sync(0xffffffffu, cls == c);
+            if (lane == 0) wcount[warp][c] = __popc(m[c]);
         }
+        __syncthreads();
+        if (threadIdx.x < 3) {
+            const int c = int(threadIdx.x);
+            int tot = 0;
+            for (int w = 0; w < kClassifyThreads / 32; ++w) {
+                const int k = wcount[w][c];
+                wcount[w][c] = tot;                       // exclusive offset of warp w
+                tot += k;
+            }
+            base[c] = tot ? atomicAdd(Q.n_cls + c, tot) : 0;
+        }
+        __syncthreads();
+        if (cls >= 0) {
+            const unsigned mine = cls == 0 ? m[0] : cls == 1 ? m[1] : m[2];
+            Q.cls[size_t(cls) * cap + base[cls] + wcount[warp][cls] + __popc(mine & ((1u << lane) - 1u))] = e;
+        }
+        __syncthreads();
     }
 }
 
 // The hits of one material class (list MAT of k_classify).
+// 5 blocks of 128 threads per SM: 96 registers, no spills in the Lambert and
+// GGX class kernels (measured per step of C3: 8 blocks 9.6 ms of shading,
+// 6 blocks 9.3 ms, 5 blocks 8.8 ms)
 #ifndef BG_SHADE_CLASS_BLOCKS
-#define BG_SHADE_CLASS_BLOCKS 8
+#define BG_SHADE_CLASS_BLOCKS 5
 #endif
 template <int KIND, bool CACHE, bool AREA, int MAT>
 __global__ void __launch_bounds__(kShadeThreads, BG_SHADE_CLASS_BLOCKS)
@@ -642,7 +661,7 @@ template <int KIND, bool CACHE, bool AREA>
 static int launch_shade_split(const DevScene& d, int nb, int nbc, cudaStream_t st, const ShadeArgs& A,
                               const PathState& P, const Queues& Q) {
     BG_CUDA(cudaMemsetAsync(Q.n_cls, 0, 3 * sizeof(int), st));
-    k_classify<<<nb, kShadeThreads, 0, st>>>(d, Q, A.cap);
+    k_classify<<<nb, kClassifyThreads, 0, st>>>(Q, A.cap);
     k_shade_class<KIND, CACHE, AREA, kMatOther><<<nbc, kShadeThreads, 0, st>>>(d, A, P, Q);
     k_shade_class<KIND, CACHE, AREA, BG_MAT_LAMBERT><<<nbc, kShadeThreads, 0, st>>>(d, A, P, Q);
     k_shade_class<KIND, CACHE, AREA, BG_MAT_MICROFACET_GGX><<<nbc, kShadeThreads, 0, st>>>(d, A, P, Q);
@@ -1018,7 +1037,7 @@ static int enqueue_pass(bg_scene* s, RenderState* rs, cudaStream_t st, const Pas
             BG_CUDA(cudaMemsetAsync(cnt + (par ? kCntSh1 : kCntSh), 0, 3 * sizeof(int), st));
             if (b == 0) {
                 if ((rc = launch_trace(s, false, Q.ext_rays_in, 0, Q.n_ext_in, Q.ext_hits, nullptr, st, nullptr, 1, wk,
-                                       Q.ext_root_in)))
+                                       Q.ext_root_in, &kExtTrace)))
                     return rc;
                 if (ins) { ++ins->launches; ++ins->launches_extend; }
             }
@@ -1047,7 +1066,7 @@ static int enqueue_pass(bg_scene* s, RenderState* rs, cudaStream_t st, const Pas
                 Queues Qn;
                 pass_queues(rs, cur, c.batched, Qn, par ^ 1);
                 if ((rc = launch_trace(s, false, Qn.ext_rays_in, 0, Qn.n_ext_in, Qn.ext_hits, nullptr, st, nullptr, 1,
-                                       wk + 6, Qn.ext_root_in)))
+                                       wk + 6, Qn.ext_root_in, &kExtTrace)))
                     return rc;
                 if (ins) { ++ins->launches; ++ins->launches_extend; }
             }
@@ -1060,7 +1079,7 @@ static int enqueue_pass(bg_scene* s, RenderState* rs, cudaStream_t st, const Pas
         BG_CUDA(cudaMemsetAsync(cnt + kCntSh, 0, 3 * sizeof(int), st));
         if (!fork || b == 0) {
             if (ins) ins->mark(0);
-            if ((rc = launch_trace(s, false, Q.ext_rays_in, 0, Q.n_ext_in, Q.ext_hits, nullptr, st, nullptr, 1, wk, Q.ext_root_in))) return rc;
+            if ((rc = launch_trace(s, false, Q.ext_rays_in, 0, Q.n_ext_in, Q.ext_hits, nullptr, st, nullptr, 1, wk, Q.ext_root_in, &kExtTrace))) return rc;
             if (ins) { ins->mark(0); ++ins->launches; ++ins->launches_extend; }
         }
         if (ins && ins->count_trav) {
@@ -1086,7 +1105,7 @@ static int enqueue_pass(bg_scene* s, RenderState* rs, cudaStream_t st, const Pas
             BG_CUDA(cudaEventRecord(rs->ev_fork, st));
             BG_CUDA(cudaStreamWaitEvent(rs->fstream, rs->ev_fork, 0));
             if ((rc = launch_trace(s, false, Qn.ext_rays_in, 0, Qn.n_ext_in, Qn.ext_hits, nullptr, rs->fstream, nullptr, 1,
-                                   wk + 6, Qn.ext_root_in)))
+                                   wk + 6, Qn.ext_root_in, &kExtTrace)))
                 return rc;
             BG_CUDA(cudaEventRecord(rs->ev_join, rs->fstream));
             if (ins) { ++ins->launches; ++ins->launches_extend; }
@@ -1094,10 +1113,12 @@ static int enqueue_pass(bg_scene* s, RenderState* rs, cudaStream_t st, const Pas
         if (fork) {   // MIS trace and its resolve beside the shadow trace (they write different slots)
             if (!forked) BG_CUDA(cudaEventRecord(rs->ev_fork, st));
             BG_CUDA(cudaStreamWaitEvent(rs->mstream, rs->ev_fork, 0));
-            if ((rc = launch_trace(s, false, Q.mis_rays, 0, Q.n_mis, Q.mis_hits, nullptr, rs->mstream, nullptr, 1, wk + 3,
-                                   Q.mis_root)))
-                return rc;
-            k_resolve_mis<<<nb, kShadeThreads, 0, rs->mstream>>>(s->dev, P, Q);
+            if (s->dev.has_area) {   // MIS rays go to area lights only (the queue is empty otherwise)
+                if ((rc = launch_trace(s, false, Q.mis_rays, 0, Q.n_mis, Q.mis_hits, nullptr, rs->mstream, nullptr, 1,
+                                       wk + 3, Q.mis_root)))
+                    return rc;
+                k_resolve_mis<<<nb, kShadeThreads, 0, rs->mstream>>>(s->dev, P, Q);
+            }
             if (query_here) {   // the cache query too: it adds to P.rad of ended paths, the resolves write P.slots
                 if (wait_here)
                     BG_CUDA(cudaStreamWaitEvent(rs->mstream, rs->ev_train, ins ? 0u : unsigned(cudaEventWaitExternal)));
@@ -1113,16 +1134,17 @@ static int enqueue_pass(bg_scene* s, RenderState* rs, cudaStream_t st, const Pas
         if ((rc = launch_trace(s, true, Q.sh_rays, 0, Q.n_sh, nullptr, nullptr, st, nullptr, 1, wk + 2, Q.sh_root, &sr)))
             return rc;
         if (ins) { ins->mark(1); ins->mark(2); }
-        if (!fork && (rc = launch_trace(s, false, Q.mis_rays, 0, Q.n_mis, Q.mis_hits, nullptr, st, nullptr, 1, wk + 3, Q.mis_root)))
+        if (!fork && s->dev.has_area &&
+            (rc = launch_trace(s, false, Q.mis_rays, 0, Q.n_mis, Q.mis_hits, nullptr, st, nullptr, 1, wk + 3, Q.mis_root)))
             return rc;
-        if (ins) { ins->mark(2); ins->launches += 2; }
+        if (ins) { ins->mark(2); ins->launches += s->dev.has_area ? 2 : 1; }
         if (ins && ins->count_trav) {
             if ((rc = launch_trace(s, true, Q.sh_rays, 0, Q.n_sh, nullptr, cnt_occ, st, Q.totals + 6, 64, wk + 4, Q.sh_root))) return rc;
             if ((rc = launch_trace(s, false, Q.mis_rays, 0, Q.n_mis, cnt_hits, nullptr, st, Q.totals + 9, 64, wk + 5, Q.mis_root))) return rc;
             ins->launches += 2;
         }
         if (fork) BG_CUDA(cudaStreamWaitEvent(st, rs->ev_mjoin, 0));
-        else k_resolve_mis<<<nb, kShadeThreads, 0, st>>>(s->dev, P, Q);
+        else if (s->dev.has_area) k_resolve_mis<<<nb, kShadeThreads, 0, st>>>(s->dev, P, Q);
         if (query_here && !fork) {
             // paths that ended into the cache here: encode, infer, add throughput * prediction
             if (ins) ins->mark(3);
@@ -1134,7 +1156,7 @@ static int enqueue_pass(bg_scene* s, RenderState* rs, cudaStream_t st, const Pas
         }
         k_finalize<<<nb, kShadeThreads, 0, st>>>(P, Q, rs->kmax, c.maxdepth, c.cache ? c.train_stride : 0,
                                                  c.cache ? c.cache_depth : 0, b, 0, int(rs->cap));
-        if (ins) ins->launches += 2;
+        if (ins) ins->launches += s->dev.has_area ? 2 : 1;
         if (forked) BG_CUDA(cudaStreamWaitEvent(st, rs->ev_join, 0));
         cur = 1 - cur;
         pass_queues(rs, cur, c.batched, Q);

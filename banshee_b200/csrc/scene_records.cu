@@ -92,7 +92,8 @@ __global__ void k_world_boxes(int64_t ntris, const int32_t* __restrict__ bundle,
 __global__ void k_tri_records(int64_t ntris, const int32_t* __restrict__ order, const int32_t* __restrict__ bundle,
                               const MeshOff* __restrict__ offs, const float* __restrict__ verts,
                               const int32_t* __restrict__ vi, const BundleRec* __restrict__ bundles,
-                              TriRec* __restrict__ tris, int vertices) {
+                              TriRec* __restrict__ tris, int vertices, const int32_t* __restrict__ mat,
+                              const int32_t* __restrict__ mat_class, int nmat) {
     for (int64_t k = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; k < ntris; k += int64_t(gridDim.x) * blockDim.x) {
         const int64_t t = order[k];
         const int b = bundle[t];
@@ -104,7 +105,8 @@ __global__ void k_tri_records(int64_t ntris, const int32_t* __restrict__ order, 
         TriRec r;
         r.v0 = make_float4(p1.x, p1.y, p1.z, __int_as_float(bcode));
         r.e1 = make_float4(e1.x, e1.y, e1.z, __int_as_float(int32_t(t)));
-        r.e2 = make_float4(e2.x, e2.y, e2.z, 0.f);
+        const int m = mat[t];
+        r.e2 = make_float4(e2.x, e2.y, e2.z, __int_as_float(m >= 0 && m < nmat ? mat_class[m] : 0));
         tris[k] = r;
     }
 }
@@ -202,9 +204,10 @@ int device_world_boxes(MeshArrays& A, const BundleRec* bundles, int64_t ntris, f
 }
 
 int device_records(const MeshArrays& A, const BundleRec* bundles, const int32_t* order, int64_t ntris, TriRec* tris,
-                   ShadeRec* shade, bool vertices) {
+                   ShadeRec* shade, bool vertices, const int32_t* mat_class, int nmat) {
     k_tri_records<<<grid_for(ntris), kRT>>>(ntris, order, A.bundle.as<int32_t>(), A.offs.as<MeshOff>(),
-                                            A.verts.as<float>(), A.vi.as<int32_t>(), bundles, tris, vertices ? 1 : 0);
+                                            A.verts.as<float>(), A.vi.as<int32_t>(), bundles, tris, vertices ? 1 : 0,
+                                            A.mat.as<int32_t>(), mat_class, nmat);
     k_shade_records<<<grid_for(ntris), kRT>>>(ntris, A.bundle.as<int32_t>(), A.offs.as<MeshOff>(), A.verts.as<float>(),
                                               A.normals.as<float>(), A.uvs.as<float>(), A.vi.as<int32_t>(),
                                               A.ni.as<int32_t>(), A.ti.as<int32_t>(), A.mat.as<int32_t>(), shade);

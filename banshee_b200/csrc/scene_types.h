@@ -17,9 +17,10 @@ namespace bg {
 
 // Moller-Trumbore operands in object space: v0 = p1, e1 = p2 - p1, e2 = p3 - p1
 // (computed once with the same float subtraction as primitive/mesh.cpp:13-14).
-// v0.w = bundle index (int bits), e1.w = global primitive id (int bits).  A
-// scene committed with the watertight test holds the vertices themselves:
-// v0 = p1, e1 = p2, e2 = p3 (same .w fields).
+// v0.w = bundle index (int bits), e1.w = global primitive id (int bits), e2.w
+// = material class of the face (int bits: 0 emissive, 1 Lambert, 2 GGX; what
+// the renderer splits its shading by).  A scene committed with the watertight
+// test holds the vertices themselves: v0 = p1, e1 = p2, e2 = p3 (same .w fields).
 struct alignas(16) TriRec {
     float4 v0, e1, e2;
 };

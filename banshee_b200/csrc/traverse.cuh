@@ -37,19 +37,15 @@ __host__ __device__ constexpr int stack_entries() { return WIDTH == 8 ? kStackSi
 constexpr int kRefillStepsClosest = 24;
 constexpr int kRefillStepsAny = 16;
 constexpr float kBoxSlack = 4e-7f;
-
-#ifndef BG_BOX_FMA
-#define BG_BOX_FMA 1
-#endif
+// (Measured and rejected: slab distances as one fmaf(P, 1/d, -o/d) each, with a
+// per-ray absolute error bound added to the slack.  The bound, 2^-24 max|o/d|,
+// is huge for rays nearly parallel to an axis, so such rays visited most of the
+// tree: C3 ran at 8 instead of 500 Msamples/s.)
 
 struct Ray {
     v3 o, d, inv;
     float tmin, tmax;
     uint32_t oct;    // bit k set: direction component k is negative (sign of 1/d)
-#if BG_BOX_FMA
-    v3 oinv;         // o * inv, rounded: a slab distance is fmaf(P, inv, -oinv)
-    float eabs;      // bound on the absolute rounding error that adds: 2^-24 max |o * inv| (+ margin)
-#endif
 };
 
 __device__ __forceinline__ Ray make_ray(float4 a, float4 b) {
@@ -58,10 +54,6 @@ __device__ __forceinline__ Ray make_ray(float4 a, float4 b) {
     r.d = mk(b.x, b.y, b.z); r.tmax = b.w;
     r.inv = mk(1.f / r.d.x, 1.f / r.d.y, 1.f / r.d.z);
     r.oct = (signbit(r.inv.x) ? 1u : 0u) | (signbit(r.inv.y) ? 2u : 0u) | (signbit(r.inv.z) ? 4u : 0u);
-#if BG_BOX_FMA
-    r.oinv = mk(r.o.x * r.inv.x, r.o.y * r.inv.y, r.o.z * r.inv.z);
-    r.eabs = fmaxf(fmaxf(fabsf(r.oinv.x), fabsf(r.oinv.y)), fabsf(r.oinv.z)) * 6.0e-8f;
-#endif
     return r;
 }
 
@@ -183,17 +175,6 @@ __device__ __forceinline__ uint32_t box4(const WideNode4* __restrict__ nodes, in
     uint32_t mask = 0;
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-#if BG_BOX_FMA
-        float ax = fmaf(nxa[i], r.inv.x, -r.oinv.x);
-        float bx = fmaf(fxa[i], r.inv.x, -r.oinv.x);
-        float ay = fmaf(nya[i], r.inv.y, -r.oinv.y);
-        float by = fmaf(fya[i], r.inv.y, -r.oinv.y);
-        float az = fmaf(nza[i], r.inv.z, -r.oinv.z);
-        float bz = fmaf(fza[i], r.inv.z, -r.oinv.z);
-        float t0 = fmaxf(fmaxf(ax, ay), fmaxf(az, r.tmin)) - r.eabs;
-        float t1 = fminf(fminf(bx, by), fminf(bz, best));
-        t1 = fmaf(fabsf(t1), kBoxSlack, t1) + r.eabs;
-#else
         float ax = (nxa[i] - r.o.x) * r.inv.x;
         float bx = (fxa[i] - r.o.x) * r.inv.x;
         float ay = (nya[i] - r.o.y) * r.inv.y;
@@ -203,7 +184,6 @@ __device__ __forceinline__ uint32_t box4(const WideNode4* __restrict__ nodes, in
         float t0 = fmaxf(fmaxf(ax, ay), fmaxf(az, r.tmin));
         float t1 = fminf(fminf(bx, by), fminf(bz, best));
         t1 = t1 + fabsf(t1) * kBoxSlack;
-#endif
         tn[i] = t0;
         if (t0 <= t1) mask |= 1u << i;
     }
@@ -248,17 +228,6 @@ __device__ __forceinline__ uint32_t box8(const QNode8* __restrict__ nodes, int n
         const float fqy = __uint_as_float(__byte_perm(i < 4 ? qfy.x : qfy.y, 0x4B000000u, sel));
         const float nqz = __uint_as_float(__byte_perm(i < 4 ? qnz.x : qnz.y, 0x4B000000u, sel));
         const float fqz = __uint_as_float(__byte_perm(i < 4 ? qfz.x : qfz.y, 0x4B000000u, sel));
-#if BG_BOX_FMA
-        const float ax = fmaf(fmaf(nqx, sx, hd.x), r.inv.x, -r.oinv.x);
-        const float bx = fmaf(fmaf(fqx, sx, hd.x), r.inv.x, -r.oinv.x);
-        const float ay = fmaf(fmaf(nqy, sy, hd.y), r.inv.y, -r.oinv.y);
-        const float by = fmaf(fmaf(fqy, sy, hd.y), r.inv.y, -r.oinv.y);
-        const float az = fmaf(fmaf(nqz, sz, hd.z), r.inv.z, -r.oinv.z);
-        const float bz = fmaf(fmaf(fqz, sz, hd.z), r.inv.z, -r.oinv.z);
-        float t0 = fmaxf(fmaxf(ax, ay), fmaxf(az, r.tmin)) - r.eabs;
-        float t1 = fminf(fminf(bx, by), fminf(bz, best));
-        t1 = fmaf(fabsf(t1), kBoxSlack, t1) + r.eabs;
-#else
         const float ax = (fmaf(nqx, sx, hd.x) - r.o.x) * r.inv.x;
         const float bx = (fmaf(fqx, sx, hd.x) - r.o.x) * r.inv.x;
         const float ay = (fmaf(nqy, sy, hd.y) - r.o.y) * r.inv.y;
@@ -268,7 +237,6 @@ __device__ __forceinline__ uint32_t box8(const QNode8* __restrict__ nodes, int n
         float t0 = fmaxf(fmaxf(ax, ay), fmaxf(az, r.tmin));
         float t1 = fminf(fminf(bx, by), fminf(bz, best));
         t1 = t1 + fabsf(t1) * kBoxSlack;
-#endif
         tn[i] = t0;
         if (t0 <= t1) mask |= 1u << i;
     }
@@ -311,6 +279,7 @@ struct TravState {
     typename std::conditional<WT, ObjRayWT, ObjRay>::type cache;
     float best, u, v;
     int prim;
+    int cls;        // material class of the closest hit so far (TriRec e2.w)
     int item;       // current node / leaf code; kNone when the stack must be popped
     int sp;
 };
@@ -322,6 +291,7 @@ __device__ __forceinline__ void trav_init(TS& s, float4 a, float4 b) {
     s.cache.bundle = -2;
     s.best = s.r.tmax;
     s.prim = -1;
+    s.cls = 0;
     s.u = s.v = 0.f;
     s.item = 0;      // root
     s.sp = 0;
@@ -434,6 +404,7 @@ __device__ __forceinline__ bool trav_leaf(const DevScene& S, TravState<WT>& s, i
             s.prim = __float_as_int(e1.w);
             if (ANY) return true;
             s.best = t; s.u = a; s.v = b;
+            s.cls = __float_as_int(e2.w);
         }
     }
     return false;

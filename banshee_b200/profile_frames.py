@@ -4,10 +4,11 @@
   python -m banshee_b200.profile_frames --workload c5 --frames 2
   python -m banshee_b200.profile_frames --workload c2 [--width 8]
 
-c3: the 6.09M-triangle production scene at 1920x1080, plain GiTracer(8), one
-    camera sample per pixel per frame (one pass of 2^21 paths, 128-thread
-    traversal blocks: no autotuning); k_trace launches per bounce are, in
-    capture order, extension (closest hit), shadow (any hit), MIS (closest hit).
+c3: the 6.09M-triangle production scene at 1920x1080, plain GiTracer(8), --spp
+    camera samples per pixel per frame (default 1: one pass of 2^21 paths;
+    128-thread traversal blocks: no autotuning); k_trace launches per bounce
+    are, in capture order, extension (closest hit) and shadow (any hit), plus
+    MIS (closest hit) in scenes with area lights.
 c5: the same scene through the radiance cache (2^19-entry hash grid levels,
     65,536 training paths per frame ending into the cache one bounce after the
     rendering paths, which end after 2 bounces; training one frame behind).
@@ -25,6 +26,7 @@ def main():
     ap.add_argument("--workload", choices=["c2", "c3", "c5"], default="c3")
     ap.add_argument("--frames", type=int, default=1)
     ap.add_argument("--width", type=int, default=0, help="node layout (4 or 8; 0 = scene default)")
+    ap.add_argument("--spp", type=int, default=1, help="camera samples per pixel per frame (c3, c5)")
     args = ap.parse_args()
     import numpy as np
     import torch
@@ -55,10 +57,11 @@ def main():
                                        learning_rate=1e-2, train_suffix=1)
 
             def frame(f):
-                cache.render(acc.data_ptr(), 1920, 1080, 1, seed=1, sample_offset=f, maxdepth=8)
+                cache.render(acc.data_ptr(), 1920, 1080, args.spp, seed=1, sample_offset=f * args.spp, maxdepth=8)
         else:
             def frame(f):
-                gs.render(acc.data_ptr(), 1920, 1080, 1, seed=1, sample_offset=f, maxdepth=8, stats=False)
+                gs.render(acc.data_ptr(), 1920, 1080, args.spp, seed=1, sample_offset=f * args.spp, maxdepth=8,
+                          stats=False)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     e0.record()

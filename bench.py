@@ -397,6 +397,7 @@ def _ratio(a, b):
     return (a / b) if (a and b) else None
 
 
+WARM_FRAMES, WARM_W, WARM_H = 32, 384, 216   # the cache's training-only warm-up frames
 CACHE_CFG = dict(log2_table_size=19, base_resolution=16, max_resolution=2048, train_paths=65536, cache_depth=2,
                  train_batch=65536, train_steps=1, learning_rate=1e-2, train_suffix=1)
 CACHE_DESC = ("hash grid 16 levels x 2 features, 2^19 entries/level, res 16..2048; MLP 64x5 bf16; Adam lr 1e-2; "
@@ -411,8 +412,10 @@ def time_to_relmse(gs, sc, args, target=1e-3):
     plain GiTracer(8) render at args.gt_spp spp accumulated in float64 (the
     reference's own noise, estimated from two halves, subtracted).  The plain
     tracer runs at 1 spp per frame and at SPP per call (its throughput
-    configuration, the headline comparison); the cache renders 1 spp per frame
-    and trains once per frame.  The cache's bias floor is its error, after
+    configuration, the headline comparison); the cache renders SPP per frame
+    after 32 training-only frames (every path of a 384x216 frame trains; their
+    time counts) and trains once per frame; it is also timed at 1 spp per frame
+    against the plain tracer at 1 spp per frame.  The cache's bias floor is its error, after
     convergence, once its image noise and the reference's are taken out.  The
     bound for any cache that ends paths after 2 bounces is the plain tracer
     truncated there (max depth 2) against its own float64 reference."""
@@ -436,18 +439,35 @@ def time_to_relmse(gs, sc, args, target=1e-3):
     torch.cuda.synchronize()
     warm.close()
     del wbuf
+    # the cache at 1 spp per frame (one Adam step per frame)
+    cache1 = capi.RadianceCache(gs, **CACHE_CFG)
+    cached1 = run(lambda p, f: cache1.render(p, WIDTH, HEIGHT, 1, seed=SEED, sample_offset=f, maxdepth=MAXDEPTH), 4)
+    cache1.close()
+    # the cache at its throughput configuration: WARM_FRAMES training-only frames
+    # (the same camera at 384x216, 1 spp: every path is a training path, nothing
+    # is kept), then SPP samples per pixel per frame; the warm-up is timed
     cache = capi.RadianceCache(gs, **CACHE_CFG)
-    render_cached = lambda p, f: cache.render(p, WIDTH, HEIGHT, 1, seed=SEED, sample_offset=f, maxdepth=MAXDEPTH)
-    cached = run(render_cached, 4)
+    scratch = torch.zeros((WARM_H, WARM_W, 4), dtype=torch.float32, device="cuda")
+
+    def render_cached(p, f):
+        if f < WARM_FRAMES:
+            cache.render(scratch.data_ptr(), WARM_W, WARM_H, 1, seed=SEED + 99, sample_offset=f, maxdepth=MAXDEPTH)
+        else:
+            cache.render(p, WIDTH, HEIGHT, SPP, seed=SEED, sample_offset=(f - WARM_FRAMES) * SPP, maxdepth=MAXDEPTH)
+
+    cached = run(render_cached, 1)
     # the cache keeps training while the floor is measured
-    floor = CV.bias_floor(render_cached, WIDTH, HEIGHT, gt, gt_var, args.floor_frames, first_frame=cached["frames"])
+    floor = CV.bias_floor(lambda p, f: cache.render(p, WIDTH, HEIGHT, SPP, seed=SEED, sample_offset=f * SPP,
+                                                    maxdepth=MAXDEPTH),
+                          WIDTH, HEIGHT, gt, gt_var, args.floor_frames, first_frame=cached["frames"])
     cache.close()
+    del scratch
     gt2, gt2_var, gt2_s, _ = _ground_truth(gs, args, 2, args.gt_spp_bound)
     trunc = CV.converge_frame(lambda p, f: gs.render(p, WIDTH, HEIGHT, 1, seed=SEED, sample_offset=f, maxdepth=2,
                                                      stats=False),
                               WIDTH, HEIGHT, gt2, gt2_var, args.conv_seconds, 100000, target=target, every=4)
     del gt, gt_var, gt2, gt2_var
-    ratio = _ratio(cached["t_target"], plain["t_target"])
+    ratio = _ratio(cached1["t_target"], plain["t_target"])
     ratio_spp = _ratio(cached["t_target"], plain_spp["t_target"])
     bound = _ratio(trunc["t_target"], plain["t_target"])
     return {"target_relmse": target, "frame": [WIDTH, HEIGHT], "reference_spp": args.gt_spp,
@@ -457,8 +477,9 @@ def time_to_relmse(gs, sc, args, target=1e-3):
                       "reference's own variance (from its two halves)",
             "cache_config": CACHE_DESC,
             "plain": _summ(plain), "plain_spp_per_call": {"spp_per_call": SPP, **_summ(plain_spp)},
-            "cache": _summ(cached), "cache_bias_floor": floor,
-            "cache_over_plain_time": ratio, "cache_over_plain_spp_per_call_time": ratio_spp,
+            "cache": {"spp_per_frame": SPP, "warm_up_frames": [WARM_FRAMES, WARM_W, WARM_H], **_summ(cached)},
+            "cache_1spp": _summ(cached1), "cache_bias_floor": floor,
+            "cache_over_plain_time": ratio_spp, "cache_1spp_over_plain_1spp_time": ratio,
             "perfect_cache_bound": {
                 "what": "plain tracer truncated after 2 bounces (max depth 2) against its own reference at "
                         "%d spp: the time-to-target of a free, exact cache ending paths there" % args.gt_spp_bound,
