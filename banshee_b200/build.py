@@ -2,7 +2,8 @@
 
 nvcc compiles every .cu for sm_100a only (-gencode arch=compute_100a,code=sm_100a)
 with -fmad=false and IEEE division / square root, which the bit-exact
-Moller-Trumbore path relies on.  Host C++ is compiled by g++ with
+Moller-Trumbore path relies on (cache.cu, the radiance cache, is off that path
+and contracts multiply-adds).  Host C++ is compiled by g++ with
 -ffp-contract=off.  No GPU is needed to build.
 """
 import os
@@ -21,6 +22,11 @@ CXX_SOURCES = ["bvh_build.cpp", "image.cpp"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false",
               "-Xcompiler", "-fPIC,-ffp-contract=off", "--expt-relaxed-constexpr", "-Xptxas", "-warn-spills"]
+
+
+# The radiance cache's kernels (encoding, MLP, Adam) are not part of the
+# bit-exact path: they may contract multiply-adds.
+FMAD_FILES = {"cache.cu"}
 
 
 def _newer(target, deps):
@@ -45,7 +51,8 @@ def build(verbose=False, force=False):
             continue
         path = os.path.join(CSRC, src)
         if src.endswith(".cu"):
-            cmd = [NVCC] + NVCC_FLAGS + ["-c", path, "-o", obj]
+            flags = [("-fmad=true" if (f == "-fmad=false" and src in FMAD_FILES) else f) for f in NVCC_FLAGS]
+            cmd = [NVCC] + flags + ["-c", path, "-o", obj]
         else:
             cmd = ["g++", "-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-pthread",
                    "-I" + os.path.join(CUDA_HOME, "include"), "-c", path, "-o", obj]

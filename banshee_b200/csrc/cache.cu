@@ -148,6 +148,12 @@ __device__ __forceinline__ void mlp_forward(const __nv_bfloat16* sw, const uint3
     mlp_layer<4, 2>(h[4], sw + kFwW5, kS5, out);
 }
 
+// two floats -> bf16 pair (round to nearest even), low half first
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+    const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<const uint32_t*>(&v);
+}
+
 // ------------------------------------------------------------- encoding
 __device__ __forceinline__ uint32_t grid_index(const NrcDev& C, int level, int x, int y, int z) {
     const uint32_t T = 1u << C.log2_T;
@@ -175,11 +181,12 @@ __device__ __forceinline__ void norm_pos(const NrcDev& C, const float* f, float*
     for (int k = 0; k < 3; ++k) u[k] = fminf(fmaxf((f[k] - C.bmin[k]) * C.bscale[k], 0.f), 1.f);
 }
 
-__device__ __forceinline__ void one_blob(float v, __nv_bfloat16* dst) {
+// one-blob encoding of v in [0,1] into 16 bf16 values, packed two per word
+__device__ __forceinline__ void one_blob(float v, uint32_t* w) {
 #pragma unroll
-    for (int b = 0; b < 16; ++b) {
-        float d = v - (b + 0.5f) * (1.f / 16.f);
-        dst[b] = __float2bfloat16_rn(__expf(-d * d * 128.f));
+    for (int b = 0; b < 16; b += 2) {
+        const float d0 = v - (b + 0.5f) * (1.f / 16.f), d1 = v - (b + 1.5f) * (1.f / 16.f);
+        w[b / 2] = pack_bf16(__expf(-d0 * d0 * 128.f), __expf(-d1 * d1 * 128.f));
     }
 }
 
@@ -188,52 +195,51 @@ __device__ __forceinline__ void sph(float x, float y, float z, float& th, float&
     ph = atan2f(y, x) * (0.5f / BG_PI) + 0.5f;
 }
 
-// raw query records [n][16] -> encoded bf16 rows [n][128]
+// raw query records [n][16] -> encoded bf16 rows [n][128].  The row is built in
+// 64 registers (two bf16 per word, every index static) and stored as 16-byte
+// chunks: no local-memory copy of the row.
 __global__ void __launch_bounds__(128) k_nrc_encode(NrcDev C, const float* __restrict__ feat, const int* n_dev, int64_t n_static,
                                                     int offset, int limit, __nv_bfloat16* __restrict__ X) {
     int64_t n = n_dev ? int64_t(*n_dev) : n_static;
     n = n - offset;
     if (limit > 0 && n > limit) n = limit;
     for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
-        const float* f = feat + (size_t(offset) + size_t(i)) * kNrcFeatFloats;
-        float fr[13];
-#pragma unroll
-        for (int k = 0; k < 13; ++k) fr[k] = f[k];
-        __nv_bfloat16 row[kNrcIn];
+        const float4* f4 = reinterpret_cast<const float4*>(feat + (size_t(offset) + size_t(i)) * kNrcFeatFloats);
+        const float4 q0 = f4[0], q1 = f4[1], q2 = f4[2], q3 = f4[3];
+        const float fr[13] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w, q2.x, q2.y, q2.z, q2.w, q3.x};
+        uint32_t w[kNrcIn / 2];
         float u[3];
         norm_pos(C, fr, u);
+#pragma unroll
         for (int l = 0; l < kNrcLevels; ++l) {
             GridCorner g = grid_cell(C, l, u);
             float a0 = 0.f, a1 = 0.f;
 #pragma unroll
             for (int cidx = 0; cidx < 8; ++cidx) {
                 const int dx = cidx & 1, dy = (cidx >> 1) & 1, dz = (cidx >> 2) & 1;
-                const float w = (dx ? g.fx : 1.f - g.fx) * (dy ? g.fy : 1.f - g.fy) * (dz ? g.fz : 1.f - g.fz);
+                const float wt = (dx ? g.fx : 1.f - g.fx) * (dy ? g.fy : 1.f - g.fy) * (dz ? g.fz : 1.f - g.fz);
                 const uint32_t idx = grid_index(C, l, g.x0 + dx, g.y0 + dy, g.z0 + dz);
-                const float2 v = *reinterpret_cast<const float2*>(C.grid + (size_t(l) << C.log2_T) * 2 + size_t(idx) * 2);
-                a0 += w * v.x;
-                a1 += w * v.y;
+                const float2 v = __ldg(reinterpret_cast<const float2*>(C.grid + (size_t(l) << C.log2_T) * 2 + size_t(idx) * 2));
+                a0 += wt * v.x;
+                a1 += wt * v.y;
             }
-            row[2 * l] = __float2bfloat16_rn(a0);
-            row[2 * l + 1] = __float2bfloat16_rn(a1);
+            w[l] = pack_bf16(a0, a1);
         }
         float th, ph;
         sph(fr[3], fr[4], fr[5], th, ph);
-        one_blob(th, row + 32);
-        one_blob(ph, row + 48);
+        one_blob(th, w + 16);
+        one_blob(ph, w + 24);
         sph(fr[6], fr[7], fr[8], th, ph);
-        one_blob(th, row + 64);
-        one_blob(ph, row + 80);
-        row[96] = __float2bfloat16_rn(fr[9]);
-        row[97] = __float2bfloat16_rn(fr[10]);
-        row[98] = __float2bfloat16_rn(fr[11]);
-        row[99] = __float2bfloat16_rn(fr[12]);
-        row[100] = __float2bfloat16_rn(1.f);
-        for (int k = 101; k < kNrcIn; ++k) row[k] = __float2bfloat16_rn(0.f);
-        uint4* dst = reinterpret_cast<uint4*>(X + size_t(i) * kNrcIn);
-        const uint4* src = reinterpret_cast<const uint4*>(row);
+        one_blob(th, w + 32);
+        one_blob(ph, w + 40);
+        w[48] = pack_bf16(fr[9], fr[10]);
+        w[49] = pack_bf16(fr[11], fr[12]);
+        w[50] = pack_bf16(1.f, 0.f);
 #pragma unroll
-        for (int k = 0; k < kNrcIn / 8; ++k) dst[k] = src[k];
+        for (int k = 51; k < kNrcIn / 2; ++k) w[k] = 0u;
+        uint4* dst = reinterpret_cast<uint4*>(X + size_t(i) * kNrcIn);
+#pragma unroll
+        for (int k = 0; k < kNrcIn / 8; ++k) dst[k] = make_uint4(w[4 * k], w[4 * k + 1], w[4 * k + 2], w[4 * k + 3]);
     }
 }
 

@@ -636,11 +636,9 @@ k_classify(Queues Q, int cap) {
 // 5 blocks of 128 threads per SM: 96 registers, no spills in the Lambert and
 // GGX class kernels (measured per step of C3: 8 blocks 9.6 ms of shading,
 // 6 blocks 9.3 ms, 5 blocks 8.8 ms)
-#ifndef BG_SHADE_CLASS_BLOCKS
-#define BG_SHADE_CLASS_BLOCKS 5
-#endif
+constexpr int kShadeClassBlocks = 5;
 template <int KIND, bool CACHE, bool AREA, int MAT>
-__global__ void __launch_bounds__(kShadeThreads, BG_SHADE_CLASS_BLOCKS)
+__global__ void __launch_bounds__(kShadeThreads, kShadeClassBlocks)
 k_shade_class(DevScene S, ShadeArgs A, PathState P, Queues Q) {
     constexpr int c = MAT == BG_MAT_LAMBERT ? 1 : MAT == BG_MAT_MICROFACET_GGX ? 2 : 0;
     const int n = Q.n_cls[c];
@@ -651,12 +649,10 @@ k_shade_class(DevScene S, ShadeArgs A, PathState P, Queues Q) {
         shade_path<KIND, CACHE, AREA, MAT>(S, A, P, Q, list[i]);
 }
 
-#ifndef BG_SHADE_SPLIT
-#define BG_SHADE_SPLIT 1
-#endif
-
 // Material-class kernels of one configuration: classify, then misses and
 // emissive hits, Lambert hits and GGX hits, each by its own kernel.
+// (Measured: one kernel for every material, 64 registers and out-of-line BSDF
+// calls, shaded a C3 step in 11.6 ms; the class kernels take 6.3 ms.)
 template <int KIND, bool CACHE, bool AREA>
 static int launch_shade_split(const DevScene& d, int nb, int nbc, cudaStream_t st, const ShadeArgs& A,
                               const PathState& P, const Queues& Q) {
@@ -668,8 +664,9 @@ static int launch_shade_split(const DevScene& d, int nb, int nbc, cudaStream_t s
     return BG_OK;
 }
 
-// The shading kernel(s) for a tracer kind, cache mode and the scene's lights.
-// Returns the number of kernels launched (< 0: an error code).
+// The shading kernels for a tracer kind, cache mode and the scene's lights.
+// Returns the number of kernels launched (< 0: an error code).  AoTracer has no
+// BSDF: its paths are shaded by one kernel.
 static int launch_shade(const DevScene& d, int kind, bool cache, int nb, int nbc, cudaStream_t st,
                         const ShadeArgs& A, const PathState& P, const Queues& Q) {
     const bool area = d.has_area != 0;
@@ -677,30 +674,17 @@ static int launch_shade(const DevScene& d, int kind, bool cache, int nb, int nbc
         k_shade<BG_TRACER_AO, false, false><<<nb, kShadeThreads, 0, st>>>(d, A, P, Q);
         return 1;
     }
-    if (BG_SHADE_SPLIT) {
-        int rc;
-        if (kind == BG_TRACER_DI)
-            rc = area ? launch_shade_split<BG_TRACER_DI, false, true>(d, nb, nbc, st, A, P, Q)
-                      : launch_shade_split<BG_TRACER_DI, false, false>(d, nb, nbc, st, A, P, Q);
-        else if (cache)
-            rc = area ? launch_shade_split<BG_TRACER_GI, true, true>(d, nb, nbc, st, A, P, Q)
-                      : launch_shade_split<BG_TRACER_GI, true, false>(d, nb, nbc, st, A, P, Q);
-        else
-            rc = area ? launch_shade_split<BG_TRACER_GI, false, true>(d, nb, nbc, st, A, P, Q)
-                      : launch_shade_split<BG_TRACER_GI, false, false>(d, nb, nbc, st, A, P, Q);
-        return rc ? rc : 4;
-    }
-    if (kind == BG_TRACER_DI) {
-        if (area) k_shade<BG_TRACER_DI, false, true><<<nb, kShadeThreads, 0, st>>>(d, A, P, Q);
-        else k_shade<BG_TRACER_DI, false, false><<<nb, kShadeThreads, 0, st>>>(d, A, P, Q);
-    } else if (cache) {
-        if (area) k_shade<BG_TRACER_GI, true, true><<<nb, kShadeThreads, 0, st>>>(d, A, P, Q);
-        else k_shade<BG_TRACER_GI, true, false><<<nb, kShadeThreads, 0, st>>>(d, A, P, Q);
-    } else {
-        if (area) k_shade<BG_TRACER_GI, false, true><<<nb, kShadeThreads, 0, st>>>(d, A, P, Q);
-        else k_shade<BG_TRACER_GI, false, false><<<nb, kShadeThreads, 0, st>>>(d, A, P, Q);
-    }
-    return 1;
+    int rc;
+    if (kind == BG_TRACER_DI)
+        rc = area ? launch_shade_split<BG_TRACER_DI, false, true>(d, nb, nbc, st, A, P, Q)
+                  : launch_shade_split<BG_TRACER_DI, false, false>(d, nb, nbc, st, A, P, Q);
+    else if (cache)
+        rc = area ? launch_shade_split<BG_TRACER_GI, true, true>(d, nb, nbc, st, A, P, Q)
+                  : launch_shade_split<BG_TRACER_GI, true, false>(d, nb, nbc, st, A, P, Q);
+    else
+        rc = area ? launch_shade_split<BG_TRACER_GI, false, true>(d, nb, nbc, st, A, P, Q)
+                  : launch_shade_split<BG_TRACER_GI, false, false>(d, nb, nbc, st, A, P, Q);
+    return rc ? rc : 4;
 }
 
 // BSDF-sampled rays towards area lights: the closest hit must be on a bundle
@@ -710,10 +694,6 @@ __global__ void __launch_bounds__(kShadeThreads)
 k_resolve_mis(DevScene S, PathState P, Queues Q) {
     const int n = *Q.n_mis;
     const int nthreads = gridDim.x * blockDim.x;
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        Q.totals[1] += (unsigned long long)*Q.n_sh;
-        Q.totals[2] += (unsigned long long)n;
-    }
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += nthreads) {
         const bg_hit hit = Q.mis_hits[e];
         if (hit.primid < 0) continue;   // area lights emit nothing on a miss
@@ -742,6 +722,10 @@ k_finalize(PathState P, Queues Q, int kmax, int maxdepth, int train_stride, int 
            int cap) {
     const int n = *Q.n_end;
     const int nthreads = gridDim.x * blockDim.x;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {   // the bounce's shadow and MIS rays (statistics)
+        Q.totals[1] += (unsigned long long)*Q.n_sh;
+        Q.totals[2] += (unsigned long long)*Q.n_mis;
+    }
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += nthreads) {
         const int path = Q.end_path[e];
         float4 r4 = P.rad[path];
@@ -879,7 +863,7 @@ static int alloc_state(bg_scene* s, RenderState* rs, int64_t cap, int L) {
         (rc = rs->work.ensure(size_t(kMaxBounceCounters) * 8)))
         return rc;
     int nb = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_shade<BG_TRACER_GI, false, true>, kShadeThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_shade<BG_TRACER_AO, false, false>, kShadeThreads, 0);
     rs->blocks = std::max(1, nb) * s->ctx->num_sms;
     nb = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_shade_class<BG_TRACER_GI, false, false, BG_MAT_MICROFACET_GGX>,
