@@ -236,7 +236,38 @@ def raycast_c2(ctx, nrays=1 << 24, reps=5):
     # same soup: build time and traversal speed of their trees
     for builder, name in ((1, "device_lbvh"), (2, "device_ploc"), (3, "device_sah")):
         out[name] = _device_build_traversal(ctx, builder, nrays, reps)
+    out["watertight"] = _watertight_traversal(ctx, nrays, reps)
     return out
+
+
+def _watertight_traversal(ctx, nrays, reps):
+    """The optional watertight ray / triangle test (not in the reference) on the
+    same soup and rays, host SAH tree: Mrays/s per set and node layout."""
+    import torch
+    from banshee_b200 import abi, capi, scenes
+    gw = capi.GpuScene(ctx, scenes.soup(1 << 20, seed=1), intersect=abi.BG_INTERSECT_WATERTIGHT)
+    res = {}
+    for kind, anyhit in (("coherent", False), ("incoherent", False), ("incoherent", True)):
+        rays = scenes.soup_rays(nrays, kind, seed=2, any_hit=anyhit)
+        dr = torch.from_numpy(rays.view(np.uint8)).cuda()
+        out = torch.zeros(nrays * (1 if anyhit else 16), dtype=torch.uint8, device="cuda")
+        fn = gw.intersect_any if anyhit else gw.intersect_closest
+        for width in (4, 8):
+            gw.set_node_width(width)
+            for _ in range(2):
+                fn(dr.data_ptr(), out.data_ptr(), nrays)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(reps):
+                fn(dr.data_ptr(), out.data_ptr(), nrays)
+            e1.record()
+            torch.cuda.synchronize()
+            res["layout%d_%s_%s_mrays_per_s" % (width, kind, "any" if anyhit else "closest")] = round(
+                nrays / (e0.elapsed_time(e1) / reps) / 1e3, 1)
+        del dr, out
+    gw.close()
+    return res
 
 
 def _device_build_traversal(ctx, builder, nrays, reps):
@@ -505,6 +536,8 @@ def summary(line):
         for w in (4, 8):
             for k in ("coherent_closest", "incoherent_closest", "incoherent_any", "coherent_shadow_any"):
                 out["c2_w%d_%s_mrays" % (w, k)] = g(c2, "layout%d" % w, k, "mrays_per_s")
+    out["c2_watertight_w4_incoherent_closest_mrays"] = g(line, "raycast_c2", "watertight",
+                                                        "layout4_incoherent_closest_mrays_per_s")
     out["c1_msamples_per_s"] = g(line, "cornell_c1", "gpu_msamples_per_s")
     out["c1_relmse_vs_reference"] = g(line, "cornell_c1", "relmse_gpu_vs_reference")
     out["c4_msamples_per_s"] = g(line, "batch_c4", "msamples_per_s")
