@@ -22,6 +22,7 @@
 #include <cstdint>
 
 #include "cache.h"
+#include "nrc_encode.cuh"
 
 namespace bg {
 
@@ -115,9 +116,13 @@ __device__ __forceinline__ void tc_load_weights(const __nv_bfloat16* __restrict_
     }
 }
 
+// feat != nullptr: the input rows are encoded here from the raw query records
+// (16 floats each; thread r encodes tile row r straight into the A tile), so
+// no encoded row goes through global memory; otherwise they are read from X.
 __global__ void __launch_bounds__(128, 2) k_nrc_infer_tc(NrcDev C, const __nv_bfloat16* __restrict__ X,
                                                          const int* n_dev, int64_t n_static, float4* __restrict__ out,
-                                                         unsigned* __restrict__ errflags) {
+                                                         unsigned* __restrict__ errflags,
+                                                         const float* __restrict__ feat) {
     extern __shared__ __align__(1024) unsigned char tc_smem[];
     unsigned char* smem = tc_smem;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -151,14 +156,30 @@ __global__ void __launch_bounds__(128, 2) k_nrc_infer_tc(NrcDev C, const __nv_bf
     uint32_t phase = 0;
     for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const int64_t row0 = tile * kTcRows;
-        // input rows -> A0; 8 lanes write 8 rows of one chunk (conflict-free), 4 chunks per warp
-        for (int j = 0; j < 16; ++j) {
-            const int u = j * 4 + warp, rg = u >> 2, kq4 = u & 3;
-            const int r = rg * 8 + (lane & 7), kc = kq4 * 4 + (lane >> 3);
-            const int64_t g = row0 + r;
-            uint4 v = make_uint4(0u, 0u, 0u, 0u);
-            if (g < n) v = *reinterpret_cast<const uint4*>(X + size_t(g) * kNrcIn + kc * 8);
-            *reinterpret_cast<uint4*>(smem + kTcA0 + tc_off(r, kc, 16)) = v;
+        if (feat) {
+            // thread tid encodes row tid of the tile into A0 (16 chunks of 16 bytes)
+            uint32_t w[kNrcIn / 2];
+            const int64_t g = row0 + tid;
+            if (g < n) {
+                encode_row(C, feat + size_t(g) * kNrcFeatFloats, w);
+            } else {
+#pragma unroll
+                for (int k = 0; k < kNrcIn / 2; ++k) w[k] = 0u;
+            }
+#pragma unroll
+            for (int kc = 0; kc < 16; ++kc)
+                *reinterpret_cast<uint4*>(smem + kTcA0 + tc_off(tid, kc, 16)) =
+                    make_uint4(w[4 * kc], w[4 * kc + 1], w[4 * kc + 2], w[4 * kc + 3]);
+        } else {
+            // input rows -> A0; 8 lanes write 8 rows of one chunk (conflict-free), 4 chunks per warp
+            for (int j = 0; j < 16; ++j) {
+                const int u = j * 4 + warp, rg = u >> 2, kq4 = u & 3;
+                const int r = rg * 8 + (lane & 7), kc = kq4 * 4 + (lane >> 3);
+                const int64_t g = row0 + r;
+                uint4 v = make_uint4(0u, 0u, 0u, 0u);
+                if (g < n) v = *reinterpret_cast<const uint4*>(X + size_t(g) * kNrcIn + kc * 8);
+                *reinterpret_cast<uint4*>(smem + kTcA0 + tc_off(r, kc, 16)) = v;
+            }
         }
         tc_fence_async_smem();
         tc_fence_before();

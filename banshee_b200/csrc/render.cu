@@ -34,6 +34,7 @@ namespace bg {
 int nrc_prepare(bg_cache* c, int64_t rows);
 int nrc_encode(bg_cache* c, const float* feat, const int* n_dev, int64_t n_static, int offset, int limit, cudaStream_t st);
 int nrc_infer(bg_cache* c, const int* n_dev, int64_t n_static, float4* out, cudaStream_t st);
+int nrc_query(bg_cache* c, const float* feat, const int* n_dev, int64_t n_static, float4* out, cudaStream_t st);
 int nrc_train_step(bg_cache* c, const float* feat, const float4* target, const int* n_dev, int offset, int B, bool apply,
                    cudaStream_t st);
 const bg_cache_desc* nrc_desc(const bg_cache* c);
@@ -1107,10 +1108,9 @@ static int enqueue_pass(bg_scene* s, RenderState* rs, cudaStream_t st, const Pas
                 if (wait_here)
                     BG_CUDA(cudaStreamWaitEvent(rs->mstream, rs->ev_train, ins ? 0u : unsigned(cudaEventWaitExternal)));
                 float4* qo = rs->q_out.as<float4>();
-                if ((rc = nrc_encode(c.cache, rs->q_feat.as<float>(), Q.n_query, 0, 0, 0, rs->mstream))) return rc;
-                if ((rc = nrc_infer(c.cache, Q.n_query, 0, qo, rs->mstream))) return rc;
+                if ((rc = nrc_query(c.cache, rs->q_feat.as<float>(), Q.n_query, 0, qo, rs->mstream))) return rc;
                 k_cache_resolve<<<nb, kShadeThreads, 0, rs->mstream>>>(P, Q, qo);
-                if (ins) ins->launches += 3;
+                if (ins) ins->launches += nrc_desc(c.cache)->mlp_kernel == 0 ? 2 : 3;
             }
             BG_CUDA(cudaEventRecord(rs->ev_mjoin, rs->mstream));
         }
@@ -1133,10 +1133,9 @@ static int enqueue_pass(bg_scene* s, RenderState* rs, cudaStream_t st, const Pas
             // paths that ended into the cache here: encode, infer, add throughput * prediction
             if (ins) ins->mark(3);
             float4* qo = rs->q_out.as<float4>();
-            if ((rc = nrc_encode(c.cache, rs->q_feat.as<float>(), Q.n_query, 0, 0, 0, st))) return rc;
-            if ((rc = nrc_infer(c.cache, Q.n_query, 0, qo, st))) return rc;
+            if ((rc = nrc_query(c.cache, rs->q_feat.as<float>(), Q.n_query, 0, qo, st))) return rc;
             k_cache_resolve<<<nb, kShadeThreads, 0, st>>>(P, Q, qo);
-            if (ins) { ins->launches += 3; ins->mark(3); }
+            if (ins) { ins->launches += nrc_desc(c.cache)->mlp_kernel == 0 ? 2 : 3; ins->mark(3); }
         }
         k_finalize<<<nb, kShadeThreads, 0, st>>>(P, Q, rs->kmax, c.maxdepth, c.cache ? c.train_stride : 0,
                                                  c.cache ? c.cache_depth : 0, b, 0, int(rs->cap));

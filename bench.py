@@ -527,7 +527,7 @@ def summary(line):
             if not isinstance(d, dict) or d.get(k) is None:
                 return None
             d = d[k]
-        return round(d, 6) if isinstance(d, float) else d
+        return float("%.6g" % d) if isinstance(d, float) else d
     out = {"c3_msamples_per_s": g(line, "value"), "c3_e2e_msamples_per_s": g(line, "e2e", "value"),
            "c3_parity_relmse": g(line, "c3_parity", "relmse"), "c3_parity_pixels": g(line, "c3_parity", "pixels"),
            "traversal_frac_hbm": g(line, "roofline", "frac"), "error_flags": line.get("error_flags")}
