@@ -267,6 +267,8 @@ static void launch_width(bg_scene* s, bool any_hit, const float4* rays, int64_t 
 static void launch_layout(bg_scene* s, bool any_hit, const float4* rays, int64_t n_static, const int* n_dev,
                           bg_hit* hits, uint8_t* occ, cudaStream_t st, unsigned long long* counters, int stride,
                           unsigned long long* w, const int* roots, ShadowResolve res) {
+    // (Measured and rejected: any-hit rays on the 8-wide nodes while closest-hit
+    // rays use the 4-wide ones: the C3 shadow traversal took 16.6 instead of 13.6 ms.)
     const bool w8 = s->dev.width == 8, wt = s->dev.watertight != 0;
     if (w8 && wt) launch_width<8, true>(s, any_hit, rays, n_static, n_dev, hits, occ, st, counters, stride, w, roots, res);
     else if (w8) launch_width<8, false>(s, any_hit, rays, n_static, n_dev, hits, occ, st, counters, stride, w, roots, res);

@@ -636,10 +636,11 @@ k_classify(Queues Q, int cap) {
 // The hits of one material class (list MAT of k_classify).
 // 5 blocks of 128 threads per SM: 96 registers, no spills in the Lambert and
 // GGX class kernels (measured per step of C3: 8 blocks 9.6 ms of shading,
-// 6 blocks 9.3 ms, 5 blocks 8.8 ms)
+// 6 blocks 9.3 ms, 5 blocks 8.8 ms, 4 blocks 0.3 ms slower than 5)
 constexpr int kShadeClassBlocks = 5;
+// The misses-and-emissive kernel mostly ends paths: 8 blocks / SM (64 registers).
 template <int KIND, bool CACHE, bool AREA, int MAT>
-__global__ void __launch_bounds__(kShadeThreads, kShadeClassBlocks)
+__global__ void __launch_bounds__(kShadeThreads, MAT == kMatOther ? 8 : kShadeClassBlocks)
 k_shade_class(DevScene S, ShadeArgs A, PathState P, Queues Q) {
     constexpr int c = MAT == BG_MAT_LAMBERT ? 1 : MAT == BG_MAT_MICROFACET_GGX ? 2 : 0;
     const int n = Q.n_cls[c];
@@ -659,7 +660,7 @@ static int launch_shade_split(const DevScene& d, int nb, int nbc, cudaStream_t s
                               const PathState& P, const Queues& Q) {
     BG_CUDA(cudaMemsetAsync(Q.n_cls, 0, 3 * sizeof(int), st));
     k_classify<<<nb, kClassifyThreads, 0, st>>>(Q, A.cap);
-    k_shade_class<KIND, CACHE, AREA, kMatOther><<<nbc, kShadeThreads, 0, st>>>(d, A, P, Q);
+    k_shade_class<KIND, CACHE, AREA, kMatOther><<<nb, kShadeThreads, 0, st>>>(d, A, P, Q);
     k_shade_class<KIND, CACHE, AREA, BG_MAT_LAMBERT><<<nbc, kShadeThreads, 0, st>>>(d, A, P, Q);
     k_shade_class<KIND, CACHE, AREA, BG_MAT_MICROFACET_GGX><<<nbc, kShadeThreads, 0, st>>>(d, A, P, Q);
     return BG_OK;
