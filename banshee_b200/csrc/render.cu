@@ -587,6 +587,12 @@ k_shade(DevScene S, ShadeArgs A, PathState P, Queues Q) {
         shade_path<KIND, CACHE, AREA, kMatAny>(S, A, P, Q, e);
 }
 
+// (Measured and rejected: tracing the secondary extension and shadow queues in
+// the order of their rays' direction octants, a counting sort in 256-entry
+// blocks: every k_trace launch of a C3 frame got 4-7 % slower, as a lane refill
+// then draws its rays from an 8 times wider stretch of the queue, i.e. of the
+// image, and the sort cost 3 % of the frame besides.)
+
 // Splits the extension queue by material class: list c of Q.cls (entries
 // c * cap ..) receives the queue indices of the hits of class c (0 = misses and
 // emissive, 1 = Lambert, 2 = GGX), in queue order within a block.  The class
@@ -638,9 +644,10 @@ k_classify(Queues Q, int cap) {
 // GGX class kernels (measured per step of C3: 8 blocks 9.6 ms of shading,
 // 6 blocks 9.3 ms, 5 blocks 8.8 ms, 4 blocks 0.3 ms slower than 5)
 constexpr int kShadeClassBlocks = 5;
-// The misses-and-emissive kernel mostly ends paths: 8 blocks / SM (64 registers).
+// (Measured and rejected: the misses-and-emissive kernel at 8 blocks / SM on
+// the full grid, 0.15 ms per C3 step slower in the serial phase timing.)
 template <int KIND, bool CACHE, bool AREA, int MAT>
-__global__ void __launch_bounds__(kShadeThreads, MAT == kMatOther ? 8 : kShadeClassBlocks)
+__global__ void __launch_bounds__(kShadeThreads, kShadeClassBlocks)
 k_shade_class(DevScene S, ShadeArgs A, PathState P, Queues Q) {
     constexpr int c = MAT == BG_MAT_LAMBERT ? 1 : MAT == BG_MAT_MICROFACET_GGX ? 2 : 0;
     const int n = Q.n_cls[c];
@@ -660,7 +667,7 @@ static int launch_shade_split(const DevScene& d, int nb, int nbc, cudaStream_t s
                               const PathState& P, const Queues& Q) {
     BG_CUDA(cudaMemsetAsync(Q.n_cls, 0, 3 * sizeof(int), st));
     k_classify<<<nb, kClassifyThreads, 0, st>>>(Q, A.cap);
-    k_shade_class<KIND, CACHE, AREA, kMatOther><<<nb, kShadeThreads, 0, st>>>(d, A, P, Q);
+    k_shade_class<KIND, CACHE, AREA, kMatOther><<<nbc, kShadeThreads, 0, st>>>(d, A, P, Q);
     k_shade_class<KIND, CACHE, AREA, BG_MAT_LAMBERT><<<nbc, kShadeThreads, 0, st>>>(d, A, P, Q);
     k_shade_class<KIND, CACHE, AREA, BG_MAT_MICROFACET_GGX><<<nbc, kShadeThreads, 0, st>>>(d, A, P, Q);
     return BG_OK;
