@@ -501,7 +501,7 @@ int nrc_encode(bg_cache* c, const float* feat, const int* n_dev, int64_t n_stati
 
 int nrc_infer(bg_cache* c, const int* n_dev, int64_t n_static, float4* out, cudaStream_t st) {
     if (c->desc.mlp_kernel == 0)
-        k_nrc_infer_tc<<<c->sms * 2, 128, kTcSmem, st>>>(c->dev, c->X.as<__nv_bfloat16>(), n_dev, n_static, out,
+        k_nrc_infer_tc<<<c->sms * kTiCtasPerSm, kTiThreads, kTiSmem, st>>>(c->dev, c->X.as<__nv_bfloat16>(), n_dev, n_static, out,
                                                           c->scene->dev.errflags, nullptr);
     else
         k_nrc_infer<<<c->sms * 4, 128, kInferSmem, st>>>(c->dev, c->X.as<__nv_bfloat16>(), n_dev, n_static, out);
@@ -513,7 +513,7 @@ int nrc_infer(bg_cache* c, const int* n_dev, int64_t n_static, float4* out, cuda
 // into the inference kernel; the mma.sync path encodes into X first.
 int nrc_query(bg_cache* c, const float* feat, const int* n_dev, int64_t n_static, float4* out, cudaStream_t st) {
     if (c->desc.mlp_kernel == 0) {
-        k_nrc_infer_tc<<<c->sms * 2, 128, kTcSmem, st>>>(c->dev, nullptr, n_dev, n_static, out, c->scene->dev.errflags,
+        k_nrc_infer_tc<<<c->sms * kTiCtasPerSm, kTiThreads, kTiSmem, st>>>(c->dev, nullptr, n_dev, n_static, out, c->scene->dev.errflags,
                                                           feat);
         BG_CUDA(cudaGetLastError());
         return BG_OK;
@@ -650,7 +650,7 @@ int bg_cache_create(bg_scene* s, const bg_cache_desc* d, bg_cache** out) {
         return set_error(BG_ERR_INVALID_ARG, "train_suffix %d < 0", d->train_suffix);
     }
     cudaFuncSetAttribute(k_nrc_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, kInferSmem);
-    cudaFuncSetAttribute(k_nrc_infer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
+    cudaFuncSetAttribute(k_nrc_infer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kTiSmem);
     cudaFuncSetAttribute(k_nrc_train_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kTtSmem);
     cudaFuncSetAttribute(k_nrc_train, cudaFuncAttributeMaxDynamicSharedMemorySize, kTrainSmem);
     if ((rc = cache_init_params(c))) { bg_cache_destroy(c); return rc; }

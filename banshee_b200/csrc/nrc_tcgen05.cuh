@@ -1,6 +1,7 @@
 // Radiance-cache MLP inference on the 5th-generation tensor cores (tcgen05).
 //
-// One persistent CTA of 128 threads per tile of 128 query rows:
+// Persistent CTAs; each group of 128 threads works on one tile of 128 query
+// rows at a time (the inference kernel's layout is described above it):
 //   * the six weight matrices live in shared memory for the whole kernel, in
 //     the K-major no-swizzle canonical layout of the UMMA shared-memory
 //     descriptors: 8x8 bf16 core matrices of 128 contiguous bytes, core
@@ -116,96 +117,129 @@ __device__ __forceinline__ void tc_load_weights(const __nv_bfloat16* __restrict_
     }
 }
 
+// Inference: CTAs of kTiGroups x 128 threads.  Each group of four warps runs
+// its own 128-row tiles through the six layers with its own mbarrier, its own
+// 64 TMEM columns and its own 32 KB activation slot: the 128-wide input tile,
+// whose first 16 KB the 64-wide hidden tiles reuse once the layer-0 MMA has
+// completed (82 KB of shared memory per group with the weights, against
+// 100 KB with a separate hidden tile).  Groups synchronise on named barriers
+// (ids 1..kTiGroups), the CTA only at start and end.  The kernel is bound by
+// the encoding's hash-grid gathers, not by the MMA chain: measured on the C3
+// frame's queries, one group per CTA at two CTAs per SM (the smaller shared
+// footprint leaves more L1 to the gathers) took 103 us per launch, four groups
+// in one CTA per SM 126 us; the previous layout (separate hidden tile) 1.07 ms
+// per 8-spp frame against 0.68 ms now.
 // feat != nullptr: the input rows are encoded here from the raw query records
-// (16 floats each; thread r encodes tile row r straight into the A tile), so
-// no encoded row goes through global memory; otherwise they are read from X.
-__global__ void __launch_bounds__(128, 2) k_nrc_infer_tc(NrcDev C, const __nv_bfloat16* __restrict__ X,
-                                                         const int* n_dev, int64_t n_static, float4* __restrict__ out,
-                                                         unsigned* __restrict__ errflags,
-                                                         const float* __restrict__ feat) {
+// (16 floats each; thread r of a group encodes row r of its tile straight into
+// the A tile), so no encoded row goes through global memory; otherwise they
+// are read from X.
+constexpr int kTiGroups = 1;
+constexpr int kTiCtasPerSm = 2;                            // CTAs per SM in the grid
+constexpr int kTiThreads = 128 * kTiGroups;
+constexpr int kTiSlot0 = kTcA0;                            // group g's slot at kTiSlot0 + g * kTiSlotBytes
+constexpr int kTiSlotBytes = kTcRows * 128 * 2;            // 32 KB: the [128 x 128] input tile
+constexpr int kTiBar = kTiSlot0 + kTiGroups * kTiSlotBytes;   // kTiGroups mbarriers + TMEM base
+constexpr int kTiSmem = kTiBar + 8 * kTiGroups + 16;
+constexpr uint32_t kTiCols = 64 * kTiGroups;               // TMEM columns (a power of two >= 32)
+static_assert(kTiSmem <= 227 * 1024, "inference shared memory");
+static_assert((kTiCols & (kTiCols - 1)) == 0 && kTiCols <= 512, "TMEM allocation");
+
+__device__ __forceinline__ void group_sync(int g) {
+    asm volatile("bar.sync %0, 128;" ::"r"(g + 1) : "memory");
+}
+
+__global__ void __launch_bounds__(kTiThreads, kTiCtasPerSm) k_nrc_infer_tc(NrcDev C, const __nv_bfloat16* __restrict__ X,
+                                                                const int* n_dev, int64_t n_static,
+                                                                float4* __restrict__ out,
+                                                                unsigned* __restrict__ errflags,
+                                                                const float* __restrict__ feat) {
     extern __shared__ __align__(1024) unsigned char tc_smem[];
     unsigned char* smem = tc_smem;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int g = warp >> 2;              // tile group
+    const int gt = tid & 127;             // thread within the group = tile row = TMEM lane
+    const int gw = warp & 3;              // warp within the group (TMEM lanes 32 gw .. 32 gw + 31)
     const uint32_t sbase = uint32_t(__cvta_generic_to_shared(smem));
-    const uint32_t bar = sbase + kTcBar;
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + kTcBar + 8);
-    __shared__ int abort_flag;
+    const uint32_t bar = sbase + kTiBar + 8 * g;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + kTiBar + 8 * kTiGroups);
+    __shared__ int abort_flag[kTiGroups];
+    unsigned char* slot = smem + kTiSlot0 + g * kTiSlotBytes;
+    const uint32_t sslot = sbase + kTiSlot0 + g * kTiSlotBytes;
 
     tc_load_weights(C.wb + kNrcW0, 64, 128, smem + kTcW0);
     for (int l = 0; l < 4; ++l) tc_load_weights(C.wb + kNrcW1 + l * 4096, 64, 64, smem + kTcW1 + l * 8192);
     tc_load_weights(C.wb + kNrcW5, 16, 64, smem + kTcW5);
-    if (tid == 0) {
-        abort_flag = 0;
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(bar) : "memory");
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    if (tid < kTiGroups) {
+        abort_flag[tid] = 0;
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(sbase + kTiBar + 8 * tid) : "memory");
     }
+    if (tid == 0) asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
-                     :: "r"(sbase + kTcBar + 8), "r"(kTcCols) : "memory");
+                     :: "r"(sbase + kTiBar + 8 * kTiGroups), "r"(kTiCols) : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     tc_fence_async_smem();
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    const uint32_t tmem = *tmem_slot;
-    const uint32_t trow = tmem + (uint32_t(warp * 32) << 16);   // this warp's 32 lanes
+    const uint32_t tmem = *tmem_slot + uint32_t(64 * g);           // this group's accumulator columns
+    const uint32_t trow = tmem + (uint32_t(gw * 32) << 16);        // this warp's 32 lanes
 
     const int64_t n = n_dev ? int64_t(*n_dev) : n_static;
     const int64_t ntiles = (n + kTcRows - 1) / kTcRows;
     uint32_t phase = 0;
-    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    for (int64_t tile = int64_t(blockIdx.x) * kTiGroups + g; tile < ntiles; tile += int64_t(gridDim.x) * kTiGroups) {
         const int64_t row0 = tile * kTcRows;
         if (feat) {
-            // thread tid encodes row tid of the tile into A0 (16 chunks of 16 bytes)
+            // thread gt encodes row gt of the tile into the input tile (16 chunks of 16 bytes)
             uint32_t w[kNrcIn / 2];
-            const int64_t g = row0 + tid;
-            if (g < n) {
-                encode_row(C, feat + size_t(g) * kNrcFeatFloats, w);
+            const int64_t gr = row0 + gt;
+            if (gr < n) {
+                encode_row(C, feat + size_t(gr) * kNrcFeatFloats, w);
             } else {
 #pragma unroll
                 for (int k = 0; k < kNrcIn / 2; ++k) w[k] = 0u;
             }
 #pragma unroll
             for (int kc = 0; kc < 16; ++kc)
-                *reinterpret_cast<uint4*>(smem + kTcA0 + tc_off(tid, kc, 16)) =
+                *reinterpret_cast<uint4*>(slot + tc_off(gt, kc, 16)) =
                     make_uint4(w[4 * kc], w[4 * kc + 1], w[4 * kc + 2], w[4 * kc + 3]);
         } else {
-            // input rows -> A0; 8 lanes write 8 rows of one chunk (conflict-free), 4 chunks per warp
+            // input rows -> input tile; 8 lanes write 8 rows of one chunk (conflict-free), 4 chunks per warp
             for (int j = 0; j < 16; ++j) {
-                const int u = j * 4 + warp, rg = u >> 2, kq4 = u & 3;
+                const int u = j * 4 + gw, rg = u >> 2, kq4 = u & 3;
                 const int r = rg * 8 + (lane & 7), kc = kq4 * 4 + (lane >> 3);
-                const int64_t g = row0 + r;
+                const int64_t gr = row0 + r;
                 uint4 v = make_uint4(0u, 0u, 0u, 0u);
-                if (g < n) v = *reinterpret_cast<const uint4*>(X + size_t(g) * kNrcIn + kc * 8);
-                *reinterpret_cast<uint4*>(smem + kTcA0 + tc_off(r, kc, 16)) = v;
+                if (gr < n) v = *reinterpret_cast<const uint4*>(X + size_t(gr) * kNrcIn + kc * 8);
+                *reinterpret_cast<uint4*>(slot + tc_off(r, kc, 16)) = v;
             }
         }
         tc_fence_async_smem();
         tc_fence_before();
-        __syncthreads();
+        group_sync(g);
         for (int layer = 0; layer < 6; ++layer) {
-            if (tid == 0) {
+            if (gt == 0) {
                 tc_fence_after();
                 const int KC = layer == 0 ? 16 : 8;
-                const uint32_t a = sbase + (layer == 0 ? kTcA0 : kTcA1);
                 const uint32_t b = sbase + (layer == 0 ? kTcW0 : layer < 5 ? kTcW1 + (layer - 1) * 8192 : kTcW5);
                 const uint32_t idesc = tc_idesc(layer < 5 ? 64 : 16);
                 for (int s = 0; s < KC / 2; ++s)
-                    tc_mma(tmem, tc_desc(a + s * 256, 128, KC * 128), tc_desc(b + s * 256, 128, KC * 128), idesc,
+                    tc_mma(tmem, tc_desc(sslot + s * 256, 128, KC * 128), tc_desc(b + s * 256, 128, KC * 128), idesc,
                            s > 0 ? 1u : 0u);
                 tc_commit(bar);
             }
             if (!tc_wait(bar, phase, C.wait_polls)) {
                 atomicOr(errflags, BG_FLAG_TIMEOUT);
-                abort_flag = 1;
+                abort_flag[g] = 1;
             }
             phase ^= 1u;
             tc_fence_after();
-            __syncthreads();
-            if (abort_flag) break;
-            const int r = tid;                       // TMEM lane = tile row
+            group_sync(g);
+            if (abort_flag[g]) break;
             if (layer < 5) {
+                // ReLU, bf16, into the hidden tile (the slot's first 16 KB: the MMA that read them is done)
 #pragma unroll
                 for (int c4 = 0; c4 < 4; ++c4) {
                     float v[16];
@@ -219,26 +253,27 @@ __global__ void __launch_bounds__(128, 2) k_nrc_infer_tc(NrcDev C, const __nv_bf
                     p1.y = tc_pack(fmaxf(v[10], 0.f), fmaxf(v[11], 0.f));
                     p1.z = tc_pack(fmaxf(v[12], 0.f), fmaxf(v[13], 0.f));
                     p1.w = tc_pack(fmaxf(v[14], 0.f), fmaxf(v[15], 0.f));
-                    *reinterpret_cast<uint4*>(smem + kTcA1 + tc_off(r, 2 * c4, 8)) = p0;
-                    *reinterpret_cast<uint4*>(smem + kTcA1 + tc_off(r, 2 * c4 + 1, 8)) = p1;
+                    *reinterpret_cast<uint4*>(slot + tc_off(gt, 2 * c4, 8)) = p0;
+                    *reinterpret_cast<uint4*>(slot + tc_off(gt, 2 * c4 + 1, 8)) = p1;
                 }
                 tc_fence_async_smem();
             } else {
                 float v[16];
                 tc_ld16(trow, v);
-                if (row0 + r < n) out[row0 + r] = make_float4(v[0], v[1], v[2], 0.f);
+                if (row0 + gt < n) out[row0 + gt] = make_float4(v[0], v[1], v[2], 0.f);
             }
             tc_fence_before();
-            __syncthreads();
+            group_sync(g);
         }
-        if (abort_flag) break;
+        if (abort_flag[g]) break;
     }
-    // after a timeout, give the outstanding MMA group one more bounded wait before freeing its TMEM
-    if (abort_flag && tid == 0) tc_wait(bar, phase ^ 1u);
+    // after a timeout, give the group's outstanding MMA one more bounded wait before the TMEM is freed
+    if (abort_flag[g] && gt == 0) tc_wait(bar, phase ^ 1u);
+    tc_fence_before();
     __syncthreads();
     if (warp == 0) {
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(kTcCols) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(*tmem_slot), "r"(kTiCols) : "memory");
     }
 }
 

@@ -33,7 +33,12 @@ __host__ __device__ constexpr int smem_stack_entries() { return WIDTH == 4 ? 8 :
 template <int WIDTH>
 __host__ __device__ constexpr int stack_entries() { return WIDTH == 8 ? kStackSize8 : kStackSize; }
 // traversal steps between warp refill points (measured on passes of 2^24 paths:
-// closest hit 24 > 16 > 12 by about 1 % of the frame; any hit 16 > 8, 32)
+// closest hit 24 > 16 > 12 by about 1 % of the frame; any hit 16 > 8, 32).
+// (Measured and rejected: each lane's next ray prefetched into shared memory by
+// cp.async from a per-warp pool of 32 indices, refilling every 24 / 12 / 8 / 4
+// steps: C3 567 -> 528 / 519 / 511 / 280 Msamples/s with 4-wide nodes; and
+// registers capped at 48 or 40 for 40 or 48 resident warps per SM: spills,
+// 559 -> 544 / 495 Msamples/s.)
 constexpr int kRefillStepsClosest = 24;
 constexpr int kRefillStepsAny = 16;
 constexpr float kBoxSlack = 4e-7f;
@@ -378,8 +383,12 @@ __device__ __forceinline__ bool trav_node(const DevScene& S, TS& s, const STACK&
     return true;
 }
 
-// Tests the triangles of leaf code `item` (bit 31 set, count-1 in bits 27..30,
-// first triangle in bits 0..26).  True when an any-hit query found its hit.
+// Tests the first triangle of leaf code `item` (bit 31 set, count-1 in bits
+// 27..30, first triangle in bits 0..26) and sets the lane's next item: the
+// rest of the leaf, or a pop.  True when an any-hit query found its hit.  One
+// triangle per traversal step keeps lanes that are in a leaf in step with
+// lanes that are in a node (measured against the whole leaf in one step: C2
+// incoherent closest hits +4 %, any hits +3.5 %, C3 frame +1-2 %).
 // WT: the scene's records hold the vertices (p1, p2, p3) and the test is the
 // watertight one; otherwise they hold (p1, e1, e2) for Moller-Trumbore.
 template <bool ANY, bool COUNT, bool WT>
@@ -387,25 +396,25 @@ __device__ __forceinline__ bool trav_leaf(const DevScene& S, TravState<WT>& s, i
     const uint32_t code = uint32_t(item);
     const int count = int((code >> kLeafStartBits) & 15u) + 1;
     const int start = int(code & uint32_t(kMaxLeafStart));
-    for (int k = 0; k < count; ++k) {
-        const float4* tp = reinterpret_cast<const float4*>(S.tris + start + k);
-        float4 v0 = __ldg(tp), e1 = __ldg(tp + 1), e2 = __ldg(tp + 2);
-        if (COUNT) ++cnt.tris;
-        obj_ray(S, s.r, __float_as_int(v0.w), s.cache);
-        float t, a, b;
-        bool hit;
-        if constexpr (WT)
-            hit = wt_test(s.cache, mk(v0.x, v0.y, v0.z), mk(e1.x, e1.y, e1.z), mk(e2.x, e2.y, e2.z), s.r.tmin,
-                          ANY ? s.r.tmax : s.best, t, a, b);
-        else
-            hit = mt_test(s.cache.o, s.cache.d, mk(v0.x, v0.y, v0.z), mk(e1.x, e1.y, e1.z), mk(e2.x, e2.y, e2.z),
-                          s.r.tmin, ANY ? s.r.tmax : s.best, t, a, b);
-        if (hit) {
-            s.prim = __float_as_int(e1.w);
-            if (ANY) return true;
-            s.best = t; s.u = a; s.v = b;
-            s.cls = __float_as_int(e2.w);
-        }
+    // the rest of the leaf: one triangle fewer, starting one later
+    s.item = count > 1 ? int(code - (1u << kLeafStartBits) + 1u) : kNone;
+    const float4* tp = reinterpret_cast<const float4*>(S.tris + start);
+    float4 v0 = __ldg(tp), e1 = __ldg(tp + 1), e2 = __ldg(tp + 2);
+    if (COUNT) ++cnt.tris;
+    obj_ray(S, s.r, __float_as_int(v0.w), s.cache);
+    float t, a, b;
+    bool hit;
+    if constexpr (WT)
+        hit = wt_test(s.cache, mk(v0.x, v0.y, v0.z), mk(e1.x, e1.y, e1.z), mk(e2.x, e2.y, e2.z), s.r.tmin,
+                      ANY ? s.r.tmax : s.best, t, a, b);
+    else
+        hit = mt_test(s.cache.o, s.cache.d, mk(v0.x, v0.y, v0.z), mk(e1.x, e1.y, e1.z), mk(e2.x, e2.y, e2.z),
+                      s.r.tmin, ANY ? s.r.tmax : s.best, t, a, b);
+    if (hit) {
+        s.prim = __float_as_int(e1.w);
+        if (ANY) return true;
+        s.best = t; s.u = a; s.v = b;
+        s.cls = __float_as_int(e2.w);
     }
     return false;
 }
@@ -424,7 +433,6 @@ __device__ __forceinline__ bool trav_steps(const DevScene& S, TravState<WT>& s, 
             if (!trav_node<COUNT, WIDTH>(S, s, stack, item, cnt)) return true;
         } else {
             if (trav_leaf<ANY, COUNT>(S, s, item, cnt)) return true;
-            s.item = kNone;
         }
     }
     return false;

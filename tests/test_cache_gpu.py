@@ -184,7 +184,8 @@ def test_trained_cache_recovers_truncated_radiance(ctx):
 def test_tcgen05_and_mma_sync_inference_agree(ctx):
     """The tcgen05 kernel (TMEM accumulators) and the mma.sync kernel compute the
     same bf16 network; only the fp32 summation order differs.  Ragged row counts
-    exercise partial 128-row tiles."""
+    exercise partial 128-row tiles; the largest gives every tile group of the
+    tcgen05 kernel several tiles."""
     import torch
     from banshee_b200 import capi
     gs, c0 = _cache(ctx, log2t=12, mlp_kernel=0)
@@ -193,7 +194,7 @@ def test_tcgen05_and_mma_sync_inference_agree(ctx):
     m, g, _, _ = c0.params()
     c1.set_params(m, g)
     rng = np.random.default_rng(8)
-    for n in (1, 127, 129, 5000, 65536 + 77):
+    for n in (1, 127, 129, 5000, 65536 + 77, 300_005):
         fd = torch.from_numpy(_features(n, rng)).cuda()
         o0 = torch.zeros((n, 4), dtype=torch.float32, device="cuda")
         o1 = torch.zeros((n, 4), dtype=torch.float32, device="cuda")

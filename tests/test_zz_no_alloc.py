@@ -69,10 +69,13 @@ def test_noalloc_allocates_nothing():
     want = gs.traversal_counts(dr.data_ptr(), rays.shape[0])
     gs.traversal_counts_noalloc(dr.data_ptr(), rays.shape[0])       # the device's scratch address is looked up
     before = capi.alloc_stats()
+    torch.cuda.synchronize()
+    free_before = torch.cuda.mem_get_info()[0]      # the device's free memory, whoever allocates
     capi.alloc_limit(0)
     try:
         for _ in range(2):
             assert gs.traversal_counts_noalloc(dr.data_ptr(), rays.shape[0]) == want
+        assert torch.cuda.mem_get_info()[0] == free_before
         after = capi.alloc_stats()
         assert after["calls"] == before["calls"] and after["bytes"] == before["bytes"]
         with pytest.raises(capi.BansheeError) as ei:
