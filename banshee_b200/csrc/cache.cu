@@ -429,8 +429,9 @@ struct bg_cache {
     bg_cache_desc desc{};
     bg::NrcDev dev{};
     bg::DevBuf grid, grid_grad, grid_m, grid_v, w, w_grad, w_m, w_v, wb, step;
-    bg::DevBuf X, H, DZ, DZ5, dX, feat, target, out, loss;   // training / query scratch
-    int64_t cap = 0;
+    bg::DevBuf X, H, DZ, DZ5, dX, loss;   // training scratch; X also holds encoded mma.sync queries
+    int64_t train_cap = 0;                // training rows H, DZ, DZ5 and dX hold
+    int64_t x_cap = 0;                    // encoded rows X holds
     int sms = 0;
     int64_t frame = 0;
     uint64_t id = 0;          // unique over the process (captured passes key on it)
@@ -443,15 +444,27 @@ static int64_t grid_params(const bg_cache* c) { return int64_t(kNrcLevels) * (in
 
 static std::atomic<uint64_t> g_cache_ids{1};
 
-static int cache_scratch(bg_cache* c, int64_t rows) {
-    if (rows <= c->cap) return BG_OK;
-    c->buf_epoch = g_cache_ids.fetch_add(1);
+// Scratch for up to `train_rows` rows of one Adam step (encoded rows, hidden
+// activations and layer gradients of the fused training kernels) and for
+// `query_rows` queries at a time.  The tcgen05 inference kernel encodes its
+// queries in shared memory and needs none; the mma.sync path encodes them
+// into X first.  (Sizing everything by the pass, 2^24 paths, took 28.6 GB.)
+static int cache_scratch(bg_cache* c, int64_t train_rows, int64_t query_rows) {
+    const int64_t xr = std::max(train_rows, c->desc.mlp_kernel == 0 ? int64_t(0) : query_rows);
+    if (train_rows <= c->train_cap && xr <= c->x_cap) return BG_OK;
+    c->buf_epoch = g_cache_ids.fetch_add(1);   // captured passes bake X in (mma.sync queries)
     int rc;
-    const size_t R = size_t(rows);
-    if ((rc = c->X.ensure(R * kNrcIn * 2)) || (rc = c->H.ensure(5 * R * 64 * 2)) || (rc = c->DZ.ensure(5 * R * 64 * 2)) ||
-        (rc = c->DZ5.ensure(R * 16 * 2)) || (rc = c->dX.ensure(R * 32 * 4)) || (rc = c->out.ensure(R * 16)))
-        return rc;
-    c->cap = rows;
+    if (xr > c->x_cap) {
+        if ((rc = c->X.ensure(size_t(xr) * kNrcIn * 2))) return rc;
+        c->x_cap = xr;
+    }
+    if (train_rows > c->train_cap) {
+        const size_t R = size_t(train_rows);
+        if ((rc = c->H.ensure(5 * R * 64 * 2)) || (rc = c->DZ.ensure(5 * R * 64 * 2)) || (rc = c->DZ5.ensure(R * 16 * 2)) ||
+            (rc = c->dX.ensure(R * 32 * 4)))
+            return rc;
+        c->train_cap = train_rows;
+    }
     return BG_OK;
 }
 
@@ -574,7 +587,50 @@ int nrc_train_step(bg_cache* c, const float* feat, const float4* target, const i
     return BG_OK;
 }
 
-int nrc_prepare(bg_cache* c, int64_t rows) { return cache_scratch(c, rows); }
+int nrc_prepare(bg_cache* c, int64_t train_rows, int64_t query_rows) { return cache_scratch(c, train_rows, query_rows); }
+
+// Captured passes do not depend on which cache they were captured with: the
+// only arguments of a pass's kernels that belong to a cache are the NrcDev
+// (parameters, grid, weights) and the encoded-row buffer X of the query
+// kernels.  nrc_graph_node() says whether a captured kernel node is one of
+// them and, with `exec`, points its copy in the executable graph at cache `c`
+// (every other argument is kept as captured).
+int nrc_graph_node(bg_cache* c, cudaGraphExec_t exec, cudaGraphNode_t node, bool* is_cache) {
+    cudaKernelNodeParams kp;
+    BG_CUDA(cudaGraphKernelNodeGetParams(node, &kp));
+    *is_cache = false;
+    void** a = kp.kernelParams;
+    NrcDev C = c->dev;
+    const __nv_bfloat16* Xc = c->X.as<__nv_bfloat16>();
+    if (kp.func == reinterpret_cast<void*>(k_nrc_infer_tc)) {
+        // (NrcDev, X, n_dev, n_static, out, errflags, feat); X is null when the kernel encodes
+        *is_cache = true;
+        if (!exec) return BG_OK;
+        const __nv_bfloat16* X = *static_cast<const __nv_bfloat16* const*>(a[1]) ? Xc : nullptr;
+        void* args[] = {&C, &X, a[2], a[3], a[4], a[5], a[6]};
+        kp.kernelParams = args;
+        kp.extra = nullptr;
+        BG_CUDA(cudaGraphExecKernelNodeSetParams(exec, node, &kp));
+    } else if (kp.func == reinterpret_cast<void*>(k_nrc_encode)) {
+        // (NrcDev, feat, n_dev, n_static, offset, limit, X)
+        *is_cache = true;
+        if (!exec) return BG_OK;
+        __nv_bfloat16* X = c->X.as<__nv_bfloat16>();
+        void* args[] = {&C, a[1], a[2], a[3], a[4], a[5], &X};
+        kp.kernelParams = args;
+        kp.extra = nullptr;
+        BG_CUDA(cudaGraphExecKernelNodeSetParams(exec, node, &kp));
+    } else if (kp.func == reinterpret_cast<void*>(k_nrc_infer)) {
+        // (NrcDev, X, n_dev, n_static, out)
+        *is_cache = true;
+        if (!exec) return BG_OK;
+        void* args[] = {&C, &Xc, a[2], a[3], a[4]};
+        kp.kernelParams = args;
+        kp.extra = nullptr;
+        BG_CUDA(cudaGraphExecKernelNodeSetParams(exec, node, &kp));
+    }
+    return BG_OK;
+}
 const bg_cache_desc* nrc_desc(const bg_cache* c) { return &c->desc; }
 int64_t nrc_next_frame(bg_cache* c) { return c->frame++; }
 int64_t nrc_frame(const bg_cache* c) { return c->frame; }
@@ -654,6 +710,9 @@ int bg_cache_create(bg_scene* s, const bg_cache_desc* d, bg_cache** out) {
     cudaFuncSetAttribute(k_nrc_train_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kTtSmem);
     cudaFuncSetAttribute(k_nrc_train, cudaFuncAttributeMaxDynamicSharedMemorySize, kTrainSmem);
     if ((rc = cache_init_params(c))) { bg_cache_destroy(c); return rc; }
+    // the scratch of one Adam step over train_batch rows, here rather than in
+    // the first render that trains
+    if ((rc = cache_scratch(c, c->desc.train_batch, 0))) { bg_cache_destroy(c); return rc; }
     *out = c;
     return BG_OK;
 }
@@ -662,7 +721,7 @@ int bg_cache_destroy(bg_cache* c) {
     if (!c) return BG_OK;
     cudaDeviceSynchronize();
     for (DevBuf* b : {&c->grid, &c->grid_grad, &c->grid_m, &c->grid_v, &c->w, &c->w_grad, &c->w_m, &c->w_v, &c->wb,
-                      &c->step, &c->X, &c->H, &c->DZ, &c->DZ5, &c->dX, &c->feat, &c->target, &c->out, &c->loss})
+                      &c->step, &c->X, &c->H, &c->DZ, &c->DZ5, &c->dX, &c->loss})
         b->release();
     delete c;
     return BG_OK;
@@ -673,7 +732,7 @@ int bg_cache_query(bg_cache* c, const float* feat, float* out_rgba, int64_t n, v
     if (n < 0 || n > (int64_t(1) << 30)) return set_error(BG_ERR_INVALID_ARG, "bad query count");
     if (n == 0) return BG_OK;
     int rc;
-    if ((rc = cache_scratch(c, n))) return rc;
+    if ((rc = cache_scratch(c, 0, n))) return rc;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     return nrc_query(c, feat, nullptr, n, reinterpret_cast<float4*>(out_rgba), st);
 }
@@ -683,7 +742,7 @@ int bg_cache_train(bg_cache* c, const float* feat, const float* target_rgba, int
     if (!c || (n > 0 && (!feat || !target_rgba))) return set_error(BG_ERR_INVALID_ARG, "NULL argument");
     if (n <= 0 || n > (int64_t(1) << 26)) return set_error(BG_ERR_INVALID_ARG, "bad training batch size");
     int rc;
-    if ((rc = cache_scratch(c, n))) return rc;
+    if ((rc = cache_scratch(c, n, 0))) return rc;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     BG_CUDA(cudaMemsetAsync(c->loss.ptr, 0, 4, st));
     if ((rc = nrc_train_step(c, feat, reinterpret_cast<const float4*>(target_rgba), nullptr, 0, int(n), apply != 0, st)))

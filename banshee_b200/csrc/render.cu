@@ -31,7 +31,7 @@
 namespace bg {
 
 // cache.cu
-int nrc_prepare(bg_cache* c, int64_t rows);
+int nrc_prepare(bg_cache* c, int64_t train_rows, int64_t query_rows);
 int nrc_encode(bg_cache* c, const float* feat, const int* n_dev, int64_t n_static, int offset, int limit, cudaStream_t st);
 int nrc_infer(bg_cache* c, const int* n_dev, int64_t n_static, float4* out, cudaStream_t st);
 int nrc_query(bg_cache* c, const float* feat, const int* n_dev, int64_t n_static, float4* out, cudaStream_t st);
@@ -42,6 +42,7 @@ int64_t nrc_next_frame(bg_cache* c);
 int64_t nrc_frame(const bg_cache* c);   // frames rendered so far
 uint64_t nrc_id(const bg_cache* c);          // unique over the process, never reused
 uint64_t nrc_buf_epoch(const bg_cache* c);   // changes whenever the cache's scratch is reallocated
+int nrc_graph_node(bg_cache* c, cudaGraphExec_t exec, cudaGraphNode_t node, bool* is_cache);
 bg_scene* nrc_scene(const bg_cache* c);
 
 __global__ void k_clamp_count(int* n, int cap) {
@@ -50,7 +51,7 @@ __global__ void k_clamp_count(int* n, int cap) {
 
 constexpr int kShadeThreads = 128;
 constexpr int kMaxBounceCounters = 6 * 1024;   // 6 work counters per bounce, maxdepth <= 1024
-constexpr int kGraphKey = 16;                    // int64 fields identifying a captured pass
+constexpr int kGraphKey = 15;                    // int64 fields identifying a captured pass
 
 
 // A pass segment: `ns` samples of pixels [p0, p0 + np) of job `job`, as paths
@@ -111,14 +112,17 @@ struct RenderState {
     // this bounce's MIS trace + resolve (mstream), with fork / join events
     cudaStream_t fstream = nullptr, mstream = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_mjoin = nullptr;
-    // captured passes, two kept (a cached render alternates its training-row sets)
+    // captured passes, eight kept, least recently used replaced (a cached
+    // render alternates between two training-row sets, and the training-path
+    // stride, which a captured pass bakes in, follows the frame's size)
     struct PassGraph {
         cudaGraph_t graph = nullptr;
         cudaGraphExec_t exec = nullptr;
         cudaGraphNode_t gen_node = nullptr, acc_node = nullptr;
+        std::vector<cudaGraphNode_t> cache_nodes;   // kernels whose arguments belong to the cache
         int64_t key[kGraphKey] = {};
         uint64_t used = 0;
-    } graphs[2];
+    } graphs[8];
     uint64_t graph_clock = 0;
 };
 
@@ -1163,14 +1167,15 @@ static int enqueue_pass(bg_scene* s, RenderState* rs, cudaStream_t st, const Pas
 
 // Captures one pass into a CUDA graph (once per bounce-loop shape) and finds
 // the two kernel nodes whose arguments (the segment slice, the training-path
-// phase) change per pass.
+// phase) change per pass, and the radiance-cache kernel nodes, which are
+// pointed at the rendering cache on every replay (a cache of the same
+// configuration replays the same graph).
 static int pass_graph(bg_scene* s, RenderState* rs, const PassCfg& c, RenderState::PassGraph*& out) {
     uint32_t aob;
     memcpy(&aob, &c.ao_radius, sizeof(aob));
     const int64_t key[kGraphKey] = {c.maxdepth, c.kind, c.batched ? 1 : 0, rs->kmax, int64_t(rs->cap), s->tune_threads,
                                     s->dev.width, int64_t(aob), s->ev_accum ? 1 : 0,
-                                    c.cache ? int64_t(nrc_id(c.cache)) : 0,
-                                    c.cache ? int64_t(nrc_buf_epoch(c.cache)) : 0,
+                                    c.cache ? int64_t(nrc_desc(c.cache)->mlp_kernel) + 1 : 0,
                                     c.cache ? c.cache_depth : -1, c.cache ? c.train_end : -1,
                                     c.cache ? c.train_stride : 0, c.cache ? rs->tr_set : 0,
                                     int64_t(rs->buf_epoch)};
@@ -1194,6 +1199,7 @@ static int pass_graph(bg_scene* s, RenderState* rs, const PassCfg& c, RenderStat
     std::vector<cudaGraphNode_t> nodes(nn);
     BG_CUDA(cudaGraphGetNodes(g, nodes.data(), &nn));
     pg->gen_node = pg->acc_node = nullptr;
+    pg->cache_nodes.clear();
     for (cudaGraphNode_t n : nodes) {
         cudaGraphNodeType t;
         BG_CUDA(cudaGraphNodeGetType(n, &t));
@@ -1202,6 +1208,11 @@ static int pass_graph(bg_scene* s, RenderState* rs, const PassCfg& c, RenderStat
         BG_CUDA(cudaGraphKernelNodeGetParams(n, &kp));
         if (kp.func == reinterpret_cast<void*>(k_generate)) pg->gen_node = n;
         if (kp.func == reinterpret_cast<void*>(k_accumulate)) pg->acc_node = n;
+        if (c.cache) {
+            bool is_cache = false;
+            if ((rc = nrc_graph_node(c.cache, nullptr, n, &is_cache))) return rc;
+            if (is_cache) pg->cache_nodes.push_back(n);
+        }
     }
     if (!pg->gen_node || !pg->acc_node) return set_error(BG_ERR_STATE, "pass graph: kernel nodes not found");
     BG_CUDA(cudaGraphInstantiate(&pg->exec, g, 0));
@@ -1232,6 +1243,12 @@ static int launch_pass_graph(bg_scene* s, RenderState* rs, const PassCfg& c) {
     kp.kernelParams = aargs;
     kp.extra = nullptr;
     BG_CUDA(cudaGraphExecKernelNodeSetParams(pg->exec, pg->acc_node, &kp));
+    // the cache's kernels read the cache this render uses (graphs are keyed by
+    // the cache's configuration, not by the cache)
+    for (cudaGraphNode_t n : pg->cache_nodes) {
+        bool is_cache = false;
+        if ((rc = nrc_graph_node(c.cache, pg->exec, n, &is_cache))) return rc;
+    }
     BG_CUDA(cudaGraphLaunch(pg->exec, rs->gstream));
     return BG_OK;
 }
@@ -1424,7 +1441,7 @@ int render_jobs(bg_scene* s, bg_cache* cache, const std::vector<JobSpec>& jobs, 
             rs->tr_cap = tr_cap;
             rs->pending_cache = 0;                   // the sets were reallocated
         }
-        if ((rc = nrc_prepare(cache, std::max<int64_t>(cap, tbatch)))) return rc;
+        if ((rc = nrc_prepare(cache, tbatch, cap))) return rc;
         // Online training is one frame behind: this frame's training rows go to
         // one set while the previous frame's rows (the other set) are trained on
         // a side stream, beside this frame's first bounces, which do not read

@@ -460,20 +460,25 @@ def time_to_relmse(gs, sc, args, target=1e-3):
                                        stats=False), 4)
     plain_spp = run(lambda p, f: gs.render(p, WIDTH, HEIGHT, SPP, seed=SEED, sample_offset=f * SPP,
                                            maxdepth=MAXDEPTH, stats=False), 1)
-    # warm the process as the plain tracer's timing is warm: a throwaway cache
-    # renders a few frames (kernel modules loaded, scratch memory pooled); the
-    # timed cache then starts untrained
+    # warm the process as the plain tracer's timing is warm (its pass graph was
+    # captured by the steps above): a throwaway cache of the same configuration
+    # renders two frames of each shape the timed caches render (kernel modules
+    # loaded, scratch memory pooled, pass graphs captured for both training-row
+    # sets); the timed caches then start untrained
     warm = capi.RadianceCache(gs, **CACHE_CFG)
     wbuf = torch.zeros((HEIGHT, WIDTH, 4), dtype=torch.float32, device="cuda")
-    for f in range(4):
+    wscr = torch.zeros((WARM_H, WARM_W, 4), dtype=torch.float32, device="cuda")
+    for f in range(2):
         warm.render(wbuf.data_ptr(), WIDTH, HEIGHT, 1, seed=SEED, sample_offset=f, maxdepth=MAXDEPTH)
+    for f in range(2):
+        warm.render(wscr.data_ptr(), WARM_W, WARM_H, 1, seed=SEED, sample_offset=f, maxdepth=MAXDEPTH)
+    for f in range(2):
+        warm.render(wbuf.data_ptr(), WIDTH, HEIGHT, SPP, seed=SEED, sample_offset=f * SPP, maxdepth=MAXDEPTH)
     torch.cuda.synchronize()
-    warm.close()
-    del wbuf
+    del wbuf, wscr
     # the cache at 1 spp per frame (one Adam step per frame)
     cache1 = capi.RadianceCache(gs, **CACHE_CFG)
     cached1 = run(lambda p, f: cache1.render(p, WIDTH, HEIGHT, 1, seed=SEED, sample_offset=f, maxdepth=MAXDEPTH), 4)
-    cache1.close()
     # the cache at its throughput configuration: WARM_FRAMES training-only frames
     # (the same camera at 384x216, 1 spp: every path is a training path, nothing
     # is kept), then SPP samples per pixel per frame; the warm-up is timed
@@ -491,7 +496,10 @@ def time_to_relmse(gs, sc, args, target=1e-3):
     floor = CV.bias_floor(lambda p, f: cache.render(p, WIDTH, HEIGHT, SPP, seed=SEED, sample_offset=f * SPP,
                                                     maxdepth=MAXDEPTH),
                           WIDTH, HEIGHT, gt, gt_var, args.floor_frames, first_frame=cached["frames"])
-    cache.close()
+    # the caches are released after every timed leg that uses one (a release
+    # synchronises the device and frees about 0.6 GB)
+    for c in (warm, cache1, cache):
+        c.close()
     del scratch
     gt2, gt2_var, gt2_s, _ = _ground_truth(gs, args, 2, args.gt_spp_bound)
     trunc = CV.converge_frame(lambda p, f: gs.render(p, WIDTH, HEIGHT, 1, seed=SEED, sample_offset=f, maxdepth=2,
