@@ -561,10 +561,17 @@ int nrc_train_step(bg_cache* c, const float* feat, const float4* target, const i
     const __nv_bfloat16* DZ = c->DZ.as<__nv_bfloat16>();
     float* dW = c->w_grad.as<float>();
     const size_t L = size_t(B) * 64;
-    k_nrc_wgrad<64, 128><<<wg, 256, 0, st>>>(DZ, T.X, n_dev, offset, B, B, dW + kNrcW0);
-    for (int l = 1; l < 5; ++l)
-        k_nrc_wgrad<64, 64><<<wg, 256, 0, st>>>(DZ + l * L, H + (l - 1) * L, n_dev, offset, B, B, dW + kNrcW1 + (l - 1) * 4096);
-    k_nrc_wgrad<16, 64><<<wg, 256, 0, st>>>(T.DZ5, H + 4 * L, n_dev, offset, B, B, dW + kNrcW5);
+    if (c->desc.mlp_kernel == 0) {
+        // all six weight gradients in one tcgen05 kernel
+        TcWgradArgs W{T.X, H, DZ, T.DZ5, dW, B};
+        k_nrc_wgrad_tc<<<wg, kWgThreads, kWgSmem, st>>>(c->dev, W, n_dev, offset, B, c->scene->dev.errflags);
+    } else {
+        k_nrc_wgrad<64, 128><<<wg, 256, 0, st>>>(DZ, T.X, n_dev, offset, B, B, dW + kNrcW0);
+        for (int l = 1; l < 5; ++l)
+            k_nrc_wgrad<64, 64><<<wg, 256, 0, st>>>(DZ + l * L, H + (l - 1) * L, n_dev, offset, B, B,
+                                                    dW + kNrcW1 + (l - 1) * 4096);
+        k_nrc_wgrad<16, 64><<<wg, 256, 0, st>>>(T.DZ5, H + 4 * L, n_dev, offset, B, B, dW + kNrcW5);
+    }
     k_nrc_grid_bwd<<<c->sms * 8, 128, 0, st>>>(c->dev, feat, T.dX, n_dev, offset, B, B);
     BG_CUDA(cudaGetLastError());
     if (apply) {
@@ -708,6 +715,7 @@ int bg_cache_create(bg_scene* s, const bg_cache_desc* d, bg_cache** out) {
     cudaFuncSetAttribute(k_nrc_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, kInferSmem);
     cudaFuncSetAttribute(k_nrc_infer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kTiSmem);
     cudaFuncSetAttribute(k_nrc_train_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kTtSmem);
+    cudaFuncSetAttribute(k_nrc_wgrad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kWgSmem);
     cudaFuncSetAttribute(k_nrc_train, cudaFuncAttributeMaxDynamicSharedMemorySize, kTrainSmem);
     if ((rc = cache_init_params(c))) { bg_cache_destroy(c); return rc; }
     // the scratch of one Adam step over train_batch rows, here rather than in

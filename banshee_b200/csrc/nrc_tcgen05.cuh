@@ -498,4 +498,180 @@ __global__ void __launch_bounds__(128, 2) k_nrc_train_tc(NrcDev C, TcTrainArgs T
     }
 }
 
+
+// ------------------------------------------------------------- weight gradients
+// The six weight-gradient GEMMs of one Adam step, dW_l[o][i] = sum_s dZ_l[s][o]
+// A_l[s][i] (A_0 = the encoded rows X, A_l = H_{l-1}), on tcgen05 in one kernel.
+// The samples s are the reduction dimension K: a CTA stages kWgS samples of
+// every operand as plain row copies (row s of an operand at tc_off(s, chunk,
+// width / 8)), which read as MN-major operands (8 K-rows of 8 contiguous
+// M / N elements per core matrix: LBO = the stride between groups of 8
+// samples, SBO = 128 bytes between groups of 8 features), exactly as the
+// training backward reads its weights.  Every MMA has M = 128: layer 0's A is
+// X (128 features); the 64-wide inputs of two layers are stacked into one
+// 128-wide A (P1 = [H0 | H1], P2 = [H2 | H3], P3 = [H4 | 0]), and each of them
+// is multiplied by the two layers' dZ in turn, so the products needed sit in
+// the accumulator's top or bottom 64 lanes (the other half of each product is
+// not used).  Accumulators (transposed, D[i][o]) stay in TMEM over the CTA's
+// chunks: cols 0-63 dW0^T, 64-127 dW1^T (lanes 0-63), 128-191 dW2^T (lanes
+// 64-127), 192-255 dW3^T (0-63), 256-319 dW4^T (64-127), 320-335 dW5^T (0-63);
+// at the end each CTA adds them into dW with coalesced float atomics (split K
+// over CTAs, as the mma.sync kernels do).
+constexpr int kWgS = 128;                                  // samples per staged chunk
+constexpr int kWgThreads = 256;
+constexpr int kWgX = 0;                                    // [kWgS x 128] A tiles: X, P1, P2, P3
+constexpr int kWgA = kWgS * 128 * 2;                       // bytes per A tile
+constexpr int kWgDz = 4 * kWgA;                            // [kWgS x 64] x 5: dZ0..dZ4
+constexpr int kWgDzB = kWgS * 64 * 2;
+constexpr int kWgDz5 = kWgDz + 5 * kWgDzB;                 // [kWgS x 16]
+constexpr int kWgBar = kWgDz5 + kWgS * 16 * 2;
+constexpr int kWgSmem = kWgBar + 16;
+constexpr uint32_t kWgCols = 512;
+static_assert(kWgSmem <= 227 * 1024, "weight-gradient shared memory");
+
+struct TcWgradArgs {
+    const __nv_bfloat16* X;      // [B][128] encoded rows
+    const __nv_bfloat16* H;      // [5][B][64]
+    const __nv_bfloat16* DZ;     // [5][B][64]
+    const __nv_bfloat16* DZ5;    // [B][16]
+    float* dW;                   // [kNrcParams], accumulated
+    int B;
+};
+
+__global__ void __launch_bounds__(kWgThreads, 1) k_nrc_wgrad_tc(NrcDev C, TcWgradArgs T, const int* n_dev, int offset,
+                                                                int limit, unsigned* __restrict__ errflags) {
+    extern __shared__ __align__(1024) unsigned char wg_smem[];
+    unsigned char* smem = wg_smem;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const uint32_t sbase = uint32_t(__cvta_generic_to_shared(smem));
+    const uint32_t bar = sbase + kWgBar;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + kWgBar + 8);
+    __shared__ int abort_flag;
+
+    int n = n_dev ? *n_dev - offset : T.B;
+    if (limit > 0 && n > limit) n = limit;
+    if (n < 0) n = 0;
+    const int nchunks = (n + kWgS - 1) / kWgS;
+    if (int(blockIdx.x) >= nchunks) return;   // (uniform per CTA, before any TMEM allocation)
+
+    // the zero half of P3 is written once
+    for (int v = tid; v < kWgS * 8; v += kWgThreads) {
+        const int sl = v >> 3, kc = 8 + (v & 7);
+        *reinterpret_cast<uint4*>(smem + kWgX + 3 * kWgA + tc_off(sl, kc, 16)) = make_uint4(0u, 0u, 0u, 0u);
+    }
+    if (tid == 0) {
+        abort_flag = 0;
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(bar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     :: "r"(sbase + kWgBar + 8), "r"(kWgCols) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+    const size_t L = size_t(T.B) * 64;
+    uint32_t phase = 0;
+    bool first = true;
+    for (int chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x) {
+        const int s0 = chunk * kWgS;
+        // stage: 16-byte pieces of sample rows; rows past n are zero
+        for (int v = tid; v < kWgS * 16; v += kWgThreads) {              // X: 16 chunks per row
+            const int sl = v >> 4, kc = v & 15;
+            uint4 x = make_uint4(0u, 0u, 0u, 0u);
+            if (s0 + sl < n) x = *reinterpret_cast<const uint4*>(T.X + size_t(s0 + sl) * 128 + kc * 8);
+            *reinterpret_cast<uint4*>(smem + kWgX + tc_off(sl, kc, 16)) = x;
+        }
+        for (int v = tid; v < kWgS * 8 * 5; v += kWgThreads) {           // H0..H4 into P1, P2, P3
+            const int l = v / (kWgS * 8), r = v % (kWgS * 8), sl = r >> 3, kc = r & 7;
+            uint4 x = make_uint4(0u, 0u, 0u, 0u);
+            if (s0 + sl < n) x = *reinterpret_cast<const uint4*>(T.H + size_t(l) * L + size_t(s0 + sl) * 64 + kc * 8);
+            const int tile = 1 + (l >> 1), half = l & 1;
+            *reinterpret_cast<uint4*>(smem + kWgX + tile * kWgA + tc_off(sl, kc + 8 * half, 16)) = x;
+        }
+        for (int v = tid; v < kWgS * 8 * 5; v += kWgThreads) {           // dZ0..dZ4
+            const int l = v / (kWgS * 8), r = v % (kWgS * 8), sl = r >> 3, kc = r & 7;
+            uint4 x = make_uint4(0u, 0u, 0u, 0u);
+            if (s0 + sl < n) x = *reinterpret_cast<const uint4*>(T.DZ + size_t(l) * L + size_t(s0 + sl) * 64 + kc * 8);
+            *reinterpret_cast<uint4*>(smem + kWgDz + l * kWgDzB + tc_off(sl, kc, 8)) = x;
+        }
+        for (int v = tid; v < kWgS * 2; v += kWgThreads) {               // dZ5
+            const int sl = v >> 1, kc = v & 1;
+            uint4 x = make_uint4(0u, 0u, 0u, 0u);
+            if (s0 + sl < n) x = *reinterpret_cast<const uint4*>(T.DZ5 + size_t(s0 + sl) * 16 + kc * 8);
+            *reinterpret_cast<uint4*>(smem + kWgDz5 + tc_off(sl, kc, 2)) = x;
+        }
+        tc_fence_async_smem();
+        tc_fence_before();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+            // (A tile, its LBO) x (B tile, its LBO, N) -> TMEM columns
+            auto gemm = [&](uint32_t a, uint32_t b, uint32_t b_lbo, int N, uint32_t col) {
+                const uint32_t idesc = tc_idesc(N, true) | (1u << 15);   // A and B MN-major
+                for (int k = 0; k < kWgS / 16; ++k)
+                    tc_mma(tmem + col, tc_desc(a + k * 2 * 2048, 2048, 128), tc_desc(b + k * 2 * b_lbo, b_lbo, 128),
+                           idesc, (first && k == 0) ? 0u : 1u);
+            };
+            const uint32_t A0 = sbase + kWgX, P1 = A0 + kWgA, P2 = A0 + 2 * kWgA, P3 = A0 + 3 * kWgA;
+            const uint32_t Z = sbase + kWgDz;
+            gemm(A0, Z + 0 * kWgDzB, 1024, 64, 0);
+            gemm(P1, Z + 1 * kWgDzB, 1024, 64, 64);
+            gemm(P1, Z + 2 * kWgDzB, 1024, 64, 128);
+            gemm(P2, Z + 3 * kWgDzB, 1024, 64, 192);
+            gemm(P2, Z + 4 * kWgDzB, 1024, 64, 256);
+            gemm(P3, sbase + kWgDz5, 256, 16, 320);
+            tc_commit(bar);
+        }
+        first = false;
+        if (!tc_wait(bar, phase, C.wait_polls)) {
+            atomicOr(errflags, BG_FLAG_TIMEOUT);
+            abort_flag = 1;
+        }
+        phase ^= 1u;
+        tc_fence_after();
+        __syncthreads();   // the MMAs have read this chunk's tiles before they are overwritten
+        if (abort_flag) break;
+    }
+    if (!abort_flag) {
+        // warp w reads TMEM lanes 32 (w % 4) .. + 31 (lane = feature i); warps w and w + 4
+        // split the columns
+        const int q = warp & 3, half = warp >> 2;
+        const int i = q * 32 + (tid & 31);
+        const uint32_t trow = tmem + (uint32_t(q * 32) << 16);
+        auto out = [&](uint32_t col0, int ncols, float* dst, int ld, int ioff) {
+            for (int c = 0; c < ncols; c += 16) {
+                float v[16];
+                tc_ld16(trow + col0 + uint32_t(c), v);
+#pragma unroll
+                for (int j = 0; j < 16; ++j) atomicAdd(dst + size_t(c + j) * ld + (i - ioff), v[j]);
+            }
+        };
+        float* dW = T.dW;
+        if (half == 0) {
+            out(0, 64, dW + kNrcW0, 128, 0);                                   // dW0[o][i], i = 0..127
+            if (i < 64) out(64, 64, dW + kNrcW1, 64, 0);                       // dW1 = H0^T dZ1
+            else out(128, 64, dW + kNrcW1 + 4096, 64, 64);                     // dW2 = H1^T dZ2
+        } else {
+            if (i < 64) {
+                out(192, 64, dW + kNrcW1 + 2 * 4096, 64, 0);                   // dW3 = H2^T dZ3
+                out(320, 16, dW + kNrcW5, 64, 0);                              // dW5 = H4^T dZ5
+            } else {
+                out(256, 64, dW + kNrcW1 + 3 * 4096, 64, 64);                  // dW4 = H3^T dZ4
+            }
+        }
+    }
+    // after a timeout, give the outstanding MMA group one more bounded wait before freeing its TMEM
+    if (abort_flag && tid == 0) tc_wait(bar, phase ^ 1u);
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(kWgCols) : "memory");
+    }
+}
+
 }  // namespace bg

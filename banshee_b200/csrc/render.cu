@@ -1463,7 +1463,9 @@ int render_jobs(bg_scene* s, bg_cache* cache, const std::vector<JobSpec>& jobs, 
             k_clamp_count<<<1, 1, 0, ts>>>(ntr_prev, int(rs->tr_cap));
             for (int i = 0; i < tsteps; ++i)
                 if ((rc = nrc_train_step(cache, feat, target, ntr_prev, i * tbatch, tbatch, true, ts))) return rc;
-            ins.launches += 1 + 11 * tsteps;
+            // per step: encode, forward + backward, weight gradients (one tcgen05 kernel or six
+            // mma.sync ones), grid backward, step counter, two Adam kernels
+            ins.launches += 1 + (cd->mlp_kernel == 0 ? 7 : 12) * tsteps;
             ins.mark(4);
             if (side) BG_CUDA(cudaEventRecord(rs->ev_train, ts));
             wait_train = side;
