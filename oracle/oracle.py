@@ -72,6 +72,8 @@ def _lib(kind):
             lib = _load_ref(REF_GPU_SO)
             lib.ref_world_use_gpu.restype = C.c_int32
             lib.ref_world_use_gpu.argtypes = [_vp, _vp]
+            lib.ref_world_use_gpu_world.restype = C.c_int32
+            lib.ref_world_use_gpu_world.argtypes = [_vp, _vp, C.POINTER(_vp)]
             lib.ref_gpu_renderer.restype = C.c_int32
             lib.ref_gpu_renderer.argtypes = [_vp, _vp, _vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
                                              C.c_int32, C.c_uint64, _vp]
@@ -237,3 +239,12 @@ class ReferenceOnGpu(Reference):
     def use_gpu(self, gpu_scene_handle):
         if self.lib.ref_world_use_gpu(self.w, gpu_scene_handle) != 0:
             raise ValueError("GpuAccelerator rejected the world")
+
+    def use_gpu_world(self, gpu_ctx_handle):
+        """GpuAccelerator over a device scene built from this committed World
+        (gpu_scene_from_world); returns the scene handle, which the caller
+        destroys (bg_scene_destroy) after close()."""
+        h = _vp()
+        if self.lib.ref_world_use_gpu_world(self.w, gpu_ctx_handle, C.byref(h)) != 0:
+            raise ValueError("gpu_scene_from_world or GpuAccelerator failed")
+        return h.value

@@ -50,6 +50,7 @@
 #ifdef BANSHEE_GPU_ADAPTER
 #include "adapters/gpu_accelerator.h"
 #include "adapters/gpu_renderer.h"
+#include "adapters/world_scene.h"
 #endif
 #include "tracer/aotracer.h"
 #include "sampler/sobol_sampler.h"
@@ -293,6 +294,22 @@ int ref_world_use_gpu(void* w, void* gpu_scene) {
     RefWorld* rw = static_cast<RefWorld*>(w);
     try {
         rw->world.accel_.reset(new GpuAccelerator(rw->world, static_cast<bg_scene*>(gpu_scene)));
+    } catch (...) {
+        return -1;
+    }
+    return 0;
+}
+
+/* Builds the device scene from the committed World itself
+ * (gpu_scene_from_world: the bundles' public accessors) and installs
+ * GpuAccelerator over it.  *scene_out receives that scene; the caller destroys
+ * it (bg_scene_destroy) after the world. */
+int ref_world_use_gpu_world(void* w, void* gpu_ctx, void** scene_out) {
+    RefWorld* rw = static_cast<RefWorld*>(w);
+    try {
+        bg_scene* s = gpu_scene_from_world(static_cast<bg_ctx*>(gpu_ctx), rw->world);
+        *scene_out = s;
+        rw->world.accel_.reset(new GpuAccelerator(rw->world, s));
     } catch (...) {
         return -1;
     }

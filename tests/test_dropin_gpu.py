@@ -3,6 +3,7 @@
 GpuAccelerator adapter over the C ABI.  Every closest hit and every shadow
 query of the reference's GiTracer / DiTracer then comes from the GPU, and the
 images must be bit-identical to the same code running on its own Bvh."""
+import ctypes as C
 import os
 
 import numpy as np
@@ -41,6 +42,32 @@ def test_reference_tracer_over_gpu_accelerator(ctx, ref_gpu, tracer, width):
     gpu = ref.render(**kw)                 # the same reference code, hits from the GPU
     assert (own.view(np.uint32) == gpu.view(np.uint32)).all()
     assert gs.error_flags() == 0
+
+
+@pytest.mark.parametrize("scene", ["cornell", "production"])
+def test_gpu_accelerator_over_scene_built_from_the_world(ctx, ref_gpu, scene):
+    """gpu_scene_from_world builds the device scene from the committed World's
+    own bundles (vertices, faces, transforms through public accessors), with no
+    scene description from the caller; the reference's tracer over it renders
+    the same image, bit for bit, as over its own Bvh."""
+    from banshee_b200 import capi
+    if scene == "cornell":
+        sc = scenes.cornell(20, 20)
+        kw = dict(spp=4, seed=9, tracer=abi.BG_TRACER_GI, maxdepth=5, nthreads=4)
+    else:   # transformed bundles
+        sc = scenes.production(20, 12, nterrain=32, nspheres=6, sphere_seg=10, seed=4)
+        kw = dict(spp=2, seed=3, maxdepth=8, nthreads=4)
+    ref = ref_gpu.ReferenceOnGpu(sc)
+    own = ref.render(**kw)
+    handle = ref.use_gpu_world(ctx.h.value)
+    try:
+        gpu = ref.render(**kw)
+        assert (own.view(np.uint32) == gpu.view(np.uint32)).all()
+        flags = C.c_uint32()
+        assert capi.lib().bg_scene_error_flags(C.c_void_p(handle), C.byref(flags), 1) == 0 and flags.value == 0
+    finally:
+        ref.close()
+        capi.lib().bg_scene_destroy(C.c_void_p(handle))
 
 
 def test_reference_production_scene_over_gpu_accelerator(ctx, ref_gpu):
