@@ -528,6 +528,48 @@ def time_to_relmse(gs, sc, args, target=1e-3):
             "summary_reference_spp": args.gt_spp}
 
 
+def cache_bias_scenes(ctx, args, warm_frames=64):
+    """The cache's bias floor on two more scenes than C5's: the C1 Cornell box
+    (256^2, GiTracer(5): an indoor scene whose light comes from paths of many
+    bounces) and a reduced production scene (512^2, 200k-triangle terrain and
+    20 spheres, GiTracer(8)).  Same cache configuration and measurement as
+    C5: after `warm_frames` training frames at SPP per frame, the relMSE of
+    args.floor_frames more frames against a plain render at args.gt_spp_bound
+    spp accumulated in float64, split into the image's noise, the reference's
+    noise and the rest, the squared bias.  Also with the training paths traced
+    to full depth instead of ending into the cache (unbiased training targets:
+    what remains is the network's and the grid's fitting error)."""
+    from banshee_b200 import capi, scenes
+    from banshee_b200 import convergence as CV
+    out = []
+    for name, sc, maxdepth in (("cornell_c1", scenes.cornell(256, 256), 5),
+                               ("production_512", scenes.production(512, 512, nterrain=320, nspheres=20,
+                                                                    sphere_seg=60, seed=11), MAXDEPTH)):
+        gs = capi.GpuScene(ctx, sc)
+        W, H = sc.width, sc.height
+        gt, gt_var, gt_s, _ = _ground_truth(gs, args, maxdepth, args.gt_spp_bound, width=W, height=H, name=name)
+        import torch
+        tmp = torch.zeros((H, W, 4), dtype=torch.float32, device="cuda")
+        rec = {"scene": name, "frame": [W, H], "maxdepth": maxdepth, "triangles": gs.info()["ntriangles"],
+               "reference_spp": args.gt_spp_bound, "reference_seconds": gt_s, "warm_frames": warm_frames}
+        # the C5 configuration (training paths end into the cache one bounce after
+        # the rendering paths), and training paths traced to full depth
+        for key, cfg in (("", CACHE_CFG), ("full_depth_training_", dict(CACHE_CFG, train_suffix=0))):
+            cache = capi.RadianceCache(gs, **cfg)
+            for f in range(warm_frames):
+                cache.render(tmp.data_ptr(), W, H, SPP, seed=SEED, sample_offset=f * SPP, maxdepth=maxdepth)
+            floor = CV.bias_floor(lambda p, f: cache.render(p, W, H, SPP, seed=SEED, sample_offset=f * SPP,
+                                                            maxdepth=maxdepth),
+                                  W, H, gt, gt_var, args.floor_frames, first_frame=warm_frames)
+            torch.cuda.synchronize()
+            cache.close()
+            rec.update({key + k: v for k, v in floor.items()})
+        out.append(rec)
+        del gt, gt_var, tmp
+        gs.close()
+    return out
+
+
 def summary(line):
     """A few numbers per config, kept short so the end of the JSON line carries them."""
     def g(d, *ks):
@@ -555,6 +597,9 @@ def summary(line):
         for k, v in rt.items():
             if k.startswith("summary_"):
                 out["c5_" + k[len("summary_"):]] = v
+        for r in rt.get("bias_per_scene") or []:
+            out["c5_bias_floor_" + r["scene"]] = g(r, "bias_floor")
+            out["c5_bias_floor_full_depth_training_" + r["scene"]] = g(r, "full_depth_training_bias_floor")
     return out
 
 
@@ -756,6 +801,7 @@ def main():
     cache_res = c2 = c1 = None
     if rank == 0 and world == 1 and not args.no_cache:
         cache_res = time_to_relmse(gs, sc, args)
+        cache_res["bias_per_scene"] = cache_bias_scenes(ctx, args)
     if rank == 0 and world == 1 and not args.no_extra:
         gs.close()
         c2 = raycast_c2(ctx)
