@@ -440,6 +440,8 @@ struct bg_cache {
 
 namespace bg {
 
+void render_forget_cache(bg_scene* s, const bg_cache* c);   // render.cu
+
 static int64_t grid_params(const bg_cache* c) { return int64_t(kNrcLevels) * (int64_t(1) << c->dev.log2_T) * kNrcFeat; }
 
 static std::atomic<uint64_t> g_cache_ids{1};
@@ -728,6 +730,7 @@ int bg_cache_create(bg_scene* s, const bg_cache_desc* d, bg_cache** out) {
 int bg_cache_destroy(bg_cache* c) {
     if (!c) return BG_OK;
     cudaDeviceSynchronize();
+    render_forget_cache(c->scene, c);   // its pending training rows, if any, are dropped
     for (DevBuf* b : {&c->grid, &c->grid_grad, &c->grid_m, &c->grid_v, &c->w, &c->w_grad, &c->w_m, &c->w_v, &c->wb,
                       &c->step, &c->X, &c->H, &c->DZ, &c->DZ5, &c->dX, &c->loss})
         b->release();

@@ -88,6 +88,7 @@ struct RenderState {
     // rows of the other set wait to be trained at the start of the next frame
     // of the same cache (pending_frame: that cache's frame index which wrote them)
     uint64_t pending_cache = 0;         // id (nrc_id) of the cache whose training rows are pending
+    bg_cache* pending_ptr = nullptr;    // that cache (cleared when it is destroyed)
     // bumped whenever a buffer that captured passes bake in is reallocated
     // (segment / job tables, cache-mode queues and training sets): graphs
     // captured before then hold stale pointers and must not be replayed
@@ -1440,6 +1441,7 @@ int render_jobs(bg_scene* s, bg_cache* cache, const std::vector<JobSpec>& jobs, 
                 return rc;
             rs->tr_cap = tr_cap;
             rs->pending_cache = 0;                   // the sets were reallocated
+            rs->pending_ptr = nullptr;
         }
         if ((rc = nrc_prepare(cache, tbatch, cap))) return rc;
         // Online training is one frame behind: this frame's training rows go to
@@ -1447,6 +1449,26 @@ int render_jobs(bg_scene* s, bg_cache* cache, const std::vector<JobSpec>& jobs, 
         // a side stream, beside this frame's first bounces, which do not read
         // the cache; the first query stage waits for that training.
         const int64_t frame = nrc_frame(cache) - 1;
+        if (rs->pending_cache != 0 && rs->pending_cache != nrc_id(cache) && rs->pending_ptr) {
+            // Rows another cache of this scene left pending (renders of several
+            // caches interleaved): train them into that cache now, so that every
+            // cache trains on each of its frames once.  Synchronous, as that
+            // cache's next render may come on another stream.
+            bg_cache* other = rs->pending_ptr;
+            const bg_cache_desc* od = nrc_desc(other);
+            const int oset = rs->tr_set;             // the set its last render wrote
+            int* ntr = rs->counts.as<int>() + kCntTrain + oset;
+            const float* feat = rs->tr_feat.as<float>() + size_t(oset) * rs->tr_cap * 16;
+            const float4* target = rs->tr_target.as<float4>() + size_t(oset) * rs->tr_cap;
+            k_clamp_count<<<1, 1, 0, st>>>(ntr, int(rs->tr_cap));
+            for (int i = 0; i < std::max(0, od->train_steps); ++i)
+                if ((rc = nrc_train_step(other, feat, target, ntr, i * std::max(1, od->train_batch),
+                                         std::max(1, od->train_batch), true, st)))
+                    return rc;
+            BG_CUDA(cudaStreamSynchronize(st));
+            rs->pending_cache = 0;
+            rs->pending_ptr = nullptr;
+        }
         train_prev = tsteps > 0 && rs->pending_cache == nrc_id(cache) && rs->pending_frame == frame - 1;
         rs->tr_set ^= 1;
         int* ntr_prev = rs->counts.as<int>() + kCntTrain + (rs->tr_set ^ 1);
@@ -1474,6 +1496,7 @@ int render_jobs(bg_scene* s, bg_cache* cache, const std::vector<JobSpec>& jobs, 
         if (use_graph && !wait_train) BG_CUDA(cudaEventRecord(rs->ev_train, st));
         BG_CUDA(cudaMemsetAsync(rs->counts.as<int>() + kCntTrain + rs->tr_set, 0, sizeof(int), st));
         rs->pending_cache = nrc_id(cache);
+        rs->pending_ptr = cache;
         rs->pending_frame = frame;
     }
     int64_t done_samples = 0;
@@ -1632,6 +1655,17 @@ static int scene_autotune(bg_scene* s, const bg_camera_desc* cam, const bg_trace
         result->node_width = best_w;
     }
     return BG_OK;
+}
+
+// A destroyed cache's pending training rows are dropped (bg_cache_destroy).
+void render_forget_cache(bg_scene* s, const bg_cache* c) {
+    if (!s) return;
+    std::lock_guard<std::mutex> lk(s->mu);
+    RenderState* rs = s->render;
+    if (rs && rs->pending_ptr == c) {
+        rs->pending_ptr = nullptr;
+        rs->pending_cache = 0;
+    }
 }
 
 }  // namespace bg

@@ -478,7 +478,11 @@ int bg_cache_set_params(bg_cache* cache, const float* mlp, const float* grid);
 /* Renders like bg_render with GiTracer(tracer->maxdepth), except that
  * rendering paths end into the cache at vertex desc.cache_depth, and
  * desc.train_paths paths per call are traced in full and train the cache
- * (desc.train_steps Adam steps) after the frame. */
+ * (desc.train_steps Adam steps) after the frame: at the start of the cache's
+ * next call, beside its first bounces.  When calls of several caches of one
+ * scene interleave, a call that finds another cache's rows pending trains
+ * them into that cache first (synchronously), so every cache trains on each
+ * of its frames once; destroying a cache drops its pending rows. */
 int bg_render_cached(bg_scene* scene, bg_cache* cache, const bg_camera_desc* camera, const bg_tracer_desc* tracer,
                      const bg_sampler_desc* sampler, int32_t width, int32_t height, float* accum_rgbw_dev,
                      bg_render_stats* stats, void* stream);

@@ -277,3 +277,39 @@ def test_new_cache_on_the_same_scene_gets_its_own_pass_graph(ctx):
     # training uses float atomics, so the two runs agree to rounding, not bits
     assert relmse(mean_image(again), mean_image(fresh)) < 1e-2
     assert gs.error_flags() == 0
+
+
+def test_two_caches_rendering_alternately_keep_their_own_networks(ctx):
+    """Two caches of one configuration on one scene replay the same captured
+    passes (graphs are keyed by the cache's configuration), each re-pointed at
+    its own cache before every replay.  Rendering them alternately, each one's
+    frames must match the same cache rendering alone on a scene object of its
+    own; different network seeds make a mix-up visible."""
+    import torch
+    from banshee_b200 import capi, scenes
+    from banshee_b200.metrics import mean_image, relmse
+    sc = scenes.cornell(48, 48)
+    cfg = dict(log2_table_size=12, base_resolution=4, max_resolution=64, train_paths=1024, cache_depth=2,
+               train_batch=1024, train_steps=1, learning_rate=1e-2)
+
+    def frames(caches, n=4):
+        accs = [torch.zeros((48, 48, 4), dtype=torch.float32, device="cuda") for _ in caches]
+        for f in range(n):
+            for c, a in zip(caches, accs):
+                c.render(a.data_ptr(), 48, 48, 1, seed=5, sample_offset=f, maxdepth=5)
+        torch.cuda.synchronize()
+        return [a.cpu().numpy() for a in accs]
+
+    gs = capi.GpuScene(ctx, sc)
+    a, b = capi.RadianceCache(gs, seed=1, **cfg), capi.RadianceCache(gs, seed=2, **cfg)
+    both = frames([a, b])
+    alone = [frames([capi.RadianceCache(capi.GpuScene(ctx, sc), seed=k, **cfg)])[0] for k in (1, 2)]
+    for got, want in zip(both, alone):
+        assert np.isfinite(got).all() and (got[..., 3] == 4).all()
+        # training uses float atomics: the runs agree to rounding, not bits
+        assert relmse(mean_image(got), mean_image(want)) < 1e-2
+    # the two networks differ (different seeds), so each cache did read its own
+    assert relmse(mean_image(both[0]), mean_image(both[1])) > relmse(mean_image(both[0]), mean_image(alone[0]))
+    assert gs.error_flags() == 0
+    a.close()
+    b.close()
