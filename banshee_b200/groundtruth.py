@@ -1,6 +1,6 @@
 """Float64 accumulation of a progressive render, with checkpoint and resume.
 
-The radiance cache is judged against a plain GiTracer render at high spp
+The radiance cache is measured against a plain GiTracer render at high spp
 accumulated in float64.  At 1080p and 65,536 spp that is 1.36e11 camera
 samples, minutes of GPU time, so the accumulation is resumable:
 
