@@ -645,9 +645,12 @@ k_classify(Queues Q, int cap) {
 }
 
 // The hits of one material class (list MAT of k_classify).
-// 5 blocks of 128 threads per SM: 96 registers, no spills in the Lambert and
-// GGX class kernels (measured per step of C3: 8 blocks 9.6 ms of shading,
-// 6 blocks 9.3 ms, 5 blocks 8.8 ms, 4 blocks 0.3 ms slower than 5)
+// 5 blocks of 128 threads per SM: 96 registers; no spills in the Lambert
+// kernel, 4 bytes in the GGX one (measured per step of C3: 8 blocks 9.6 ms of
+// shading, 6 blocks 9.3 ms, 5 blocks 8.8 ms, 4 blocks 0.3 ms slower than 5).
+// The area-light instantiations spill 140-200 bytes at 96 registers, but the
+// same 5 blocks serve them best (C1 GiTracer: 4 blocks with 128 registers
+// 587 Msamples/s, 5 blocks 699, 6 blocks 685, 8 blocks 665).
 constexpr int kShadeClassBlocks = 5;
 // (Measured and rejected: the misses-and-emissive kernel at 8 blocks / SM on
 // the full grid, 0.15 ms per C3 step slower in the serial phase timing.)
