@@ -232,11 +232,47 @@ def raycast_c2(ctx, nrays=1 << 24, reps=5):
             "achieved_gbs": round(bpr * nrays / (ms * 1e-3) / 1e9, 1)}
         del dr, res, sub
     gs.close()
+    out["cpu_baseline"] = _raycast_c2_cpu(scenes.soup(1 << 20, seed=1), nrays)
     # the device builders (LBVH: Morton order; PLOC: clustering over it) on the
     # same soup: build time and traversal speed of their trees
     for builder, name in ((1, "device_lbvh"), (2, "device_ploc"), (3, "device_sah")):
         out[name] = _device_build_traversal(ctx, builder, nrays, reps)
     out["watertight"] = _watertight_traversal(ctx, nrays, reps)
+    return out
+
+
+def _raycast_c2_cpu(sc, nrays, sub=1 << 18, count_sub=1 << 14):
+    """C2 on the host: Banshee's own Bvh (oracle/_ref, World::Intersect) casting
+    a seeded subset (every nrays/sub-th ray) of each set with all host threads,
+    and, as the guard on the byte model, the nodes and triangles per ray of the
+    reference's binary tree (the oracle's restatement of Bvh::Build and
+    Bvh::Intersect, the same tree) on a smaller subset."""
+    try:
+        from oracle.oracle import Oracle, Reference
+        t0 = time.perf_counter()
+        ref = Reference(sc, raycast=True)
+        build_s = time.perf_counter() - t0
+        orc = Oracle(sc)
+    except Exception as exc:   # the checker libraries may be absent
+        return {"unavailable": str(exc)}
+    from banshee_b200 import scenes
+    out = {"kind": "reference", "cores": os.cpu_count() or 1, "reference_build_s": build_s,
+           "sample": "every %dth ray of each 16M-ray set (%d rays), all host threads" % (nrays // sub, sub)}
+    for kind, anyhit, trange in [("coherent", False, None), ("incoherent", False, None),
+                                 ("incoherent", True, None), ("coherent", True, (1.5, 2.5))]:
+        rays = scenes.soup_rays(nrays, kind, seed=2, any_hit=anyhit, **({"tmax_range": trange} if trange else {}))
+        r = np.ascontiguousarray(rays[:: nrays // sub])
+        t0 = time.perf_counter()
+        (ref.intersect_any if anyhit else ref.intersect_closest)(r, nthreads=0)
+        dt = time.perf_counter() - t0
+        c = np.ascontiguousarray(rays[:: nrays // count_sub])
+        nodes, tris = orc.traversal_counts(c, any_hit=anyhit)
+        name = ("coherent_shadow" if trange else kind) + ("_any" if anyhit else "_closest")
+        out[name] = {"mrays_per_s": round(r.shape[0] / dt / 1e6, 3),
+                     "reference_nodes_per_ray": round(nodes / c.shape[0], 2),
+                     "reference_tris_per_ray": round(tris / c.shape[0], 2)}
+    ref.close()
+    orc.close()
     return out
 
 
@@ -588,6 +624,8 @@ def summary(line):
                 out["c2_w%d_%s_mrays" % (w, k)] = g(c2, "layout%d" % w, k, "mrays_per_s")
     out["c2_watertight_w4_incoherent_closest_mrays"] = g(line, "raycast_c2", "watertight",
                                                         "layout4_incoherent_closest_mrays_per_s")
+    out["c2_cpu_reference_incoherent_closest_mrays"] = g(line, "raycast_c2", "cpu_baseline", "incoherent_closest",
+                                                         "mrays_per_s")
     out["c1_msamples_per_s"] = g(line, "cornell_c1", "gpu_msamples_per_s")
     out["c1_relmse_vs_reference"] = g(line, "cornell_c1", "relmse_gpu_vs_reference")
     out["c4_msamples_per_s"] = g(line, "batch_c4", "msamples_per_s")
