@@ -840,6 +840,13 @@ def main():
     if rank == 0 and world == 1 and not args.no_cache:
         cache_res = time_to_relmse(gs, sc, args)
         cache_res["bias_per_scene"] = cache_bias_scenes(ctx, args)
+        # the reference CPU tracer's time to the same target: the samples the plain
+        # GPU tracer needed (same estimator) at the CPU rate measured above
+        ps = cache_res["plain_spp_per_call"]
+        if cpu and cpu.get("value") and ps.get("seconds_to_target"):
+            samples = ps["seconds_to_target"] / (ps["ms_per_frame"] * 1e-3) * SPP * npix
+            cache_res["cpu_reference_seconds_to_target"] = samples / (cpu["value"] * 1e6)
+            cache_res["summary_cpu_reference_seconds_to_target"] = cache_res["cpu_reference_seconds_to_target"]
     if rank == 0 and world == 1 and not args.no_extra:
         gs.close()
         c2 = raycast_c2(ctx)
